@@ -1,0 +1,390 @@
+"""Benchmark of the KT RK2 step (gpu-vh's hot path) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one "step" = one Heun RK2 step over the whole lattice): the full single event of
+the benchmark configuration -- 131x131x61 cells, dx = dy = deta = 0.1, tau0 = 0.6,
+dtau = 0.01, QCD equation of state, eta/s = 0.16, shear + bulk, plain FP64, on a seeded
+Glauber-hotspot initial state (synthetic, see gvh/workloads.py). Metric: cell-updates/s
+(one interior cell advanced by one full RK2 step). With N GPUs each rank advances its own
+event (different seed): independent events, no collective in the step (weak scaling).
+
+Timing: W untimed warm-up steps, then K steps bracketed by barrier + synchronize, timed
+with CUDA events on the stream the kernels run on; the job time is the max over ranks.
+The lattice state (~380 MB) is larger than L2 (126 MB), so no flush is needed between
+steps. `e2e` times the same step through the C ABI with host buffers: each step copies the
+full state from pinned host memory to the device (gvh_set_state), steps, and copies it
+back (gvh_get_state).
+
+--impl reference times the reference's own KT step (its rhic/src sources compiled for the
+CPU by oracle/build_ref.py, OpenMP over the launch grid) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "gpu-vh_b200"))
+
+import numpy as np  # noqa: E402
+
+from gvh import workloads  # noqa: E402
+
+METRIC = "cell-updates/s"
+HBM_FALLBACK_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_info():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return HBM_FALLBACK_GBS, "fallback"
+
+
+def bytes_per_cell_update(nq: int) -> int:
+    """Algorithmic bytes of one cell-update (both stages), FP64: stage 1 reads q^n (nq), e,
+    u^n (4), u^{n-1} (4) and writes q* (nq), e*, u* (4); stage 2 reads q* (nq), e*, u* (4),
+    u^n (4), q^n (nq) and writes q^{n+1} (nq), e, u (4): 5 nq + 28 values. Pressure is a
+    function of e and is not counted."""
+    return (5 * nq + 28) * 8
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.dev)], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def make_event(w, rank):
+    import dataclasses
+    w = dataclasses.replace(w, seed=w.seed + rank)
+    prim = workloads.glauber_hotspots(w)
+    meta = prim.pop("_meta")
+    return w, prim, meta
+
+
+def central_planes(w, prim, nz_s):
+    """The nz_s rapidity planes around eta = 0 of a ghosted event, as a ghosted sub-lattice."""
+    k0 = (w.nz - nz_s) // 2
+    ncx, ncy = w.nx + 4, w.ny + 4
+    return {key: np.asarray(v).reshape(w.nz + 4, ncy, ncx)[k0: k0 + nz_s + 4].reshape(-1) if np.ndim(v) else v
+            for key, v in prim.items()}
+
+
+def cpu_baseline(w, prim, budget_s=20.0):
+    """The oracle (this project's C restatement, OpenMP) timed on the host cores on a bounded
+    sample of the workload: the first nz_s rapidity planes of the same event, sized so the
+    timed steps take about budget_s."""
+    import oracle
+
+    threads = os.cpu_count() or 1
+    kw = w.lattice_kwargs()
+
+    def run(nz_s, steps):
+        k = dict(kw, nz=nz_s)
+        L = oracle.OracleLattice(**k)
+        ncx, ncy = w.nx + 4, w.ny + 4
+        L.set_primitive(central_planes(w, prim, nz_s))
+        t0 = time.perf_counter()
+        t = w.tau0
+        for n in range(steps):
+            L.step(t, w.dtau)
+            t = w.tau0 + (n + 1) * w.dtau
+        return time.perf_counter() - t0
+
+    probe_nz = 2
+    dt_probe = run(probe_nz, 1)
+    per_cell = dt_probe / (w.nx * w.ny * probe_nz)
+    nz_s = int(max(2, min(w.nz, budget_s / 2 / max(per_cell * w.nx * w.ny, 1e-9))))
+    steps = 2
+    el = run(nz_s, steps)
+    cells = w.nx * w.ny * nz_s
+    return {"value": cells * steps / el, "unit": METRIC, "cores": threads, "kind": "port",
+            "sample": f"oracle (kt_oracle.c, OpenMP {threads} threads): {steps} RK2 steps of the first {nz_s} of "
+                      f"{w.nz} rapidity planes of the same event ({cells} cells), {el:.1f} s"}
+
+
+def run_reference(args):
+    """Reference arm: the reference's own KT step built for the CPU, all host threads."""
+    rank, world, local = dist_info()
+    if rank != 0:
+        return 0
+    w = workloads.CONFIG2
+    import oracle
+
+    if not oracle.ref_available("fp64_qcd_bulk"):
+        print(json.dumps({"impl": "reference", "unavailable": "reference CPU build oracle/_ref/libref_fp64_qcd_bulk.so "
+                                                              "missing (build needs the reference tree)"}))
+        return 0
+    w, prim, meta = make_event(w, 0)
+    threads = os.cpu_count() or 1
+    kw = w.lattice_kwargs()
+    ncx, ncy = w.nx + 4, w.ny + 4
+    # size the per-step sample so the whole run (warm-up + steps) ends within ~3 minutes
+    total_budget = 180.0
+    n_calls = args.warmup + args.steps
+
+    def make(nz_s):
+        R = oracle.RefLattice(threads=threads, **dict(kw, nz=nz_s))
+        R.set_primitive(central_planes(w, prim, nz_s))
+        return R
+
+    R = make(2)
+    t0 = time.perf_counter()
+    R.step(w.tau0, w.dtau)
+    per_cell = (time.perf_counter() - t0) / (w.nx * w.ny * 2)
+    nz_s = int(max(2, min(w.nz, total_budget / max(n_calls, 1) / max(per_cell * w.nx * w.ny, 1e-9))))
+    R = make(nz_s)
+    t = w.tau0
+    for n in range(args.warmup):
+        R.step(t, w.dtau)
+        t += w.dtau
+    t0 = time.perf_counter()
+    for n in range(args.steps):
+        R.step(t, w.dtau)
+        t += w.dtau
+    el = time.perf_counter() - t0
+    cells = w.nx * w.ny * nz_s
+    value = cells * args.steps / el
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": w.name, "lattice": [w.nx, w.ny, w.nz], "sample_lattice": [w.nx, w.ny, nz_s],
+                   "eos": "qcd", "shear": True, "bulk": True, "theta": w.theta, "impact_b_fm": meta["b"]},
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "reference",
+                         "sample": f"reference rhic/src KT step built for the CPU (g++ -O2, OpenMP {threads} threads) "
+                                   f"on the central {nz_s} of {w.nz} rapidity planes of the event"},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(args):
+    import torch
+
+    import gvh
+
+    rank, world, local = dist_info()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    w, prim, meta = make_event(workloads.CONFIG2, rank)
+    L = gvh.Lattice(device=local, **w.lattice_kwargs())
+    L.set_primitive(prim)
+    stream = torch.cuda.Stream(device=local)
+    L.set_stream(stream.cuda_stream)
+    t = w.tau0
+    n_done = 0
+
+    def step():
+        nonlocal t, n_done
+        L.step(t, w.dtau)
+        n_done += 1
+        t = w.tau0 + n_done * w.dtau
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        with torch.cuda.stream(stream):
+            ev0.record(stream)
+            for _ in range(args.steps):
+                step()
+            ev1.record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    flags = L.status()
+    if flags:
+        raise RuntimeError(f"status flags {flags} raised during the timed steps")
+    ms_max = ms
+    if dist:
+        tt = torch.tensor([ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms_max = float(tt.item())
+    cells = w.cells
+    value = world * cells * args.steps / (ms_max / 1e3)
+    launches = L.launches_per_step * args.steps
+
+    # end to end through the C ABI with pinned host buffers
+    e2e = None
+    n_fields = len(L.field_names)
+    host_in = torch.empty((n_fields, L.ng), dtype=torch.float64, pin_memory=True)
+    host_out = torch.empty((n_fields, L.ng), dtype=torch.float64, pin_memory=True)
+    st = L.get_state()
+    for f, k in enumerate(L.field_names):
+        host_in[f].copy_(torch.from_numpy(st[k]))
+    ptr_in = [host_in[f].data_ptr() for f in range(n_fields)]
+    ptr_out = [host_out[f].data_ptr() for f in range(n_fields)]
+    L.set_stream(None)
+    L.set_stream(stream.cuda_stream)
+    for _ in range(2):
+        L.set_state_ptrs(ptr_in)
+        step()
+        L.get_state_ptrs(ptr_out)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.e2e_steps):
+        L.set_state_ptrs(ptr_in)
+        step()
+        L.get_state_ptrs(ptr_out)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = e0.elapsed_time(e1)
+    if dist:
+        tt = torch.tensor([ms_e2e], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms_e2e = float(tt.item())
+    bytes_io = n_fields * L.ng * 8
+    e2e = {"value": world * cells * args.e2e_steps / (ms_e2e / 1e3), "unit": METRIC,
+           "h2d_bytes_per_step": bytes_io, "d2h_bytes_per_step": bytes_io,
+           "ms_per_step": ms_e2e / args.e2e_steps, "steps": args.e2e_steps}
+
+    peak, peak_kind = measured_peaks()
+    b_cell = bytes_per_cell_update(L.nq)
+    achieved = cells * b_cell / (ms / args.steps / 1e3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        try:
+            traffic = json.load(open(tp)).get("bytes_per_step")
+        except Exception:
+            traffic = None
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "peak_source": peak_kind,
+                "algorithmic_bytes_per_step": cells * b_cell,
+                "kernel": "kt_stage_kernel (stage 1 + stage 2 per step)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline(w, prim)
+        except Exception as ex:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": METRIC, "cores": os.cpu_count(), "kind": "port", "sample": f"failed: {ex}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": w.name, "lattice": [w.nx, w.ny, w.nz], "spacing_fm": [w.dx, w.dy, w.dz],
+                       "tau0": w.tau0, "dtau": w.dtau, "eos": "qcd", "eta_over_s": w.etabar, "shear": True,
+                       "bulk": True, "theta": w.theta, "precision": "fp64", "events": world,
+                       "impact_b_fm": meta["b"], "n_part": meta["n_part"],
+                       "l2_policy": "state (~%.0f MB) larger than L2; no flush" % (L.ng * (2 * L.nq + 15) * 8 / 1e6),
+                       "parallelism": f"events x{world}"},
+            "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line))
+    L.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

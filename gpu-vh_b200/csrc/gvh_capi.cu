@@ -1,0 +1,406 @@
+// gvh_capi.cu -- libgvh.so: the C ABI declared in include/gvh.h.
+//
+// A handle owns one lattice in HBM (interior cells only, component-major SoA, see
+// gvh_stage.cuh) and a CUDA stream. gvh_rk2_step launches two fused stage kernels; the
+// reference issues ~21 launches, 12 stream creations/destructions and a device-wide
+// synchronisation for the same step (FullyDiscreteKurganovTadmorScheme.cu:109-139,
+// GhostCells.cu:19-28).
+//
+// Buffers (one allocation): qA, qB (conserved, nq each), e, pA, pB, u[3] (4 each).
+//   stage 1: q^n=qA -> q*=qB,  p^n=pA -> p*=pB,  u^n, u^{n-1} -> u* (over u^{n-1}), e in place
+//   stage 2: q*=qB, q^n=qA -> q^{n+1}=qA (in place: q^n is read at the centre only),
+//            p* -> pA,  u*, u^n -> u^{n+1} (third buffer), e in place
+// after the step u^{n+1} is current and u^n previous, as after the reference's
+// swapFluidVelocity (FullyDiscreteKurganovTadmorScheme.cu:131).
+#include <cuda_runtime.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <string>
+
+#include "../../include/gvh.h"
+#include "gvh_stage.cuh"
+
+using namespace gvh;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+#define GVH_CUDA(call)                                                                          \
+  do {                                                                                          \
+    cudaError_t err_ = (call);                                                                  \
+    if (err_ != cudaSuccess) return fail(GVH_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(err_)); \
+  } while (0)
+
+constexpr int kThreads = 128;
+
+}  // namespace
+
+struct gvh_handle {
+  int nx, ny, nz, nq;
+  long long ncells, ng;     // interior cells, ghosted cells
+  long long sy, sz, cs;     // internal strides
+  double dx, dy, dz, dt_lattice, etabar, theta;
+  int eos, shear, bulk, precision, device;
+  cudaStream_t stream;      // where work is queued (own_stream unless the caller set one)
+  cudaStream_t own_stream;
+  double *block;
+  double *qA, *qB, *e, *pA, *pB, *u[3];
+  int ucur, uprev, ufree;
+  unsigned *status;
+  double *staging;          // reference-layout fields for set/get, allocated on first use
+};
+
+namespace {
+
+// --------------------------------------------------------------------------------------
+// layout conversion kernels (reference ghosted layout <-> internal interior-only layout)
+// --------------------------------------------------------------------------------------
+struct Pack {
+  int nx, ny, nz;
+  long long sy, sz;   // internal strides
+  long long ng;       // ghosted size (field stride in staging)
+};
+
+__device__ __forceinline__ long long ref_index(const Pack &p, int i, int j, int k) {
+  return (long long)(i + 2) + (long long)(p.nx + 4) * ((j + 2) + (long long)(p.ny + 4) * (k + 2));
+}
+
+// staging (nf fields, ghosted) -> internal fields dst[f] (interior)
+__global__ void pack_kernel(Pack p, int nf, const double *__restrict__ staging, double *const *dst) {
+  long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long n = (long long)p.nx * p.ny * p.nz;
+  if (id >= n) return;
+  int i = id % p.nx, j = (id / p.nx) % p.ny, k = id / ((long long)p.nx * p.ny);
+  long long r = ref_index(p, i, j, k), s = i + p.sy * j + p.sz * k;
+  for (int f = 0; f < nf; ++f)
+    if (dst[f]) dst[f][s] = staging[f * p.ng + r];
+}
+
+// internal fields src[f] -> staging (ghosted, every ghost cell filled from the nearest
+// interior cell: the reference's zero-gradient faces, edges and corners alike)
+__global__ void unpack_kernel(Pack p, int nf, const double *const *src, double *__restrict__ staging) {
+  long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long n = p.ng;
+  if (id >= n) return;
+  int gi = id % (p.nx + 4), gj = (id / (p.nx + 4)) % (p.ny + 4), gk = id / ((long long)(p.nx + 4) * (p.ny + 4));
+  int i = min(max(gi - 2, 0), p.nx - 1), j = min(max(gj - 2, 0), p.ny - 1), k = min(max(gk - 2, 0), p.nz - 1);
+  long long s = i + p.sy * j + p.sz * k;
+  for (int f = 0; f < nf; ++f)
+    if (src[f]) staging[f * p.ng + id] = src[f][s];
+}
+
+// T^{tau mu} from primitives (DynamicalVariables.cu:349-392 with EnergyMomentumTensor.cu
+// :159-177) and p = p(e) (InitialConditions.cpp:124-127), in the internal layout.
+template <int EOS>
+__global__ void init_conserved_kernel(long long n, int nq, long long cs, double *q, double *e, double *p,
+                                      double *u, double *up) {
+  long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  double es = e[s];
+  double ps = eq_pressure<EOS>(es);
+  p[s] = ps;
+  double ut = u[s], ux = u[cs + s], uy = u[2 * cs + s], un = u[3 * cs + s];
+  double pitt = 0, pitx = 0, pity = 0, pitn = 0, Pi = 0;
+  if (nq >= 14) { pitt = q[4 * cs + s]; pitx = q[5 * cs + s]; pity = q[6 * cs + s]; pitn = q[7 * cs + s]; }
+  if (nq == 15) Pi = q[14 * cs + s];
+  double pp = ps + Pi;
+  q[s] = (es + pp) * ut * ut - pp + pitt;
+  q[cs + s] = (es + pp) * ut * ux + pitx;
+  q[2 * cs + s] = (es + pp) * ut * uy + pity;
+  q[3 * cs + s] = (es + pp) * ut * un + pitn;
+  for (int m = 0; m < 4; ++m) up[m * cs + s] = u[m * cs + s];
+}
+
+template <int EOS, bool SHEAR, bool BULK>
+int launch_stage(const gvh_handle *h, const StageArgs &a, bool stage2) {
+  const long long blocks = (h->ncells + kThreads - 1) / kThreads;
+  if (stage2) kt_stage_kernel<EOS, SHEAR, BULK, true><<<(unsigned)blocks, kThreads, 0, h->stream>>>(a);
+  else kt_stage_kernel<EOS, SHEAR, BULK, false><<<(unsigned)blocks, kThreads, 0, h->stream>>>(a);
+  GVH_CUDA(cudaGetLastError());
+  return GVH_OK;
+}
+
+template <int EOS>
+int dispatch_physics(const gvh_handle *h, const StageArgs &a, bool stage2) {
+  if (!h->shear) return launch_stage<EOS, false, false>(h, a, stage2);
+  if (!h->bulk) return launch_stage<EOS, true, false>(h, a, stage2);
+  return launch_stage<EOS, true, true>(h, a, stage2);
+}
+
+int dispatch(const gvh_handle *h, const StageArgs &a, bool stage2) {
+  if (h->eos == GVH_EOS_CONFORMAL) return dispatch_physics<EOS_CONFORMAL>(h, a, stage2);
+  return dispatch_physics<EOS_QCD>(h, a, stage2);
+}
+
+Pack make_pack(const gvh_handle *h) { return Pack{h->nx, h->ny, h->nz, h->sy, h->sz, h->ng}; }
+
+int ensure_staging(gvh_handle *h) {
+  if (h->staging) return GVH_OK;
+  size_t bytes = (size_t)(h->nq + 10) * h->ng * sizeof(double) + 64 * sizeof(double *);
+  if (cudaMalloc(&h->staging, bytes) != cudaSuccess) return fail(GVH_ERR_NOMEM, "staging allocation failed");
+  return GVH_OK;
+}
+
+// device array of field pointers lives after the staging fields
+double **staging_ptr_table(gvh_handle *h) {
+  return reinterpret_cast<double **>(h->staging + (size_t)(h->nq + 10) * h->ng);
+}
+
+void internal_fields(const gvh_handle *h, double **f) {
+  for (int n = 0; n < h->nq; ++n) f[n] = h->qA + n * h->cs;
+  f[h->nq] = h->e;
+  f[h->nq + 1] = h->pA;
+  for (int m = 0; m < 4; ++m) f[h->nq + 2 + m] = h->u[h->ucur] + m * h->cs;
+  for (int m = 0; m < 4; ++m) f[h->nq + 6 + m] = h->u[h->uprev] + m * h->cs;
+}
+
+int set_device(const gvh_handle *h) {
+  GVH_CUDA(cudaSetDevice(h->device));
+  return GVH_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void gvh_default_options(gvh_options *o) {
+  if (!o) return;
+  o->eos = GVH_EOS_QCD;
+  o->shear = 1;
+  o->bulk = 1;
+  o->precision = GVH_PRECISION_FP64;
+  o->theta = 2.0;
+  o->device = -1;
+}
+
+const char *gvh_last_error(void) { return g_last_error.c_str(); }
+
+int gvh_create(const gvh_lattice_params *L, const gvh_hydro_params *H, const gvh_options *opts, gvh_handle **out) {
+  if (!L || !H || !out) return fail(GVH_ERR_INVALID, "gvh_create: null argument");
+  *out = nullptr;
+  gvh_options o;
+  if (opts) o = *opts; else gvh_default_options(&o);
+  if (L->numLatticePointsX < 1 || L->numLatticePointsY < 1 || L->numLatticePointsRapidity < 1)
+    return fail(GVH_ERR_INVALID, "gvh_create: lattice sizes must be >= 1");
+  if (!(L->latticeSpacingX > 0) || !(L->latticeSpacingY > 0) || !(L->latticeSpacingRapidity > 0) ||
+      !(L->latticeSpacingProperTime > 0))
+    return fail(GVH_ERR_INVALID, "gvh_create: lattice spacings must be > 0");
+  if (o.eos != GVH_EOS_QCD && o.eos != GVH_EOS_CONFORMAL) return fail(GVH_ERR_INVALID, "gvh_create: unknown eos");
+  if (o.bulk && !o.shear) return fail(GVH_ERR_INVALID, "gvh_create: bulk needs shear (component 14 layout)");
+  if (o.precision != GVH_PRECISION_FP64)
+    return fail(GVH_ERR_INVALID, "gvh_create: precision mode %d not built", o.precision);
+  if (o.shear && !(H->shearViscosityToEntropyDensity > 0))
+    return fail(GVH_ERR_INVALID, "gvh_create: eta/s must be > 0 with shear");
+  int dev = o.device;
+  if (dev < 0) GVH_CUDA(cudaGetDevice(&dev));
+  GVH_CUDA(cudaSetDevice(dev));
+
+  gvh_handle *h = new gvh_handle();
+  memset(h, 0, sizeof(*h));
+  h->nx = L->numLatticePointsX; h->ny = L->numLatticePointsY; h->nz = L->numLatticePointsRapidity;
+  h->nq = 4 + (o.shear ? 10 : 0) + (o.bulk ? 1 : 0);
+  h->ncells = (long long)h->nx * h->ny * h->nz;
+  h->ng = (long long)(h->nx + 4) * (h->ny + 4) * (h->nz + 4);
+  h->sy = h->nx;
+  h->sz = (long long)h->nx * h->ny;
+  h->cs = (h->ncells + 31) / 32 * 32;  // 256-byte aligned components
+  h->dx = L->latticeSpacingX; h->dy = L->latticeSpacingY; h->dz = L->latticeSpacingRapidity;
+  h->dt_lattice = L->latticeSpacingProperTime;
+  h->etabar = H->shearViscosityToEntropyDensity;
+  h->theta = o.theta;
+  h->eos = o.eos; h->shear = o.shear; h->bulk = o.bulk; h->precision = o.precision; h->device = dev;
+  h->ucur = 0; h->uprev = 1; h->ufree = 2;
+
+  size_t nbuf = 2 * (size_t)h->nq + 3 + 12;
+  size_t bytes = nbuf * h->cs * sizeof(double) + 256;
+  if (cudaMalloc(&h->block, bytes) != cudaSuccess) {
+    delete h;
+    return fail(GVH_ERR_NOMEM, "gvh_create: cannot allocate %zu bytes", bytes);
+  }
+  cudaMemset(h->block, 0, bytes);
+  double *b = h->block;
+  h->qA = b; b += h->nq * h->cs;
+  h->qB = b; b += h->nq * h->cs;
+  h->e = b; b += h->cs;
+  h->pA = b; b += h->cs;
+  h->pB = b; b += h->cs;
+  for (int m = 0; m < 3; ++m) { h->u[m] = b; b += 4 * h->cs; }
+  h->status = reinterpret_cast<unsigned *>(b);
+  if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaFree(h->block);
+    delete h;
+    return fail(GVH_ERR_CUDA, "gvh_create: stream creation failed");
+  }
+  h->stream = h->own_stream;
+  *out = h;
+  return GVH_OK;
+}
+
+int gvh_destroy(gvh_handle *h) {
+  if (!h) return GVH_OK;
+  cudaSetDevice(h->device);
+  cudaStreamSynchronize(h->stream);
+  cudaStreamSynchronize(h->own_stream);
+  cudaStreamDestroy(h->own_stream);
+  cudaFree(h->block);
+  if (h->staging) cudaFree(h->staging);
+  delete h;
+  return GVH_OK;
+}
+
+int gvh_num_conserved(const gvh_handle *h) { return h ? h->nq : GVH_ERR_INVALID; }
+int gvh_num_fields(const gvh_handle *h) { return h ? h->nq + 10 : GVH_ERR_INVALID; }
+long long gvh_num_lattice_cells(const gvh_handle *h) { return h ? h->ng : GVH_ERR_INVALID; }
+int gvh_launches_per_step(const gvh_handle *h) { return h ? 2 : GVH_ERR_INVALID; }
+
+int gvh_set_state(gvh_handle *h, const double *const *fields, int n_fields) {
+  if (!h || !fields) return fail(GVH_ERR_INVALID, "gvh_set_state: null argument");
+  if (n_fields != h->nq + 10) return fail(GVH_ERR_INVALID, "gvh_set_state: expected %d fields", h->nq + 10);
+  int rc;
+  if ((rc = set_device(h)) || (rc = ensure_staging(h))) return rc;
+  const size_t fb = h->ng * sizeof(double);
+  for (int f = 0; f < n_fields; ++f) {
+    const double *src = fields[f];
+    if (!src && f >= h->nq + 6) src = fields[f - 4];  // up defaults to u
+    if (!src) return fail(GVH_ERR_INVALID, "gvh_set_state: field %d is null", f);
+    GVH_CUDA(cudaMemcpyAsync(h->staging + f * h->ng, src, fb, cudaMemcpyDefault, h->stream));
+  }
+  double *dst[32];
+  internal_fields(h, dst);
+  double **table = staging_ptr_table(h);
+  GVH_CUDA(cudaMemcpyAsync(table, dst, n_fields * sizeof(double *), cudaMemcpyHostToDevice, h->stream));
+  pack_kernel<<<(unsigned)((h->ncells + 255) / 256), 256, 0, h->stream>>>(make_pack(h), n_fields, h->staging, table);
+  GVH_CUDA(cudaGetLastError());
+  GVH_CUDA(cudaStreamSynchronize(h->stream));  // the host pointer table above is on the stack
+  return GVH_OK;
+}
+
+int gvh_get_state(gvh_handle *h, double *const *fields, int n_fields) {
+  if (!h || !fields) return fail(GVH_ERR_INVALID, "gvh_get_state: null argument");
+  if (n_fields != h->nq + 10) return fail(GVH_ERR_INVALID, "gvh_get_state: expected %d fields", h->nq + 10);
+  int rc;
+  if ((rc = set_device(h)) || (rc = ensure_staging(h))) return rc;
+  double *src[32];
+  internal_fields(h, src);
+  for (int f = 0; f < n_fields; ++f)
+    if (!fields[f]) src[f] = nullptr;
+  double **table = staging_ptr_table(h);
+  GVH_CUDA(cudaMemcpyAsync(table, src, n_fields * sizeof(double *), cudaMemcpyHostToDevice, h->stream));
+  unpack_kernel<<<(unsigned)((h->ng + 255) / 256), 256, 0, h->stream>>>(make_pack(h), n_fields, table, h->staging);
+  GVH_CUDA(cudaGetLastError());
+  const size_t fb = h->ng * sizeof(double);
+  for (int f = 0; f < n_fields; ++f)
+    if (fields[f]) GVH_CUDA(cudaMemcpyAsync(fields[f], h->staging + f * h->ng, fb, cudaMemcpyDefault, h->stream));
+  GVH_CUDA(cudaStreamSynchronize(h->stream));
+  return GVH_OK;
+}
+
+int gvh_set_primitive_state(gvh_handle *h, const double *const *prim, int n_prim) {
+  if (!h || !prim) return fail(GVH_ERR_INVALID, "gvh_set_primitive_state: null argument");
+  const int want = 5 + (h->nq - 4);
+  if (n_prim != want) return fail(GVH_ERR_INVALID, "gvh_set_primitive_state: expected %d arrays", want);
+  for (int f = 0; f < n_prim; ++f)
+    if (!prim[f]) return fail(GVH_ERR_INVALID, "gvh_set_primitive_state: array %d is null", f);
+  int rc;
+  if ((rc = set_device(h)) || (rc = ensure_staging(h))) return rc;
+  const size_t fb = h->ng * sizeof(double);
+  for (int f = 0; f < n_prim; ++f)
+    GVH_CUDA(cudaMemcpyAsync(h->staging + f * h->ng, prim[f], fb, cudaMemcpyDefault, h->stream));
+  double *dst[32];
+  dst[0] = h->e;
+  for (int m = 0; m < 4; ++m) dst[1 + m] = h->u[h->ucur] + m * h->cs;
+  for (int n = 4; n < h->nq; ++n) dst[5 + n - 4] = h->qA + n * h->cs;
+  double **table = staging_ptr_table(h);
+  GVH_CUDA(cudaMemcpyAsync(table, dst, n_prim * sizeof(double *), cudaMemcpyHostToDevice, h->stream));
+  pack_kernel<<<(unsigned)((h->ncells + 255) / 256), 256, 0, h->stream>>>(make_pack(h), n_prim, h->staging, table);
+  GVH_CUDA(cudaGetLastError());
+  const unsigned blocks = (unsigned)((h->ncells + 255) / 256);
+  if (h->eos == GVH_EOS_CONFORMAL)
+    init_conserved_kernel<EOS_CONFORMAL><<<blocks, 256, 0, h->stream>>>(h->ncells, h->nq, h->cs, h->qA, h->e, h->pA,
+                                                                        h->u[h->ucur], h->u[h->uprev]);
+  else
+    init_conserved_kernel<EOS_QCD><<<blocks, 256, 0, h->stream>>>(h->ncells, h->nq, h->cs, h->qA, h->e, h->pA,
+                                                                  h->u[h->ucur], h->u[h->uprev]);
+  GVH_CUDA(cudaGetLastError());
+  GVH_CUDA(cudaStreamSynchronize(h->stream));
+  return GVH_OK;
+}
+
+int gvh_rk2_step(gvh_handle *h, double t, double dt, double T_reg) {
+  if (!h) return fail(GVH_ERR_INVALID, "gvh_rk2_step: null handle");
+  int rc;
+  if ((rc = set_device(h))) return rc;
+  StageArgs a;
+  memset(&a, 0, sizeof a);
+  a.nx = h->nx; a.ny = h->ny; a.nz = h->nz;
+  a.sy = h->sy; a.sz = h->sz; a.cs = h->cs; a.ncells = h->ncells;
+  a.dx = h->dx; a.dy = h->dy; a.dz = h->dz; a.dt = h->dt_lattice;
+  a.etabar = h->etabar; a.theta = h->theta;
+  a.e_reg = (h->eos == GVH_EOS_CONFORMAL) ? energy_density_of_T<EOS_CONFORMAL>(T_reg)
+                                          : energy_density_of_T<EOS_QCD>(T_reg);
+  a.status = h->status;
+  a.e = h->e;
+  const double t1 = t + dt;
+  // stage 1 (predictor)
+  a.t_euler = t; a.t_after = t1;
+  a.qin = h->qA; a.qn = nullptr; a.qout = h->qB;
+  a.pin = h->pA; a.pout = h->pB;
+  a.uin = h->u[h->ucur]; a.uprev = h->u[h->uprev]; a.uout = h->u[h->uprev];
+  if ((rc = dispatch(h, a, false))) return rc;
+  // stage 2 (corrector + Heun combination)
+  a.t_euler = t1; a.t_after = t1;
+  a.qin = h->qB; a.qn = h->qA; a.qout = h->qA;
+  a.pin = h->pB; a.pout = h->pA;
+  a.uin = h->u[h->uprev]; a.uprev = h->u[h->ucur]; a.uout = h->u[h->ufree];
+  if ((rc = dispatch(h, a, true))) return rc;
+  const int nc = h->ufree, np = h->ucur, nf = h->uprev;
+  h->ucur = nc; h->uprev = np; h->ufree = nf;
+  return GVH_OK;
+}
+
+int gvh_set_stream(gvh_handle *h, void *stream) {
+  if (!h) return fail(GVH_ERR_INVALID, "null handle");
+  GVH_CUDA(cudaSetDevice(h->device));
+  GVH_CUDA(cudaStreamSynchronize(h->stream));
+  h->stream = stream ? reinterpret_cast<cudaStream_t>(stream) : h->own_stream;
+  return GVH_OK;
+}
+
+int gvh_synchronize(gvh_handle *h) {
+  if (!h) return fail(GVH_ERR_INVALID, "null handle");
+  GVH_CUDA(cudaSetDevice(h->device));
+  GVH_CUDA(cudaStreamSynchronize(h->stream));
+  return GVH_OK;
+}
+
+int gvh_status(gvh_handle *h, unsigned *flags) {
+  if (!h) return fail(GVH_ERR_INVALID, "null handle");
+  GVH_CUDA(cudaSetDevice(h->device));
+  unsigned v = 0;
+  GVH_CUDA(cudaMemcpyAsync(&v, h->status, sizeof v, cudaMemcpyDeviceToHost, h->stream));
+  GVH_CUDA(cudaStreamSynchronize(h->stream));
+  if (flags) *flags = v;
+  return v ? GVH_ERR_NUMERIC : GVH_OK;
+}
+
+int gvh_clear_status(gvh_handle *h) {
+  if (!h) return fail(GVH_ERR_INVALID, "null handle");
+  GVH_CUDA(cudaSetDevice(h->device));
+  GVH_CUDA(cudaMemsetAsync(h->status, 0, sizeof(unsigned), h->stream));
+  return GVH_OK;
+}
+
+}  // extern "C"

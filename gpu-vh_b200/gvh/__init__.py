@@ -1,0 +1,222 @@
+"""Python host binding of libgvh.so, the B200 KT RK2 step of gpu-vh.
+
+The binding mirrors the reference's interface for this path: the lattice/hydro parameter
+structs (LatticeParameters.h:17-31, HydroParameters.h:15-22), the ghosted SoA state arrays
+(DynamicalVariables.cu:32-35) and one call per Heun step (twoStepRungeKutta,
+FullyDiscreteKurganovTadmorScheme.cu:109-139). All compute runs in the CUDA library; if
+the library is missing this module raises instead of computing anything itself.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import build as _build
+
+LIB_PATH = _build.LIB
+
+GVH_EOS_QCD = 0
+GVH_EOS_CONFORMAL = 1
+GVH_PRECISION_FP64 = 0
+GVH_PRECISION_MIXED = 1
+GVH_STATUS_NAN = 1
+GVH_STATUS_NEWTON = 2
+
+Q_NAMES = ["ttt", "ttx", "tty", "ttn", "pitt", "pitx", "pity", "pitn",
+           "pixx", "pixy", "pixn", "piyy", "piyn", "pinn", "Pi"]
+PRIM_NAMES = ["e", "p", "ut", "ux", "uy", "un", "utp", "uxp", "uyp", "unp"]
+HBARC = 0.197326938  # GeV fm (HydroPlugin.cpp:132)
+
+
+class GvhError(RuntimeError):
+    pass
+
+
+class LatticeParams(ctypes.Structure):
+    """Layout-compatible with the reference's struct LatticeParameters."""
+    _fields_ = [("numLatticePointsX", ctypes.c_int), ("numLatticePointsY", ctypes.c_int),
+                ("numLatticePointsRapidity", ctypes.c_int), ("numComputationalLatticePointsX", ctypes.c_int),
+                ("numComputationalLatticePointsY", ctypes.c_int),
+                ("numComputationalLatticePointsRapidity", ctypes.c_int), ("numProperTimePoints", ctypes.c_int),
+                ("latticeSpacingX", ctypes.c_double), ("latticeSpacingY", ctypes.c_double),
+                ("latticeSpacingRapidity", ctypes.c_double), ("latticeSpacingProperTime", ctypes.c_double)]
+
+
+class HydroParams(ctypes.Structure):
+    """Layout-compatible with the reference's struct HydroParameters."""
+    _fields_ = [("initialProperTimePoint", ctypes.c_double), ("shearViscosityToEntropyDensity", ctypes.c_double),
+                ("freezeoutTemperatureGeV", ctypes.c_double), ("initializePimunuNavierStokes", ctypes.c_int),
+                ("regulationTemperatureGeV", ctypes.c_double)]
+
+
+class Options(ctypes.Structure):
+    _fields_ = [("eos", ctypes.c_int), ("shear", ctypes.c_int), ("bulk", ctypes.c_int),
+                ("precision", ctypes.c_int), ("theta", ctypes.c_double), ("device", ctypes.c_int)]
+
+
+_lib = None
+
+EXPORTS = [
+    "gvh_default_options", "gvh_create", "gvh_destroy", "gvh_num_conserved", "gvh_num_fields",
+    "gvh_num_lattice_cells", "gvh_set_primitive_state", "gvh_set_state", "gvh_get_state", "gvh_rk2_step",
+    "gvh_status", "gvh_clear_status", "gvh_synchronize", "gvh_launches_per_step", "gvh_last_error",
+    "gvh_set_stream",
+]
+
+
+def load(path: str | None = None):
+    """Load libgvh.so (the CUDA implementation). Raises if it is not built."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise GvhError(f"libgvh.so not found at {p}: build it with __graft_entry__.build()")
+    L = ctypes.CDLL(p)
+    vp, ip, dp = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+    L.gvh_default_options.argtypes = [ctypes.POINTER(Options)]
+    L.gvh_default_options.restype = None
+    L.gvh_create.argtypes = [ctypes.POINTER(LatticeParams), ctypes.POINTER(HydroParams), ctypes.POINTER(Options),
+                             ctypes.POINTER(vp)]
+    L.gvh_destroy.argtypes = [vp]
+    L.gvh_num_conserved.argtypes = [vp]
+    L.gvh_num_fields.argtypes = [vp]
+    L.gvh_num_lattice_cells.argtypes = [vp]
+    L.gvh_num_lattice_cells.restype = ctypes.c_longlong
+    L.gvh_set_primitive_state.argtypes = [vp, vp, ip]
+    L.gvh_set_state.argtypes = [vp, vp, ip]
+    L.gvh_get_state.argtypes = [vp, vp, ip]
+    L.gvh_rk2_step.argtypes = [vp, dp, dp, dp]
+    L.gvh_status.argtypes = [vp, ctypes.POINTER(ctypes.c_uint)]
+    L.gvh_clear_status.argtypes = [vp]
+    L.gvh_synchronize.argtypes = [vp]
+    L.gvh_launches_per_step.argtypes = [vp]
+    L.gvh_set_stream.argtypes = [vp, vp]
+    L.gvh_last_error.restype = ctypes.c_char_p
+    if path is None:
+        _lib = L
+    return L
+
+
+def _check(rc: int, what: str):
+    if rc != 0:
+        msg = load().gvh_last_error().decode(errors="replace")
+        raise GvhError(f"{what} failed ({rc}): {msg}")
+
+
+def _ptr_array(ptrs):
+    return (ctypes.c_void_p * len(ptrs))(*ptrs)
+
+
+def q_names(shear: bool, bulk: bool) -> list[str]:
+    names = Q_NAMES[:4]
+    if shear:
+        names += Q_NAMES[4:14]
+    if bulk:
+        names += ["Pi"]
+    return names
+
+
+class Lattice:
+    """One hydro lattice on the GPU (a libgvh handle)."""
+
+    def __init__(self, nx, ny, nz, dx, dy, dz, dt, etabar, theta=2.0, conformal=False, shear=True, bulk=True,
+                 precision="fp64", device=-1, tau0=0.5, T_fo_GeV=0.15, T_reg_GeV=0.0):
+        self._L = load()
+        self.nx, self.ny, self.nz = nx, ny, nz
+        self.ncx, self.ncy, self.ncz = nx + 4, ny + 4, nz + 4
+        self.ng = self.ncx * self.ncy * self.ncz
+        self.shear, self.bulk, self.conformal = bool(shear), bool(bulk), bool(conformal)
+        self.qnames = q_names(self.shear, self.bulk)
+        self.nq = len(self.qnames)
+        self.field_names = self.qnames + PRIM_NAMES
+        self.lattice = LatticeParams(nx, ny, nz, nx + 4, ny + 4, nz + 4, 0, dx, dy, dz, dt)
+        self.hydro = HydroParams(tau0, etabar, T_fo_GeV, 0, T_reg_GeV)
+        o = Options()
+        self._L.gvh_default_options(ctypes.byref(o))
+        o.eos = GVH_EOS_CONFORMAL if conformal else GVH_EOS_QCD
+        o.shear, o.bulk, o.theta, o.device = int(shear), int(bulk), float(theta), int(device)
+        o.precision = {"fp64": GVH_PRECISION_FP64, "mixed": GVH_PRECISION_MIXED}[precision]
+        self.options = o
+        h = ctypes.c_void_p()
+        _check(self._L.gvh_create(ctypes.byref(self.lattice), ctypes.byref(self.hydro), ctypes.byref(o),
+                                  ctypes.byref(h)), "gvh_create")
+        self._h = h
+        assert self._L.gvh_num_conserved(h) == self.nq
+        assert self._L.gvh_num_lattice_cells(h) == self.ng
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.gvh_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- state ---------------------------------------------------------------------------
+    def _as_ghosted(self, a):
+        a = np.ascontiguousarray(np.broadcast_to(np.asarray(a, np.float64).reshape(-1), (self.ng,)))
+        return a
+
+    def set_primitive(self, prim: dict):
+        order = ["e", "ut", "ux", "uy", "un"] + self.qnames[4:]
+        arrs = [self._as_ghosted(prim.get(k, 0.0)) for k in order]
+        _check(self._L.gvh_set_primitive_state(self._h, _ptr_array([a.ctypes.data for a in arrs]), len(arrs)),
+               "gvh_set_primitive_state")
+
+    def set_state(self, state: dict):
+        arrs = [None if state.get(k) is None else self._as_ghosted(state[k]) for k in self.field_names]
+        ptrs = [None if a is None else a.ctypes.data for a in arrs]
+        _check(self._L.gvh_set_state(self._h, _ptr_array(ptrs), len(ptrs)), "gvh_set_state")
+
+    def get_state(self, names=None) -> dict:
+        want = set(names) if names else set(self.field_names)
+        arrs = [np.empty(self.ng) if k in want else None for k in self.field_names]
+        ptrs = [None if a is None else a.ctypes.data for a in arrs]
+        _check(self._L.gvh_get_state(self._h, _ptr_array(ptrs), len(ptrs)), "gvh_get_state")
+        return {k: a for k, a in zip(self.field_names, arrs) if a is not None}
+
+    def set_state_ptrs(self, ptrs):
+        _check(self._L.gvh_set_state(self._h, _ptr_array(list(ptrs)), len(ptrs)), "gvh_set_state")
+
+    def get_state_ptrs(self, ptrs):
+        _check(self._L.gvh_get_state(self._h, _ptr_array(list(ptrs)), len(ptrs)), "gvh_get_state")
+
+    def interior(self, a):
+        return np.asarray(a).reshape(self.ncz, self.ncy, self.ncx)[2:-2, 2:-2, 2:-2]
+
+    # -- stepping ------------------------------------------------------------------------
+    def step(self, t, dt, T_reg=0.0):
+        _check(self._L.gvh_rk2_step(self._h, float(t), float(dt), float(T_reg)), "gvh_rk2_step")
+
+    def set_stream(self, stream_ptr: int | None):
+        """Queue this lattice's work on a caller-owned CUDA stream (raw cudaStream_t value)."""
+        _check(self._L.gvh_set_stream(self._h, stream_ptr or None), "gvh_set_stream")
+
+    def synchronize(self):
+        _check(self._L.gvh_synchronize(self._h), "gvh_synchronize")
+
+    def status(self) -> int:
+        f = ctypes.c_uint(0)
+        rc = self._L.gvh_status(self._h, ctypes.byref(f))
+        if rc not in (0, -3):
+            _check(rc, "gvh_status")
+        return int(f.value)
+
+    def clear_status(self):
+        _check(self._L.gvh_clear_status(self._h), "gvh_clear_status")
+
+    @property
+    def launches_per_step(self) -> int:
+        return int(self._L.gvh_launches_per_step(self._h))

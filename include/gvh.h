@@ -1,0 +1,141 @@
+/*
+ * gvh.h -- C ABI of the B200 KT RK2 step (gpu-vh's hot path), libgvh.so.
+ *
+ * Plain C types only (no CUDA or torch types), so any FFI can bind it. Every function
+ * returns an int status: GVH_OK (0) or a negative GVH_ERR_* code; gvh_last_error() gives
+ * a one-line reason for the calling thread's last failure.
+ *
+ * What it replaces in the reference (gpu-vh, paths within its tree):
+ *   gvh_create / gvh_destroy     allocateDeviceMemory / freeDeviceMemory
+ *                                (DynamicalVariables.cu:147-269, 443-485) and the
+ *                                constant set-up initializeCUDAConstantParameters
+ *                                (CudaConfiguration.cu:209-248)
+ *   gvh_set_primitive_state      setConservedVariables + copyHostToDeviceMemory +
+ *                                setGhostCells (HydroPlugin.cpp:214-220,
+ *                                DynamicalVariables.cu:271-308, 349-392)
+ *   gvh_set_state / gvh_get_state
+ *                                copyHostToDeviceMemory / copyDeviceToHostMemory
+ *                                (DynamicalVariables.cu:271-347), full state
+ *   gvh_rk2_step                 twoStepRungeKutta (FullyDiscreteKurganovTadmorScheme.cuh:18,
+ *                                FullyDiscreteKurganovTadmorScheme.cu:109-139) followed by
+ *                                the host swap setCurrentConservedVariables
+ *                                (HydroPlugin.cpp:422)
+ *   gvh_status                   (none: the reference printf()s NaN and Newton failures,
+ *                                EnergyMomentumTensor.cu:43, 92-94)
+ *
+ * State arrays use the reference's layout: one array per field over the ghosted lattice
+ * (nx+4)(ny+4)(nz+4), index i + (nx+4)*(j + (ny+4)*k) (DynamicalVariables.cu:32-35), interior
+ * at i,j,k in [2, n+2) (LatticeParameters.h:13-15). Host or device pointers are accepted
+ * (unified addressing). Field order (gvh_set_state / gvh_get_state): the evolved conserved
+ * components in CONSERVED_VARIABLES order (DynamicalVariables.cuh:50-71) -- ttt ttx tty ttn,
+ * then pitt pitx pity pitn pixx pixy pixn piyy piyn pinn if shear is evolved, then Pi if bulk
+ * is evolved -- followed by e, p, ut, ux, uy, un, utp, uxp, uyp, unp (u one step earlier).
+ */
+#ifndef GVH_H_
+#define GVH_H_
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GVH_OK 0
+#define GVH_ERR_INVALID -1   /* bad argument or configuration */
+#define GVH_ERR_CUDA -2      /* a CUDA call failed (message in gvh_last_error) */
+#define GVH_ERR_NUMERIC -3   /* the step raised a status bit (see gvh_status) */
+#define GVH_ERR_NOMEM -4     /* device allocation failed */
+
+/* status bits (gvh_status) */
+#define GVH_STATUS_NAN 1u          /* an energy density came out NaN */
+#define GVH_STATUS_NEWTON 2u       /* the QCD-EoS Newton solve hit its iteration cap */
+
+#define GVH_EOS_QCD 0              /* Wuppertal-Budapest fit (the reference default) */
+#define GVH_EOS_CONFORMAL 1        /* p = e/3 (CONFORMAL_EOS, EquationOfState.cuh:16) */
+
+#define GVH_PRECISION_FP64 0       /* plain FP64 path */
+#define GVH_PRECISION_MIXED 1      /* FP32 fluxes/limiter/sources, FP64 state and root find */
+
+/* Same members, order and types as the reference's struct LatticeParameters
+ * (LatticeParameters.h:17-31), so a pointer to one can be passed as the other. */
+typedef struct gvh_lattice_params {
+	int numLatticePointsX;
+	int numLatticePointsY;
+	int numLatticePointsRapidity;
+	int numComputationalLatticePointsX;
+	int numComputationalLatticePointsY;
+	int numComputationalLatticePointsRapidity;
+	int numProperTimePoints;
+	double latticeSpacingX;
+	double latticeSpacingY;
+	double latticeSpacingRapidity;
+	double latticeSpacingProperTime;
+} gvh_lattice_params;
+
+/* Same layout as the reference's struct HydroParameters (HydroParameters.h:15-22). */
+typedef struct gvh_hydro_params {
+	double initialProperTimePoint;
+	double shearViscosityToEntropyDensity;
+	double freezeoutTemperatureGeV;
+	int initializePimunuNavierStokes;
+	double regulationTemperatureGeV;
+} gvh_hydro_params;
+
+/* The reference's compile-time switches, chosen at run time here. */
+typedef struct gvh_options {
+	int eos;        /* GVH_EOS_* (reference: CONFORMAL_EOS macro) */
+	int shear;      /* evolve pi^{mu nu} (reference: PIMUNU macro, DynamicalVariables.cuh:13) */
+	int bulk;       /* evolve Pi, needs shear (reference: PI macro, DynamicalVariables.cuh:14) */
+	int precision;  /* GVH_PRECISION_* (reference: PRECISION macro, DynamicalVariables.cuh:44) */
+	double theta;   /* minmod limiter slope (reference: THETA 2.0, FluxLimiter.cu:15) */
+	int device;     /* CUDA device ordinal; -1 = current device */
+} gvh_options;
+
+typedef struct gvh_handle gvh_handle;
+
+/* Fills opts with the reference's shipped configuration: QCD EoS, shear + bulk, theta 2.0,
+ * FP64, current device. */
+void gvh_default_options(gvh_options *opts);
+
+int gvh_create(const gvh_lattice_params *lattice, const gvh_hydro_params *hydro, const gvh_options *opts,
+               gvh_handle **out);
+int gvh_destroy(gvh_handle *h);
+
+/* Number of evolved conserved components (4, 14 or 15) and of state fields (+10). */
+int gvh_num_conserved(const gvh_handle *h);
+int gvh_num_fields(const gvh_handle *h);
+/* Ghosted lattice size (nx+4)(ny+4)(nz+4): the length of every state array. */
+long long gvh_num_lattice_cells(const gvh_handle *h);
+
+/* Initial state from primitive fields on the interior of ghosted arrays: prim[0]=e,
+ * prim[1..4]=ut,ux,uy,un, then the evolved dissipative components (pitt..pinn, Pi).
+ * Sets p = p(e), T^{tau mu} from (e, p, u, pi, Pi), u one step earlier = u. */
+int gvh_set_primitive_state(gvh_handle *h, const double *const *prim, int n_prim);
+int gvh_set_state(gvh_handle *h, const double *const *fields, int n_fields);
+/* Null entries are skipped. Ghost layers come back zero-gradient filled, edges and
+ * corners included. Synchronises the handle's stream. */
+int gvh_get_state(gvh_handle *h, double *const *fields, int n_fields);
+
+/* One Heun RK2 step from time t (t and dt as twoStepRungeKutta takes them). Cells with
+ * e <= e(T_reg) have pi^{mu nu} regulated; T_reg is in fm^-1 and 0 (the reference's default
+ * configuration) regulates nothing, since e(0) lies below every energy density.
+ * Asynchronous on the handle's stream. */
+int gvh_rk2_step(gvh_handle *h, double t, double dt, double T_reg);
+
+/* Waits for the handle's stream; returns GVH_OK, or GVH_ERR_NUMERIC with *flags set when a
+ * step raised a status bit since the last gvh_clear_status. flags may be null. */
+int gvh_status(gvh_handle *h, unsigned *flags);
+int gvh_clear_status(gvh_handle *h);
+int gvh_synchronize(gvh_handle *h);
+
+/* Runs the handle's work on a caller-owned stream (a cudaStream_t passed as void*); NULL
+ * returns to the handle's own stream. Waits for work already queued on the old stream. */
+int gvh_set_stream(gvh_handle *h, void *stream);
+
+/* Number of stage-kernel launches one gvh_rk2_step issues. */
+int gvh_launches_per_step(const gvh_handle *h);
+
+const char *gvh_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GVH_H_ */

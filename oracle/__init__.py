@@ -1,0 +1,253 @@
+"""Oracle package: CPU checkers for the KT RK2 step. TEST INFRASTRUCTURE ONLY.
+
+Two engines with one Python interface (ctypes, numpy arrays in the reference's ghosted
+SoA layout):
+
+* ``OracleLattice`` -- kt_oracle.c, this project's own C restatement of the reference
+  algorithm (FP64 semantics), built into oracle/_build/.
+* ``RefLattice`` -- the reference's own hot-path sources compiled for the CPU
+  (oracle/build_ref.py -> oracle/_ref/), used to pin the restatement and as the
+  benchmark's reference arm. Each variant library holds one lattice (the reference keeps
+  its state in globals).
+
+Only tests/, the smoke check and the CPU-baseline/reference legs of bench.py use this
+package; the product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+BUILD_DIR = os.path.join(HERE, "_build")
+ORACLE_LIB = os.path.join(BUILD_DIR, "libkt_oracle.so")
+REF_DIR = os.path.join(HERE, "_ref")
+
+Q_NAMES = ["ttt", "ttx", "tty", "ttn", "pitt", "pitx", "pity", "pitn",
+           "pixx", "pixy", "pixn", "piyy", "piyn", "pinn", "Pi"]
+PRIM_NAMES = ["e", "p", "ut", "ux", "uy", "un", "utp", "uxp", "uyp", "unp"]
+
+
+def q_names(shear: bool, bulk: bool) -> list[str]:
+    names = Q_NAMES[:4]
+    if shear:
+        names += Q_NAMES[4:14]
+    if bulk:
+        names += ["Pi"]
+    return names
+
+
+def build_oracle(verbose: bool = True) -> str:
+    """Compile kt_oracle.c (no FMA contraction, like the reference CPU build)."""
+    os.makedirs(BUILD_DIR, exist_ok=True)
+    src = os.path.join(HERE, "kt_oracle.c")
+    cmd = ["gcc", "-std=c99", "-O2", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off", "-o", ORACLE_LIB, src, "-lm"]
+    r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + r.stdout)
+    if verbose:
+        print(f"[oracle] built {ORACLE_LIB}")
+    return ORACLE_LIB
+
+
+class KtParams(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+                ("dx", ctypes.c_double), ("dy", ctypes.c_double), ("dz", ctypes.c_double),
+                ("dt", ctypes.c_double), ("etabar", ctypes.c_double), ("theta", ctypes.c_double),
+                ("conformal", ctypes.c_int), ("shear", ctypes.c_int), ("bulk", ctypes.c_int)]
+
+
+_oracle = None
+
+
+def _load_oracle():
+    global _oracle
+    if _oracle is None:
+        if not os.path.exists(ORACLE_LIB):
+            build_oracle(verbose=False)
+        L = ctypes.CDLL(ORACLE_LIB)
+        L.kt_create.restype = ctypes.c_void_p
+        L.kt_create.argtypes = [ctypes.POINTER(KtParams)]
+        L.kt_destroy.argtypes = [ctypes.c_void_p]
+        L.kt_nq.argtypes = [ctypes.POINTER(KtParams)]
+        for fn in ("kt_set_state", "kt_get_state", "kt_set_primitive_state"):
+            getattr(L, fn).argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.kt_rk2_step.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+        L.kt_rk2_step.restype = None
+        for fn in ("kt_equilibrium_pressure", "kt_speed_of_sound_squared", "kt_effective_temperature",
+                   "kt_equilibrium_energy_density"):
+            getattr(L, fn).argtypes = [ctypes.POINTER(KtParams), ctypes.c_double]
+            getattr(L, fn).restype = ctypes.c_double
+        L.kt_get_inferred_variables.argtypes = [ctypes.POINTER(KtParams), ctypes.c_double, ctypes.c_void_p,
+                                                ctypes.c_double] + [ctypes.POINTER(ctypes.c_double)] * 6
+        L.kt_get_inferred_variables.restype = None
+        _oracle = L
+    return _oracle
+
+
+def _ptrs(arrays):
+    return (ctypes.c_void_p * len(arrays))(*[None if a is None else a.ctypes.data for a in arrays])
+
+
+class _Base:
+    """Shared geometry and numpy plumbing."""
+
+    def __init__(self, nx, ny, nz, dx, dy, dz, dt, etabar, theta, conformal, shear, bulk):
+        self.nx, self.ny, self.nz = nx, ny, nz
+        self.ncx, self.ncy, self.ncz = nx + 4, ny + 4, nz + 4
+        self.ng = self.ncx * self.ncy * self.ncz
+        self.conformal, self.shear, self.bulk = bool(conformal), bool(shear), bool(bulk)
+        self.params = dict(nx=nx, ny=ny, nz=nz, dx=dx, dy=dy, dz=dz, dt=dt, etabar=etabar, theta=theta,
+                           conformal=int(conformal), shear=int(shear), bulk=int(bulk))
+        self.qnames = q_names(shear, bulk)
+        self.nq = len(self.qnames)
+        self.field_names = self.qnames + PRIM_NAMES
+
+    def _prim_list(self, prim: dict):
+        order = ["e", "ut", "ux", "uy", "un"] + self.qnames[4:]
+        out = []
+        for k in order:
+            a = prim.get(k)
+            if a is None:
+                a = np.zeros(self.ng)
+            out.append(np.ascontiguousarray(np.broadcast_to(np.asarray(a, np.float64).reshape(-1), (self.ng,))))
+        return out
+
+    def _field_list(self, state: dict):
+        out = []
+        for k in self.field_names:
+            a = state.get(k)
+            out.append(None if a is None else np.ascontiguousarray(np.asarray(a, np.float64).reshape(-1)))
+        return out
+
+    def interior(self, a):
+        return np.asarray(a).reshape(self.ncz, self.ncy, self.ncx)[2:-2, 2:-2, 2:-2]
+
+
+class OracleLattice(_Base):
+    """kt_oracle.c behind the shared interface."""
+
+    def __init__(self, **kw):
+        super().__init__(**kw)
+        self._L = _load_oracle()
+        self._p = KtParams(**self.params)
+        self._h = self._L.kt_create(ctypes.byref(self._p))
+        if not self._h:
+            raise ValueError("kt_create rejected the parameters")
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            self._L.kt_destroy(self._h)
+            self._h = None
+
+    def set_primitive(self, prim: dict):
+        arrs = self._prim_list(prim)
+        self._L.kt_set_primitive_state(self._h, _ptrs(arrs))
+
+    def set_state(self, state: dict):
+        arrs = self._field_list(state)
+        self._L.kt_set_state(self._h, _ptrs(arrs))
+
+    def get_state(self) -> dict:
+        arrs = [np.zeros(self.ng) for _ in self.field_names]
+        self._L.kt_get_state(self._h, _ptrs(arrs))
+        return dict(zip(self.field_names, arrs))
+
+    def step(self, t, dt, T_reg=0.0):
+        self._L.kt_rk2_step(self._h, t, dt, T_reg)
+
+    # scalar physics, for unit tests
+    def pressure(self, e):
+        return self._L.kt_equilibrium_pressure(ctypes.byref(self._p), e)
+
+    def temperature(self, e):
+        return self._L.kt_effective_temperature(ctypes.byref(self._p), e)
+
+    def energy_density(self, T):
+        return self._L.kt_equilibrium_energy_density(ctypes.byref(self._p), T)
+
+    def inferred(self, t, q, e_prev):
+        qa = np.zeros(15)
+        qa[:len(q)] = q
+        outs = [ctypes.c_double() for _ in range(6)]
+        self._L.kt_get_inferred_variables(ctypes.byref(self._p), t, qa.ctypes.data, e_prev, *outs)
+        return [o.value for o in outs]
+
+
+def ref_variant(precision: str, conformal: bool, shear: bool, bulk: bool) -> str:
+    phys = "bulk" if bulk else ("shear" if shear else "ideal")
+    return f"{precision}_{'conf' if conformal else 'qcd'}_{phys}"
+
+
+def ref_available(variant: str = "fp64_conf_shear") -> bool:
+    return os.path.exists(os.path.join(REF_DIR, f"libref_{variant}.so"))
+
+
+class RefLattice(_Base):
+    """The reference's own sources built for the CPU (one lattice per variant library)."""
+
+    def __init__(self, precision="fp64", threads=None, **kw):
+        super().__init__(**kw)
+        if self.bulk and not self.shear:
+            raise ValueError("bulk without shear is not a valid reference build")
+        self.variant = ref_variant(precision, self.conformal, self.shear, self.bulk)
+        path = os.path.join(REF_DIR, f"libref_{self.variant}.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        L = ctypes.CDLL(path)
+        L.gvh_ref_init.argtypes = [ctypes.c_int] * 3 + [ctypes.c_double] * 6
+        L.gvh_ref_rk2_step.argtypes = [ctypes.c_double] * 3
+        for fn in ("gvh_ref_set_state", "gvh_ref_get_state", "gvh_ref_set_primitive_state"):
+            getattr(L, fn).argtypes = [ctypes.c_void_p]
+        for fn in ("gvh_ref_equilibrium_pressure", "gvh_ref_effective_temperature",
+                   "gvh_ref_equilibrium_energy_density", "gvh_ref_speed_of_sound_squared"):
+            getattr(L, fn).argtypes = [ctypes.c_double]
+            getattr(L, fn).restype = ctypes.c_double
+        L.gvh_ref_inferred.argtypes = [ctypes.c_double, ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p]
+        L.gvh_ref_set_threads.argtypes = [ctypes.c_int]
+        self._L = L
+        if threads:
+            L.gvh_ref_set_threads(int(threads))
+        assert L.gvh_ref_nq() == self.nq, (L.gvh_ref_nq(), self.nq)
+        p = self.params
+        rc = L.gvh_ref_init(p["nx"], p["ny"], p["nz"], p["dx"], p["dy"], p["dz"], p["dt"], p["etabar"], p["theta"])
+        if rc != 0:
+            raise ValueError("gvh_ref_init failed")
+
+    def max_threads(self) -> int:
+        return int(self._L.gvh_ref_max_threads())
+
+    def set_primitive(self, prim: dict):
+        arrs = self._prim_list(prim)  # keep the arrays alive across the call
+        self._L.gvh_ref_set_primitive_state(_ptrs(arrs))
+
+    def set_state(self, state: dict):
+        arrs = self._field_list(state)
+        self._L.gvh_ref_set_state(_ptrs(arrs))
+
+    def get_state(self) -> dict:
+        arrs = [np.zeros(self.ng) for _ in self.field_names]
+        self._L.gvh_ref_get_state(_ptrs(arrs))
+        return dict(zip(self.field_names, arrs))
+
+    def step(self, t, dt, T_reg=0.0):
+        self._L.gvh_ref_rk2_step(t, dt, T_reg)
+
+    def pressure(self, e):
+        return self._L.gvh_ref_equilibrium_pressure(e)
+
+    def temperature(self, e):
+        return self._L.gvh_ref_effective_temperature(e)
+
+    def energy_density(self, T):
+        return self._L.gvh_ref_equilibrium_energy_density(T)
+
+    def inferred(self, t, q, e_prev):
+        qa = np.zeros(15)
+        qa[:len(q)] = q
+        out = np.zeros(6)
+        self._L.gvh_ref_inferred(t, qa.ctypes.data, e_prev, out.ctypes.data)
+        return list(out)

@@ -1,0 +1,126 @@
+"""Build recipe for oracle/_ref: the reference's own hot-path sources compiled for the CPU.
+
+Test infrastructure only (the pinning oracle and the benchmark's reference arm). It
+compiles gpu-vh's rhic/src/*.cu files IN PLACE from the reference tree with g++ through
+the host shim in oracle/ref_shim, links them with oracle/ref_driver.cpp, and writes one
+shared library per physics variant into oracle/_ref/ (git-ignored; it travels with the
+working tree to the GPU host like every other built .so).
+
+One file needs a generated overlay copy: FluxLimiter.cu hard-codes `#define THETA 2.0`
+(FluxLimiter.cu:15) after its includes, so no header can override it. The copy, written to
+oracle/_ref/overlay/, only turns THETA into a runtime double so one build serves both the
+shipped theta=2.0 and the theta=1.8 configuration. Every other source is compiled unchanged.
+
+Variants (compile-time switches the reference exposes as macros):
+  precision  fp64 (PRECISION double + double intrinsics, via the shim) | fp32 (as shipped)
+  eos        conf (CONFORMAL_EOS, EquationOfState.cuh:16) | qcd (default WB fit)
+  physics    bulk (PIMUNU+PI: 15 components) | shear (PI off: 14) | ideal (4)
+"""
+from __future__ import annotations
+
+import itertools
+import os
+import shutil
+import subprocess
+import sys
+from concurrent.futures import ThreadPoolExecutor
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_ROOT = os.environ.get("GVH_REFERENCE_ROOT", "/root/reference")
+OUT = os.path.join(HERE, "_ref")
+
+SOURCES = [
+    "EulerStep.cu",
+    "SemiDiscreteKurganovTadmorScheme.cu",
+    "HalfSiteExtrapolation.cu",
+    "LocalPropagationSpeed.cu",
+    "SpectralRadius.cu",
+    "FluxFunctions.cu",
+    "SourceTerms.cu",
+    "TransportCoefficients.cu",
+    "EnergyMomentumTensor.cu",
+    "EquationOfState.cu",
+    "RegulateDissipativeCurrents.cu",
+]
+
+PRECISIONS = {"fp64": ["-DGVH_REF_FP64"], "fp32": []}
+EOS = {"conf": ["-DCONFORMAL_EOS"], "qcd": []}
+PHYSICS = {"bulk": [], "shear": ["-DGVH_REF_NO_BULK"], "ideal": ["-DGVH_REF_IDEAL"]}
+
+
+def variant_names():
+    return ["_".join(v) for v in itertools.product(PRECISIONS, EOS, PHYSICS)]
+
+
+def lib_path(name: str) -> str:
+    return os.path.join(OUT, f"libref_{name}.so")
+
+
+def _overlay_flux_limiter() -> str:
+    src = os.path.join(REF_ROOT, "rhic", "src", "FluxLimiter.cu")
+    with open(src) as f:
+        text = f.read()
+    needle = "#define THETA 2.0"
+    if needle not in text:
+        raise RuntimeError(f"{src}: expected '{needle}' not found")
+    text = text.replace(needle, "extern double gvh_ref_theta;\n#define THETA gvh_ref_theta")
+    d = os.path.join(OUT, "overlay")
+    os.makedirs(d, exist_ok=True)
+    dst = os.path.join(d, "FluxLimiter.cu")
+    with open(dst, "w") as f:
+        f.write(text)
+    return dst
+
+
+def _run(cmd):
+    r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("command failed: " + " ".join(cmd) + "\n" + r.stdout)
+
+
+def build_variant(name: str, flux_limiter: str) -> str:
+    prec, eos, phys = name.split("_")
+    flags = PRECISIONS[prec] + EOS[eos] + PHYSICS[phys]
+    obj_dir = os.path.join(OUT, "obj", name)
+    os.makedirs(obj_dir, exist_ok=True)
+    src_dir = os.path.join(REF_ROOT, "rhic", "src")
+    inc = [
+        "-I", os.path.join(HERE, "ref_shim"),
+        "-I", os.path.join(REF_ROOT, "rhic", "include"),
+        "-I", src_dir,
+    ]
+    common = ["g++", "-std=c++14", "-O2", "-fPIC", "-fopenmp", "-ffp-contract=off", "-w"] + inc + flags
+    objs = []
+    for s in [os.path.join(src_dir, x) for x in SOURCES] + [flux_limiter]:
+        o = os.path.join(obj_dir, os.path.basename(s) + ".o")
+        _run(common + ["-x", "c++", "-c", s, "-o", o])
+        objs.append(o)
+    o = os.path.join(obj_dir, "ref_driver.o")
+    _run(common + ["-c", os.path.join(HERE, "ref_driver.cpp"), "-o", o])
+    objs.append(o)
+    lib = lib_path(name)
+    _run(["g++", "-shared", "-fopenmp", "-o", lib] + objs)
+    return lib
+
+
+def build(jobs: int | None = None, verbose: bool = True) -> list[str]:
+    """Build every variant; returns the library paths. Skips (returns []) when the
+    reference tree is not present, e.g. on a host that only runs prebuilt files."""
+    if not os.path.isdir(os.path.join(REF_ROOT, "rhic", "src")):
+        if verbose:
+            print(f"[oracle/_ref] reference tree not found at {REF_ROOT}; skipping")
+        return []
+    os.makedirs(OUT, exist_ok=True)
+    fl = _overlay_flux_limiter()
+    names = variant_names()
+    with ThreadPoolExecutor(max_workers=jobs or min(12, os.cpu_count() or 4)) as ex:
+        libs = list(ex.map(lambda n: build_variant(n, fl), names))
+    shutil.rmtree(os.path.join(OUT, "obj"), ignore_errors=True)
+    if verbose:
+        print(f"[oracle/_ref] built {len(libs)} variants into {OUT}")
+    return libs
+
+
+if __name__ == "__main__":
+    build()
+    sys.exit(0)

@@ -1,0 +1,1 @@
+#include "gvh_ref_shim.h"

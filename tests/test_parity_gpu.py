@@ -1,0 +1,168 @@
+"""Parity of the CUDA KT step (libgvh.so, through its C ABI) with the oracle and the
+reference's golden outputs.
+
+Tolerance (plain FP64 path): per field, max over cells |cuda - ref| / max over cells |ref|
+<= 1e-12 (REL_TOL). The CUDA path contracts multiply-adds into FMAs and uses the device's
+pow/exp/tanh, so it agrees with the reference to rounding, not bit for bit. The QCD
+equation of state is solved by Newton's method with a relative stop test of 1e-3
+(EnergyMomentumTensor.cu:39); a rounding-level difference can move a cell across that
+test, so QCD cases allow QCD_TOL.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import gvh
+import oracle
+from gvh import workloads
+from helpers import rel_err, rich_state
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+import importlib.util
+
+_spec = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLDEN, "make_golden.py"))
+make_golden = importlib.util.module_from_spec(_spec)
+_spec.loader.exec_module(make_golden)
+
+REL_TOL = 1e-12
+QCD_TOL = 1e-9
+
+
+def tol_for(lat_kw):
+    return REL_TOL if lat_kw["conformal"] else QCD_TOL
+
+
+@pytest.mark.parametrize("case", sorted(make_golden.CASES))
+def test_cuda_matches_golden(case):
+    lat_kw, steps, T_reg, st_kw = make_golden.CASES[case]
+    g = dict(np.load(os.path.join(GOLDEN, f"{case}.npz")))
+    L, _, s0, s1 = make_golden.run_case(gvh.Lattice, lat_kw, steps, T_reg, st_kw)
+    assert L.status() == 0
+    tol = tol_for(lat_kw)
+    for k in L.field_names:
+        assert rel_err(L.interior(s0[k]), g["init_" + k]) <= REL_TOL, f"{case} init {k}"
+        err = rel_err(L.interior(s1[k]), g["final_" + k])
+        assert err <= tol, f"{case} final {k}: rel err {err:.3e} > {tol:g}"
+
+
+def test_config1_100_steps_matches_oracle():
+    """The benchmark's small event (33x33x17, conformal, shear, theta 1.8, 100 steps)."""
+    w = workloads.CONFIG1
+    kw = w.lattice_kwargs()
+    G = gvh.Lattice(**kw)
+    O = oracle.OracleLattice(**kw)
+    prim = workloads.gaussian_profile(w)
+    G.set_primitive(prim)
+    O.set_primitive(prim)
+    t = w.tau0
+    for n in range(1, w.steps + 1):
+        G.step(t, w.dtau)
+        O.step(t, w.dtau)
+        t = w.tau0 + n * w.dtau
+    sg, so = G.get_state(), O.get_state()
+    assert G.status() == 0
+    for k in G.field_names:
+        err = rel_err(G.interior(sg[k]), O.interior(so[k]))
+        assert err <= REL_TOL, f"{k}: {err:.3e}"
+    e_g, e_o = G.interior(sg["e"]), O.interior(so["e"])
+    assert np.max(np.abs(e_g - e_o) / np.abs(e_o)) <= REL_TOL
+
+
+def test_ghost_cells_are_zero_gradient():
+    lat_kw, _, _, st_kw = make_golden.CASES["conf_shear"]
+    L = gvh.Lattice(**lat_kw)
+    L.set_primitive(rich_state(L, **st_kw))
+    L.step(0.5, lat_kw["dt"])
+    s = L.get_state()
+    e = s["e"].reshape(L.ncz, L.ncy, L.ncx)
+    np.testing.assert_array_equal(e[:, :, 0], e[:, :, 2])
+    np.testing.assert_array_equal(e[:, :, 1], e[:, :, 2])
+    np.testing.assert_array_equal(e[:, :, -1], e[:, :, -3])
+    np.testing.assert_array_equal(e[0], e[2])
+    np.testing.assert_array_equal(e[:, -2], e[:, -3])
+
+
+def test_set_get_state_round_trip():
+    lat_kw, _, _, st_kw = make_golden.CASES["qcd_bulk"]
+    O = oracle.OracleLattice(**lat_kw)
+    O.set_primitive(rich_state(O, **st_kw))
+    O.step(0.5, lat_kw["dt"])
+    ref = O.get_state()
+    G = gvh.Lattice(**lat_kw)
+    G.set_state(ref)
+    back = G.get_state()
+    for k in G.field_names:
+        np.testing.assert_array_equal(G.interior(back[k]), O.interior(ref[k]), err_msg=k)
+    # continuing from a set state gives the oracle's next step
+    G.step(0.5 + lat_kw["dt"], lat_kw["dt"])
+    O.step(0.5 + lat_kw["dt"], lat_kw["dt"])
+    sg, so = G.get_state(), O.get_state()
+    for k in G.field_names:
+        assert rel_err(G.interior(sg[k]), O.interior(so[k])) <= QCD_TOL, k
+
+
+def test_status_reports_nan_without_faulting():
+    lat_kw, _, _, st_kw = make_golden.CASES["qcd_bulk"]
+    G = gvh.Lattice(**lat_kw)
+    prim = rich_state(G, **st_kw)
+    prim["e"] = prim["e"].copy()
+    prim["e"][G.ng // 2] = np.nan
+    G.set_primitive(prim)
+    assert G.status() == 0
+    G.step(0.5, lat_kw["dt"])
+    flags = G.status()
+    assert flags & gvh.GVH_STATUS_NAN
+    G.clear_status()
+    assert G.status() == 0
+
+
+def test_mirror_symmetry_full_config2_lattice():
+    """Size-independent property at the full 131x131x61 QCD + bulk lattice: an initial state
+    even under x -> -x, y -> -y, eta -> -eta stays exactly even (odd in the matching
+    velocity) step after step."""
+    w = workloads.CONFIG2
+    G = gvh.Lattice(**w.lattice_kwargs())
+    Z, Y, X = workloads.coords(w)
+    e0 = 40.0 / workloads.HBARC
+    e = e0 * np.exp(-(X ** 2 / 18 + Y ** 2 / 8)) * np.exp(-np.maximum(np.abs(Z) - 1, 0) ** 2 / 0.72) + 1e-3
+    e = e.astype(np.float32).astype(np.float64)
+    G.set_primitive(dict(e=e.reshape(-1), ut=1.0, ux=0.0, uy=0.0, un=0.0))
+    t = w.tau0
+    for n in range(1, 6):
+        G.step(t, w.dtau)
+        t = w.tau0 + n * w.dtau
+    assert G.status() == 0
+    s = G.get_state()
+    E = G.interior(s["e"])
+    np.testing.assert_array_equal(E, E[::-1, :, :])
+    np.testing.assert_array_equal(E, E[:, ::-1, :])
+    np.testing.assert_array_equal(E, E[:, :, ::-1])
+    UX = G.interior(s["ux"])
+    np.testing.assert_array_equal(UX, -UX[:, :, ::-1])
+    assert np.abs(UX).max() > 0
+
+
+def test_config2_lattice_two_steps_matches_oracle():
+    """Full-size QCD + bulk lattice with the seeded Glauber-hotspot event: two steps against
+    the (OpenMP) oracle."""
+    w = workloads.CONFIG2
+    kw = w.lattice_kwargs()
+    prim = workloads.glauber_hotspots(w)
+    prim.pop("_meta")
+    G = gvh.Lattice(**kw)
+    O = oracle.OracleLattice(**kw)
+    G.set_primitive(prim)
+    O.set_primitive(prim)
+    t = w.tau0
+    for n in range(1, 3):
+        G.step(t, w.dtau)
+        O.step(t, w.dtau)
+        t = w.tau0 + n * w.dtau
+    sg, so = G.get_state(), O.get_state()
+    assert G.status() == 0
+    for k in G.field_names:
+        err = rel_err(G.interior(sg[k]), O.interior(so[k]))
+        assert err <= QCD_TOL, f"{k}: {err:.3e}"
