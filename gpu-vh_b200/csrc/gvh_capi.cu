@@ -44,7 +44,7 @@ int fail(int code, const char *fmt, ...) {
     if (err_ != cudaSuccess) return fail(GVH_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(err_)); \
   } while (0)
 
-constexpr int kThreads = 128;
+constexpr int kThreads = gvh::kBlock;
 
 }  // namespace
 

@@ -30,23 +30,24 @@ constexpr double kF16 = (double)1.6f;      // SourceTerms.cu:57
 // Equation of state (EquationOfState.cu)
 // ------------------------------------------------------------------------------------
 
-// p(e): EquationOfState.cu:30-80 (Wuppertal-Budapest rational fit, nested fma in double);
-// conformal p = e/3.
+// The QCD fits of EquationOfState.cu are rational functions of e; they are evaluated here
+// in Horner form (the reference builds explicit powers e^2..e^13 first). The two agree to
+// rounding.
+
+// p(e): EquationOfState.cu:30-80; conformal p = e/3.
 template <int EOS>
 __device__ __forceinline__ double eq_pressure(double e) {
   if (EOS == EOS_CONFORMAL) return e / 3;
-  double e1 = e, e2 = e * e, e3 = e2 * e, e4 = e3 * e, e5 = e4 * e, e6 = e5 * e;
-  double e7 = e6 * e, e8 = e7 * e, e9 = e8 * e, e10 = e9 * e, e11 = e10 * e, e12 = e11 * e;
-  double a = fma(1.9531729608963267e-11, e12, fma(3.1188455176941583e-7, e11, fma(0.0009417586777847889, e10,
-             fma(0.7158279081255019, e9, fma(141.5073484468774, e8, fma(6340.448389300905, e7,
-             fma(41913.439282708554, e6, fma(334334.4309240126, e5, fma(1.6357487344679043e6, e4,
-             fma(3.1729694865420084e6, e3, fma(1.077580993288114e6, e2, fma(9737.845799644809, e1,
-             -0.25181736420168666))))))))))));
-  double b = fma(3.2581066229887368e-18, e12, fma(5.928138360995685e-11, e11, fma(9.601103399348206e-7, e10,
-             fma(0.002962497695527404, e9, fma(2.3405487982094204, e8, fma(499.04919730607065, e7,
-             fma(26452.34905933697, e6, fma(278581.2989342773, e5, fma(1.7851642641834426e6, e4,
-             fma(1.3512402226067686e7, e3, fma(2.0931169138134286e7, e2, fma(4.0574329080826794e6, e1,
-             45829.44617893836))))))))))));
+  double a = 1.9531729608963267e-11;
+  a = fma(a, e, 3.1188455176941583e-7); a = fma(a, e, 0.0009417586777847889); a = fma(a, e, 0.7158279081255019);
+  a = fma(a, e, 141.5073484468774); a = fma(a, e, 6340.448389300905); a = fma(a, e, 41913.439282708554);
+  a = fma(a, e, 334334.4309240126); a = fma(a, e, 1.6357487344679043e6); a = fma(a, e, 3.1729694865420084e6);
+  a = fma(a, e, 1.077580993288114e6); a = fma(a, e, 9737.845799644809); a = fma(a, e, -0.25181736420168666);
+  double b = 3.2581066229887368e-18;
+  b = fma(b, e, 5.928138360995685e-11); b = fma(b, e, 9.601103399348206e-7); b = fma(b, e, 0.002962497695527404);
+  b = fma(b, e, 2.3405487982094204); b = fma(b, e, 499.04919730607065); b = fma(b, e, 26452.34905933697);
+  b = fma(b, e, 278581.2989342773); b = fma(b, e, 1.7851642641834426e6); b = fma(b, e, 1.3512402226067686e7);
+  b = fma(b, e, 2.0931169138134286e7); b = fma(b, e, 4.0574329080826794e6); b = fma(b, e, 45829.44617893836);
   return a / b;
 }
 
@@ -55,34 +56,36 @@ __device__ __forceinline__ double eq_pressure(double e) {
 template <int EOS>
 __device__ __forceinline__ double sound_speed2(double e) {
   if (EOS == EOS_CONFORMAL) return 0.0;
-  double e2 = e * e, e3 = e2 * e, e4 = e3 * e, e5 = e4 * e, e6 = e5 * e, e7 = e6 * e;
-  double e8 = e7 * e, e9 = e8 * e, e10 = e9 * e, e11 = e10 * e, e12 = e11 * e, e13 = e12 * e;
-  return (5.191934309650155e-32 + 4.123605749683891e-23 * e + 3.1955868410879504e-16 * e2
-          + 1.4170364808063119e-10 * e3 + 6.087136671592452e-6 * e4 + 0.02969737949090831 * e5
-          + 15.382615282179595 * e6 + 460.6487249985994 * e7 + 1612.4245252438795 * e8
-          + 275.0492627924299 * e9 + 58.60283714484669 * e10 + 6.504847576502024 * e11
-          + 0.03009027913262399 * e12 + 8.189430244031285e-6 * e13)
-       / (1.4637868900982493e-30 + 6.716598285341542e-22 * e + 3.5477700458515908e-15 * e2
-          + 1.1225580509306008e-9 * e3 + 0.00003551782901018317 * e4 + 0.13653226327408863 * e5
-          + 60.85769171450653 * e6 + 1800.5461219450308 * e7 + 15190.225535036281 * e8
-          + 590.2572000057821 * e9 + 293.99144775704605 * e10 + 21.461303090563028 * e11
-          + 0.09301685073435291 * e12 + 0.000024810902623582917 * e13);
+  double c = 8.189430244031285e-6;
+  c = fma(c, e, 0.03009027913262399); c = fma(c, e, 6.504847576502024); c = fma(c, e, 58.60283714484669);
+  c = fma(c, e, 275.0492627924299); c = fma(c, e, 1612.4245252438795); c = fma(c, e, 460.6487249985994);
+  c = fma(c, e, 15.382615282179595); c = fma(c, e, 0.02969737949090831); c = fma(c, e, 6.087136671592452e-6);
+  c = fma(c, e, 1.4170364808063119e-10); c = fma(c, e, 3.1955868410879504e-16);
+  c = fma(c, e, 4.123605749683891e-23); c = fma(c, e, 5.191934309650155e-32);
+  double d = 0.000024810902623582917;
+  d = fma(d, e, 0.09301685073435291); d = fma(d, e, 21.461303090563028); d = fma(d, e, 293.99144775704605);
+  d = fma(d, e, 590.2572000057821); d = fma(d, e, 15190.225535036281); d = fma(d, e, 1800.5461219450308);
+  d = fma(d, e, 60.85769171450653); d = fma(d, e, 0.13653226327408863); d = fma(d, e, 0.00003551782901018317);
+  d = fma(d, e, 1.1225580509306008e-9); d = fma(d, e, 3.5477700458515908e-15);
+  d = fma(d, e, 6.716598285341542e-22); d = fma(d, e, 1.4637868900982493e-30);
+  return c / d;
 }
 
 // T(e): EquationOfState.cu:118-148; conformal T = (e/13.8997)^(1/4).
 template <int EOS>
 __device__ __forceinline__ double temperature(double e) {
   if (EOS == EOS_CONFORMAL) return pow(e / kEosFactor, 0.25);
-  double e2 = e * e, e3 = e2 * e, e4 = e3 * e, e5 = e4 * e, e6 = e5 * e, e7 = e6 * e;
-  double e8 = e7 * e, e9 = e8 * e, e10 = e9 * e, e11 = e10 * e;
-  return (1.510073201405604e-29 + 8.014062800678687e-18 * e + 2.4954778310451065e-10 * e2
-          + 0.000063810382643387 * e3 + 0.4873490574161924 * e4 + 207.48582344326206 * e5
-          + 6686.07424325115 * e6 + 14109.766109389702 * e7 + 1471.6180520527757 * e8
-          + 14.055788949565482 * e9 + 0.015421252394182246 * e10 + 1.5780479034557783e-6 * e11)
-       / (7.558667139355393e-28 + 1.3686372302041508e-16 * e + 2.998130743142826e-9 * e2
-          + 0.0005036835870305458 * e3 + 2.316902328874072 * e4 + 578.0778724946719 * e5
-          + 11179.193315394154 * e6 + 17965.67607192861 * e7 + 1051.0730543534657 * e8
-          + 5.916312075925817 * e9 + 0.003778342768228011 * e10 + 1.8472801679382593e-7 * e11);
+  double a = 1.5780479034557783e-6;
+  a = fma(a, e, 0.015421252394182246); a = fma(a, e, 14.055788949565482); a = fma(a, e, 1471.6180520527757);
+  a = fma(a, e, 14109.766109389702); a = fma(a, e, 6686.07424325115); a = fma(a, e, 207.48582344326206);
+  a = fma(a, e, 0.4873490574161924); a = fma(a, e, 0.000063810382643387); a = fma(a, e, 2.4954778310451065e-10);
+  a = fma(a, e, 8.014062800678687e-18); a = fma(a, e, 1.510073201405604e-29);
+  double b = 1.8472801679382593e-7;
+  b = fma(b, e, 0.003778342768228011); b = fma(b, e, 5.916312075925817); b = fma(b, e, 1051.0730543534657);
+  b = fma(b, e, 17965.67607192861); b = fma(b, e, 11179.193315394154); b = fma(b, e, 578.0778724946719);
+  b = fma(b, e, 2.316902328874072); b = fma(b, e, 0.0005036835870305458); b = fma(b, e, 2.998130743142826e-9);
+  b = fma(b, e, 1.3686372302041508e-16); b = fma(b, e, 7.558667139355393e-28);
+  return a / b;
 }
 
 // e(T): EquationOfState.cu:150-204; conformal e = 13.8997 T^4. Host-callable: the host
@@ -132,39 +135,119 @@ enum : unsigned { STATUS_NAN = 1u, STATUS_NEWTON = 2u };
 // returns the last iterate (as the reference does at its cap) and raises STATUS_NEWTON.
 constexpr int kNewtonMaxIters = 500;
 
-// e from (M0, M, Pi): EnergyMomentumTensor.cu:18-48.
+// p(e) and c_s^2(e) of the QCD fit together, both rational functions evaluated in Horner
+// form (the reference evaluates the same polynomials from explicit powers,
+// EquationOfState.cu:30-116; the two agree to rounding).
+__device__ __forceinline__ void qcd_p_cs2(double e, double &p, double &cs2) {
+  double a = 1.9531729608963267e-11;
+  a = fma(a, e, 3.1188455176941583e-7); a = fma(a, e, 0.0009417586777847889); a = fma(a, e, 0.7158279081255019);
+  a = fma(a, e, 141.5073484468774); a = fma(a, e, 6340.448389300905); a = fma(a, e, 41913.439282708554);
+  a = fma(a, e, 334334.4309240126); a = fma(a, e, 1.6357487344679043e6); a = fma(a, e, 3.1729694865420084e6);
+  a = fma(a, e, 1.077580993288114e6); a = fma(a, e, 9737.845799644809); a = fma(a, e, -0.25181736420168666);
+  double b = 3.2581066229887368e-18;
+  b = fma(b, e, 5.928138360995685e-11); b = fma(b, e, 9.601103399348206e-7); b = fma(b, e, 0.002962497695527404);
+  b = fma(b, e, 2.3405487982094204); b = fma(b, e, 499.04919730607065); b = fma(b, e, 26452.34905933697);
+  b = fma(b, e, 278581.2989342773); b = fma(b, e, 1.7851642641834426e6); b = fma(b, e, 1.3512402226067686e7);
+  b = fma(b, e, 2.0931169138134286e7); b = fma(b, e, 4.0574329080826794e6); b = fma(b, e, 45829.44617893836);
+  double c = 8.189430244031285e-6;
+  c = fma(c, e, 0.03009027913262399); c = fma(c, e, 6.504847576502024); c = fma(c, e, 58.60283714484669);
+  c = fma(c, e, 275.0492627924299); c = fma(c, e, 1612.4245252438795); c = fma(c, e, 460.6487249985994);
+  c = fma(c, e, 15.382615282179595); c = fma(c, e, 0.02969737949090831); c = fma(c, e, 6.087136671592452e-6);
+  c = fma(c, e, 1.4170364808063119e-10); c = fma(c, e, 3.1955868410879504e-16);
+  c = fma(c, e, 4.123605749683891e-23); c = fma(c, e, 5.191934309650155e-32);
+  double d = 0.000024810902623582917;
+  d = fma(d, e, 0.09301685073435291); d = fma(d, e, 21.461303090563028); d = fma(d, e, 293.99144775704605);
+  d = fma(d, e, 590.2572000057821); d = fma(d, e, 15190.225535036281); d = fma(d, e, 1800.5461219450308);
+  d = fma(d, e, 60.85769171450653); d = fma(d, e, 0.13653226327408863); d = fma(d, e, 0.00003551782901018317);
+  d = fma(d, e, 1.1225580509306008e-9); d = fma(d, e, 3.5477700458515908e-15);
+  d = fma(d, e, 6.716598285341542e-22); d = fma(d, e, 1.4637868900982493e-30);
+  p = a / b;
+  cs2 = c / d;
+}
+
+// The QCD fit at the Newton guess. Every solve of one cell starts from the same guess (the
+// cell's energy density), so the first iteration's p and c_s^2 are computed once per cell.
+struct GuessEos {
+  double e, inv_e, p, cs2;
+};
 template <int EOS>
-__device__ __forceinline__ double energy_from_conserved(double ePrev, double M0, double M, double Pi,
-                                                        unsigned &status) {
-  if (EOS == EOS_CONFORMAL) return fabs(sqrt(fabs(4 * M0 * M0 - 3 * M)) - M0);
-  double e0 = ePrev;
-  for (int j = 0; j < kNewtonMaxIters; ++j) {
-    double p = eq_pressure<EOS>(e0);
-    double cs2 = sound_speed2<EOS>(e0);
-    double cst2 = p / e0;
-    double A = fma(M0, 1 - cst2, Pi);
-    double B = fma(M0, M0 + Pi, -M);
-    double H = sqrt(fabs(A * A + 4 * cst2 * B));
-    double D = (A - H) / (2 * cst2);
-    double f = e0 + D;
-    double fp = 1 - ((cs2 - cst2) * (B + D * H - ((cs2 - cst2) * cst2 * D * M0) / e0)) / (cst2 * e0 * H);
-    double e = e0 - f / fp;
-    if (fabs(e - e0) <= 0.001 * fabs(e)) return e;
-    e0 = e;
+__device__ __forceinline__ GuessEos guess_eos(double ePrev) {
+  GuessEos g;
+  g.e = ePrev;
+  g.inv_e = 1.0 / ePrev;
+  if (EOS == EOS_CONFORMAL) {
+    g.p = 0.0;
+    g.cs2 = 0.0;
+  } else {
+    qcd_p_cs2(ePrev, g.p, g.cs2);
   }
-  status |= STATUS_NEWTON;
-  return e0;
+  return g;
+}
+
+// One Newton update of EnergyMomentumTensor.cu:22-40 (divisions by e0 and by cst2*e0*H =
+// p*H taken through a shared reciprocal / the product p*H; equal to rounding).
+__device__ __forceinline__ double newton_update(double e0, double inv_e0, double p, double cs2, double M0, double M,
+                                                double Pi) {
+  double cst2 = p * inv_e0;
+  double A = fma(M0, 1 - cst2, Pi);
+  double B = fma(M0, M0 + Pi, -M);
+  double H = sqrt(fabs(A * A + 4 * cst2 * B));
+  double D = (A - H) / (2 * cst2);
+  double f = e0 + D;
+  double g = cs2 - cst2;
+  double fp = 1 - (g * (B + D * H - (g * cst2 * D * M0) * inv_e0)) / (p * H);
+  return e0 - f / fp;
+}
+
+// N independent Newton solves (EnergyMomentumTensor.cu:18-48) iterated together: each
+// follows its own sequence of iterates and stops at its own iteration (|de| <= 1e-3 |e|),
+// while the independent chains give the FP64 pipe instruction-level parallelism.
+template <int EOS, int N>
+__device__ __forceinline__ void energy_from_conserved_n(const GuessEos &g0, const double (&M0)[N],
+                                                        const double (&M)[N], const double (&Pi)[N],
+                                                        double (&out)[N], unsigned &status) {
+  if (EOS == EOS_CONFORMAL) {
+#pragma unroll
+    for (int n = 0; n < N; ++n) out[n] = fabs(sqrt(fabs(4 * M0[n] * M0[n] - 3 * M[n])) - M0[n]);
+    return;
+  }
+  double e0[N];
+  bool done[N];
+  bool all = true;
+#pragma unroll
+  for (int n = 0; n < N; ++n) {
+    double e = newton_update(g0.e, g0.inv_e, g0.p, g0.cs2, M0[n], M[n], Pi[n]);
+    done[n] = fabs(e - g0.e) <= 0.001 * fabs(e);
+    e0[n] = e;
+    out[n] = e;
+    all = all && done[n];
+  }
+  for (int j = 1; j < kNewtonMaxIters && !all; ++j) {
+    all = true;
+#pragma unroll
+    for (int n = 0; n < N; ++n) {
+      if (done[n]) continue;
+      double p, cs2;
+      qcd_p_cs2(e0[n], p, cs2);
+      double e = newton_update(e0[n], 1.0 / e0[n], p, cs2, M0[n], M[n], Pi[n]);
+      done[n] = fabs(e - e0[n]) <= 0.001 * fabs(e);
+      e0[n] = e;
+      out[n] = e;
+      all = all && done[n];
+    }
+  }
+  if (!all) status |= STATUS_NEWTON;
 }
 
 struct Prim {
   double e, p, ut, ux, uy, un;
 };
 
-// getInferredVariables: EnergyMomentumTensor.cu:50-108. The Pi clamp guarded by the
-// never-defined `Pi` macro (lines 82-85) is not part of the reference's behaviour.
+// getInferredVariables: EnergyMomentumTensor.cu:50-108, guess g0.e. The Pi clamp guarded
+// by the never-defined `Pi` macro (lines 82-85) is not part of the reference's behaviour.
 template <int EOS>
 __device__ __forceinline__ Prim inferred(double t, double ttt, double ttx, double tty, double ttn, double pitt,
-                                         double pitx, double pity, double pitn, double Pi, double ePrev,
+                                         double pitx, double pity, double pitn, double Pi, const GuessEos &g0,
                                          unsigned &status) {
   Prim r;
   double M0 = ttt - pitt;
@@ -172,8 +255,13 @@ __device__ __forceinline__ Prim inferred(double t, double ttt, double ttx, doubl
   double M2 = tty - pity;
   double M3 = ttn - pitn;
   double M = M1 * M1 + M2 * M2 + t * t * M3 * M3;
-  if (ePrev <= 0.1) r.e = M0 - M / M0;
-  else r.e = energy_from_conserved<EOS>(ePrev, M0, M, Pi, status);
+  if (g0.e <= 0.1) {
+    r.e = M0 - M / M0;
+  } else {
+    double m0[1] = {M0}, mm[1] = {M}, pi[1] = {Pi}, e[1];
+    energy_from_conserved_n<EOS, 1>(g0, m0, mm, pi, e, status);
+    r.e = e[0];
+  }
   if (isnan(r.e)) status |= STATUS_NAN;
   r.p = eq_pressure<EOS>(r.e);
   if (r.e < 1.e-7) { r.e = 1.e-7; r.p = 1.e-7; }
@@ -187,6 +275,47 @@ __device__ __forceinline__ Prim inferred(double t, double ttt, double ttx, doubl
   return r;
 }
 
+// N primitive recoveries sharing one guess-independent formulation (EnergyMomentumTensor.cu
+// :50-108), the Newton solves iterated together. Outputs e, p, u^tau and w = u^axis/u^tau
+// for the axis the KT face flux needs (the only velocity the flux uses).
+template <int EOS, int N, int AXIS>
+__device__ __forceinline__ void inferred_face_n(double t, const double (&ttt)[N], const double (&ttx)[N],
+                                                const double (&tty)[N], const double (&ttn)[N],
+                                                const double (&pitt)[N], const double (&pitx)[N],
+                                                const double (&pity)[N], const double (&pitn)[N],
+                                                const double (&Pi)[N], const GuessEos &g0, double (&w)[N],
+                                                unsigned &status) {
+  const double ePrev = g0.e;
+  double M0[N], M[N], Mi[N], e[N];
+#pragma unroll
+  for (int n = 0; n < N; ++n) {
+    M0[n] = ttt[n] - pitt[n];
+    double M1 = ttx[n] - pitx[n];
+    double M2 = tty[n] - pity[n];
+    double M3 = ttn[n] - pitn[n];
+    M[n] = M1 * M1 + M2 * M2 + t * t * M3 * M3;
+    Mi[n] = AXIS == 0 ? M1 : AXIS == 1 ? M2 : M3;
+  }
+  if (ePrev <= 0.1) {
+#pragma unroll
+    for (int n = 0; n < N; ++n) e[n] = M0[n] - M[n] / M0[n];
+  } else {
+    energy_from_conserved_n<EOS, N>(g0, M0, M, Pi, e, status);
+  }
+#pragma unroll
+  for (int n = 0; n < N; ++n) {
+    if (isnan(e[n])) status |= STATUS_NAN;
+    double p = eq_pressure<EOS>(e[n]);
+    double en = e[n];
+    if (en < 1.e-7) { en = 1.e-7; p = 1.e-7; }
+    double P = p + Pi[n];
+    double E = 1 / (en + P);
+    double ut = sqrt(fabs((M0[n] + P) * E));
+    double E2 = E / ut;
+    w[n] = (Mi[n] * E2) / ut;
+  }
+}
+
 // ------------------------------------------------------------------------------------
 // Limiter (FluxLimiter.cu:17-39): generalised minmod, sign(0) = +1.
 // ------------------------------------------------------------------------------------
@@ -194,12 +323,17 @@ template <class R>
 __device__ __forceinline__ R sgn1(R x) { return x < R(0) ? R(-1) : R(1); }
 template <class R>
 __device__ __forceinline__ R minmod2(R x, R y) { return (sgn1(x) + sgn1(y)) * fmin(fabs(x), fabs(y)) / R(2); }
+// minmod(left, minmod(ctr, right)) of FluxLimiter.cu:33-38 in closed form: the smallest of
+// the three when all are positive, the largest when all are negative, else 0 (a zero
+// argument counts as positive there and yields 0 here too). Same values, fewer operations.
 template <class R>
 __device__ __forceinline__ R limited_slope(R theta, R x, R y, R z) {
   R left = theta * (y - x);
   R ctr = (z - x) / R(2);
   R right = theta * (z - y);
-  return minmod2(left, minmod2(ctr, right));
+  R lo = fmin(left, fmin(ctr, right));
+  R hi = fmax(left, fmax(ctr, right));
+  return lo > R(0) ? lo : (hi < R(0) ? hi : R(0));
 }
 
 }  // namespace gvh

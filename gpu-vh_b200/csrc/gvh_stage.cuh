@@ -1,4 +1,4 @@
-// gvh_stage.cuh -- the fused KT stage kernel.
+// gvh_stage.cuh -- the fused KT stage kernel (plain FP64 path).
 //
 // One launch is one RK substep of twoStepRungeKutta (FullyDiscreteKurganovTadmorScheme.cu
 // :109-139) over every interior cell. Per cell it does what the reference spreads over
@@ -8,7 +8,17 @@
 // regulateDissipativeCurrents (RegulateDissipativeCurrents.cu:15-134), keeping everything
 // in registers and writing each output once. setGhostCells (GhostCells.cu:15-144) is
 // replaced by clamped neighbour indices: a zero-gradient ghost always equals the nearest
-// interior cell, and the stencils are axis-aligned, so clamping reads the same values.
+// interior cell, and every stencil is axis-aligned, so clamping reads the same values.
+//
+// Each cell evaluates both faces of each axis with its own energy density as the Newton
+// guess, as the reference does (EulerStep.cu:1054-1062): for the QCD equation of state the
+// face solution depends on that guess through the solver's stop test, so sharing a face
+// between two cells would change the answer.
+//
+// Per axis the flux is done in two phases to keep few values live: (A) the face states of
+// the components the root find needs (T^{tau mu}, pi^{tau mu}, Pi) give u^axis/u^tau on both
+// sides of both faces (4 Newton solves iterated together); (B) every component is then
+// streamed through: 5 loads, 3 limited slopes, two KT fluxes, accumulate.
 //
 // Layout in HBM (interior only, no ghosts): component-major SoA, cell index
 // s = i + sy*j + sz*k, component c at c*cs + s.
@@ -43,136 +53,150 @@ struct StageArgs {
   unsigned *status;       // or-ed STATUS_* bits
 };
 
+constexpr int kBlock = 128;  // threads per block of the stage kernel
+
 template <bool SHEAR, bool BULK>
 struct NComp {
   static constexpr int value = 4 + (SHEAR ? 10 : 0) + (BULK ? 1 : 0);
 };
 
-// Half-cell states of one face from the 4 cells around it (HalfSiteExtrapolation.cu:15-30):
-// qL = q0 + D(q-1,q0,q1)/2, qR = q1 - D(q0,q1,q2)/2.
-__device__ __forceinline__ void face_states(double theta, double qa, double qb, double qc, double qd, double &qL,
-                                            double &qR) {
-  qL = qb + limited_slope(theta, qa, qb, qc) / 2;
-  qR = qc - limited_slope(theta, qb, qc, qd) / 2;
+// u^axis/u^tau on the left and right of the faces i+1/2 (fwd) and i-1/2 (bwd), and the
+// local propagation speed of each face (LocalPropagationSpeed.cu:15-24, SpectralRadius.cu).
+struct FaceSpeeds {
+  double wLf, wRf, af, wLb, wRb, ab;
+};
+
+// Phase A. Half-cell states (HalfSiteExtrapolation.cu:15-30) of the root-find components
+// at both faces, then primitive recovery of all four (SemiDiscreteKurganovTadmorScheme.cu
+// :41-44) with the cell's own energy density as guess.
+template <int EOS, bool SHEAR, bool BULK, int AXIS>
+__device__ __forceinline__ FaceSpeeds face_speeds(const StageArgs &a, long long s, const long long (&o)[5],
+                                                  const GuessEos &g0, unsigned &status) {
+  // index 0: fwd R, 1: fwd L, 2: bwd R, 3: bwd L
+  double st[9][4];
+  constexpr int NR = 4 + (SHEAR ? 4 : 0) + (BULK ? 1 : 0);
+#pragma unroll
+  for (int r = 0; r < NR; ++r) {
+    const int c = (r < 8) ? r : 14;
+    const double *q = a.qin + c * a.cs + s;
+    const double q0 = __ldg(q + o[0]), q1 = __ldg(q + o[1]), q2 = __ldg(q), q3 = __ldg(q + o[3]), q4 = __ldg(q + o[4]);
+    const double Dm = limited_slope(a.theta, q0, q1, q2);
+    const double D0 = limited_slope(a.theta, q1, q2, q3);
+    const double Dp = limited_slope(a.theta, q2, q3, q4);
+    st[r][0] = q3 - Dp / 2;   // fwd qR
+    st[r][1] = q2 + D0 / 2;   // fwd qL
+    st[r][2] = q2 - D0 / 2;   // bwd qR
+    st[r][3] = q1 + Dm / 2;   // bwd qL
+  }
+#pragma unroll
+  for (int r = NR; r < 9; ++r)
+#pragma unroll
+    for (int f = 0; f < 4; ++f) st[r][f] = 0.0;
+  double w[4];
+  inferred_face_n<EOS, 4, AXIS>(a.t_euler, st[0], st[1], st[2], st[3], st[4], st[5], st[6], st[7], st[8], g0, w,
+                                status);
+  FaceSpeeds f;
+  f.wRf = w[0]; f.wLf = w[1]; f.wRb = w[2]; f.wLb = w[3];
+  f.af = fmax(fabs(f.wLf), fabs(f.wRf));
+  f.ab = fmax(fabs(f.wLb), fabs(f.wRb));
+  return f;
 }
 
-// KT numerical flux at one face (SemiDiscreteKurganovTadmorScheme.cu:15-57):
-// H = (F(qR) + F(qL) - a (qR - qL)) / 2, F = q v^axis, a = max |v^axis| over both sides.
-// off[0..3] are the (clamped) offsets of the 4 cells around the face; H is combined into
-// acc with sign `sgn` (-1 for the face at i+1/2, +1 for i-1/2).
-template <int EOS, int NQ, int AXIS>
-__device__ __forceinline__ void face_flux(const StageArgs &a, long long s, const long long off[4], double ePrev,
-                                          double t, double sgn, double acc[NQ], unsigned &status) {
-  double qL[NQ], qR[NQ];
-#pragma unroll
-  for (int n = 0; n < NQ; ++n) {
-    const double *c = a.qin + n * a.cs + s;
-    face_states(a.theta, __ldg(c + off[0]), __ldg(c + off[1]), __ldg(c + off[2]), __ldg(c + off[3]), qL[n], qR[n]);
-  }
-  const bool shear = NQ >= 14;
-  const bool bulk = NQ == 15;
-  Prim R = inferred<EOS>(t, qR[0], qR[1], qR[2], qR[3], shear ? qR[4] : 0.0, shear ? qR[5] : 0.0,
-                         shear ? qR[6] : 0.0, shear ? qR[7] : 0.0, bulk ? qR[NQ - 1] : 0.0, ePrev, status);
-  Prim L = inferred<EOS>(t, qL[0], qL[1], qL[2], qL[3], shear ? qL[4] : 0.0, shear ? qL[5] : 0.0,
-                         shear ? qL[6] : 0.0, shear ? qL[7] : 0.0, bulk ? qL[NQ - 1] : 0.0, ePrev, status);
-  const double vR = AXIS == 0 ? R.ux : AXIS == 1 ? R.uy : R.un;
-  const double vL = AXIS == 0 ? L.ux : AXIS == 1 ? L.uy : L.un;
-  const double sp = fmax(fabs(vL / L.ut), fabs(vR / R.ut));
-#pragma unroll
-  for (int n = 0; n < NQ; ++n) {
-    double FqR = vR * qR[n] / R.ut;
-    double FqL = vL * qL[n] / L.ut;
-    double h = (FqR + FqL - sp * (qR[n] - qL[n])) / 2;
-    acc[n] = (sgn < 0) ? -h : acc[n] + h;
-  }
+// Phase B for one component: the KT fluxes H(i+1/2), H(i-1/2)
+// (SemiDiscreteKurganovTadmorScheme.cu:48-56, F = q u^axis/u^tau, FluxFunctions.cu:18-31)
+// and their difference (EulerStep.cu:1054-1062).
+__device__ __forceinline__ double flux_difference(const StageArgs &a, const double *q, const long long (&o)[5],
+                                                  const FaceSpeeds &f) {
+  const double q0 = __ldg(q + o[0]), q1 = __ldg(q + o[1]), q2 = __ldg(q), q3 = __ldg(q + o[3]), q4 = __ldg(q + o[4]);
+  const double Dm = limited_slope(a.theta, q0, q1, q2);
+  const double D0 = limited_slope(a.theta, q1, q2, q3);
+  const double Dp = limited_slope(a.theta, q2, q3, q4);
+  const double fR = q3 - Dp / 2, fL = q2 + D0 / 2;
+  const double bR = q2 - D0 / 2, bL = q1 + Dm / 2;
+  // F(qR) and F(qL) are rounded separately (no fused multiply-add across the pair), which
+  // keeps the scheme exactly mirror-symmetric.
+  const double Hf = (__dmul_rn(fR, f.wRf) + __dmul_rn(fL, f.wLf) - f.af * (fR - fL)) * 0.5;
+  const double Hb = (__dmul_rn(bR, f.wRb) + __dmul_rn(bL, f.wLb) - f.ab * (bR - bL)) * 0.5;
+  return -Hf + Hb;
 }
 
 // One axis of the Euler update (EulerStep.cu:1011-1277, one of X/Y/Z):
 // out += dt * ( (H(i-1/2) - H(i+1/2)) / d + S_axis ), S_axis from SourceTerms.cu:443-567.
 template <int EOS, bool SHEAR, bool BULK, int AXIS>
 __device__ __forceinline__ void axis_update(const StageArgs &a, long long s, int idx, int n_axis, long long stride,
-                                            double ePrev, const double *uc, double out[NComp<SHEAR, BULK>::value],
+                                            const GuessEos &g0, const double *uc, double *out,
                                             unsigned &status) {
   constexpr int NQ = NComp<SHEAR, BULK>::value;
-  const long long m2 = (long long)(max(idx - 2, 0) - idx) * stride;
-  const long long m1 = (long long)(max(idx - 1, 0) - idx) * stride;
-  const long long p1 = (long long)(min(idx + 1, n_axis - 1) - idx) * stride;
-  const long long p2 = (long long)(min(idx + 2, n_axis - 1) - idx) * stride;
+  const long long o[5] = {(long long)(max(idx - 2, 0) - idx) * stride, (long long)(max(idx - 1, 0) - idx) * stride,
+                          0, (long long)(min(idx + 1, n_axis - 1) - idx) * stride,
+                          (long long)(min(idx + 2, n_axis - 1) - idx) * stride};
   const double d = AXIS == 0 ? a.dx : AXIS == 1 ? a.dy : a.dz;
-  double res[NQ];
-  {
-    const long long off[4] = {m1, 0, p1, p2};
-    face_flux<EOS, NQ, AXIS>(a, s, off, ePrev, a.t_euler, -1.0, res, status);
-  }
-  {
-    const long long off[4] = {m2, m1, 0, p1};
-    face_flux<EOS, NQ, AXIS>(a, s, off, ePrev, a.t_euler, +1.0, res, status);
-  }
-#pragma unroll
-  for (int n = 0; n < NQ; ++n) res[n] /= d;
+  const double inv_d = 1.0 / d;
+  const FaceSpeeds f = face_speeds<EOS, SHEAR, BULK, AXIS>(a, s, o, g0, status);
+
+  double Sa[4] = {0.0, 0.0, 0.0, 0.0};
   if (SHEAR) {
-    // centred differences of pi^{mu nu} (and Pi) along this axis
-    const double fac = 1 / d / 2;
+    // centred differences of pi^{mu nu} (and Pi) along this axis (SourceTerms.cu:443-567)
+    const double fac = inv_d / 2;
     auto der = [&](int c) {
       const double *q = a.qin + c * a.cs + s;
-      return (__ldg(q + p1) - __ldg(q + m1)) * fac;
+      return (__ldg(q + o[3]) - __ldg(q + o[1])) * fac;
     };
-    const double ut = uc[0];
-    double S0, S1, S2, S3;
+    const double v = uc[1 + AXIS] / uc[0];
     if (AXIS == 0) {
-      double vx = uc[1] / ut;
       double dpitt = der(4), dpitx = der(5), dpity = der(6), dpitn = der(7), dpixx = der(8), dpixy = der(9),
              dpixn = der(10);
       if (!BULK) {
-        S0 = dpitt * vx - dpitx;
-        S1 = dpitx * vx - dpixx;
+        Sa[0] = dpitt * v - dpitx;
+        Sa[1] = dpitx * v - dpixx;
       } else {
         double dPi = der(14);
-        S0 = dpitt * vx - dpitx - vx * dPi;
-        S1 = dpitx * vx - dpixx - dPi;
+        Sa[0] = dpitt * v - dpitx - v * dPi;
+        Sa[1] = dpitx * v - dpixx - dPi;
       }
-      S2 = dpity * vx - dpixy;
-      S3 = dpitn * vx - dpixn;
+      Sa[2] = dpity * v - dpixy;
+      Sa[3] = dpitn * v - dpixn;
     } else if (AXIS == 1) {
-      double vy = uc[2] / ut;
       double dpitt = der(4), dpitx = der(5), dpity = der(6), dpitn = der(7), dpixy = der(9), dpiyy = der(11),
              dpiyn = der(12);
       if (!BULK) {
-        S0 = dpitt * vy - dpity;
-        S2 = dpity * vy - dpiyy;
+        Sa[0] = dpitt * v - dpity;
+        Sa[2] = dpity * v - dpiyy;
       } else {
         double dPi = der(14);
-        S0 = dpitt * vy - dpity - vy * dPi;
-        S2 = dpity * vy - dpiyy - dPi;
+        Sa[0] = dpitt * v - dpity - v * dPi;
+        Sa[2] = dpity * v - dpiyy - dPi;
       }
-      S1 = dpitx * vy - dpixy;
-      S3 = dpitn * vy - dpiyn;
+      Sa[1] = dpitx * v - dpixy;
+      Sa[3] = dpitn * v - dpiyn;
     } else {
-      double vn = uc[3] / ut;
       double dpitt = der(4), dpitx = der(5), dpity = der(6), dpitn = der(7), dpixn = der(10), dpiyn = der(12),
              dpinn = der(13);
       if (!BULK) {
-        S0 = dpitt * vn - dpitn;
-        S3 = dpitn * vn - dpinn;
+        Sa[0] = dpitt * v - dpitn;
+        Sa[3] = dpitn * v - dpinn;
       } else {
         double dPi = der(14);
-        S0 = dpitt * vn - dpitn - vn * dPi;
-        S3 = dpitn * vn - dpinn - dPi / (a.t_euler * a.t_euler);
+        Sa[0] = dpitt * v - dpitn - v * dPi;
+        Sa[3] = dpitn * v - dpinn - dPi / (a.t_euler * a.t_euler);
       }
-      S1 = dpitx * vn - dpixn;
-      S2 = dpity * vn - dpiyn;
+      Sa[1] = dpitx * v - dpixn;
+      Sa[2] = dpity * v - dpiyn;
     }
-    res[0] += S0;
-    res[1] += S1;
-    res[2] += S2;
-    res[3] += S3;
   }
 #pragma unroll
-  for (int n = 0; n < NQ; ++n) out[n] += res[n] * a.dt;
+  for (int n = 0; n < NQ; ++n) {
+    double r = flux_difference(a, a.qin + n * a.cs + s, o, f) * inv_d;
+    if (SHEAR && n < 4) r += Sa[n];
+    out[n * kBlock] += r * a.dt;
+  }
 }
 
 template <int EOS, bool SHEAR, bool BULK, bool STAGE2>
-__global__ void __launch_bounds__(128) kt_stage_kernel(const StageArgs a) {
+#ifndef GVH_MIN_BLOCKS
+#define GVH_MIN_BLOCKS 3
+#endif
+__global__ void __launch_bounds__(kBlock, GVH_MIN_BLOCKS) kt_stage_kernel(const StageArgs a) {
   constexpr int NQ = NComp<SHEAR, BULK>::value;
   const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (id >= a.ncells) return;
@@ -182,64 +206,66 @@ __global__ void __launch_bounds__(128) kt_stage_kernel(const StageArgs a) {
   const long long s = i + a.sy * j + a.sz * k;
   unsigned status = 0;
 
-  // ---- centre state -------------------------------------------------------------------
-  double q[NQ];
-#pragma unroll
-  for (int n = 0; n < NQ; ++n) q[n] = __ldg(a.qin + n * a.cs + s);
   const double ePrev = a.e[s];
-  const double pc = __ldg(a.pin + s);
-  double uc[4], up[4];
+  double uc[4];
 #pragma unroll
-  for (int m = 0; m < 4; ++m) {
-    uc[m] = __ldg(a.uin + m * a.cs + s);
-    up[m] = a.uprev[m * a.cs + s];
-  }
+  for (int m = 0; m < 4; ++m) uc[m] = __ldg(a.uin + m * a.cs + s);
 
   // ---- source term: out = q + dt * S (EulerStep.cu:946-1009, SourceTerms.cu:569-755) ---
-  double out[NQ];
+  // The running update of each component lives in shared memory (this thread's column of
+  // s_out): it is read-modified-written once per axis, and keeping it out of registers
+  // leaves them to the Newton solves and the source algebra.
+  __shared__ double s_out[NQ * kBlock];
+  double *out = s_out + threadIdx.x;
   {
+    double q[NQ];
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) q[n] = __ldg(a.qin + n * a.cs + s);
+    const double pc = __ldg(a.pin + s);
     const double th = a.theta;
+    const double idx_ = 1.0 / a.dx, idy = 1.0 / a.dy, idz = 1.0 / a.dz;
     const long long xm = (i > 0) ? -1 : 0, xp = (i < a.nx - 1) ? 1 : 0;
     const long long ym = (j > 0) ? -a.sy : 0, yp = (j < a.ny - 1) ? a.sy : 0;
     const long long zm = (k > 0) ? -a.sz : 0, zp = (k < a.nz - 1) ? a.sz : 0;
     CellFlow f;
     f.ut = uc[0]; f.ux = uc[1]; f.uy = uc[2]; f.un = uc[3];
-    f.utp = up[0]; f.uxp = up[1]; f.uyp = up[2]; f.unp = up[3];
+    f.utp = a.uprev[s]; f.uxp = a.uprev[a.cs + s]; f.uyp = a.uprev[2 * a.cs + s]; f.unp = a.uprev[3 * a.cs + s];
     double du[3][4];
 #pragma unroll
     for (int m = 0; m < 4; ++m) {
       const double *u = a.uin + m * a.cs + s;
-      du[0][m] = limited_slope(th, __ldg(u + xm), uc[m], __ldg(u + xp)) / a.dx;
-      du[1][m] = limited_slope(th, __ldg(u + ym), uc[m], __ldg(u + yp)) / a.dy;
-      du[2][m] = limited_slope(th, __ldg(u + zm), uc[m], __ldg(u + zp)) / a.dz;
+      du[0][m] = limited_slope(th, __ldg(u + xm), uc[m], __ldg(u + xp)) * idx_;
+      du[1][m] = limited_slope(th, __ldg(u + ym), uc[m], __ldg(u + yp)) * idy;
+      du[2][m] = limited_slope(th, __ldg(u + zm), uc[m], __ldg(u + zp)) * idz;
     }
     f.dxut = du[0][0]; f.dyut = du[1][0]; f.dnut = du[2][0];
     f.dxux = du[0][1]; f.dyux = du[1][1]; f.dnux = du[2][1];
     f.dxuy = du[0][2]; f.dyuy = du[1][2]; f.dnuy = du[2][2];
     f.dxun = du[0][3]; f.dyun = du[1][3]; f.dnun = du[2][3];
     const double *p = a.pin + s;
-    const double dxp = limited_slope(th, __ldg(p + xm), pc, __ldg(p + xp)) / a.dx;
-    const double dyp = limited_slope(th, __ldg(p + ym), pc, __ldg(p + yp)) / a.dy;
-    const double dnp = limited_slope(th, __ldg(p + zm), pc, __ldg(p + zp)) / a.dz;
+    const double dxp = limited_slope(th, __ldg(p + xm), pc, __ldg(p + xp)) * idx_;
+    const double dyp = limited_slope(th, __ldg(p + ym), pc, __ldg(p + yp)) * idy;
+    const double dnp = limited_slope(th, __ldg(p + zm), pc, __ldg(p + zp)) * idz;
 
     const double t = a.t_euler;
     const double Pi = BULK ? q[NQ - 1] : 0.0;
     const double pitt = SHEAR ? q[4] : 0.0, pitx = SHEAR ? q[5] : 0.0, pity = SHEAR ? q[6] : 0.0;
     const double pitn = SHEAR ? q[7] : 0.0, pinn = SHEAR ? q[13] : 0.0;
     const double ut = uc[0], ux = uc[1], uy = uc[2], un = uc[3];
+    const double iut = 1.0 / ut, it = 1.0 / t;
     // Tnn (EnergyMomentumTensor.cu:205-207) with p + Pi
     const double pP = pc + Pi;
-    const double tnn = (ePrev + pP) * un * un + pP / t / t + pinn;
-    const double vx = ux / ut, vy = uy / ut, vn = un / ut;
-    const double dxvx = (f.dxux - vx * f.dxut) / ut;
-    const double dyvy = (f.dyuy - vy * f.dyut) / ut;
-    const double dnvn = (f.dnun - vn * f.dnut) / ut;
+    const double tnn = (ePrev + pP) * un * un + pP * it * it + pinn;
+    const double vx = ux * iut, vy = uy * iut, vn = un * iut;
+    const double dxvx = (f.dxux - vx * f.dxut) * iut;
+    const double dyvy = (f.dyuy - vy * f.dyut) * iut;
+    const double dnvn = (f.dnun - vn * f.dnut) * iut;
     const double dkvk = dxvx + dyvy + dnvn;
     double S[NQ];
-    S[0] = -(q[0] / t + t * tnn) + dkvk * (pitt - pc - Pi) - vx * dxp - vy * dyp - vn * dnp;
-    S[1] = -q[1] / t - dxp + dkvk * pitx;
-    S[2] = -q[2] / t - dyp + dkvk * pity;
-    S[3] = -3 * q[3] / t - dnp / (t * t) + dkvk * pitn;
+    S[0] = -(q[0] * it + t * tnn) + dkvk * (pitt - pc - Pi) - vx * dxp - vy * dyp - vn * dnp;
+    S[1] = -q[1] * it - dxp + dkvk * pitx;
+    S[2] = -q[2] * it - dyp + dkvk * pity;
+    S[3] = -3 * q[3] * it - dnp * it * it + dkvk * pitn;
     if (SHEAR) {
       Shear pi{q[4], q[5], q[6], q[7], q[8], q[9], q[10], q[11], q[12], q[13]};
       double rhs[11];
@@ -248,32 +274,33 @@ __global__ void __launch_bounds__(128) kt_stage_kernel(const StageArgs a) {
       for (int n = 4; n < NQ; ++n) S[n] = rhs[n - 4];
     }
 #pragma unroll
-    for (int n = 0; n < NQ; ++n) out[n] = q[n] + a.dt * S[n];
+    for (int n = 0; n < NQ; ++n) out[n * kBlock] = q[n] + a.dt * S[n];
   }
 
   // ---- flux divergence along x, y, eta (EulerStep.cu:1011-1277) -------------------------
-  axis_update<EOS, SHEAR, BULK, 0>(a, s, i, a.nx, 1, ePrev, uc, out, status);
-  axis_update<EOS, SHEAR, BULK, 1>(a, s, j, a.ny, a.sy, ePrev, uc, out, status);
-  axis_update<EOS, SHEAR, BULK, 2>(a, s, k, a.nz, a.sz, ePrev, uc, out, status);
+  const GuessEos g0 = guess_eos<EOS>(ePrev);
+  axis_update<EOS, SHEAR, BULK, 0>(a, s, i, a.nx, 1, g0, uc, out, status);
+  axis_update<EOS, SHEAR, BULK, 1>(a, s, j, a.ny, a.sy, g0, uc, out, status);
+  axis_update<EOS, SHEAR, BULK, 2>(a, s, k, a.nz, a.sz, g0, uc, out, status);
 
   // ---- Heun combination Q = (Q + q^n)/2 (FullyDiscreteKurganovTadmorScheme.cu:60-104) ---
+  double o[NQ];
+#pragma unroll
+  for (int n = 0; n < NQ; ++n) o[n] = out[n * kBlock];
   if (STAGE2) {
 #pragma unroll
-    for (int n = 0; n < NQ; ++n) {
-      out[n] += a.qn[n * a.cs + s];
-      out[n] /= 2;
-    }
+    for (int n = 0; n < NQ; ++n) o[n] = (o[n] + a.qn[n * a.cs + s]) * 0.5;
   }
 
   // ---- primitive recovery at the new time (EnergyMomentumTensor.cu:110-154) ---------------
   const double tn = a.t_after;
-  Prim pr = inferred<EOS>(tn, out[0], out[1], out[2], out[3], SHEAR ? out[4] : 0.0, SHEAR ? out[5] : 0.0,
-                          SHEAR ? out[6] : 0.0, SHEAR ? out[7] : 0.0, BULK ? out[NQ - 1] : 0.0, ePrev, status);
+  Prim pr = inferred<EOS>(tn, o[0], o[1], o[2], o[3], SHEAR ? o[4] : 0.0, SHEAR ? o[5] : 0.0,
+                          SHEAR ? o[6] : 0.0, SHEAR ? o[7] : 0.0, BULK ? o[NQ - 1] : 0.0, g0, status);
 
   // ---- regulation (RegulateDissipativeCurrents.cu:15-134) ----------------------------------
-  if (SHEAR) {
-    const double pitt = out[4], pitx = out[5], pity = out[6], pitn = out[7], pixx = out[8], pixy = out[9];
-    const double pixn = out[10], piyy = out[11], piyn = out[12], pinn = out[13];
+  if (SHEAR && pr.e <= a.e_reg) {
+    const double pitt = o[4], pitx = o[5], pity = o[6], pitn = o[7], pixx = o[8], pixy = o[9];
+    const double pixn = o[10], piyy = o[11], piyn = o[12], pinn = o[13];
     const double t2 = tn * tn;
     const double xi0 = 0.1, rhomax = 1.0;
     double pipi = pitt * pitt - 2 * pitx * pitx - 2 * pity * pity + pixx * pixx + 2 * pixy * pixy + piyy * piyy
@@ -291,14 +318,13 @@ __global__ void __launch_bounds__(128) kt_stage_kernel(const StageArgs a) {
     if (fabs(rho) < 1.e-7) facShear = 1.0;
     // The reference reads Pi as 0 here (its `#ifdef Pi` is never true), so rho_bulk = 0
     // and the bulk factor is always 1 (RegulateDissipativeCurrents.cu:54-58, 106-109).
-    if (pr.e > a.e_reg) facShear = 1.0;
 #pragma unroll
-    for (int n = 4; n < 14; ++n) out[n] *= facShear;
+    for (int n = 4; n < 14; ++n) o[n] *= facShear;
   }
 
   // ---- write ----------------------------------------------------------------------------
 #pragma unroll
-  for (int n = 0; n < NQ; ++n) a.qout[n * a.cs + s] = out[n];
+  for (int n = 0; n < NQ; ++n) a.qout[n * a.cs + s] = o[n];
   a.e[s] = pr.e;
   a.pout[s] = pr.p;
   a.uout[s] = pr.ut;

@@ -109,7 +109,8 @@ def test_status_reports_nan_without_faulting():
     G = gvh.Lattice(**lat_kw)
     prim = rich_state(G, **st_kw)
     prim["e"] = prim["e"].copy()
-    prim["e"][G.ng // 2] = np.nan
+    centre = 2 + G.ncx * (2 + G.ny // 2 + G.ncy * (2 + G.nz // 2)) + G.nx // 2  # an interior cell
+    prim["e"][centre] = np.nan
     G.set_primitive(prim)
     assert G.status() == 0
     G.step(0.5, lat_kw["dt"])
