@@ -278,8 +278,8 @@ __device__ __forceinline__ Prim inferred(double t, double ttt, double ttx, doubl
 // N primitive recoveries sharing one guess-independent formulation (EnergyMomentumTensor.cu
 // :50-108), the Newton solves iterated together. Outputs e, p, u^tau and w = u^axis/u^tau
 // for the axis the KT face flux needs (the only velocity the flux uses).
-template <int EOS, int N, int AXIS>
-__device__ __forceinline__ void inferred_face_n(double t, const double (&ttt)[N], const double (&ttx)[N],
+template <int EOS, int N>
+__device__ __forceinline__ void inferred_face_n(double t, int axis, const double (&ttt)[N], const double (&ttx)[N],
                                                 const double (&tty)[N], const double (&ttn)[N],
                                                 const double (&pitt)[N], const double (&pitx)[N],
                                                 const double (&pity)[N], const double (&pitn)[N],
@@ -294,7 +294,7 @@ __device__ __forceinline__ void inferred_face_n(double t, const double (&ttt)[N]
     double M2 = tty[n] - pity[n];
     double M3 = ttn[n] - pitn[n];
     M[n] = M1 * M1 + M2 * M2 + t * t * M3 * M3;
-    Mi[n] = AXIS == 0 ? M1 : AXIS == 1 ? M2 : M3;
+    Mi[n] = axis == 0 ? M1 : axis == 1 ? M2 : M3;
   }
   if (ePrev <= 0.1) {
 #pragma unroll

@@ -69,8 +69,8 @@ struct FaceSpeeds {
 // Phase A. Half-cell states (HalfSiteExtrapolation.cu:15-30) of the root-find components
 // at both faces, then primitive recovery of all four (SemiDiscreteKurganovTadmorScheme.cu
 // :41-44) with the cell's own energy density as guess.
-template <int EOS, bool SHEAR, bool BULK, int AXIS>
-__device__ __forceinline__ FaceSpeeds face_speeds(const StageArgs &a, long long s, const long long (&o)[5],
+template <int EOS, bool SHEAR, bool BULK>
+__device__ __forceinline__ FaceSpeeds face_speeds(const StageArgs &a, int s, int axis, const int (&o)[5],
                                                   const GuessEos &g0, unsigned &status) {
   // index 0: fwd R, 1: fwd L, 2: bwd R, 3: bwd L
   double st[9][4];
@@ -78,7 +78,7 @@ __device__ __forceinline__ FaceSpeeds face_speeds(const StageArgs &a, long long 
 #pragma unroll
   for (int r = 0; r < NR; ++r) {
     const int c = (r < 8) ? r : 14;
-    const double *q = a.qin + c * a.cs + s;
+    const double *q = a.qin + (size_t)c * a.cs + s;
     const double q0 = __ldg(q + o[0]), q1 = __ldg(q + o[1]), q2 = __ldg(q), q3 = __ldg(q + o[3]), q4 = __ldg(q + o[4]);
     const double Dm = limited_slope(a.theta, q0, q1, q2);
     const double D0 = limited_slope(a.theta, q1, q2, q3);
@@ -93,8 +93,8 @@ __device__ __forceinline__ FaceSpeeds face_speeds(const StageArgs &a, long long 
 #pragma unroll
     for (int f = 0; f < 4; ++f) st[r][f] = 0.0;
   double w[4];
-  inferred_face_n<EOS, 4, AXIS>(a.t_euler, st[0], st[1], st[2], st[3], st[4], st[5], st[6], st[7], st[8], g0, w,
-                                status);
+  inferred_face_n<EOS, 4>(a.t_euler, axis, st[0], st[1], st[2], st[3], st[4], st[5], st[6], st[7], st[8], g0, w,
+                          status);
   FaceSpeeds f;
   f.wRf = w[0]; f.wLf = w[1]; f.wRb = w[2]; f.wLb = w[3];
   f.af = fmax(fabs(f.wLf), fabs(f.wRf));
@@ -105,12 +105,12 @@ __device__ __forceinline__ FaceSpeeds face_speeds(const StageArgs &a, long long 
 // Phase B for one component: the KT fluxes H(i+1/2), H(i-1/2)
 // (SemiDiscreteKurganovTadmorScheme.cu:48-56, F = q u^axis/u^tau, FluxFunctions.cu:18-31)
 // and their difference (EulerStep.cu:1054-1062).
-__device__ __forceinline__ double flux_difference(const StageArgs &a, const double *q, const long long (&o)[5],
+__device__ __forceinline__ double flux_difference(double theta, const double *q, const int (&o)[5],
                                                   const FaceSpeeds &f) {
   const double q0 = __ldg(q + o[0]), q1 = __ldg(q + o[1]), q2 = __ldg(q), q3 = __ldg(q + o[3]), q4 = __ldg(q + o[4]);
-  const double Dm = limited_slope(a.theta, q0, q1, q2);
-  const double D0 = limited_slope(a.theta, q1, q2, q3);
-  const double Dp = limited_slope(a.theta, q2, q3, q4);
+  const double Dm = limited_slope(theta, q0, q1, q2);
+  const double D0 = limited_slope(theta, q1, q2, q3);
+  const double Dp = limited_slope(theta, q2, q3, q4);
   const double fR = q3 - Dp / 2, fL = q2 + D0 / 2;
   const double bR = q2 - D0 / 2, bL = q1 + Dm / 2;
   // F(qR) and F(qL) are rounded separately (no fused multiply-add across the pair), which
@@ -120,73 +120,50 @@ __device__ __forceinline__ double flux_difference(const StageArgs &a, const doub
   return -Hf + Hb;
 }
 
-// One axis of the Euler update (EulerStep.cu:1011-1277, one of X/Y/Z):
-// out += dt * ( (H(i-1/2) - H(i+1/2)) / d + S_axis ), S_axis from SourceTerms.cu:443-567.
-template <int EOS, bool SHEAR, bool BULK, int AXIS>
-__device__ __forceinline__ void axis_update(const StageArgs &a, long long s, int idx, int n_axis, long long stride,
-                                            const GuessEos &g0, const double *uc, double *out,
+// pi^{m a} component index for spatial m, a in {x, y, eta}.
+__device__ __forceinline__ int pi_spatial(int m, int a) {
+  // xx=8 xy=9 xn=10 yy=11 yn=12 nn=13
+  return (m == 0) ? 8 + a : (m == 1) ? (a == 0 ? 9 : 10 + a) : (a == 0 ? 10 : 11 + a);
+}
+
+// One axis of the Euler update (EulerStep.cu:1011-1277, one of X/Y/Z, the axis chosen at
+// run time so the code exists once): out += dt * ( (H(i-1/2) - H(i+1/2)) / d + S_axis ),
+// with S_axis of SourceTerms.cu:443-567:
+//   S_0     = d(pi^{tt}) v - d(pi^{t a}) [- v d(Pi)]
+//   S_{m+1} = d(pi^{t m}) v - d(pi^{m a}) [- d(Pi), divided by tau^2 along eta, when m = a]
+template <int EOS, bool SHEAR, bool BULK>
+__device__ __forceinline__ void axis_update(const StageArgs &a, int s, int axis, int idx, int n_axis, int stride,
+                                            double d, const GuessEos &g0, const double *uc, double *out,
                                             unsigned &status) {
   constexpr int NQ = NComp<SHEAR, BULK>::value;
-  const long long o[5] = {(long long)(max(idx - 2, 0) - idx) * stride, (long long)(max(idx - 1, 0) - idx) * stride,
-                          0, (long long)(min(idx + 1, n_axis - 1) - idx) * stride,
-                          (long long)(min(idx + 2, n_axis - 1) - idx) * stride};
-  const double d = AXIS == 0 ? a.dx : AXIS == 1 ? a.dy : a.dz;
+  const int o[5] = {(max(idx - 2, 0) - idx) * stride, (max(idx - 1, 0) - idx) * stride, 0,
+                    (min(idx + 1, n_axis - 1) - idx) * stride, (min(idx + 2, n_axis - 1) - idx) * stride};
   const double inv_d = 1.0 / d;
-  const FaceSpeeds f = face_speeds<EOS, SHEAR, BULK, AXIS>(a, s, o, g0, status);
+  const FaceSpeeds f = face_speeds<EOS, SHEAR, BULK>(a, s, axis, o, g0, status);
 
   double Sa[4] = {0.0, 0.0, 0.0, 0.0};
   if (SHEAR) {
-    // centred differences of pi^{mu nu} (and Pi) along this axis (SourceTerms.cu:443-567)
     const double fac = inv_d / 2;
     auto der = [&](int c) {
-      const double *q = a.qin + c * a.cs + s;
+      const double *q = a.qin + (size_t)c * a.cs + s;
       return (__ldg(q + o[3]) - __ldg(q + o[1])) * fac;
     };
-    const double v = uc[1 + AXIS] / uc[0];
-    if (AXIS == 0) {
-      double dpitt = der(4), dpitx = der(5), dpity = der(6), dpitn = der(7), dpixx = der(8), dpixy = der(9),
-             dpixn = der(10);
-      if (!BULK) {
-        Sa[0] = dpitt * v - dpitx;
-        Sa[1] = dpitx * v - dpixx;
-      } else {
-        double dPi = der(14);
-        Sa[0] = dpitt * v - dpitx - v * dPi;
-        Sa[1] = dpitx * v - dpixx - dPi;
-      }
-      Sa[2] = dpity * v - dpixy;
-      Sa[3] = dpitn * v - dpixn;
-    } else if (AXIS == 1) {
-      double dpitt = der(4), dpitx = der(5), dpity = der(6), dpitn = der(7), dpixy = der(9), dpiyy = der(11),
-             dpiyn = der(12);
-      if (!BULK) {
-        Sa[0] = dpitt * v - dpity;
-        Sa[2] = dpity * v - dpiyy;
-      } else {
-        double dPi = der(14);
-        Sa[0] = dpitt * v - dpity - v * dPi;
-        Sa[2] = dpity * v - dpiyy - dPi;
-      }
-      Sa[1] = dpitx * v - dpixy;
-      Sa[3] = dpitn * v - dpiyn;
-    } else {
-      double dpitt = der(4), dpitx = der(5), dpity = der(6), dpitn = der(7), dpixn = der(10), dpiyn = der(12),
-             dpinn = der(13);
-      if (!BULK) {
-        Sa[0] = dpitt * v - dpitn;
-        Sa[3] = dpitn * v - dpinn;
-      } else {
-        double dPi = der(14);
-        Sa[0] = dpitt * v - dpitn - v * dPi;
-        Sa[3] = dpitn * v - dpinn - dPi / (a.t_euler * a.t_euler);
-      }
-      Sa[1] = dpitx * v - dpixn;
-      Sa[2] = dpity * v - dpiyn;
+    const double v = uc[1 + axis] / uc[0];
+    const double dPi = BULK ? der(14) : 0.0;
+    const double dPi_aa = (axis == 2) ? dPi / (a.t_euler * a.t_euler) : dPi;
+    double s0 = der(4) * v - der(5 + axis);
+    if (BULK) s0 = s0 - v * dPi;
+    Sa[0] = s0;
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      double sm = der(5 + m) * v - der(pi_spatial(m, axis));
+      if (BULK && m == axis) sm = sm - dPi_aa;
+      Sa[1 + m] = sm;
     }
   }
-#pragma unroll
+#pragma unroll 1
   for (int n = 0; n < NQ; ++n) {
-    double r = flux_difference(a, a.qin + n * a.cs + s, o, f) * inv_d;
+    double r = flux_difference(a.theta, a.qin + (size_t)n * a.cs + s, o, f) * inv_d;
     if (SHEAR && n < 4) r += Sa[n];
     out[n * kBlock] += r * a.dt;
   }
@@ -279,9 +256,14 @@ __global__ void __launch_bounds__(kBlock, GVH_MIN_BLOCKS) kt_stage_kernel(const 
 
   // ---- flux divergence along x, y, eta (EulerStep.cu:1011-1277) -------------------------
   const GuessEos g0 = guess_eos<EOS>(ePrev);
-  axis_update<EOS, SHEAR, BULK, 0>(a, s, i, a.nx, 1, g0, uc, out, status);
-  axis_update<EOS, SHEAR, BULK, 1>(a, s, j, a.ny, a.sy, g0, uc, out, status);
-  axis_update<EOS, SHEAR, BULK, 2>(a, s, k, a.nz, a.sz, g0, uc, out, status);
+#pragma unroll 1
+  for (int axis = 0; axis < 3; ++axis) {
+    const int idx = axis == 0 ? i : axis == 1 ? j : k;
+    const int n_axis = axis == 0 ? a.nx : axis == 1 ? a.ny : a.nz;
+    const int stride = axis == 0 ? 1 : axis == 1 ? (int)a.sy : (int)a.sz;
+    const double d = axis == 0 ? a.dx : axis == 1 ? a.dy : a.dz;
+    axis_update<EOS, SHEAR, BULK>(a, (int)s, axis, idx, n_axis, stride, d, g0, uc, out, status);
+  }
 
   // ---- Heun combination Q = (Q + q^n)/2 (FullyDiscreteKurganovTadmorScheme.cu:60-104) ---
   double o[NQ];
