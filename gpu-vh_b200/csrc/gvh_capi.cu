@@ -124,13 +124,19 @@ __global__ void init_conserved_kernel(long long n, int nq, long long cs, double 
   for (int m = 0; m < 4; ++m) up[m * cs + s] = u[m * cs + s];
 }
 
-template <int EOS, bool SHEAR, bool BULK>
-int launch_stage(const gvh_handle *h, const StageArgs &a, bool stage2) {
+template <int EOS, bool SHEAR, bool BULK, bool MIXED>
+int launch_stage_p(const gvh_handle *h, const StageArgs &a, bool stage2) {
   const long long blocks = (h->ncells + kThreads - 1) / kThreads;
-  if (stage2) kt_stage_kernel<EOS, SHEAR, BULK, true><<<(unsigned)blocks, kThreads, 0, h->stream>>>(a);
-  else kt_stage_kernel<EOS, SHEAR, BULK, false><<<(unsigned)blocks, kThreads, 0, h->stream>>>(a);
+  if (stage2) kt_stage_kernel<EOS, SHEAR, BULK, true, MIXED><<<(unsigned)blocks, kThreads, 0, h->stream>>>(a);
+  else kt_stage_kernel<EOS, SHEAR, BULK, false, MIXED><<<(unsigned)blocks, kThreads, 0, h->stream>>>(a);
   GVH_CUDA(cudaGetLastError());
   return GVH_OK;
+}
+
+template <int EOS, bool SHEAR, bool BULK>
+int launch_stage(const gvh_handle *h, const StageArgs &a, bool stage2) {
+  if (h->precision == GVH_PRECISION_MIXED) return launch_stage_p<EOS, SHEAR, BULK, true>(h, a, stage2);
+  return launch_stage_p<EOS, SHEAR, BULK, false>(h, a, stage2);
 }
 
 template <int EOS>
@@ -200,8 +206,8 @@ int gvh_create(const gvh_lattice_params *L, const gvh_hydro_params *H, const gvh
     return fail(GVH_ERR_INVALID, "gvh_create: lattice spacings must be > 0");
   if (o.eos != GVH_EOS_QCD && o.eos != GVH_EOS_CONFORMAL) return fail(GVH_ERR_INVALID, "gvh_create: unknown eos");
   if (o.bulk && !o.shear) return fail(GVH_ERR_INVALID, "gvh_create: bulk needs shear (component 14 layout)");
-  if (o.precision != GVH_PRECISION_FP64)
-    return fail(GVH_ERR_INVALID, "gvh_create: precision mode %d not built", o.precision);
+  if (o.precision != GVH_PRECISION_FP64 && o.precision != GVH_PRECISION_MIXED)
+    return fail(GVH_ERR_INVALID, "gvh_create: unknown precision mode %d", o.precision);
   if (o.shear && !(H->shearViscosityToEntropyDensity > 0))
     return fail(GVH_ERR_INVALID, "gvh_create: eta/s must be > 0 with shear");
   int dev = o.device;

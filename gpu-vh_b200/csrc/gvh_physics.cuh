@@ -337,3 +337,206 @@ __device__ __forceinline__ R limited_slope(R theta, R x, R y, R z) {
 }
 
 }  // namespace gvh
+
+// ====================================================================================
+// Single-precision versions used by the mixed-precision path (fluxes, limiter, sources
+// and the face states' primitive recovery in FP32; the state, the cell-centre recovery,
+// the RK accumulation and the regulation stay FP64).
+// ====================================================================================
+namespace gvh {
+
+// Coefficients of the QCD fits (EquationOfState.cu), index k = power of e, as floats.
+__constant__ float kPa_f[13] = {-0.25181736420168666f, 9737.845799644809f, 1.077580993288114e6f,
+                                3.1729694865420084e6f, 1.6357487344679043e6f, 334334.4309240126f,
+                                41913.439282708554f, 6340.448389300905f, 141.5073484468774f,
+                                0.7158279081255019f, 0.0009417586777847889f, 3.1188455176941583e-7f,
+                                1.9531729608963267e-11f};
+__constant__ float kPb_f[13] = {45829.44617893836f, 4.0574329080826794e6f, 2.0931169138134286e7f,
+                                1.3512402226067686e7f, 1.7851642641834426e6f, 278581.2989342773f,
+                                26452.34905933697f, 499.04919730607065f, 2.3405487982094204f,
+                                0.002962497695527404f, 9.601103399348206e-7f, 5.928138360995685e-11f,
+                                3.2581066229887368e-18f};
+__constant__ float kCn_f[14] = {5.191934309650155e-32f, 4.123605749683891e-23f, 3.1955868410879504e-16f,
+                                1.4170364808063119e-10f, 6.087136671592452e-6f, 0.02969737949090831f,
+                                15.382615282179595f, 460.6487249985994f, 1612.4245252438795f,
+                                275.0492627924299f, 58.60283714484669f, 6.504847576502024f,
+                                0.03009027913262399f, 8.189430244031285e-6f};
+__constant__ float kCd_f[14] = {1.4637868900982493e-30f, 6.716598285341542e-22f, 3.5477700458515908e-15f,
+                                1.1225580509306008e-9f, 0.00003551782901018317f, 0.13653226327408863f,
+                                60.85769171450653f, 1800.5461219450308f, 15190.225535036281f,
+                                590.2572000057821f, 293.99144775704605f, 21.461303090563028f,
+                                0.09301685073435291f, 0.000024810902623582917f};
+__constant__ float kTn_f[12] = {1.510073201405604e-29f, 8.014062800678687e-18f, 2.4954778310451065e-10f,
+                                0.000063810382643387f, 0.4873490574161924f, 207.48582344326206f,
+                                6686.07424325115f, 14109.766109389702f, 1471.6180520527757f,
+                                14.055788949565482f, 0.015421252394182246f, 1.5780479034557783e-6f};
+__constant__ float kTd_f[12] = {7.558667139355393e-28f, 1.3686372302041508e-16f, 2.998130743142826e-9f,
+                                0.0005036835870305458f, 2.316902328874072f, 578.0778724946719f,
+                                11179.193315394154f, 17965.67607192861f, 1051.0730543534657f,
+                                5.916312075925817f, 0.003778342768228011f, 1.8472801679382593e-7f};
+
+// num(e)/den(e) for polynomials of degree N-1 in float. Above e = 1 both are divided by
+// e^(N-1) and evaluated in y = 1/e, which keeps every partial sum inside float range (the
+// degree-13 sums alone reach ~1e38 near e ~ 2000 fm^-4).
+template <int N>
+__device__ __forceinline__ void poly_pair_f(const float *num, const float *den, float e, float &pn, float &pd) {
+  if (e <= 1.f) {
+    pn = num[N - 1];
+    pd = den[N - 1];
+#pragma unroll
+    for (int k = N - 2; k >= 0; --k) {
+      pn = fmaf(pn, e, num[k]);
+      pd = fmaf(pd, e, den[k]);
+    }
+  } else {
+    const float y = __fdividef(1.f, e);
+    pn = num[0];
+    pd = den[0];
+#pragma unroll
+    for (int k = 1; k < N; ++k) {
+      pn = fmaf(pn, y, num[k]);
+      pd = fmaf(pd, y, den[k]);
+    }
+  }
+}
+
+__device__ __forceinline__ void qcd_p_cs2(float e, float &p, float &cs2) {
+  float a, b, c, d;
+  poly_pair_f<13>(kPa_f, kPb_f, e, a, b);
+  poly_pair_f<14>(kCn_f, kCd_f, e, c, d);
+  p = __fdividef(a, b);
+  cs2 = __fdividef(c, d);
+}
+
+template <int EOS>
+__device__ __forceinline__ float eq_pressure(float e) {
+  if (EOS == EOS_CONFORMAL) return e / 3.f;
+  float a, b;
+  poly_pair_f<13>(kPa_f, kPb_f, e, a, b);
+  return __fdividef(a, b);
+}
+
+template <int EOS>
+__device__ __forceinline__ float sound_speed2(float e) {
+  if (EOS == EOS_CONFORMAL) return 0.f;
+  float c, d;
+  poly_pair_f<14>(kCn_f, kCd_f, e, c, d);
+  return __fdividef(c, d);
+}
+
+template <int EOS>
+__device__ __forceinline__ float temperature(float e) {
+  if (EOS == EOS_CONFORMAL) return sqrtf(sqrtf(e * (float)(1.0 / kEosFactor)));
+  float a, b;
+  poly_pair_f<12>(kTn_f, kTd_f, e, a, b);
+  return __fdividef(a, b);
+}
+
+__device__ __forceinline__ float bulk_zeta_over_s(float T) {
+  float x = T * (float)(1.0 / 1.01355);
+  if (x > 1.05f) return 0.9f * __expf(-(x - 1) * 40.f) + 0.25f * __expf(-(x - 1) * (float)(1.0 / 0.13)) + 0.001f;
+  else if (x < 0.995f) return 0.9f * __expf((x - 1) * 400.f) + 0.22f * __expf((x - 1) * (float)(1.0 / 0.022)) + 0.03f;
+  return -13.77f * x * x + 27.55f * x - 13.45f;
+}
+
+struct GuessEosF {
+  float e, inv_e, p, cs2;
+};
+template <int EOS>
+__device__ __forceinline__ GuessEosF guess_eos_f(double ePrev) {
+  GuessEosF g;
+  g.e = (float)ePrev;
+  g.inv_e = __fdividef(1.f, g.e);
+  if (EOS == EOS_CONFORMAL) {
+    g.p = 0.f;
+    g.cs2 = 0.f;
+  } else {
+    qcd_p_cs2(g.e, g.p, g.cs2);
+  }
+  return g;
+}
+
+__device__ __forceinline__ float newton_update_f(float e0, float inv_e0, float p, float cs2, float M0, float M,
+                                                 float Pi) {
+  float cst2 = p * inv_e0;
+  float A = fmaf(M0, 1.f - cst2, Pi);
+  float B = fmaf(M0, M0 + Pi, -M);
+  float H = sqrtf(fabsf(A * A + 4.f * cst2 * B));
+  float D = __fdividef(A - H, 2.f * cst2);
+  float f = e0 + D;
+  float g = cs2 - cst2;
+  float fp = 1.f - __fdividef(g * (B + D * H - (g * cst2 * D * M0) * inv_e0), p * H);
+  return e0 - __fdividef(f, fp);
+}
+
+// FP32 face-state recovery (EnergyMomentumTensor.cu:18-108 in single precision) returning
+// w = u^axis/u^tau. A state whose FP32 solution is not a finite positive energy density is
+// recovered again in FP64 (ok[n] = false tells the caller to do so).
+template <int EOS, int N>
+__device__ __forceinline__ void inferred_face_n_f(float t, int axis, const float (&ttt)[N], const float (&ttx)[N],
+                                                  const float (&tty)[N], const float (&ttn)[N],
+                                                  const float (&pitt)[N], const float (&pitx)[N],
+                                                  const float (&pity)[N], const float (&pitn)[N],
+                                                  const float (&Pi)[N], const GuessEosF &g0, float (&w)[N],
+                                                  bool (&ok)[N]) {
+  float M0[N], M[N], Mi[N], e[N];
+#pragma unroll
+  for (int n = 0; n < N; ++n) {
+    M0[n] = ttt[n] - pitt[n];
+    float M1 = ttx[n] - pitx[n];
+    float M2 = tty[n] - pity[n];
+    float M3 = ttn[n] - pitn[n];
+    M[n] = M1 * M1 + M2 * M2 + t * t * M3 * M3;
+    Mi[n] = axis == 0 ? M1 : axis == 1 ? M2 : M3;
+  }
+  bool conv = true;
+  if (g0.e <= 0.1f) {
+#pragma unroll
+    for (int n = 0; n < N; ++n) e[n] = M0[n] - __fdividef(M[n], M0[n]);
+  } else if (EOS == EOS_CONFORMAL) {
+#pragma unroll
+    for (int n = 0; n < N; ++n) e[n] = fabsf(sqrtf(fabsf(4.f * M0[n] * M0[n] - 3.f * M[n])) - M0[n]);
+  } else {
+    float e0[N];
+    bool done[N];
+    bool all = true;
+#pragma unroll
+    for (int n = 0; n < N; ++n) {
+      float en = newton_update_f(g0.e, g0.inv_e, g0.p, g0.cs2, M0[n], M[n], Pi[n]);
+      done[n] = fabsf(en - g0.e) <= 0.001f * fabsf(en);
+      e0[n] = en;
+      e[n] = en;
+      all = all && done[n];
+    }
+    for (int j = 1; j < kNewtonMaxIters && !all; ++j) {
+      all = true;
+#pragma unroll
+      for (int n = 0; n < N; ++n) {
+        if (done[n]) continue;
+        float p, cs2;
+        qcd_p_cs2(e0[n], p, cs2);
+        float en = newton_update_f(e0[n], __fdividef(1.f, e0[n]), p, cs2, M0[n], M[n], Pi[n]);
+        done[n] = fabsf(en - e0[n]) <= 0.001f * fabsf(en);
+        e0[n] = en;
+        e[n] = en;
+        all = all && done[n];
+      }
+    }
+    conv = all;
+  }
+#pragma unroll
+  for (int n = 0; n < N; ++n) {
+    ok[n] = conv && e[n] > 0.f && e[n] < 3.0e37f;
+    float p = eq_pressure<EOS>(e[n]);
+    float en = e[n];
+    if (en < 1.e-7f) { en = 1.e-7f; p = 1.e-7f; }
+    float P = p + Pi[n];
+    float E = __fdividef(1.f, en + P);
+    float ut = sqrtf(fabsf((M0[n] + P) * E));
+    float E2 = __fdividef(E, ut);
+    w[n] = __fdividef(Mi[n] * E2, ut);
+    ok[n] = ok[n] && isfinite(w[n]);
+  }
+}
+
+}  // namespace gvh

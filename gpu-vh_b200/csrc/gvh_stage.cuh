@@ -26,6 +26,8 @@
 
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "gvh_physics.cuh"
 #include "gvh_sources.cuh"
 
@@ -62,16 +64,17 @@ struct NComp {
 
 // u^axis/u^tau on the left and right of the faces i+1/2 (fwd) and i-1/2 (bwd), and the
 // local propagation speed of each face (LocalPropagationSpeed.cu:15-24, SpectralRadius.cu).
+template <class R>
 struct FaceSpeeds {
-  double wLf, wRf, af, wLb, wRb, ab;
+  R wLf, wRf, af, wLb, wRb, ab;
 };
 
 // Phase A. Half-cell states (HalfSiteExtrapolation.cu:15-30) of the root-find components
 // at both faces, then primitive recovery of all four (SemiDiscreteKurganovTadmorScheme.cu
 // :41-44) with the cell's own energy density as guess.
 template <int EOS, bool SHEAR, bool BULK>
-__device__ __forceinline__ FaceSpeeds face_speeds(const StageArgs &a, int s, int axis, const int (&o)[5],
-                                                  const GuessEos &g0, unsigned &status) {
+__device__ __forceinline__ FaceSpeeds<double> face_speeds(const StageArgs &a, int s, int axis, const int (&o)[5],
+                                                       const GuessEos &g0, unsigned &status) {
   // index 0: fwd R, 1: fwd L, 2: bwd R, 3: bwd L
   double st[9][4];
   constexpr int NR = 4 + (SHEAR ? 4 : 0) + (BULK ? 1 : 0);
@@ -95,28 +98,83 @@ __device__ __forceinline__ FaceSpeeds face_speeds(const StageArgs &a, int s, int
   double w[4];
   inferred_face_n<EOS, 4>(a.t_euler, axis, st[0], st[1], st[2], st[3], st[4], st[5], st[6], st[7], st[8], g0, w,
                           status);
-  FaceSpeeds f;
+  FaceSpeeds<double> f;
   f.wRf = w[0]; f.wLf = w[1]; f.wRb = w[2]; f.wLb = w[3];
   f.af = fmax(fabs(f.wLf), fabs(f.wRf));
   f.ab = fmax(fabs(f.wLb), fabs(f.wRb));
   return f;
 }
 
+// Out-of-line copy for the mixed path's rare FP64 redo (keeps it out of the hot code).
+template <int EOS, bool SHEAR, bool BULK>
+__device__ __noinline__ FaceSpeeds<double> face_speeds_fallback(const StageArgs &a, int s, int axis,
+                                                                const int (&o)[5], const GuessEos &g0,
+                                                                unsigned &status) {
+  return face_speeds<EOS, SHEAR, BULK>(a, s, axis, o, g0, status);
+}
+
+// Mixed path: the same face states and recoveries in FP32. States whose FP32 recovery is
+// not a finite positive energy density (ok = false) are redone by the FP64 routine above.
+template <int EOS, bool SHEAR, bool BULK>
+__device__ __forceinline__ FaceSpeeds<float> face_speeds_f(const StageArgs &a, int s, int axis, const int (&o)[5],
+                                                           const GuessEosF &g0f, const GuessEos &g0,
+                                                           unsigned &status) {
+  float st[9][4];
+  constexpr int NR = 4 + (SHEAR ? 4 : 0) + (BULK ? 1 : 0);
+  const float th = (float)a.theta;
+#pragma unroll
+  for (int r = 0; r < NR; ++r) {
+    const int c = (r < 8) ? r : 14;
+    const double *q = a.qin + (size_t)c * a.cs + s;
+    const float q0 = (float)__ldg(q + o[0]), q1 = (float)__ldg(q + o[1]), q2 = (float)__ldg(q);
+    const float q3 = (float)__ldg(q + o[3]), q4 = (float)__ldg(q + o[4]);
+    const float Dm = limited_slope(th, q0, q1, q2);
+    const float D0 = limited_slope(th, q1, q2, q3);
+    const float Dp = limited_slope(th, q2, q3, q4);
+    st[r][0] = q3 - Dp * 0.5f;
+    st[r][1] = q2 + D0 * 0.5f;
+    st[r][2] = q2 - D0 * 0.5f;
+    st[r][3] = q1 + Dm * 0.5f;
+  }
+#pragma unroll
+  for (int r = NR; r < 9; ++r)
+#pragma unroll
+    for (int f = 0; f < 4; ++f) st[r][f] = 0.f;
+  float w[4];
+  bool ok[4];
+  inferred_face_n_f<EOS, 4>((float)a.t_euler, axis, st[0], st[1], st[2], st[3], st[4], st[5], st[6], st[7], st[8],
+                            g0f, w, ok);
+  FaceSpeeds<float> f;
+  if (ok[0] && ok[1] && ok[2] && ok[3]) {
+    f.wRf = w[0]; f.wLf = w[1]; f.wRb = w[2]; f.wLb = w[3];
+  } else {
+    const FaceSpeeds<double> d = face_speeds_fallback<EOS, SHEAR, BULK>(a, s, axis, o, g0, status);
+    f.wRf = (float)d.wRf; f.wLf = (float)d.wLf; f.wRb = (float)d.wRb; f.wLb = (float)d.wLb;
+  }
+  f.af = fmaxf(fabsf(f.wLf), fabsf(f.wRf));
+  f.ab = fmaxf(fabsf(f.wLb), fabsf(f.wRb));
+  return f;
+}
+
 // Phase B for one component: the KT fluxes H(i+1/2), H(i-1/2)
 // (SemiDiscreteKurganovTadmorScheme.cu:48-56, F = q u^axis/u^tau, FluxFunctions.cu:18-31)
 // and their difference (EulerStep.cu:1054-1062).
-__device__ __forceinline__ double flux_difference(double theta, const double *q, const int (&o)[5],
-                                                  const FaceSpeeds &f) {
-  const double q0 = __ldg(q + o[0]), q1 = __ldg(q + o[1]), q2 = __ldg(q), q3 = __ldg(q + o[3]), q4 = __ldg(q + o[4]);
-  const double Dm = limited_slope(theta, q0, q1, q2);
-  const double D0 = limited_slope(theta, q1, q2, q3);
-  const double Dp = limited_slope(theta, q2, q3, q4);
-  const double fR = q3 - Dp / 2, fL = q2 + D0 / 2;
-  const double bR = q2 - D0 / 2, bL = q1 + Dm / 2;
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+
+template <class R>
+__device__ __forceinline__ R flux_difference(R theta, const double *q, const int (&o)[5], const FaceSpeeds<R> &f) {
+  const R q0 = (R)__ldg(q + o[0]), q1 = (R)__ldg(q + o[1]), q2 = (R)__ldg(q), q3 = (R)__ldg(q + o[3]);
+  const R q4 = (R)__ldg(q + o[4]);
+  const R Dm = limited_slope(theta, q0, q1, q2);
+  const R D0 = limited_slope(theta, q1, q2, q3);
+  const R Dp = limited_slope(theta, q2, q3, q4);
+  const R fR = q3 - Dp / R(2), fL = q2 + D0 / R(2);
+  const R bR = q2 - D0 / R(2), bL = q1 + Dm / R(2);
   // F(qR) and F(qL) are rounded separately (no fused multiply-add across the pair), which
   // keeps the scheme exactly mirror-symmetric.
-  const double Hf = (__dmul_rn(fR, f.wRf) + __dmul_rn(fL, f.wLf) - f.af * (fR - fL)) * 0.5;
-  const double Hb = (__dmul_rn(bR, f.wRb) + __dmul_rn(bL, f.wLb) - f.ab * (bR - bL)) * 0.5;
+  const R Hf = (mul_rn(fR, f.wRf) + mul_rn(fL, f.wLf) - f.af * (fR - fL)) * R(0.5);
+  const R Hb = (mul_rn(bR, f.wRb) + mul_rn(bL, f.wLb) - f.ab * (bR - bL)) * R(0.5);
   return -Hf + Hb;
 }
 
@@ -131,49 +189,57 @@ __device__ __forceinline__ int pi_spatial(int m, int a) {
 // with S_axis of SourceTerms.cu:443-567:
 //   S_0     = d(pi^{tt}) v - d(pi^{t a}) [- v d(Pi)]
 //   S_{m+1} = d(pi^{t m}) v - d(pi^{m a}) [- d(Pi), divided by tau^2 along eta, when m = a]
-template <int EOS, bool SHEAR, bool BULK>
+template <int EOS, bool SHEAR, bool BULK, bool MIXED>
 __device__ __forceinline__ void axis_update(const StageArgs &a, int s, int axis, int idx, int n_axis, int stride,
-                                            double d, const GuessEos &g0, const double *uc, double *out,
-                                            unsigned &status) {
+                                            double d, const GuessEos &g0, const GuessEosF &g0f, const double *uc,
+                                            double *out, unsigned &status) {
+  using R = typename std::conditional<MIXED, float, double>::type;
   constexpr int NQ = NComp<SHEAR, BULK>::value;
   const int o[5] = {(max(idx - 2, 0) - idx) * stride, (max(idx - 1, 0) - idx) * stride, 0,
                     (min(idx + 1, n_axis - 1) - idx) * stride, (min(idx + 2, n_axis - 1) - idx) * stride};
-  const double inv_d = 1.0 / d;
-  const FaceSpeeds f = face_speeds<EOS, SHEAR, BULK>(a, s, axis, o, g0, status);
+  const R inv_d = R(1.0 / d);
+  FaceSpeeds<R> f;
+  if constexpr (MIXED) f = face_speeds_f<EOS, SHEAR, BULK>(a, s, axis, o, g0f, g0, status);
+  else f = face_speeds<EOS, SHEAR, BULK>(a, s, axis, o, g0, status);
 
-  double Sa[4] = {0.0, 0.0, 0.0, 0.0};
+  R Sa[4] = {R(0), R(0), R(0), R(0)};
   if (SHEAR) {
-    const double fac = inv_d / 2;
+    const R fac = inv_d / R(2);
     auto der = [&](int c) {
       const double *q = a.qin + (size_t)c * a.cs + s;
-      return (__ldg(q + o[3]) - __ldg(q + o[1])) * fac;
+      return ((R)__ldg(q + o[3]) - (R)__ldg(q + o[1])) * fac;
     };
-    const double v = uc[1 + axis] / uc[0];
-    const double dPi = BULK ? der(14) : 0.0;
-    const double dPi_aa = (axis == 2) ? dPi / (a.t_euler * a.t_euler) : dPi;
-    double s0 = der(4) * v - der(5 + axis);
+    const R v = dv((R)uc[1 + axis], (R)uc[0]);
+    const R dPi = BULK ? der(14) : R(0);
+    const R dPi_aa = (axis == 2) ? dv(dPi, (R)(a.t_euler * a.t_euler)) : dPi;
+    R s0 = der(4) * v - der(5 + axis);
     if (BULK) s0 = s0 - v * dPi;
     Sa[0] = s0;
 #pragma unroll
     for (int m = 0; m < 3; ++m) {
-      double sm = der(5 + m) * v - der(pi_spatial(m, axis));
+      R sm = der(5 + m) * v - der(pi_spatial(m, axis));
       if (BULK && m == axis) sm = sm - dPi_aa;
       Sa[1 + m] = sm;
     }
   }
+  const R th = (R)a.theta;
 #pragma unroll 1
   for (int n = 0; n < NQ; ++n) {
-    double r = flux_difference(a.theta, a.qin + (size_t)n * a.cs + s, o, f) * inv_d;
+    R r = flux_difference<R>(th, a.qin + (size_t)n * a.cs + s, o, f) * inv_d;
     if (SHEAR && n < 4) r += Sa[n];
-    out[n * kBlock] += r * a.dt;
+    out[n * kBlock] += (double)r * a.dt;
   }
 }
 
-template <int EOS, bool SHEAR, bool BULK, bool STAGE2>
 #ifndef GVH_MIN_BLOCKS
 #define GVH_MIN_BLOCKS 3
 #endif
+// MIXED = false: plain FP64. MIXED = true: limiter, fluxes and source terms in FP32 (face
+// states recovered in FP32 with an FP64 redo when that fails); the state, the running
+// update, the Heun combination, the cell-centre recovery and the regulation in FP64.
+template <int EOS, bool SHEAR, bool BULK, bool STAGE2, bool MIXED>
 __global__ void __launch_bounds__(kBlock, GVH_MIN_BLOCKS) kt_stage_kernel(const StageArgs a) {
+  using R = typename std::conditional<MIXED, float, double>::type;
   constexpr int NQ = NComp<SHEAR, BULK>::value;
   const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (id >= a.ncells) return;
@@ -188,81 +254,93 @@ __global__ void __launch_bounds__(kBlock, GVH_MIN_BLOCKS) kt_stage_kernel(const 
 #pragma unroll
   for (int m = 0; m < 4; ++m) uc[m] = __ldg(a.uin + m * a.cs + s);
 
-  // ---- source term: out = q + dt * S (EulerStep.cu:946-1009, SourceTerms.cu:569-755) ---
   // The running update of each component lives in shared memory (this thread's column of
   // s_out): it is read-modified-written once per axis, and keeping it out of registers
   // leaves them to the Newton solves and the source algebra.
   __shared__ double s_out[NQ * kBlock];
   double *out = s_out + threadIdx.x;
+
+  // ---- source term: out = q + dt * S (EulerStep.cu:946-1009, SourceTerms.cu:569-755) ---
   {
-    double q[NQ];
+    R q[NQ];
 #pragma unroll
-    for (int n = 0; n < NQ; ++n) q[n] = __ldg(a.qin + n * a.cs + s);
-    const double pc = __ldg(a.pin + s);
-    const double th = a.theta;
-    const double idx_ = 1.0 / a.dx, idy = 1.0 / a.dy, idz = 1.0 / a.dz;
+    for (int n = 0; n < NQ; ++n) q[n] = (R)__ldg(a.qin + n * a.cs + s);
+    const R pc = (R)__ldg(a.pin + s);
+    const R th = (R)a.theta;
+    const R idx_ = R(1.0 / a.dx), idy = R(1.0 / a.dy), idz = R(1.0 / a.dz);
     const long long xm = (i > 0) ? -1 : 0, xp = (i < a.nx - 1) ? 1 : 0;
     const long long ym = (j > 0) ? -a.sy : 0, yp = (j < a.ny - 1) ? a.sy : 0;
     const long long zm = (k > 0) ? -a.sz : 0, zp = (k < a.nz - 1) ? a.sz : 0;
-    CellFlow f;
-    f.ut = uc[0]; f.ux = uc[1]; f.uy = uc[2]; f.un = uc[3];
-    f.utp = a.uprev[s]; f.uxp = a.uprev[a.cs + s]; f.uyp = a.uprev[2 * a.cs + s]; f.unp = a.uprev[3 * a.cs + s];
-    double du[3][4];
+    CellFlowT<R> f;
+    R ucr[4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) ucr[m] = (R)uc[m];
+    f.ut = ucr[0]; f.ux = ucr[1]; f.uy = ucr[2]; f.un = ucr[3];
+    f.utp = (R)a.uprev[s]; f.uxp = (R)a.uprev[a.cs + s]; f.uyp = (R)a.uprev[2 * a.cs + s];
+    f.unp = (R)a.uprev[3 * a.cs + s];
+    R du[3][4];
 #pragma unroll
     for (int m = 0; m < 4; ++m) {
       const double *u = a.uin + m * a.cs + s;
-      du[0][m] = limited_slope(th, __ldg(u + xm), uc[m], __ldg(u + xp)) * idx_;
-      du[1][m] = limited_slope(th, __ldg(u + ym), uc[m], __ldg(u + yp)) * idy;
-      du[2][m] = limited_slope(th, __ldg(u + zm), uc[m], __ldg(u + zp)) * idz;
+      du[0][m] = limited_slope(th, (R)__ldg(u + xm), ucr[m], (R)__ldg(u + xp)) * idx_;
+      du[1][m] = limited_slope(th, (R)__ldg(u + ym), ucr[m], (R)__ldg(u + yp)) * idy;
+      du[2][m] = limited_slope(th, (R)__ldg(u + zm), ucr[m], (R)__ldg(u + zp)) * idz;
     }
     f.dxut = du[0][0]; f.dyut = du[1][0]; f.dnut = du[2][0];
     f.dxux = du[0][1]; f.dyux = du[1][1]; f.dnux = du[2][1];
     f.dxuy = du[0][2]; f.dyuy = du[1][2]; f.dnuy = du[2][2];
     f.dxun = du[0][3]; f.dyun = du[1][3]; f.dnun = du[2][3];
     const double *p = a.pin + s;
-    const double dxp = limited_slope(th, __ldg(p + xm), pc, __ldg(p + xp)) * idx_;
-    const double dyp = limited_slope(th, __ldg(p + ym), pc, __ldg(p + yp)) * idy;
-    const double dnp = limited_slope(th, __ldg(p + zm), pc, __ldg(p + zp)) * idz;
+    const R dxp = limited_slope(th, (R)__ldg(p + xm), pc, (R)__ldg(p + xp)) * idx_;
+    const R dyp = limited_slope(th, (R)__ldg(p + ym), pc, (R)__ldg(p + yp)) * idy;
+    const R dnp = limited_slope(th, (R)__ldg(p + zm), pc, (R)__ldg(p + zp)) * idz;
 
-    const double t = a.t_euler;
-    const double Pi = BULK ? q[NQ - 1] : 0.0;
-    const double pitt = SHEAR ? q[4] : 0.0, pitx = SHEAR ? q[5] : 0.0, pity = SHEAR ? q[6] : 0.0;
-    const double pitn = SHEAR ? q[7] : 0.0, pinn = SHEAR ? q[13] : 0.0;
-    const double ut = uc[0], ux = uc[1], uy = uc[2], un = uc[3];
-    const double iut = 1.0 / ut, it = 1.0 / t;
+    const R t = (R)a.t_euler;
+    const R Pi = BULK ? q[NQ - 1] : R(0);
+    const R pitt = SHEAR ? q[4] : R(0), pitx = SHEAR ? q[5] : R(0), pity = SHEAR ? q[6] : R(0);
+    const R pitn = SHEAR ? q[7] : R(0), pinn = SHEAR ? q[13] : R(0);
+    const R ut = ucr[0], ux = ucr[1], uy = ucr[2], un = ucr[3];
+    const R iut = dv(R(1), ut), it = dv(R(1), t);
     // Tnn (EnergyMomentumTensor.cu:205-207) with p + Pi
-    const double pP = pc + Pi;
-    const double tnn = (ePrev + pP) * un * un + pP * it * it + pinn;
-    const double vx = ux * iut, vy = uy * iut, vn = un * iut;
-    const double dxvx = (f.dxux - vx * f.dxut) * iut;
-    const double dyvy = (f.dyuy - vy * f.dyut) * iut;
-    const double dnvn = (f.dnun - vn * f.dnut) * iut;
-    const double dkvk = dxvx + dyvy + dnvn;
-    double S[NQ];
+    const R pP = pc + Pi;
+    const R er = (R)ePrev;
+    const R tnn = (er + pP) * un * un + pP * it * it + pinn;
+    const R vx = ux * iut, vy = uy * iut, vn = un * iut;
+    const R dxvx = (f.dxux - vx * f.dxut) * iut;
+    const R dyvy = (f.dyuy - vy * f.dyut) * iut;
+    const R dnvn = (f.dnun - vn * f.dnut) * iut;
+    const R dkvk = dxvx + dyvy + dnvn;
+    R S[NQ];
     S[0] = -(q[0] * it + t * tnn) + dkvk * (pitt - pc - Pi) - vx * dxp - vy * dyp - vn * dnp;
     S[1] = -q[1] * it - dxp + dkvk * pitx;
     S[2] = -q[2] * it - dyp + dkvk * pity;
-    S[3] = -3 * q[3] * it - dnp * it * it + dkvk * pitn;
+    S[3] = R(-3) * q[3] * it - dnp * it * it + dkvk * pitn;
     if (SHEAR) {
-      Shear pi{q[4], q[5], q[6], q[7], q[8], q[9], q[10], q[11], q[12], q[13]};
-      double rhs[11];
-      pimunu_rhs<EOS, BULK>(rhs, t, a.dt, a.etabar, ePrev, pc, f, pi, Pi, dkvk);
+      ShearT<R> pi{q[4], q[5], q[6], q[7], q[8], q[9], q[10], q[11], q[12], q[13]};
+      R rhs[11];
+      pimunu_rhs<EOS, BULK, R>(rhs, t, (R)a.dt, (R)a.etabar, er, pc, f, pi, Pi, dkvk);
 #pragma unroll
       for (int n = 4; n < NQ; ++n) S[n] = rhs[n - 4];
     }
 #pragma unroll
-    for (int n = 0; n < NQ; ++n) out[n * kBlock] = q[n] + a.dt * S[n];
+    for (int n = 0; n < NQ; ++n) {
+      // the FP64 value of q is re-read for the accumulation (a no-op reload on the FP64 path)
+      const double qd = MIXED ? __ldg(a.qin + n * a.cs + s) : (double)q[n];
+      out[n * kBlock] = qd + a.dt * (double)S[n];
+    }
   }
 
   // ---- flux divergence along x, y, eta (EulerStep.cu:1011-1277) -------------------------
   const GuessEos g0 = guess_eos<EOS>(ePrev);
+  GuessEosF g0f;
+  if (MIXED) g0f = guess_eos_f<EOS>(ePrev);
 #pragma unroll 1
   for (int axis = 0; axis < 3; ++axis) {
     const int idx = axis == 0 ? i : axis == 1 ? j : k;
     const int n_axis = axis == 0 ? a.nx : axis == 1 ? a.ny : a.nz;
     const int stride = axis == 0 ? 1 : axis == 1 ? (int)a.sy : (int)a.sz;
     const double d = axis == 0 ? a.dx : axis == 1 ? a.dy : a.dz;
-    axis_update<EOS, SHEAR, BULK>(a, (int)s, axis, idx, n_axis, stride, d, g0, uc, out, status);
+    axis_update<EOS, SHEAR, BULK, MIXED>(a, (int)s, axis, idx, n_axis, stride, d, g0, g0f, uc, out, status);
   }
 
   // ---- Heun combination Q = (Q + q^n)/2 (FullyDiscreteKurganovTadmorScheme.cu:60-104) ---

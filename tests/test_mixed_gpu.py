@@ -1,0 +1,61 @@
+"""Mixed-precision path (FP32 limiter, fluxes, sources and face-state recovery; FP64
+state, cell-centre recovery, RK accumulation and regulation) against the FP64 oracle.
+
+Stated tolerances (max over cells): relative error in e <= 1e-4, |delta u^mu| <= 1e-4
+(u^tau >= 1, so this is relative to u^tau), |delta pi^{mu nu}| / (e + p) <= 1e-3.
+"""
+import numpy as np
+import pytest
+
+import gvh
+import oracle
+from gvh import workloads
+
+pytestmark = pytest.mark.gpu
+
+E_TOL = 1e-4
+U_TOL = 1e-4
+PI_TOL = 1e-3
+
+
+def mixed_errors(G, sg, so):
+    e_g, e_o = G.interior(sg["e"]), G.interior(so["e"])
+    p_o = G.interior(so["p"])
+    err = {"e": float(np.max(np.abs(e_g - e_o) / np.abs(e_o)))}
+    err["u"] = max(float(np.max(np.abs(G.interior(sg[k]) - G.interior(so[k])))) for k in ("ut", "ux", "uy", "un"))
+    if G.shear:
+        wpp = np.abs(e_o + p_o)
+        err["pi"] = max(float(np.max(np.abs(G.interior(sg[k]) - G.interior(so[k])) / wpp))
+                        for k in G.qnames[4:14])
+    return err
+
+
+def run_pair(w, prim, steps):
+    kw = w.lattice_kwargs()
+    G = gvh.Lattice(precision="mixed", **kw)
+    O = oracle.OracleLattice(**kw)
+    G.set_primitive(prim)
+    O.set_primitive(prim)
+    t = w.tau0
+    for n in range(1, steps + 1):
+        G.step(t, w.dtau)
+        O.step(t, w.dtau)
+        t = w.tau0 + n * w.dtau
+    assert G.status() == 0
+    return G, G.get_state(), O.get_state()
+
+
+def test_mixed_config1_100_steps():
+    w = workloads.CONFIG1
+    G, sg, so = run_pair(w, workloads.gaussian_profile(w), w.steps)
+    err = mixed_errors(G, sg, so)
+    assert err["e"] <= E_TOL and err["u"] <= U_TOL and err["pi"] <= PI_TOL, err
+
+
+def test_mixed_config2_lattice_10_steps():
+    w = workloads.CONFIG2
+    prim = workloads.glauber_hotspots(w)
+    prim.pop("_meta")
+    G, sg, so = run_pair(w, prim, 10)
+    err = mixed_errors(G, sg, so)
+    assert err["e"] <= E_TOL and err["u"] <= U_TOL and err["pi"] <= PI_TOL, err
