@@ -1,0 +1,70 @@
+// gvh_layout.cuh -- conversion between the reference's ghosted SoA layout (what the C ABI
+// takes and returns) and the interior-only layout the stage kernels use, and the initial
+// T^{tau mu} from primitive fields. Internal linkage: each translation unit gets its copy.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "gvh_physics.cuh"
+
+namespace {
+
+using namespace gvh;
+
+struct Pack {
+  int nx, ny, nz;
+  long long sy, sz;   // internal strides
+  long long ng;       // ghosted size (field stride in staging)
+};
+
+__device__ __forceinline__ long long ref_index(const Pack &p, int i, int j, int k) {
+  return (long long)(i + 2) + (long long)(p.nx + 4) * ((j + 2) + (long long)(p.ny + 4) * (k + 2));
+}
+
+// staging (nf fields, ghosted) -> internal fields dst[f] (interior)
+__global__ void pack_kernel(Pack p, int nf, const double *__restrict__ staging, double *const *dst) {
+  long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long n = (long long)p.nx * p.ny * p.nz;
+  if (id >= n) return;
+  int i = id % p.nx, j = (id / p.nx) % p.ny, k = id / ((long long)p.nx * p.ny);
+  long long r = ref_index(p, i, j, k), s = i + p.sy * j + p.sz * k;
+  for (int f = 0; f < nf; ++f)
+    if (dst[f]) dst[f][s] = staging[f * p.ng + r];
+}
+
+// internal fields src[f] -> staging (ghosted, every ghost cell filled from the nearest
+// interior cell: the reference's zero-gradient faces, edges and corners alike)
+__global__ void unpack_kernel(Pack p, int nf, const double *const *src, double *__restrict__ staging) {
+  long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long n = p.ng;
+  if (id >= n) return;
+  int gi = id % (p.nx + 4), gj = (id / (p.nx + 4)) % (p.ny + 4), gk = id / ((long long)(p.nx + 4) * (p.ny + 4));
+  int i = min(max(gi - 2, 0), p.nx - 1), j = min(max(gj - 2, 0), p.ny - 1), k = min(max(gk - 2, 0), p.nz - 1);
+  long long s = i + p.sy * j + p.sz * k;
+  for (int f = 0; f < nf; ++f)
+    if (src[f]) staging[f * p.ng + id] = src[f][s];
+}
+
+// T^{tau mu} from primitives (DynamicalVariables.cu:349-392 with EnergyMomentumTensor.cu
+// :159-177) and p = p(e) (InitialConditions.cpp:124-127), in the internal layout.
+template <int EOS>
+__global__ void init_conserved_kernel(long long n, int nq, long long cs, double *q, double *e, double *p,
+                                      double *u, double *up) {
+  long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  double es = e[s];
+  double ps = eq_pressure<EOS>(es);
+  p[s] = ps;
+  double ut = u[s], ux = u[cs + s], uy = u[2 * cs + s], un = u[3 * cs + s];
+  double pitt = 0, pitx = 0, pity = 0, pitn = 0, Pi = 0;
+  if (nq >= 14) { pitt = q[4 * cs + s]; pitx = q[5 * cs + s]; pity = q[6 * cs + s]; pitn = q[7 * cs + s]; }
+  if (nq == 15) Pi = q[14 * cs + s];
+  double pp = ps + Pi;
+  q[s] = (es + pp) * ut * ut - pp + pitt;
+  q[cs + s] = (es + pp) * ut * ux + pitx;
+  q[2 * cs + s] = (es + pp) * ut * uy + pity;
+  q[3 * cs + s] = (es + pp) * ut * un + pitn;
+  for (int m = 0; m < 4; ++m) up[m * cs + s] = u[m * cs + s];
+}
+
+}  // namespace

@@ -237,12 +237,13 @@ __device__ __forceinline__ void axis_update(const StageArgs &a, int s, int axis,
 // MIXED = false: plain FP64. MIXED = true: limiter, fluxes and source terms in FP32 (face
 // states recovered in FP32 with an FP64 redo when that fails); the state, the running
 // update, the Heun combination, the cell-centre recovery and the regulation in FP64.
+//
+// stage_cell does one cell (interior index id < a.ncells); it returns the cell's new energy
+// density so callers can reduce it (the batched engine tracks max e per event).
 template <int EOS, bool SHEAR, bool BULK, bool STAGE2, bool MIXED>
-__global__ void __launch_bounds__(kBlock, GVH_MIN_BLOCKS) kt_stage_kernel(const StageArgs a) {
+__device__ __forceinline__ double stage_cell(const StageArgs &a, long long id) {
   using R = typename std::conditional<MIXED, float, double>::type;
   constexpr int NQ = NComp<SHEAR, BULK>::value;
-  const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (id >= a.ncells) return;
   const int i = (int)(id % a.nx);
   const int j = (int)((id / a.nx) % a.ny);
   const int k = (int)(id / ((long long)a.nx * a.ny));
@@ -392,6 +393,14 @@ __global__ void __launch_bounds__(kBlock, GVH_MIN_BLOCKS) kt_stage_kernel(const 
   a.uout[2 * a.cs + s] = pr.uy;
   a.uout[3 * a.cs + s] = pr.un;
   if (status) atomicOr(a.status, status);
+  return pr.e;
+}
+
+// One RK substep over one lattice: one thread per interior cell.
+template <int EOS, bool SHEAR, bool BULK, bool STAGE2, bool MIXED>
+__global__ void __launch_bounds__(kBlock, GVH_MIN_BLOCKS) kt_stage_kernel(const StageArgs a) {
+  const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (id < a.ncells) stage_cell<EOS, SHEAR, BULK, STAGE2, MIXED>(a, id);
 }
 
 }  // namespace gvh

@@ -220,3 +220,167 @@ class Lattice:
     @property
     def launches_per_step(self) -> int:
         return int(self._L.gvh_launches_per_step(self._h))
+
+
+# ---------------------------------------------------------------------------------------
+# Batched events
+# ---------------------------------------------------------------------------------------
+class EventInfo(ctypes.Structure):
+    _fields_ = [("step", ctypes.c_longlong), ("tau", ctypes.c_double), ("max_energy_density", ctypes.c_double),
+                ("freezeout_energy_density", ctypes.c_double), ("frozen_checks", ctypes.c_int),
+                ("frozen_out", ctypes.c_int), ("status", ctypes.c_uint), ("cells", ctypes.c_longlong)]
+
+
+BATCH_EXPORTS = [
+    "gvh_batch_event_bytes", "gvh_batch_create", "gvh_batch_destroy", "gvh_batch_set_stream",
+    "gvh_batch_add_event", "gvh_batch_remove_event", "gvh_batch_num_events", "gvh_batch_free_bytes",
+    "gvh_batch_active_cells", "gvh_batch_step", "gvh_batch_synchronize", "gvh_batch_event_info",
+    "gvh_batch_get_state", "gvh_batch_launch_config", "gvh_batch_set_grid", "gvh_batch_autotune",
+    "gvh_batch_last_error",
+]
+EXPORTS += BATCH_EXPORTS
+
+
+def _bind_batch(L):
+    if getattr(L, "_batch_bound", False):
+        return L
+    vp, ip, ll = ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong
+    L.gvh_batch_event_bytes.argtypes = [ctypes.POINTER(LatticeParams), ctypes.POINTER(Options)]
+    L.gvh_batch_event_bytes.restype = ll
+    L.gvh_batch_create.argtypes = [ctypes.POINTER(Options), ll, ctypes.POINTER(vp)]
+    L.gvh_batch_destroy.argtypes = [vp]
+    L.gvh_batch_set_stream.argtypes = [vp, vp]
+    L.gvh_batch_add_event.argtypes = [vp, ctypes.POINTER(LatticeParams), ctypes.POINTER(HydroParams), vp, ip,
+                                      ctypes.POINTER(ip)]
+    L.gvh_batch_remove_event.argtypes = [vp, ip]
+    L.gvh_batch_num_events.argtypes = [vp]
+    L.gvh_batch_free_bytes.argtypes = [vp]
+    L.gvh_batch_free_bytes.restype = ll
+    L.gvh_batch_active_cells.argtypes = [vp]
+    L.gvh_batch_active_cells.restype = ll
+    L.gvh_batch_step.argtypes = [vp, ip]
+    L.gvh_batch_synchronize.argtypes = [vp]
+    L.gvh_batch_event_info.argtypes = [vp, ip, ctypes.POINTER(EventInfo)]
+    L.gvh_batch_get_state.argtypes = [vp, ip, vp, ip]
+    L.gvh_batch_launch_config.argtypes = [vp, ctypes.POINTER(ip), ctypes.POINTER(ip)]
+    L.gvh_batch_set_grid.argtypes = [vp, ip]
+    L.gvh_batch_autotune.argtypes = [vp, ip, ctypes.POINTER(ip)]
+    L.gvh_batch_last_error.restype = ctypes.c_char_p
+    L._batch_bound = True
+    return L
+
+
+def _bcheck(rc: int, what: str):
+    if rc != 0:
+        msg = load().gvh_batch_last_error().decode(errors="replace")
+        raise GvhError(f"{what} failed ({rc}): {msg}")
+
+
+GVH_ERR_NOMEM = -4
+
+
+class Batch:
+    """Many events in one HBM arena, advanced together by one persistent launch per stage
+    and a CUDA graph per RK2 step. All events share the physics options."""
+
+    def __init__(self, arena_bytes, conformal=False, shear=True, bulk=True, precision="fp64", theta=2.0, device=-1):
+        self._L = _bind_batch(load())
+        o = Options()
+        self._L.gvh_default_options(ctypes.byref(o))
+        o.eos = GVH_EOS_CONFORMAL if conformal else GVH_EOS_QCD
+        o.shear, o.bulk, o.theta, o.device = int(shear), int(bulk), float(theta), int(device)
+        o.precision = {"fp64": GVH_PRECISION_FP64, "mixed": GVH_PRECISION_MIXED}[precision]
+        self.options = o
+        self.shear, self.bulk = bool(shear), bool(bulk)
+        self.qnames = q_names(self.shear, self.bulk)
+        self.nq = len(self.qnames)
+        self.field_names = self.qnames + PRIM_NAMES
+        h = ctypes.c_void_p()
+        _bcheck(self._L.gvh_batch_create(ctypes.byref(o), int(arena_bytes), ctypes.byref(h)), "gvh_batch_create")
+        self._h = h
+        self.events = {}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.gvh_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr):
+        _bcheck(self._L.gvh_batch_set_stream(self._h, stream_ptr or None), "gvh_batch_set_stream")
+
+    def event_bytes(self, nx, ny, nz) -> int:
+        lat = LatticeParams(nx, ny, nz, nx + 4, ny + 4, nz + 4, 0, 1.0, 1.0, 1.0, 1.0)
+        return int(self._L.gvh_batch_event_bytes(ctypes.byref(lat), ctypes.byref(self.options)))
+
+    def add_event(self, nx, ny, nz, dx, dy, dz, dt, etabar, prim: dict, tau0=0.5, T_fo_GeV=0.15, T_reg_GeV=0.0):
+        """Admit an event; returns its id, or None when the arena cannot hold it."""
+        lat = LatticeParams(nx, ny, nz, nx + 4, ny + 4, nz + 4, 0, dx, dy, dz, dt)
+        hyd = HydroParams(tau0, etabar, T_fo_GeV, 0, T_reg_GeV)
+        ng = (nx + 4) * (ny + 4) * (nz + 4)
+        order = ["e", "ut", "ux", "uy", "un"] + self.qnames[4:]
+        arrs = [np.ascontiguousarray(np.broadcast_to(np.asarray(prim.get(k, 0.0), np.float64).reshape(-1), (ng,)))
+                for k in order]
+        eid = ctypes.c_int(-1)
+        rc = self._L.gvh_batch_add_event(self._h, ctypes.byref(lat), ctypes.byref(hyd),
+                                         _ptr_array([a.ctypes.data for a in arrs]), len(arrs), ctypes.byref(eid))
+        if rc == GVH_ERR_NOMEM:
+            return None
+        _bcheck(rc, "gvh_batch_add_event")
+        self.events[eid.value] = (nx, ny, nz)
+        return eid.value
+
+    def remove_event(self, eid):
+        _bcheck(self._L.gvh_batch_remove_event(self._h, int(eid)), "gvh_batch_remove_event")
+        self.events.pop(eid, None)
+
+    def step(self, nsteps=1):
+        _bcheck(self._L.gvh_batch_step(self._h, int(nsteps)), "gvh_batch_step")
+
+    def synchronize(self):
+        _bcheck(self._L.gvh_batch_synchronize(self._h), "gvh_batch_synchronize")
+
+    def info(self, eid) -> EventInfo:
+        inf = EventInfo()
+        _bcheck(self._L.gvh_batch_event_info(self._h, int(eid), ctypes.byref(inf)), "gvh_batch_event_info")
+        return inf
+
+    def get_state(self, eid, names=None) -> dict:
+        nx, ny, nz = self.events[eid]
+        ng = (nx + 4) * (ny + 4) * (nz + 4)
+        want = set(names) if names else set(self.field_names)
+        arrs = [np.empty(ng) if k in want else None for k in self.field_names]
+        ptrs = [None if a is None else a.ctypes.data for a in arrs]
+        _bcheck(self._L.gvh_batch_get_state(self._h, int(eid), _ptr_array(ptrs), len(ptrs)), "gvh_batch_get_state")
+        return {k: a for k, a in zip(self.field_names, arrs) if a is not None}
+
+    @property
+    def num_events(self) -> int:
+        return int(self._L.gvh_batch_num_events(self._h))
+
+    @property
+    def free_bytes(self) -> int:
+        return int(self._L.gvh_batch_free_bytes(self._h))
+
+    @property
+    def active_cells(self) -> int:
+        return int(self._L.gvh_batch_active_cells(self._h))
+
+    @property
+    def grid(self) -> int:
+        g, b = ctypes.c_int(), ctypes.c_int()
+        self._L.gvh_batch_launch_config(self._h, ctypes.byref(g), ctypes.byref(b))
+        return g.value
+
+    def set_grid(self, g):
+        _bcheck(self._L.gvh_batch_set_grid(self._h, int(g)), "gvh_batch_set_grid")
+
+    def autotune(self, steps=2) -> int:
+        g = ctypes.c_int()
+        _bcheck(self._L.gvh_batch_autotune(self._h, int(steps), ctypes.byref(g)), "gvh_batch_autotune")
+        return g.value

@@ -17,7 +17,7 @@ NVCC_FLAGS = [
 
 
 def sources() -> list[str]:
-    return [os.path.join(CSRC, "gvh_capi.cu")]
+    return [os.path.join(CSRC, "gvh_capi.cu"), os.path.join(CSRC, "gvh_batch.cu")]
 
 
 def needs_rebuild() -> bool:

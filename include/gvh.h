@@ -135,6 +135,54 @@ int gvh_launches_per_step(const gvh_handle *h);
 
 const char *gvh_last_error(void);
 
+/* ------------------------------------------------------------------------------------
+ * Batched events (no counterpart in the reference, which runs one event per process:
+ * HydroPlugin.cpp:107-434). A batch owns one HBM arena and advances every admitted event
+ * together: a persistent stage kernel walks a packed queue of 128-cell tiles of all events,
+ * and one RK2 step (stage 1, stage 2, per-event bookkeeping) is a CUDA graph replayed per
+ * step. All events of a batch share the options (EoS, shear/bulk, precision, theta); each
+ * has its own lattice, spacings, dtau, tau0, eta/s, T_fo and T_reg (from its parameters).
+ * Each event advances exactly as a gvh_handle with the same inputs would.
+ * ---------------------------------------------------------------------------------- */
+typedef struct gvh_batch gvh_batch;
+
+typedef struct gvh_event_info {
+	long long step;                   /* RK2 steps completed */
+	double tau;                       /* proper time reached: tau0 + step * dtau */
+	double max_energy_density;        /* max interior e after the last step (fm^-4) */
+	double freezeout_energy_density;  /* e(T_fo) */
+	int frozen_checks;                /* steps (initial state included) with max e <= e(T_fo) */
+	int frozen_out;                   /* frozen_checks >= 11, the reference's stop rule
+	                                     (FOFREQ+1 all-frozen checks, HydroPlugin.cpp:396-413) */
+	unsigned status;                  /* GVH_STATUS_* bits raised by this event */
+	long long cells;                  /* interior cells */
+} gvh_event_info;
+
+/* HBM bytes one event of this lattice takes in a batch arena. */
+long long gvh_batch_event_bytes(const gvh_lattice_params *lattice, const gvh_options *opts);
+int gvh_batch_create(const gvh_options *opts, long long arena_bytes, gvh_batch **out);
+int gvh_batch_destroy(gvh_batch *b);
+int gvh_batch_set_stream(gvh_batch *b, void *stream);
+/* Admits an event from primitive fields (same arrays as gvh_set_primitive_state). Returns
+ * GVH_ERR_NOMEM without side effects when the arena cannot hold it. */
+int gvh_batch_add_event(gvh_batch *b, const gvh_lattice_params *lattice, const gvh_hydro_params *hydro,
+                        const double *const *prim, int n_prim, int *event_id);
+int gvh_batch_remove_event(gvh_batch *b, int event_id);
+int gvh_batch_num_events(const gvh_batch *b);
+long long gvh_batch_free_bytes(const gvh_batch *b);
+long long gvh_batch_active_cells(const gvh_batch *b);
+/* Queues nsteps RK2 steps of every admitted event (asynchronous). */
+int gvh_batch_step(gvh_batch *b, int nsteps);
+int gvh_batch_synchronize(gvh_batch *b);
+int gvh_batch_event_info(gvh_batch *b, int event_id, gvh_event_info *info);
+int gvh_batch_get_state(gvh_batch *b, int event_id, double *const *fields, int n_fields);
+int gvh_batch_launch_config(const gvh_batch *b, int *grid_blocks, int *block_threads);
+int gvh_batch_set_grid(gvh_batch *b, int grid_blocks);
+/* Chooses the persistent grid by timing `steps` real steps per candidate (the events
+ * advance; every candidate computes the same values). */
+int gvh_batch_autotune(gvh_batch *b, int steps, int *chosen_grid);
+const char *gvh_batch_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif
