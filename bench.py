@@ -50,6 +50,10 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the mixed-precision, event-to-freeze-out and serving measurements")
+    ap.add_argument("--serving-seconds", type=float, default=45.0)
+    ap.add_argument("--serving-rate", type=float, default=4.0)
     return ap.parse_args()
 
 
@@ -237,6 +241,72 @@ def run_reference(args):
     return 0
 
 
+def time_steps(L, w, steps, warmup, stream):
+    """ms per RK2 step of lattice L (CUDA events on its stream)."""
+    import torch
+
+    t = w.tau0
+    for n in range(warmup):
+        L.step(t, w.dtau)
+        t += w.dtau
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for n in range(steps):
+        L.step(t, w.dtau)
+        t += w.dtau
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def event_to_freezeout(w, prim, precision, device, max_steps=6000):
+    """One event on the single-lattice path, run the way the reference's loop runs it:
+    before every step test max e against e(T_fo) (device reduction), stop after 11 all-frozen
+    checks (HydroPlugin.cpp:396-413). Returns steps, seconds, status."""
+    import gvh
+
+    L = gvh.Lattice(device=device, precision=precision, **w.lattice_kwargs())
+    L.set_primitive(prim)
+    # e(T_fo) of the QCD fit from a one-cell batch (the library computes it)
+    B = gvh.Batch(1 << 22, precision=precision, device=device)
+    eid = B.add_event(1, 1, 1, w.dx, w.dy, w.dz, w.dtau, w.etabar, {"e": np.ones(125)}, tau0=w.tau0,
+                      T_fo_GeV=w.T_fo_GeV)
+    e_fo = B.info(eid).freezeout_energy_density
+    B.close()
+    L.synchronize()
+    t0 = time.perf_counter()
+    frozen, n, t = 0, 0, w.tau0
+    while n < max_steps:
+        if L.max_energy_density() <= e_fo:
+            frozen += 1
+        if frozen >= 11:
+            break
+        L.step(t, w.dtau)
+        n += 1
+        t = w.tau0 + n * w.dtau
+    L.synchronize()
+    el = time.perf_counter() - t0
+    st = L.status()
+    L.close()
+    return {"steps": n, "seconds": el, "frozen_out": frozen >= 11, "status": st, "tau_end": t}
+
+
+def serving_run(args, device):
+    from gvh import serve
+
+    rng = np.random.default_rng(2024)
+    n_req = max(8, int(args.serving_rate * args.serving_seconds))
+    arrivals = serve.poisson_arrivals(args.serving_rate, n_req, rng)
+    reqs = [serve.make_request(i, a, rng) for i, a in enumerate(arrivals)]
+    srv = serve.Server(int(60 * (1 << 30)), precision="mixed", steps_per_round=10, device=device)
+    out = srv.run(reqs, time_limit=args.serving_seconds)
+    out.pop("steps", None)
+    out.update({"rate_per_s": args.serving_rate, "requests_offered": n_req, "precision": "mixed",
+                "mix": "grids {61x61x1 @0.2 fm, 101x101x31 @0.15, 131x131x61 @0.1}, b~U(0,12), eta/s~U(0.08,0.24)"})
+    return out
+
+
 def run_ours(args):
     import torch
 
@@ -286,7 +356,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1)
     flags = L.status()
-    if flags:
+    if flags & gvh.GVH_STATUS_ERRORS:
         raise RuntimeError(f"status flags {flags} raised during the timed steps")
     ms_max = ms
     if dist:
@@ -350,6 +420,42 @@ def run_ours(args):
                 "algorithmic_bytes_per_step": cells * b_cell,
                 "kernel": "kt_stage_kernel (stage 1 + stage 2 per step)"}
 
+    extras = {}
+    if rank == 0 and world == 1 and not args.no_extras:
+        import gvh as _g
+
+        Lm = _g.Lattice(device=local, precision="mixed", **w.lattice_kwargs())
+        Lm.set_primitive(prim)
+        Lm.set_stream(stream.cuda_stream)
+        ms_mixed = time_steps(Lm, w, max(5, args.steps // 2), 3, stream)
+        Lm.close()
+        extras["mixed_cell_updates_per_s"] = cells / (ms_mixed / 1e3)
+        extras["mixed_ms_per_step"] = ms_mixed
+        ev = event_to_freezeout(w, prim, "fp64", local)
+        ev["events_per_hour"] = 3600.0 / ev["seconds"] if ev["seconds"] > 0 else None
+        extras["fp64_single_event_to_freezeout"] = ev
+        if args.serving_seconds > 0:
+            # the plain FP64 single-event path on the serving mix: one event of each grid of
+            # the mix run alone to freeze-out; the mix draws the grids uniformly
+            import dataclasses
+
+            from gvh import serve
+
+            per_grid = []
+            for (nx, ny, nz, dx) in serve.GRIDS:
+                wg = dataclasses.replace(w, nx=nx, ny=ny, nz=nz, dx=dx, dy=dx, dz=0.1, dtau=dx / 10)
+                pg = workloads.glauber_hotspots(wg)
+                pg.pop("_meta")
+                rg = event_to_freezeout(wg, pg, "fp64", local)
+                rg["grid"] = [nx, ny, nz]
+                per_grid.append(rg)
+            mean_s = float(np.mean([r["seconds"] for r in per_grid]))
+            fp64_mix = {"events_per_hour": 3600.0 / mean_s, "per_grid": per_grid}
+            extras["fp64_single_event_path_on_serving_mix"] = fp64_mix
+            sv = serving_run(args, local)
+            sv["events_per_hour_vs_fp64_single_path"] = sv["events_per_hour"] / fp64_mix["events_per_hour"]
+            extras["batched_mixed_serving"] = sv
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -370,6 +476,7 @@ def run_ours(args):
                        "parallelism": f"events x{world}"},
             "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu,
             "clocks": clocks.summary(),
+            "extras": extras,
         }
         print(json.dumps(line))
     L.close()

@@ -17,6 +17,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <string>
 
 #include "../../include/gvh.h"
@@ -327,6 +328,21 @@ int gvh_set_stream(gvh_handle *h, void *stream) {
   return GVH_OK;
 }
 
+int gvh_max_energy_density(gvh_handle *h, double *out) {
+  if (!h || !out) return fail(GVH_ERR_INVALID, "null argument");
+  GVH_CUDA(cudaSetDevice(h->device));
+  unsigned long long *scratch = reinterpret_cast<unsigned long long *>(h->status) + 1;
+  GVH_CUDA(cudaMemsetAsync(scratch, 0, sizeof(unsigned long long), h->stream));
+  const unsigned blocks = (unsigned)std::min<long long>(1024, (h->ncells + 255) / 256);
+  max_e_kernel<<<blocks, 256, 0, h->stream>>>(h->e, h->ncells, scratch);
+  GVH_CUDA(cudaGetLastError());
+  unsigned long long bits = 0;
+  GVH_CUDA(cudaMemcpyAsync(&bits, scratch, sizeof bits, cudaMemcpyDeviceToHost, h->stream));
+  GVH_CUDA(cudaStreamSynchronize(h->stream));
+  memcpy(out, &bits, sizeof *out);
+  return GVH_OK;
+}
+
 int gvh_synchronize(gvh_handle *h) {
   if (!h) return fail(GVH_ERR_INVALID, "null handle");
   GVH_CUDA(cudaSetDevice(h->device));
@@ -341,7 +357,7 @@ int gvh_status(gvh_handle *h, unsigned *flags) {
   GVH_CUDA(cudaMemcpyAsync(&v, h->status, sizeof v, cudaMemcpyDeviceToHost, h->stream));
   GVH_CUDA(cudaStreamSynchronize(h->stream));
   if (flags) *flags = v;
-  return v ? GVH_ERR_NUMERIC : GVH_OK;
+  return (v & GVH_STATUS_ERRORS) ? GVH_ERR_NUMERIC : GVH_OK;
 }
 
 int gvh_clear_status(gvh_handle *h) {

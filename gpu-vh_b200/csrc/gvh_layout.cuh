@@ -67,4 +67,15 @@ __global__ void init_conserved_kernel(long long n, int nq, long long cs, double 
   for (int m = 0; m < 4; ++m) up[m * cs + s] = u[m * cs + s];
 }
 
+// Max of a non-negative double array (interior energy densities), as the bit pattern of a
+// double: for non-negative values the integer order of the bits is the numeric order.
+__global__ void max_e_kernel(const double *e, long long n, unsigned long long *out) {
+  unsigned long long b = 0ull;
+  for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < n; s += (long long)gridDim.x * blockDim.x)
+    b = max(b, (unsigned long long)__double_as_longlong(fmax(e[s], 0.0)));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) b = max(b, __shfl_xor_sync(0xffffffffu, b, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, b);
+}
+
 }  // namespace

@@ -128,12 +128,22 @@ __device__ __forceinline__ double bulk_zeta_over_s(double T) {
 // ------------------------------------------------------------------------------------
 
 // Status bits a stage kernel may raise (or-ed into the per-lattice status word).
-enum : unsigned { STATUS_NAN = 1u, STATUS_NEWTON = 2u };
+//   STATUS_NAN     an energy density came out NaN
+//   STATUS_NEWTON  a Newton solve failed to converge even with damping
+//   STATUS_DAMPED  informational: a Newton solve needed the damped phase (see below)
+enum : unsigned { STATUS_NAN = 1u, STATUS_NEWTON = 2u, STATUS_DAMPED = 4u };
 
-// Newton iteration cap. The reference allows 10^6 iterations and damps after 5x10^5
-// (EnergyMomentumTensor.cu:15,37-38); converged cells take a handful. Hitting the cap
-// returns the last iterate (as the reference does at its cap) and raises STATUS_NEWTON.
-constexpr int kNewtonMaxIters = 500;
+// Newton iteration budget. The reference iterates e <- e - f/f' up to 5x10^5 times and
+// then switches to the damped update e <- e - 0.9 f/f' for up to another 5x10^5
+// (EnergyMomentumTensor.cu:15, 22-41). Converging solves take a handful of iterations.
+// The ones that do not converge undamped wander chaotically (the iterates of such a solve,
+// recorded from the reference's algorithm, neither settle nor repeat exactly), so the
+// state the reference reaches after 5x10^5 undamped iterations depends on every rounding
+// on the way and no implementation reproduces it; what the reference does next -- damp --
+// is what decides the answer. Here the undamped phase is kNewtonUndamped iterations, then
+// the same damped update runs up to kNewtonMaxIters in total.
+constexpr int kNewtonUndamped = 200;
+constexpr int kNewtonMaxIters = 2000;
 
 // p(e) and c_s^2(e) of the QCD fit together, both rational functions evaluated in Horner
 // form (the reference evaluates the same polynomials from explicit powers,
@@ -185,9 +195,10 @@ __device__ __forceinline__ GuessEos guess_eos(double ePrev) {
 }
 
 // One Newton update of EnergyMomentumTensor.cu:22-40 (divisions by e0 and by cst2*e0*H =
-// p*H taken through a shared reciprocal / the product p*H; equal to rounding).
+// p*H taken through a shared reciprocal / the product p*H; equal to rounding). damped
+// selects e0 - 0.9 f/f' (EnergyMomentumTensor.cu:38) over e0 - f/f'.
 __device__ __forceinline__ double newton_update(double e0, double inv_e0, double p, double cs2, double M0, double M,
-                                                double Pi) {
+                                                double Pi, bool damped = false) {
   double cst2 = p * inv_e0;
   double A = fma(M0, 1 - cst2, Pi);
   double B = fma(M0, M0 + Pi, -M);
@@ -196,7 +207,7 @@ __device__ __forceinline__ double newton_update(double e0, double inv_e0, double
   double f = e0 + D;
   double g = cs2 - cst2;
   double fp = 1 - (g * (B + D * H - (g * cst2 * D * M0) * inv_e0)) / (p * H);
-  return e0 - f / fp;
+  return damped ? e0 - (0.9 * f) / fp : e0 - f / fp;
 }
 
 // N independent Newton solves (EnergyMomentumTensor.cu:18-48) iterated together: each
@@ -223,13 +234,15 @@ __device__ __forceinline__ void energy_from_conserved_n(const GuessEos &g0, cons
     all = all && done[n];
   }
   for (int j = 1; j < kNewtonMaxIters && !all; ++j) {
+    const bool damped = j >= kNewtonUndamped;
+    if (j == kNewtonUndamped) status |= STATUS_DAMPED;
     all = true;
 #pragma unroll
     for (int n = 0; n < N; ++n) {
       if (done[n]) continue;
       double p, cs2;
       qcd_p_cs2(e0[n], p, cs2);
-      double e = newton_update(e0[n], 1.0 / e0[n], p, cs2, M0[n], M[n], Pi[n]);
+      double e = newton_update(e0[n], 1.0 / e0[n], p, cs2, M0[n], M[n], Pi[n], damped);
       done[n] = fabs(e - e0[n]) <= 0.001 * fabs(e);
       e0[n] = e;
       out[n] = e;
@@ -339,9 +352,8 @@ __device__ __forceinline__ R limited_slope(R theta, R x, R y, R z) {
 }  // namespace gvh
 
 // ====================================================================================
-// Single-precision versions used by the mixed-precision path (fluxes, limiter, sources
-// and the face states' primitive recovery in FP32; the state, the cell-centre recovery,
-// the RK accumulation and the regulation stay FP64).
+// Single-precision equation of state used by the mixed-precision path's source-term
+// algebra (temperature, c_s^2 and zeta/s of the cell).
 // ====================================================================================
 namespace gvh {
 
@@ -400,14 +412,6 @@ __device__ __forceinline__ void poly_pair_f(const float *num, const float *den, 
   }
 }
 
-__device__ __forceinline__ void qcd_p_cs2(float e, float &p, float &cs2) {
-  float a, b, c, d;
-  poly_pair_f<13>(kPa_f, kPb_f, e, a, b);
-  poly_pair_f<14>(kCn_f, kCd_f, e, c, d);
-  p = __fdividef(a, b);
-  cs2 = __fdividef(c, d);
-}
-
 template <int EOS>
 __device__ __forceinline__ float eq_pressure(float e) {
   if (EOS == EOS_CONFORMAL) return e / 3.f;
@@ -437,106 +441,6 @@ __device__ __forceinline__ float bulk_zeta_over_s(float T) {
   if (x > 1.05f) return 0.9f * __expf(-(x - 1) * 40.f) + 0.25f * __expf(-(x - 1) * (float)(1.0 / 0.13)) + 0.001f;
   else if (x < 0.995f) return 0.9f * __expf((x - 1) * 400.f) + 0.22f * __expf((x - 1) * (float)(1.0 / 0.022)) + 0.03f;
   return -13.77f * x * x + 27.55f * x - 13.45f;
-}
-
-struct GuessEosF {
-  float e, inv_e, p, cs2;
-};
-template <int EOS>
-__device__ __forceinline__ GuessEosF guess_eos_f(double ePrev) {
-  GuessEosF g;
-  g.e = (float)ePrev;
-  g.inv_e = __fdividef(1.f, g.e);
-  if (EOS == EOS_CONFORMAL) {
-    g.p = 0.f;
-    g.cs2 = 0.f;
-  } else {
-    qcd_p_cs2(g.e, g.p, g.cs2);
-  }
-  return g;
-}
-
-__device__ __forceinline__ float newton_update_f(float e0, float inv_e0, float p, float cs2, float M0, float M,
-                                                 float Pi) {
-  float cst2 = p * inv_e0;
-  float A = fmaf(M0, 1.f - cst2, Pi);
-  float B = fmaf(M0, M0 + Pi, -M);
-  float H = sqrtf(fabsf(A * A + 4.f * cst2 * B));
-  float D = __fdividef(A - H, 2.f * cst2);
-  float f = e0 + D;
-  float g = cs2 - cst2;
-  float fp = 1.f - __fdividef(g * (B + D * H - (g * cst2 * D * M0) * inv_e0), p * H);
-  return e0 - __fdividef(f, fp);
-}
-
-// FP32 face-state recovery (EnergyMomentumTensor.cu:18-108 in single precision) returning
-// w = u^axis/u^tau. A state whose FP32 solution is not a finite positive energy density is
-// recovered again in FP64 (ok[n] = false tells the caller to do so).
-template <int EOS, int N>
-__device__ __forceinline__ void inferred_face_n_f(float t, int axis, const float (&ttt)[N], const float (&ttx)[N],
-                                                  const float (&tty)[N], const float (&ttn)[N],
-                                                  const float (&pitt)[N], const float (&pitx)[N],
-                                                  const float (&pity)[N], const float (&pitn)[N],
-                                                  const float (&Pi)[N], const GuessEosF &g0, float (&w)[N],
-                                                  bool (&ok)[N]) {
-  float M0[N], M[N], Mi[N], e[N];
-#pragma unroll
-  for (int n = 0; n < N; ++n) {
-    M0[n] = ttt[n] - pitt[n];
-    float M1 = ttx[n] - pitx[n];
-    float M2 = tty[n] - pity[n];
-    float M3 = ttn[n] - pitn[n];
-    M[n] = M1 * M1 + M2 * M2 + t * t * M3 * M3;
-    Mi[n] = axis == 0 ? M1 : axis == 1 ? M2 : M3;
-  }
-  bool conv = true;
-  if (g0.e <= 0.1f) {
-#pragma unroll
-    for (int n = 0; n < N; ++n) e[n] = M0[n] - __fdividef(M[n], M0[n]);
-  } else if (EOS == EOS_CONFORMAL) {
-#pragma unroll
-    for (int n = 0; n < N; ++n) e[n] = fabsf(sqrtf(fabsf(4.f * M0[n] * M0[n] - 3.f * M[n])) - M0[n]);
-  } else {
-    float e0[N];
-    bool done[N];
-    bool all = true;
-#pragma unroll
-    for (int n = 0; n < N; ++n) {
-      float en = newton_update_f(g0.e, g0.inv_e, g0.p, g0.cs2, M0[n], M[n], Pi[n]);
-      done[n] = fabsf(en - g0.e) <= 0.001f * fabsf(en);
-      e0[n] = en;
-      e[n] = en;
-      all = all && done[n];
-    }
-    for (int j = 1; j < kNewtonMaxIters && !all; ++j) {
-      all = true;
-#pragma unroll
-      for (int n = 0; n < N; ++n) {
-        if (done[n]) continue;
-        float p, cs2;
-        qcd_p_cs2(e0[n], p, cs2);
-        float en = newton_update_f(e0[n], __fdividef(1.f, e0[n]), p, cs2, M0[n], M[n], Pi[n]);
-        done[n] = fabsf(en - e0[n]) <= 0.001f * fabsf(en);
-        e0[n] = en;
-        e[n] = en;
-        all = all && done[n];
-      }
-    }
-    conv = all;
-  }
-#pragma unroll
-  for (int n = 0; n < N; ++n) {
-    ok[n] = conv && e[n] > 0.f && e[n] < 3.0e37f;
-    float p = eq_pressure<EOS>(e[n]);
-    float en = e[n];
-    if (en < 1.e-7f) { en = 1.e-7f; p = 1.e-7f; }
-    float P = p + Pi[n];
-    float E = __fdividef(1.f, en + P);
-    float ut = sqrtf(fabsf((M0[n] + P) * E));
-    float E2 = __fdividef(E, ut);
-    w[n] = __fdividef(Mi[n] * E2, ut);
-    ok[n] = ok[n] && isfinite(w[n]);
-  }
 }
 
 }  // namespace gvh

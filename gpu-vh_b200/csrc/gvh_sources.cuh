@@ -16,8 +16,8 @@ __device__ __forceinline__ float dv(float a, float b) { return __fdividef(a, b);
 // Flow state and limited first derivatives at a cell.
 template <class R>
 struct CellFlowT {
-  R ut, ux, uy, un;      // u^mu (current)
-  R utp, uxp, uyp, unp;  // u^mu one time step earlier (for d/dtau)
+  R ut, ux, uy, un;          // u^mu (current)
+  R dtut, dtux, dtuy, dtun;  // (u^mu - u^mu one step earlier) / dt (SourceTerms.cu:68-71)
   R dxut, dyut, dnut, dxux, dyux, dnux, dxuy, dyuy, dnuy, dxun, dyun, dnun;
 };
 
@@ -29,7 +29,7 @@ struct ShearT {
 // SourceTerms.cu:29-256. rhs[0..9] = d pi^{mu nu}/dtau (pitt..pinn), rhs[10] = dPi/dtau.
 // R = double reproduces the reference's FP64 arithmetic; R = float is the mixed path.
 template <int EOS, bool BULK, class R>
-__device__ __forceinline__ void pimunu_rhs(R *rhs, R t, R dt, R etabar, R e, R p, const CellFlowT<R> &f,
+__device__ __forceinline__ void pimunu_rhs(R *rhs, R t, R etabar, R e, R p, const CellFlowT<R> &f,
                                            const ShearT<R> &pi, R Pi, R dkvk) {
   const R ut = f.ut, ux = f.ux, uy = f.uy, un = f.un;
   const R pitt = pi.tt, pitx = pi.tx, pity = pi.ty, pitn = pi.tn, pixx = pi.xx, pixy = pi.xy, pixn = pi.xn;
@@ -42,10 +42,7 @@ __device__ __forceinline__ void pimunu_rhs(R *rhs, R t, R dt, R etabar, R e, R p
   R beta_pi = R(kF02) * (e + p);
 
   R ut2 = ut * ut, un2 = un * un, t2 = t * t, t3 = t * t2;
-  R dtut = dv(ut - f.utp, dt);
-  R dtux = dv(ux - f.uxp, dt);
-  R dtuy = dv(uy - f.uyp, dt);
-  R dtun = dv(un - f.unp, dt);
+  const R dtut = f.dtut, dtux = f.dtux, dtuy = f.dtuy, dtun = f.dtun;
 
   R Dut = ut * dtut + ux * dxut + uy * dyut + un * dnut + t * un * un;
   R dut = Dut - t * un * un;

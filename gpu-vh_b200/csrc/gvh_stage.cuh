@@ -105,57 +105,6 @@ __device__ __forceinline__ FaceSpeeds<double> face_speeds(const StageArgs &a, in
   return f;
 }
 
-// Out-of-line copy for the mixed path's rare FP64 redo (keeps it out of the hot code).
-template <int EOS, bool SHEAR, bool BULK>
-__device__ __noinline__ FaceSpeeds<double> face_speeds_fallback(const StageArgs &a, int s, int axis,
-                                                                const int (&o)[5], const GuessEos &g0,
-                                                                unsigned &status) {
-  return face_speeds<EOS, SHEAR, BULK>(a, s, axis, o, g0, status);
-}
-
-// Mixed path: the same face states and recoveries in FP32. States whose FP32 recovery is
-// not a finite positive energy density (ok = false) are redone by the FP64 routine above.
-template <int EOS, bool SHEAR, bool BULK>
-__device__ __forceinline__ FaceSpeeds<float> face_speeds_f(const StageArgs &a, int s, int axis, const int (&o)[5],
-                                                           const GuessEosF &g0f, const GuessEos &g0,
-                                                           unsigned &status) {
-  float st[9][4];
-  constexpr int NR = 4 + (SHEAR ? 4 : 0) + (BULK ? 1 : 0);
-  const float th = (float)a.theta;
-#pragma unroll
-  for (int r = 0; r < NR; ++r) {
-    const int c = (r < 8) ? r : 14;
-    const double *q = a.qin + (size_t)c * a.cs + s;
-    const float q0 = (float)__ldg(q + o[0]), q1 = (float)__ldg(q + o[1]), q2 = (float)__ldg(q);
-    const float q3 = (float)__ldg(q + o[3]), q4 = (float)__ldg(q + o[4]);
-    const float Dm = limited_slope(th, q0, q1, q2);
-    const float D0 = limited_slope(th, q1, q2, q3);
-    const float Dp = limited_slope(th, q2, q3, q4);
-    st[r][0] = q3 - Dp * 0.5f;
-    st[r][1] = q2 + D0 * 0.5f;
-    st[r][2] = q2 - D0 * 0.5f;
-    st[r][3] = q1 + Dm * 0.5f;
-  }
-#pragma unroll
-  for (int r = NR; r < 9; ++r)
-#pragma unroll
-    for (int f = 0; f < 4; ++f) st[r][f] = 0.f;
-  float w[4];
-  bool ok[4];
-  inferred_face_n_f<EOS, 4>((float)a.t_euler, axis, st[0], st[1], st[2], st[3], st[4], st[5], st[6], st[7], st[8],
-                            g0f, w, ok);
-  FaceSpeeds<float> f;
-  if (ok[0] && ok[1] && ok[2] && ok[3]) {
-    f.wRf = w[0]; f.wLf = w[1]; f.wRb = w[2]; f.wLb = w[3];
-  } else {
-    const FaceSpeeds<double> d = face_speeds_fallback<EOS, SHEAR, BULK>(a, s, axis, o, g0, status);
-    f.wRf = (float)d.wRf; f.wLf = (float)d.wLf; f.wRb = (float)d.wRb; f.wLb = (float)d.wLb;
-  }
-  f.af = fmaxf(fabsf(f.wLf), fabsf(f.wRf));
-  f.ab = fmaxf(fabsf(f.wLb), fabsf(f.wRb));
-  return f;
-}
-
 // Phase B for one component: the KT fluxes H(i+1/2), H(i-1/2)
 // (SemiDiscreteKurganovTadmorScheme.cu:48-56, F = q u^axis/u^tau, FluxFunctions.cu:18-31)
 // and their difference (EulerStep.cu:1054-1062).
@@ -191,16 +140,20 @@ __device__ __forceinline__ int pi_spatial(int m, int a) {
 //   S_{m+1} = d(pi^{t m}) v - d(pi^{m a}) [- d(Pi), divided by tau^2 along eta, when m = a]
 template <int EOS, bool SHEAR, bool BULK, bool MIXED>
 __device__ __forceinline__ void axis_update(const StageArgs &a, int s, int axis, int idx, int n_axis, int stride,
-                                            double d, const GuessEos &g0, const GuessEosF &g0f, const double *uc,
-                                            double *out, unsigned &status) {
+                                            double d, const GuessEos &g0, const double *uc, double *out,
+                                            unsigned &status) {
   using R = typename std::conditional<MIXED, float, double>::type;
   constexpr int NQ = NComp<SHEAR, BULK>::value;
   const int o[5] = {(max(idx - 2, 0) - idx) * stride, (max(idx - 1, 0) - idx) * stride, 0,
                     (min(idx + 1, n_axis - 1) - idx) * stride, (min(idx + 2, n_axis - 1) - idx) * stride};
   const R inv_d = R(1.0 / d);
+  // Face states are recovered in FP64 on both paths (the mixed path rounds only the
+  // resulting speeds): an FP32 recovery was tried and let a 2+1D hotspot event run away
+  // to NaN that the FP64 recovery keeps finite.
+  const FaceSpeeds<double> fd = face_speeds<EOS, SHEAR, BULK>(a, s, axis, o, g0, status);
   FaceSpeeds<R> f;
-  if constexpr (MIXED) f = face_speeds_f<EOS, SHEAR, BULK>(a, s, axis, o, g0f, g0, status);
-  else f = face_speeds<EOS, SHEAR, BULK>(a, s, axis, o, g0, status);
+  f.wRf = (R)fd.wRf; f.wLf = (R)fd.wLf; f.wRb = (R)fd.wRb; f.wLb = (R)fd.wLb;
+  f.af = (R)fd.af; f.ab = (R)fd.ab;
 
   R Sa[4] = {R(0), R(0), R(0), R(0)};
   if (SHEAR) {
@@ -234,9 +187,10 @@ __device__ __forceinline__ void axis_update(const StageArgs &a, int s, int axis,
 #ifndef GVH_MIN_BLOCKS
 #define GVH_MIN_BLOCKS 3
 #endif
-// MIXED = false: plain FP64. MIXED = true: limiter, fluxes and source terms in FP32 (face
-// states recovered in FP32 with an FP64 redo when that fails); the state, the running
-// update, the Heun combination, the cell-centre recovery and the regulation in FP64.
+// MIXED = false: plain FP64. MIXED = true: limiter, KT fluxes and source-term algebra in
+// FP32; the state, every primitive-variable recovery (face states and cell centre), the
+// differences feeding the source terms, the running update, the Heun combination and the
+// regulation in FP64.
 //
 // stage_cell does one cell (interior index id < a.ncells); it returns the cell's new energy
 // density so callers can reduce it (the batched engine tracks max e per event).
@@ -267,34 +221,40 @@ __device__ __forceinline__ double stage_cell(const StageArgs &a, long long id) {
 #pragma unroll
     for (int n = 0; n < NQ; ++n) q[n] = (R)__ldg(a.qin + n * a.cs + s);
     const R pc = (R)__ldg(a.pin + s);
-    const R th = (R)a.theta;
-    const R idx_ = R(1.0 / a.dx), idy = R(1.0 / a.dy), idz = R(1.0 / a.dz);
     const long long xm = (i > 0) ? -1 : 0, xp = (i < a.nx - 1) ? 1 : 0;
     const long long ym = (j > 0) ? -a.sy : 0, yp = (j < a.ny - 1) ? a.sy : 0;
     const long long zm = (k > 0) ? -a.sz : 0, zp = (k < a.nz - 1) ? a.sz : 0;
+    // Derivatives of u and p: differences of nearly equal values, so they are formed in
+    // FP64 on both paths and only the results are rounded to the working precision.
     CellFlowT<R> f;
     R ucr[4];
 #pragma unroll
     for (int m = 0; m < 4; ++m) ucr[m] = (R)uc[m];
     f.ut = ucr[0]; f.ux = ucr[1]; f.uy = ucr[2]; f.un = ucr[3];
-    f.utp = (R)a.uprev[s]; f.uxp = (R)a.uprev[a.cs + s]; f.uyp = (R)a.uprev[2 * a.cs + s];
-    f.unp = (R)a.uprev[3 * a.cs + s];
+    // d u^mu / d tau = (u - u^{n-1}) / dt (SourceTerms.cu:68-71)
+    f.dtut = (R)((uc[0] - a.uprev[s]) / a.dt);
+    f.dtux = (R)((uc[1] - a.uprev[a.cs + s]) / a.dt);
+    f.dtuy = (R)((uc[2] - a.uprev[2 * a.cs + s]) / a.dt);
+    f.dtun = (R)((uc[3] - a.uprev[3 * a.cs + s]) / a.dt);
+    const double thd = a.theta;
+    const double idxd = 1.0 / a.dx, idyd = 1.0 / a.dy, idzd = 1.0 / a.dz;
     R du[3][4];
 #pragma unroll
     for (int m = 0; m < 4; ++m) {
       const double *u = a.uin + m * a.cs + s;
-      du[0][m] = limited_slope(th, (R)__ldg(u + xm), ucr[m], (R)__ldg(u + xp)) * idx_;
-      du[1][m] = limited_slope(th, (R)__ldg(u + ym), ucr[m], (R)__ldg(u + yp)) * idy;
-      du[2][m] = limited_slope(th, (R)__ldg(u + zm), ucr[m], (R)__ldg(u + zp)) * idz;
+      du[0][m] = (R)(limited_slope(thd, __ldg(u + xm), uc[m], __ldg(u + xp)) * idxd);
+      du[1][m] = (R)(limited_slope(thd, __ldg(u + ym), uc[m], __ldg(u + yp)) * idyd);
+      du[2][m] = (R)(limited_slope(thd, __ldg(u + zm), uc[m], __ldg(u + zp)) * idzd);
     }
     f.dxut = du[0][0]; f.dyut = du[1][0]; f.dnut = du[2][0];
     f.dxux = du[0][1]; f.dyux = du[1][1]; f.dnux = du[2][1];
     f.dxuy = du[0][2]; f.dyuy = du[1][2]; f.dnuy = du[2][2];
     f.dxun = du[0][3]; f.dyun = du[1][3]; f.dnun = du[2][3];
     const double *p = a.pin + s;
-    const R dxp = limited_slope(th, (R)__ldg(p + xm), pc, (R)__ldg(p + xp)) * idx_;
-    const R dyp = limited_slope(th, (R)__ldg(p + ym), pc, (R)__ldg(p + yp)) * idy;
-    const R dnp = limited_slope(th, (R)__ldg(p + zm), pc, (R)__ldg(p + zp)) * idz;
+    const double pcd = __ldg(p);
+    const R dxp = (R)(limited_slope(thd, __ldg(p + xm), pcd, __ldg(p + xp)) * idxd);
+    const R dyp = (R)(limited_slope(thd, __ldg(p + ym), pcd, __ldg(p + yp)) * idyd);
+    const R dnp = (R)(limited_slope(thd, __ldg(p + zm), pcd, __ldg(p + zp)) * idzd);
 
     const R t = (R)a.t_euler;
     const R Pi = BULK ? q[NQ - 1] : R(0);
@@ -319,7 +279,7 @@ __device__ __forceinline__ double stage_cell(const StageArgs &a, long long id) {
     if (SHEAR) {
       ShearT<R> pi{q[4], q[5], q[6], q[7], q[8], q[9], q[10], q[11], q[12], q[13]};
       R rhs[11];
-      pimunu_rhs<EOS, BULK, R>(rhs, t, (R)a.dt, (R)a.etabar, er, pc, f, pi, Pi, dkvk);
+      pimunu_rhs<EOS, BULK, R>(rhs, t, (R)a.etabar, er, pc, f, pi, Pi, dkvk);
 #pragma unroll
       for (int n = 4; n < NQ; ++n) S[n] = rhs[n - 4];
     }
@@ -333,15 +293,13 @@ __device__ __forceinline__ double stage_cell(const StageArgs &a, long long id) {
 
   // ---- flux divergence along x, y, eta (EulerStep.cu:1011-1277) -------------------------
   const GuessEos g0 = guess_eos<EOS>(ePrev);
-  GuessEosF g0f;
-  if (MIXED) g0f = guess_eos_f<EOS>(ePrev);
 #pragma unroll 1
   for (int axis = 0; axis < 3; ++axis) {
     const int idx = axis == 0 ? i : axis == 1 ? j : k;
     const int n_axis = axis == 0 ? a.nx : axis == 1 ? a.ny : a.nz;
     const int stride = axis == 0 ? 1 : axis == 1 ? (int)a.sy : (int)a.sz;
     const double d = axis == 0 ? a.dx : axis == 1 ? a.dy : a.dz;
-    axis_update<EOS, SHEAR, BULK, MIXED>(a, (int)s, axis, idx, n_axis, stride, d, g0, g0f, uc, out, status);
+    axis_update<EOS, SHEAR, BULK, MIXED>(a, (int)s, axis, idx, n_axis, stride, d, g0, uc, out, status);
   }
 
   // ---- Heun combination Q = (Q + q^n)/2 (FullyDiscreteKurganovTadmorScheme.cu:60-104) ---

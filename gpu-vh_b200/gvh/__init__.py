@@ -23,6 +23,8 @@ GVH_PRECISION_FP64 = 0
 GVH_PRECISION_MIXED = 1
 GVH_STATUS_NAN = 1
 GVH_STATUS_NEWTON = 2
+GVH_STATUS_DAMPED = 4       # informational (see include/gvh.h)
+GVH_STATUS_ERRORS = 1       # NaN; a non-converged Newton solve is a warning, as in the reference
 
 Q_NAMES = ["ttt", "ttx", "tty", "ttn", "pitt", "pitx", "pity", "pitn",
            "pixx", "pixy", "pixn", "piyy", "piyn", "pinn", "Pi"]
@@ -62,7 +64,7 @@ EXPORTS = [
     "gvh_default_options", "gvh_create", "gvh_destroy", "gvh_num_conserved", "gvh_num_fields",
     "gvh_num_lattice_cells", "gvh_set_primitive_state", "gvh_set_state", "gvh_get_state", "gvh_rk2_step",
     "gvh_status", "gvh_clear_status", "gvh_synchronize", "gvh_launches_per_step", "gvh_last_error",
-    "gvh_set_stream",
+    "gvh_set_stream", "gvh_max_energy_density",
 ]
 
 
@@ -94,6 +96,7 @@ def load(path: str | None = None):
     L.gvh_synchronize.argtypes = [vp]
     L.gvh_launches_per_step.argtypes = [vp]
     L.gvh_set_stream.argtypes = [vp, vp]
+    L.gvh_max_energy_density.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
     L.gvh_last_error.restype = ctypes.c_char_p
     if path is None:
         _lib = L
@@ -199,6 +202,11 @@ class Lattice:
     # -- stepping ------------------------------------------------------------------------
     def step(self, t, dt, T_reg=0.0):
         _check(self._L.gvh_rk2_step(self._h, float(t), float(dt), float(T_reg)), "gvh_rk2_step")
+
+    def max_energy_density(self) -> float:
+        v = ctypes.c_double()
+        _check(self._L.gvh_max_energy_density(self._h, ctypes.byref(v)), "gvh_max_energy_density")
+        return v.value
 
     def set_stream(self, stream_ptr: int | None):
         """Queue this lattice's work on a caller-owned CUDA stream (raw cudaStream_t value)."""

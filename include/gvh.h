@@ -46,7 +46,13 @@ extern "C" {
 
 /* status bits (gvh_status) */
 #define GVH_STATUS_NAN 1u          /* an energy density came out NaN */
-#define GVH_STATUS_NEWTON 2u       /* the QCD-EoS Newton solve hit its iteration cap */
+#define GVH_STATUS_NEWTON 2u       /* warning: a QCD-EoS Newton solve did not converge, even
+                                      damped; like the reference (EnergyMomentumTensor.cu:42-44)
+                                      the last iterate is used and the run goes on */
+#define GVH_STATUS_DAMPED 4u       /* informational: a Newton solve needed the damped update
+                                      (the reference switches to it after 5e5 undamped
+                                      iterations, EnergyMomentumTensor.cu:37-38; here after 200) */
+#define GVH_STATUS_ERRORS 1u       /* the bits that mean the state is not trustworthy */
 
 #define GVH_EOS_QCD 0              /* Wuppertal-Budapest fit (the reference default) */
 #define GVH_EOS_CONFORMAL 1        /* p = e/3 (CONFORMAL_EOS, EquationOfState.cuh:16) */
@@ -120,11 +126,17 @@ int gvh_get_state(gvh_handle *h, double *const *fields, int n_fields);
  * Asynchronous on the handle's stream. */
 int gvh_rk2_step(gvh_handle *h, double t, double dt, double T_reg);
 
-/* Waits for the handle's stream; returns GVH_OK, or GVH_ERR_NUMERIC with *flags set when a
- * step raised a status bit since the last gvh_clear_status. flags may be null. */
+/* Waits for the handle's stream and reports the status bits raised since the last
+ * gvh_clear_status in *flags (may be null). Returns GVH_ERR_NUMERIC when an error bit
+ * (GVH_STATUS_ERRORS) is set, else GVH_OK. */
 int gvh_status(gvh_handle *h, unsigned *flags);
 int gvh_clear_status(gvh_handle *h);
 int gvh_synchronize(gvh_handle *h);
+
+/* Maximum interior energy density of the current state (fm^-4), reduced on the device;
+ * with e(T_fo) it gives the reference's stop test (HydroPlugin.cpp:396-413) without copying
+ * the lattice to the host. Synchronises the handle's stream. */
+int gvh_max_energy_density(gvh_handle *h, double *out);
 
 /* Runs the handle's work on a caller-owned stream (a cudaStream_t passed as void*); NULL
  * returns to the handle's own stream. Waits for work already queued on the old stream. */
@@ -176,10 +188,12 @@ int gvh_batch_step(gvh_batch *b, int nsteps);
 int gvh_batch_synchronize(gvh_batch *b);
 int gvh_batch_event_info(gvh_batch *b, int event_id, gvh_event_info *info);
 int gvh_batch_get_state(gvh_batch *b, int event_id, double *const *fields, int n_fields);
+/* Stage-kernel grid: 0 = one 128-thread block per 128-cell tile (the default), n > 0 = a
+ * persistent grid of n blocks walking the tile queue. */
 int gvh_batch_launch_config(const gvh_batch *b, int *grid_blocks, int *block_threads);
 int gvh_batch_set_grid(gvh_batch *b, int grid_blocks);
-/* Chooses the persistent grid by timing `steps` real steps per candidate (the events
- * advance; every candidate computes the same values). */
+/* Chooses the grid by timing `steps` real steps per candidate (the events advance; every
+ * candidate computes the same values). */
 int gvh_batch_autotune(gvh_batch *b, int steps, int *chosen_grid);
 const char *gvh_batch_last_error(void);
 

@@ -116,7 +116,7 @@ def test_autotune_does_not_change_results():
     ida = [A.add_event(**kw, prim=prim, tau0=t0) for kw, prim, t0 in evs]
     idb = [B.add_event(**kw, prim=prim, tau0=t0) for kw, prim, t0 in evs]
     g = B.autotune(steps=1)  # advances B by (candidates + 1) x 1 steps
-    assert g >= 1
+    assert g >= 0  # 0 = one block per tile
     nb = B.info(idb[0]).step
     A.step(nb)
     for ea, eb in zip(ida, idb):

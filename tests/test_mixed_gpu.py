@@ -59,3 +59,30 @@ def test_mixed_config2_lattice_10_steps():
     G, sg, so = run_pair(w, prim, 10)
     err = mixed_errors(G, sg, so)
     assert err["e"] <= E_TOL and err["u"] <= U_TOL and err["pi"] <= PI_TOL, err
+
+
+def test_mixed_hotspot_event_stays_finite():
+    """A 2+1D hotspot event of the serving mix (61x61, 0.2 fm) that ran away to NaN when the
+    mixed path recovered face states in FP32; with FP64 recovery it stays finite and close
+    to the FP64 path."""
+    from gvh import serve
+    rng = np.random.default_rng(2024)
+    arr = serve.poisson_arrivals(4.0, 180, rng)
+    r = [serve.make_request(i, a, rng) for i, a in enumerate(arr[:11])][10]
+    lat = r.lattice
+    kw = dict(nx=lat["nx"], ny=lat["ny"], nz=lat["nz"], dx=lat["dx"], dy=lat["dy"], dz=lat["dz"], dt=lat["dt"],
+              etabar=lat["etabar"], theta=2.0, conformal=False, shear=True, bulk=True)
+    M = gvh.Lattice(precision="mixed", **kw)
+    D = gvh.Lattice(precision="fp64", **kw)
+    M.set_primitive(r.prim)
+    D.set_primitive(r.prim)
+    t = r.tau0
+    for n in range(1, 251):
+        M.step(t, lat["dt"])
+        D.step(t, lat["dt"])
+        t = r.tau0 + n * lat["dt"]
+    assert not M.status() & gvh.GVH_STATUS_NAN
+    sm, sd = M.get_state(), D.get_state()
+    e_m, e_d = M.interior(sm["e"]), D.interior(sd["e"])
+    assert np.isfinite(e_m).all()
+    assert float(np.max(np.abs(e_m - e_d)) / np.max(e_d)) <= 1e-3

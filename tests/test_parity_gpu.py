@@ -29,6 +29,9 @@ _spec.loader.exec_module(make_golden)
 
 REL_TOL = 1e-12
 QCD_TOL = 1e-9
+# After a chaotic Newton solve the two implementations agree only to the solver's stop
+# test (|de| <= 1e-3 |e|, converged quadratically, ~1e-6 of the face state).
+DAMPED_TOL = 1e-4
 
 
 def tol_for(lat_kw):
@@ -167,3 +170,40 @@ def test_config2_lattice_two_steps_matches_oracle():
     for k in G.field_names:
         err = rel_err(G.interior(sg[k]), O.interior(so[k]))
         assert err <= QCD_TOL, f"{k}: {err:.3e}"
+
+
+def _serving_event(rid, seed=11, rate=2.0):
+    from gvh import serve
+    rng = np.random.default_rng(seed)
+    arr = serve.poisson_arrivals(rate, 80, rng)
+    for i, a in enumerate(arr):
+        r = serve.make_request(i, a, rng)
+        if i == rid:
+            return r
+
+
+def test_non_converging_newton_takes_the_damped_phase():
+    """A 61x61 hotspot event whose face states at step ~65 make the reference's Newton
+    iteration wander for its whole undamped phase (5e5 iterations) before the damped update
+    converges it. The CUDA path switches to the damped update early (informational status
+    bit), raises no error bit, and stays with the oracle (which runs the full 5e5)."""
+    r = _serving_event(7)
+    lat = r.lattice
+    kw = dict(nx=lat["nx"], ny=lat["ny"], nz=lat["nz"], dx=lat["dx"], dy=lat["dy"], dz=lat["dz"], dt=lat["dt"],
+              etabar=lat["etabar"], theta=2.0, conformal=False, shear=True, bulk=True)
+    G = gvh.Lattice(**kw)
+    O = oracle.OracleLattice(**kw)
+    G.set_primitive(r.prim)
+    O.set_primitive(r.prim)
+    t = r.tau0
+    for n in range(1, 71):
+        G.step(t, lat["dt"])
+        O.step(t, lat["dt"])
+        t = r.tau0 + n * lat["dt"]
+    flags = G.status()
+    assert flags & gvh.GVH_STATUS_DAMPED and not flags & gvh.GVH_STATUS_ERRORS, flags
+    sg, so = G.get_state(), O.get_state()
+    for k in ("e", "ut", "ux", "uy", "ttt", "pixx", "Pi"):
+        assert np.isfinite(sg[k]).all()
+        err = rel_err(G.interior(sg[k]), O.interior(so[k]))
+        assert err <= DAMPED_TOL, f"{k}: {err:.3e}"
