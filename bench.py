@@ -409,7 +409,7 @@ def run_ours(args):
     b_cell = bytes_per_cell_update(L.nq)
     achieved = cells * b_cell / (ms / args.steps / 1e3) / 1e9
     traffic = None
-    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    tp = os.path.join(ROOT, "profiles", "kt_stage_traffic.json")
     if os.path.exists(tp):
         try:
             traffic = json.load(open(tp)).get("bytes_per_step")

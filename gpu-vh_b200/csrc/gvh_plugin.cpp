@@ -1,0 +1,291 @@
+// gvh_plugin.cpp -- the host side around the KT step: the reference's run-time inputs and
+// its run loop, in C++ over the C ABI of gvh.h.
+//
+//   gvh_read_lattice_parameters / gvh_read_hydro_parameters / gvh_read_ic_parameters
+//       the positional .properties readers (LatticeParameters.cpp:65-138,
+//       HydroParameters.cpp:49-98, InitialConditionParameters.cpp:65-149): line n is field
+//       n, whitespace is dropped, the value is what follows '='; missing lines leave 0.
+//   gvh_read_ic_files
+//       the type-10 initial-condition reader (InitialConditions.cpp:98-489): one
+//       "x y z value" file per field under <root>/input/, i outermost and k innermost, each
+//       value scanned as a float; e gets +1e-3 (InitialConditions.cpp:124).
+//   gvh_run
+//       HydroPlugin.cpp:107-434 for initial-condition type 10: set-up, then per step the
+//       field dump every FREQ = 10 steps (FileIO.cpp:15-60 format), the stop test (11
+//       checks with every cell at or below e(T_fo), HydroPlugin.cpp:396-413) and one RK2
+//       step. The state stays on the device: the stop test is a device reduction and only
+//       dumps copy fields back (the reference copies 30 arrays back every step).
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <cctype>
+#include <chrono>
+#include <fstream>
+#include <string>
+#include <vector>
+
+#include "../../include/gvh.h"
+
+namespace {
+
+thread_local std::string g_plugin_error;
+
+int pfail(int code, const std::string &msg) {
+  g_plugin_error = msg;
+  return code;
+}
+
+// One positional .properties file: the value of each line (text after '=', whitespace
+// removed), in order.
+bool read_properties(const std::string &path, std::vector<std::string> &values) {
+  std::ifstream in(path);
+  if (!in.is_open()) return false;
+  std::string line;
+  while (std::getline(in, line)) {
+    line.erase(std::remove_if(line.begin(), line.end(), [](unsigned char c) { return std::isspace(c); }),
+               line.end());
+    size_t pos = line.find('=');
+    values.push_back(pos == std::string::npos ? line : line.substr(pos + 1));
+  }
+  return true;
+}
+
+double num(const std::vector<std::string> &v, size_t i) { return i < v.size() ? atof(v[i].c_str()) : 0.0; }
+int inum(const std::vector<std::string> &v, size_t i) { return i < v.size() ? atoi(v[i].c_str()) : 0; }
+
+constexpr double kHbarc = 0.197326938;  // HydroPlugin.cpp:132
+constexpr int kFreq = 10;                // HydroPlugin.cpp:39
+constexpr int kFreezeoutChecks = 11;     // FOFREQ + 1, HydroPlugin.cpp:409
+
+long long ghost_index(int i, int j, int k, int nx, int ny) {
+  return (long long)i + (long long)(nx + 4) * (j + (long long)(ny + 4) * k);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *gvh_plugin_last_error(void) { return g_plugin_error.c_str(); }
+
+int gvh_read_lattice_parameters(const char *config_dir, gvh_lattice_params *out) {
+  if (!config_dir || !out) return pfail(GVH_ERR_INVALID, "null argument");
+  std::vector<std::string> v;
+  if (!read_properties(std::string(config_dir) + "/lattice.properties", v))
+    return pfail(GVH_ERR_INVALID, std::string("cannot open ") + config_dir + "/lattice.properties");
+  out->numLatticePointsX = inum(v, 0);
+  out->numLatticePointsY = inum(v, 1);
+  out->numLatticePointsRapidity = inum(v, 2);
+  out->numProperTimePoints = inum(v, 3);
+  out->latticeSpacingX = num(v, 4);
+  out->latticeSpacingY = num(v, 5);
+  out->latticeSpacingRapidity = num(v, 6);
+  out->latticeSpacingProperTime = num(v, 7);
+  out->numComputationalLatticePointsX = out->numLatticePointsX + 4;  // N_GHOST_CELLS
+  out->numComputationalLatticePointsY = out->numLatticePointsY + 4;
+  out->numComputationalLatticePointsRapidity = out->numLatticePointsRapidity + 4;
+  return GVH_OK;
+}
+
+int gvh_read_hydro_parameters(const char *config_dir, gvh_hydro_params *out) {
+  if (!config_dir || !out) return pfail(GVH_ERR_INVALID, "null argument");
+  std::vector<std::string> v;
+  if (!read_properties(std::string(config_dir) + "/hydro.properties", v))
+    return pfail(GVH_ERR_INVALID, std::string("cannot open ") + config_dir + "/hydro.properties");
+  out->initialProperTimePoint = num(v, 0);
+  out->shearViscosityToEntropyDensity = num(v, 1);
+  out->freezeoutTemperatureGeV = num(v, 2);
+  out->initializePimunuNavierStokes = inum(v, 3);
+  out->regulationTemperatureGeV = num(v, 4);  // absent in the shipped file: stays 0
+  return GVH_OK;
+}
+
+int gvh_read_ic_parameters(const char *config_dir, gvh_ic_params *out) {
+  if (!config_dir || !out) return pfail(GVH_ERR_INVALID, "null argument");
+  std::vector<std::string> v;
+  if (!read_properties(std::string(config_dir) + "/ic.properties", v))
+    return pfail(GVH_ERR_INVALID, std::string("cannot open ") + config_dir + "/ic.properties");
+  // line order of InitialConditionParameters.cpp:65-149 (not the struct's member order)
+  out->initialConditionType = inum(v, 0);
+  out->numberOfSourceFiles = inum(v, 1);
+  out->numberOfNucleonsPerNuclei = inum(v, 2);
+  out->initialEnergyDensity = num(v, 3);
+  out->scatteringCrossSectionNN = num(v, 4);
+  out->impactParameter = num(v, 5);
+  out->fractionOfBinaryCollisions = num(v, 6);
+  out->rapidityVariance = num(v, 7);
+  out->rapidityMean = num(v, 8);
+  out->sourceType = inum(v, 9);
+  return GVH_OK;
+}
+
+int gvh_read_ic_files(const char *root_dir, const gvh_lattice_params *L, int shear, int bulk, double *const *prim,
+                      int n_prim) {
+  if (!root_dir || !L || !prim) return pfail(GVH_ERR_INVALID, "null argument");
+  const int want = 5 + (shear ? 10 : 0) + (bulk ? 1 : 0);
+  if (n_prim != want) return pfail(GVH_ERR_INVALID, "wrong number of primitive arrays");
+  const int nx = L->numLatticePointsX, ny = L->numLatticePointsY, nz = L->numLatticePointsRapidity;
+  std::vector<std::string> names = {"e", "ut", "ux", "uy", "un"};
+  if (shear)
+    for (const char *c : {"pitt", "pitx", "pity", "pitn", "pixx", "pixy", "pixn", "piyy", "piyn", "pinn"})
+      names.push_back(c);
+  if (bulk) names.push_back("bulk");
+  const long long ng = (long long)(nx + 4) * (ny + 4) * (nz + 4);
+  for (int f = 0; f < n_prim; ++f) {
+    if (!prim[f]) return pfail(GVH_ERR_INVALID, "null primitive array");
+    std::fill(prim[f], prim[f] + ng, 0.0);
+    const std::string path = std::string(root_dir) + "/input/" + names[f] + ".dat";
+    FILE *fp = fopen(path.c_str(), "r");
+    if (!fp) return pfail(GVH_ERR_INVALID, "cannot open " + path);
+    for (int i = 2; i < nx + 2; ++i)
+      for (int j = 2; j < ny + 2; ++j)
+        for (int k = 2; k < nz + 2; ++k) {
+          float x, y, z, value;
+          if (fscanf(fp, "%f %f %f %f", &x, &y, &z, &value) != 4) {
+            fclose(fp);
+            return pfail(GVH_ERR_INVALID, "short or malformed file " + path);
+          }
+          double v = (double)value;
+          if (f == 0) v += 1.0e-3;
+          prim[f][ghost_index(i, j, k, nx, ny)] = v;
+        }
+    fclose(fp);
+  }
+  return GVH_OK;
+}
+
+// FileIO.cpp:15-60: <dir>/<name>_<t %.3f>.dat, k outermost, "x y z value" lines.
+int gvh_write_field(const char *output_dir, const char *name, double t, const gvh_lattice_params *L,
+                    const double *field) {
+  if (!output_dir || !name || !L || !field) return pfail(GVH_ERR_INVALID, "null argument");
+  char fname[1024];
+  snprintf(fname, sizeof fname, "%s/%s_%.3f.dat", output_dir, name, t);
+  FILE *fp = fopen(fname, "w");
+  if (!fp) return pfail(GVH_ERR_INVALID, std::string("cannot write ") + fname);
+  const int nx = L->numLatticePointsX, ny = L->numLatticePointsY, nz = L->numLatticePointsRapidity;
+  const double dx = L->latticeSpacingX, dy = L->latticeSpacingY, dz = L->latticeSpacingRapidity;
+  for (int k = 2; k < nz + 2; ++k) {
+    double z = (k - 2 - (nz - 1) / 2.) * dz;
+    for (int j = 2; j < ny + 2; ++j) {
+      double y = (j - 2 - (ny - 1) / 2.) * dy;
+      for (int i = 2; i < nx + 2; ++i) {
+        double x = (i - 2 - (nx - 1) / 2.) * dx;
+        fprintf(fp, "%.3f\t%.3f\t%.3f\t%.8f\n", x, y, z, field[ghost_index(i, j, k, nx, ny)]);
+      }
+    }
+  }
+  fclose(fp);
+  return GVH_OK;
+}
+
+int gvh_run(const gvh_lattice_params *L, const gvh_ic_params *ic, const gvh_hydro_params *H, const char *root_dir,
+            const char *output_dir, const gvh_options *opts, int dump_fields, gvh_run_report *report) {
+  if (!L || !ic || !H || !root_dir) return pfail(GVH_ERR_INVALID, "null argument");
+  if (ic->initialConditionType != 10)
+    return pfail(GVH_ERR_INVALID, "gvh_run reads initial-condition type 10 (input/*.dat files); type " +
+                                      std::to_string(ic->initialConditionType) + " is generated by the reference's "
+                                      "own initial-condition code, which is outside this library");
+  gvh_options o;
+  if (opts) o = *opts; else gvh_default_options(&o);
+  gvh_handle *h = nullptr;
+  int rc = gvh_create(L, H, &o, &h);
+  if (rc) return pfail(rc, std::string("gvh_create: ") + gvh_last_error());
+  const int nx = L->numLatticePointsX, ny = L->numLatticePointsY, nz = L->numLatticePointsRapidity;
+  const long long ng = (long long)(nx + 4) * (ny + 4) * (nz + 4);
+  const int n_prim = 5 + (o.shear ? 10 : 0) + (o.bulk ? 1 : 0);
+  std::vector<std::vector<double>> prim(n_prim, std::vector<double>(ng));
+  std::vector<double *> pp(n_prim);
+  for (int f = 0; f < n_prim; ++f) pp[f] = prim[f].data();
+  rc = gvh_read_ic_files(root_dir, L, o.shear, o.bulk, pp.data(), n_prim);
+  if (!rc) rc = gvh_set_primitive_state(h, pp.data(), n_prim);
+  if (rc) {
+    std::string msg = g_plugin_error.empty() ? gvh_last_error() : g_plugin_error;
+    gvh_destroy(h);
+    return pfail(rc, msg);
+  }
+  prim.clear();
+
+  const double t0 = H->initialProperTimePoint, dt = L->latticeSpacingProperTime;
+  const double T_reg = H->regulationTemperatureGeV / kHbarc;
+  // e(T_fo) through a one-cell batch so the EoS is the library's (HydroPlugin.cpp:133-135)
+  double e_fo = 0.0;
+  {
+    gvh_batch *b = nullptr;
+    gvh_options ob = o;
+    ob.precision = GVH_PRECISION_FP64;
+    gvh_lattice_params one = *L;
+    one.numLatticePointsX = one.numLatticePointsY = one.numLatticePointsRapidity = 1;
+    std::vector<double> e1(125, 1.0), z1(125, 0.0);
+    std::vector<const double *> p1(n_prim, z1.data());
+    p1[0] = e1.data();
+    p1[1] = e1.data();
+    int id = -1;
+    gvh_event_info inf;
+    if (gvh_batch_create(&ob, 1 << 20, &b) || gvh_batch_add_event(b, &one, H, p1.data(), n_prim, &id) ||
+        gvh_batch_event_info(b, id, &inf)) {
+      gvh_batch_destroy(b);
+      gvh_destroy(h);
+      return pfail(GVH_ERR_CUDA, std::string("freeze-out threshold: ") + gvh_batch_last_error());
+    }
+    e_fo = inf.freezeout_energy_density;
+    gvh_batch_destroy(b);
+  }
+
+  const int nf = gvh_num_fields(h), nq = gvh_num_conserved(h);
+  std::vector<std::vector<double>> fields;
+  std::vector<double *> fp;
+  double total_ms = 0.0;
+  long long steps = 0;
+  int frozen = 0;
+  double t = t0;
+  const int nt = L->numProperTimePoints;
+  for (int n = 1; n <= nt + 1; ++n) {
+    if (dump_fields && output_dir && (n - 1) % kFreq == 0) {
+      if (fields.empty()) {
+        fields.assign(nf, std::vector<double>(ng));
+        for (int f = 0; f < nf; ++f) fp.push_back(fields[f].data());
+      }
+      if ((rc = gvh_get_state(h, fp.data(), nf))) break;
+      static const char *qn[15] = {"ttt", "ttx", "tty", "ttn", "pitt", "pitx", "pity", "pitn",
+                                   "pixx", "pixy", "pixn", "piyy", "piyn", "pinn", "Pi"};
+      // HydroPlugin.cpp:44-70: e, p, u and the dissipative components
+      const int base = nq;
+      gvh_write_field(output_dir, "e", t, L, fp[base]);
+      gvh_write_field(output_dir, "p", t, L, fp[base + 1]);
+      gvh_write_field(output_dir, "ux", t, L, fp[base + 3]);
+      gvh_write_field(output_dir, "uy", t, L, fp[base + 4]);
+      gvh_write_field(output_dir, "un", t, L, fp[base + 5]);
+      gvh_write_field(output_dir, "ut", t, L, fp[base + 2]);
+      for (int c = 4; c < nq; ++c) gvh_write_field(output_dir, qn[c], t, L, fp[c]);
+    }
+    double emax = 0.0;
+    if ((rc = gvh_max_energy_density(h, &emax))) break;
+    if (emax <= e_fo) ++frozen;
+    if (frozen >= kFreezeoutChecks) break;
+    // wall time of one step, as the reference's Stopwatch brackets twoStepRungeKutta
+    // (HydroPlugin.cpp:414-420)
+    const auto c0 = std::chrono::steady_clock::now();
+    if ((rc = gvh_rk2_step(h, t, dt, T_reg))) break;
+    if ((rc = gvh_synchronize(h))) break;
+    total_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - c0).count();
+    ++steps;
+    t = t0 + n * dt;
+  }
+  unsigned flags = 0;
+  gvh_status(h, &flags);
+  if (report) {
+    report->steps = steps;
+    report->tau_end = t;
+    report->average_ms_per_step = steps ? total_ms / steps : 0.0;
+    report->frozen_out = frozen >= kFreezeoutChecks;
+    report->status = flags;
+    report->freezeout_energy_density = e_fo;
+  }
+  gvh_destroy(h);
+  if (rc) return pfail(rc, gvh_last_error());
+  return GVH_OK;
+}
+
+}  // extern "C"

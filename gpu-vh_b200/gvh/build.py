@@ -8,6 +8,7 @@ PKG_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))  # gpu-vh
 REPO_ROOT = os.path.dirname(PKG_ROOT)
 CSRC = os.path.join(PKG_ROOT, "csrc")
 LIB = os.path.join(PKG_ROOT, "libgvh.so")
+EXE = os.path.join(PKG_ROOT, "gvh-run")
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -17,7 +18,7 @@ NVCC_FLAGS = [
 
 
 def sources() -> list[str]:
-    return [os.path.join(CSRC, "gvh_capi.cu"), os.path.join(CSRC, "gvh_batch.cu")]
+    return [os.path.join(CSRC, "gvh_capi.cu"), os.path.join(CSRC, "gvh_batch.cu"), os.path.join(CSRC, "gvh_plugin.cpp")]
 
 
 def needs_rebuild() -> bool:
@@ -34,6 +35,11 @@ def build(verbose: bool = True, ptxas_info: bool = False) -> str:
     r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
     if r.returncode != 0:
         raise RuntimeError("libgvh build failed:\n" + r.stdout)
+    exe = [nvcc, "-O2", "-std=c++17", "-o", EXE, os.path.join(CSRC, "gvh_run_main.cpp"), "-L" + PKG_ROOT, "-lgvh",
+           "-Xlinker", "-rpath=$ORIGIN"]
+    r2 = subprocess.run(exe, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    if r2.returncode != 0:
+        raise RuntimeError("gvh-run build failed:\n" + r2.stdout)
     if verbose:
-        print(f"[gvh] built {LIB}")
+        print(f"[gvh] built {LIB} and {EXE}")
     return r.stdout

@@ -197,6 +197,62 @@ int gvh_batch_set_grid(gvh_batch *b, int grid_blocks);
 int gvh_batch_autotune(gvh_batch *b, int steps, int *chosen_grid);
 const char *gvh_batch_last_error(void);
 
+/* ------------------------------------------------------------------------------------
+ * Host side of a run: the reference's run-time inputs and run loop (libgvh.so).
+ * ---------------------------------------------------------------------------------- */
+
+/* Same layout as the reference's struct InitialConditionParameters
+ * (InitialConditionParameters.h:13-26). */
+typedef struct gvh_ic_params {
+	int initialConditionType;
+	int numberOfNucleonsPerNuclei;
+	int numberOfSourceFiles;
+	double initialEnergyDensity;
+	double scatteringCrossSectionNN;
+	double impactParameter;
+	double fractionOfBinaryCollisions;
+	double rapidityVariance;
+	double rapidityMean;
+	int sourceType;
+} gvh_ic_params;
+
+typedef struct gvh_run_report {
+	long long steps;                  /* RK2 steps taken */
+	double tau_end;                   /* proper time reached */
+	double average_ms_per_step;       /* wall time per step ("Average time/step",
+	                                     HydroPlugin.cpp:426) */
+	int frozen_out;                   /* stopped by the freeze-out rule (else by numProperTimePoints) */
+	unsigned status;                  /* GVH_STATUS_* bits */
+	double freezeout_energy_density;  /* e(T_fo) in fm^-4 */
+} gvh_run_report;
+
+/* Positional .properties readers: readLatticeParameters (LatticeParameters.cpp:65-138),
+ * readHydroParameters (HydroParameters.cpp:49-98), readInitialConditionParameters
+ * (InitialConditionParameters.cpp:65-149). Line n is field n; lines a file lacks leave 0
+ * (the shipped hydro.properties has no regulation temperature: T_reg = 0). */
+int gvh_read_lattice_parameters(const char *config_dir, gvh_lattice_params *out);
+int gvh_read_hydro_parameters(const char *config_dir, gvh_hydro_params *out);
+int gvh_read_ic_parameters(const char *config_dir, gvh_ic_params *out);
+
+/* Initial-condition type 10 (setInitialTmunuFromFiles, InitialConditions.cpp:98-489): reads
+ * <root>/input/{e,ut,ux,uy,un}.dat, then pitt..pinn if shear and bulk.dat if bulk, into
+ * ghosted arrays ordered as gvh_set_primitive_state takes them; e gets +1e-3. */
+int gvh_read_ic_files(const char *root_dir, const gvh_lattice_params *lattice, int shear, int bulk,
+                      double *const *prim, int n_prim);
+
+/* One field dump in the reference's output format (output(), FileIO.cpp:15-60). */
+int gvh_write_field(const char *output_dir, const char *name, double tau, const gvh_lattice_params *lattice,
+                    const double *field_ghosted);
+
+/* The run loop of run() (HydroPlugin.cpp:107-434) for initial-condition type 10: read the
+ * input files, then for n = 1 .. numProperTimePoints+1: dump fields every 10 steps (if
+ * dump_fields and output_dir), stop after 11 checks with every cell at or below e(T_fo),
+ * take one RK2 step. Other initial-condition types return GVH_ERR_INVALID. */
+int gvh_run(const gvh_lattice_params *lattice, const gvh_ic_params *ic, const gvh_hydro_params *hydro,
+            const char *root_dir, const char *output_dir, const gvh_options *opts, int dump_fields,
+            gvh_run_report *report);
+const char *gvh_plugin_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif
