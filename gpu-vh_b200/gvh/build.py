@@ -18,7 +18,8 @@ NVCC_FLAGS = [
 
 
 def sources() -> list[str]:
-    return [os.path.join(CSRC, "gvh_capi.cu"), os.path.join(CSRC, "gvh_batch.cu"), os.path.join(CSRC, "gvh_plugin.cpp")]
+    return [os.path.join(CSRC, "gvh_capi.cu"), os.path.join(CSRC, "gvh_batch.cu"), os.path.join(CSRC, "gvh_plugin.cpp"),
+            os.path.join(CSRC, "gvh_noalloc.cu")]
 
 
 def needs_rebuild() -> bool:

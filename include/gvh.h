@@ -133,6 +133,28 @@ int gvh_status(gvh_handle *h, unsigned *flags);
 int gvh_clear_status(gvh_handle *h);
 int gvh_synchronize(gvh_handle *h);
 
+/* One RK2 step on caller-owned device arrays that allocates nothing (no counterpart in the
+ * reference). For callers that own all their device memory and cannot allocate at step
+ * time -- a run loop with a fixed memory plan, a framework pool allocator that forbids
+ * foreign cudaMalloc, a region where an allocation would synchronise the device. The
+ * intermediate RK stage lives in a 32 MiB array compiled into the library (held on every
+ * GPU that loads it until exit), so the interior lattice is limited to
+ * (gvh_rk2_step_noalloc_max_bytes() - 256) / ((nq + 5) * 8) cells (about 200k cells with
+ * shear + bulk); larger lattices are rejected with GVH_ERR_INVALID.
+ * Arrays are interior-only (no ghosts), cell s = i + nx*(j + ny*k), components stacked with
+ * stride nx*ny*nz: q (nq components; in q^n, out q^{n+1}), e and p (in/out), u_prev (u one
+ * step earlier) and u (current u^mu, 4 components each; read only), u_next (out u^{n+1};
+ * must not alias u or u_prev). The step is queued on `stream` (a cudaStream_t, NULL = the
+ * legacy default stream); if status_out is not null the call waits and stores the
+ * GVH_STATUS_* bits. The first call on a device looks up the scratch address (do it before
+ * any stream capture). All calls share the scratch and its status word, which each call
+ * clears: calls whose work overlaps on the GPU race, so order them. */
+int gvh_rk2_step_noalloc(const gvh_lattice_params *lattice, const gvh_hydro_params *hydro, const gvh_options *opts,
+                         double t, double dt, double T_reg, double *q, double *e, double *p, const double *u_prev,
+                         const double *u, double *u_next, unsigned *status_out, void *stream);
+long long gvh_rk2_step_noalloc_max_bytes(void);
+const char *gvh_noalloc_last_error(void);
+
 /* Maximum interior energy density of the current state (fm^-4), reduced on the device;
  * with e(T_fo) it gives the reference's stop test (HydroPlugin.cpp:396-413) without copying
  * the lattice to the host. Synchronises the handle's stream. */
