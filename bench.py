@@ -58,10 +58,9 @@ def parse():
 
 
 def dist_info():
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return rank, world, local
+    from gvh import dist as gdist
+
+    return gdist.rank_info()
 
 
 def measured_peaks():
@@ -137,7 +136,10 @@ class ClockSampler:
 
 def make_event(w, rank):
     import dataclasses
-    w = dataclasses.replace(w, seed=w.seed + rank)
+
+    from gvh import dist as gdist
+
+    w = dataclasses.replace(w, seed=gdist.event_seed(w.seed, rank))
     prim = workloads.glauber_hotspots(w)
     meta = prim.pop("_meta")
     return w, prim, meta
@@ -358,13 +360,11 @@ def run_ours(args):
     flags = L.status()
     if flags & gvh.GVH_STATUS_ERRORS:
         raise RuntimeError(f"status flags {flags} raised during the timed steps")
-    ms_max = ms
-    if dist:
-        tt = torch.tensor([ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms_max = float(tt.item())
+    from gvh import dist as gdist
+
+    ms_max = gdist.max_over_ranks(ms, dist, device=torch.device("cuda", local))
     cells = w.cells
-    value = world * cells * args.steps / (ms_max / 1e3)
+    value = gdist.job_value(cells, args.steps, world, ms_max)
     launches = L.launches_per_step * args.steps
 
     # end to end through the C ABI with pinned host buffers
@@ -395,13 +395,9 @@ def run_ours(args):
         L.get_state_ptrs(ptr_out)
     e1.record(stream)
     torch.cuda.synchronize()
-    ms_e2e = e0.elapsed_time(e1)
-    if dist:
-        tt = torch.tensor([ms_e2e], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms_e2e = float(tt.item())
+    ms_e2e = gdist.max_over_ranks(e0.elapsed_time(e1), dist, device=torch.device("cuda", local))
     bytes_io = n_fields * L.ng * 8
-    e2e = {"value": world * cells * args.e2e_steps / (ms_e2e / 1e3), "unit": METRIC,
+    e2e = {"value": gdist.job_value(cells, args.e2e_steps, world, ms_e2e), "unit": METRIC,
            "h2d_bytes_per_step": bytes_io, "d2h_bytes_per_step": bytes_io,
            "ms_per_step": ms_e2e / args.e2e_steps, "steps": args.e2e_steps}
 
