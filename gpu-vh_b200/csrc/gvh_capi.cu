@@ -21,6 +21,7 @@
 #include <string>
 
 #include "../../include/gvh.h"
+#include "gvh_handle.h"
 #include "gvh_layout.cuh"
 #include "gvh_stage.cuh"
 
@@ -50,20 +51,6 @@ constexpr int kThreads = gvh::kBlock;
 
 }  // namespace
 
-struct gvh_handle {
-  int nx, ny, nz, nq;
-  long long ncells, ng;     // interior cells, ghosted cells
-  long long sy, sz, cs;     // internal strides
-  double dx, dy, dz, dt_lattice, etabar, theta;
-  int eos, shear, bulk, precision, device;
-  cudaStream_t stream;      // where work is queued (own_stream unless the caller set one)
-  cudaStream_t own_stream;
-  double *block;
-  double *qA, *qB, *e, *pA, *pB, *u[3];
-  int ucur, uprev, ufree;
-  unsigned *status;
-  double *staging;          // reference-layout fields for set/get, allocated on first use
-};
 
 namespace {
 

@@ -21,6 +21,10 @@ GVH_EOS_QCD = 0
 GVH_EOS_CONFORMAL = 1
 GVH_PRECISION_FP64 = 0
 GVH_PRECISION_MIXED = 1
+GVH_OK = 0
+GVH_ERR_INVALID = -1
+GVH_ERR_CUDA = -2
+GVH_ERR_NUMERIC = -3
 GVH_STATUS_NAN = 1
 GVH_STATUS_NEWTON = 2
 GVH_STATUS_DAMPED = 4       # informational (see include/gvh.h)

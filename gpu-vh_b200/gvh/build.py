@@ -13,13 +13,14 @@ EXE = os.path.join(PKG_ROOT, "gvh-run")
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17",
-    "-Xcompiler", "-fPIC", "-shared",
+    "-Xcompiler", "-fPIC,-ffp-contract=off", "-shared",
 ]
 
 
 def sources() -> list[str]:
     return [os.path.join(CSRC, "gvh_capi.cu"), os.path.join(CSRC, "gvh_batch.cu"), os.path.join(CSRC, "gvh_plugin.cpp"),
-            os.path.join(CSRC, "gvh_noalloc.cu")]
+            os.path.join(CSRC, "gvh_noalloc.cu"), os.path.join(CSRC, "gvh_surface.cu"),
+            os.path.join(CSRC, "gvh_surface_host.cpp")]
 
 
 def needs_rebuild() -> bool:

@@ -275,6 +275,67 @@ int gvh_run(const gvh_lattice_params *lattice, const gvh_ic_params *ic, const gv
             gvh_run_report *report);
 const char *gvh_plugin_last_error(void);
 
+/* ---- Freeze-out hypersurface (surface.dat) ------------------------------------------------
+ *
+ * Replaces the reference's host freeze-out finder: the FOFREQ+1 host copies of ten fields
+ * (FreezeOut.cpp:45-160, filled from a full device-to-host copy every step,
+ * HydroPlugin.cpp:264-281), the scan of every hypercube with cornelius
+ * (HydroPlugin.cpp:283-305, freezeout/cornelius-c++-1.3/cornelius.cpp) and the
+ * interpolated surface.dat row of each element (HydroPlugin.cpp:306-372, FreezeOut.cpp:1-43,
+ * 242-280). A gvh_surface keeps one time level of u^x, u^y, u^eta, e, pi^{xx,xy,x eta,yy,y eta}
+ * and Pi of its handle on the device; gvh_surface_find marks on the device the hypercubes of
+ * the slab (that level, the handle's current level) which the surface e = e_freezeout
+ * crosses, copies only their corner data to the host, runs the cornelius algorithm there on
+ * a pool of host threads and keeps the slab's rows in the reference's order (x outer, then
+ * y, then eta). The 3+1D case (nz > 1) finds 4D elements, nz == 1 3D (tau, x, y) elements. */
+typedef struct gvh_surface gvh_surface;
+
+#define GVH_SURFACE_COLUMNS 20 /* tau x y eta, tau*dsigma_mu (4), u^x u^y u^eta, e, T, p,
+                                  pi^{xx,xy,x eta,yy,y eta}, Pi */
+
+typedef struct {
+  long long slabs;               /* gvh_surface_find calls */
+  long long hypercubes_last;     /* hypercubes crossed in the last slab */
+  long long hypercubes_total;
+  long long points_last;         /* lattice points copied to the host for the last slab */
+  long long elements_last;       /* surface elements (rows) of the last slab */
+  long long elements_total;
+  long long errors_total;        /* hypercubes where the algorithm stops (the reference exits) */
+  double bytes_to_host_total;
+  double device_seconds_total;   /* marking, compaction and copies, host wall clock */
+  double host_seconds_total;     /* cornelius, interpolation and formatting */
+} gvh_surface_info;
+
+/* e_freezeout: the surface's energy density (fm^-4), e(T_fo) in the reference
+ * (HydroPlugin.cpp:131-135). Needs nx > 1 and ny > 1 (the reference's finder handles
+ * nothing else, HydroPlugin.cpp:157-182). The handle must outlive the surface. */
+int gvh_surface_create(gvh_handle *h, double e_freezeout, gvh_surface **out);
+int gvh_surface_destroy(gvh_surface *s);
+int gvh_surface_set_threads(gvh_surface *s, int nthreads);
+/* Takes the handle's current state as the lower time level of the next slab. */
+int gvh_surface_set_lower(gvh_surface *s);
+/* Elements of the slab (lower level, handle's current level); then the current level becomes
+ * the lower one. tau_label is added to each element's centroid tau and tau_scale multiplies
+ * its normal, as the reference labels its rows (HydroPlugin.cpp:298-314). */
+int gvh_surface_find(gvh_surface *s, double tau_label, double tau_scale, long long *n_elements);
+/* The last slab's rows: n_elements x GVH_SURFACE_COLUMNS doubles, or as the text the
+ * reference writes (ostream default format, space separated, one row per line). The text
+ * stays valid until the next gvh_surface_find. */
+int gvh_surface_get_rows(gvh_surface *s, double *rows, long long max_rows);
+int gvh_surface_get_text(gvh_surface *s, const char **text, long long *length);
+int gvh_surface_get_info(const gvh_surface *s, gvh_surface_info *info);
+const char *gvh_surface_last_error(void);
+
+/* Iso-surface elements of one cube of dimension dim = 2, 3 or 4 (Cornelius::find_surface_2d,
+ * _3d, _4d; cornelius.cpp:2115-2245). corners: 2^dim values, C order over the dim axes;
+ * dx: dim edge lengths; iso: the surface value. Writes up to max_elements centroids and
+ * normals (dim values each, relative to the cube's first corner; the normal is the
+ * covariant surface vector pointing to lower values, without Jacobian factors) and their
+ * count. Returns GVH_ERR_NUMERIC where the reference exits (cornelius.cpp:1287, 1552) and
+ * GVH_ERR_INVALID for bad arguments or too small output arrays. Host only; no GPU needed. */
+int gvh_cornelius(int dim, const double *corners, const double *dx, double iso, double *centroids, double *normals,
+                  int max_elements, int *n_elements);
+
 #ifdef __cplusplus
 }
 #endif

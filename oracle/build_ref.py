@@ -103,6 +103,16 @@ def build_variant(name: str, flux_limiter: str) -> str:
     return lib
 
 
+def build_cornelius() -> str:
+    """The reference's cornelius (freezeout/cornelius-c++-1.3/cornelius.cpp, included by
+    oracle/ref_cornelius.cpp from its place in the reference tree)."""
+    lib = os.path.join(OUT, "libref_cornelius.so")
+    inc = os.path.join(REF_ROOT, "freezeout", "cornelius-c++-1.3")
+    _run(["g++", "-std=c++14", "-O2", "-fPIC", "-shared", "-ffp-contract=off", "-w", "-I", inc,
+          os.path.join(HERE, "ref_cornelius.cpp"), "-o", lib])
+    return lib
+
+
 def build(jobs: int | None = None, verbose: bool = True) -> list[str]:
     """Build every variant; returns the library paths. Skips (returns []) when the
     reference tree is not present, e.g. on a host that only runs prebuilt files."""
@@ -115,6 +125,7 @@ def build(jobs: int | None = None, verbose: bool = True) -> list[str]:
     names = variant_names()
     with ThreadPoolExecutor(max_workers=jobs or min(12, os.cpu_count() or 4)) as ex:
         libs = list(ex.map(lambda n: build_variant(n, fl), names))
+    libs.append(build_cornelius())
     shutil.rmtree(os.path.join(OUT, "obj"), ignore_errors=True)
     if verbose:
         print(f"[oracle/_ref] built {len(libs)} variants into {OUT}")
