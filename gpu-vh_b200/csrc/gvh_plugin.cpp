@@ -180,8 +180,31 @@ int gvh_write_field(const char *output_dir, const char *name, double t, const gv
   return GVH_OK;
 }
 
+void gvh_surface_slab_labels(long long k, double tau0, double dtau, double *tau_label, double *tau_scale,
+                             long long *flush_iteration) {
+  // Levels are stored at iteration n = level + 1; the finder runs at iterations n with
+  // n % 10 == 9 over the slabs stored since the last run (HydroPlugin.cpp:262-287). The first
+  // chunk labels a slab with its lower level's time, later ones with its upper level's
+  // (HydroPlugin.cpp:298-299); the normal is scaled by the loop's t of the flush iteration.
+  long long flush;
+  double label;
+  if (k <= 7) {
+    flush = 9;
+    label = tau0 + ((double)k) * dtau;
+  } else {
+    flush = 10 * ((k + 2) / 10) + 9;
+    label = tau0 + ((double)(k + 1)) * dtau;
+  }
+  if (tau_label) *tau_label = label;
+  if (tau_scale) *tau_scale = tau0 + (double)(flush - 1) * dtau;
+  if (flush_iteration) *flush_iteration = flush;
+}
+
 int gvh_run(const gvh_lattice_params *L, const gvh_ic_params *ic, const gvh_hydro_params *H, const char *root_dir,
-            const char *output_dir, const gvh_options *opts, int dump_fields, gvh_run_report *report) {
+            const char *output_dir, const gvh_options *opts, int outputs, gvh_run_report *report) {
+  g_plugin_error.clear();
+  const bool dump_fields = (outputs & GVH_RUN_FIELDS) != 0;
+  const bool want_surface = (outputs & GVH_RUN_SURFACE) != 0 && output_dir;
   if (!L || !ic || !H || !root_dir) return pfail(GVH_ERR_INVALID, "null argument");
   if (ic->initialConditionType != 10)
     return pfail(GVH_ERR_INVALID, "gvh_run reads initial-condition type 10 (input/*.dat files); type " +
@@ -233,6 +256,31 @@ int gvh_run(const gvh_lattice_params *L, const gvh_ic_params *ic, const gvh_hydr
     gvh_batch_destroy(b);
   }
 
+  // freeze-out surface (HydroPlugin.cpp:155-211 set-up, 255-393 per iteration)
+  gvh_surface *surf = nullptr;
+  FILE *surf_file = nullptr;
+  std::string chunk_text;
+  long long surf_rows = 0, chunk_rows = 0;
+  double surf_seconds = 0.0;
+  if (want_surface) {
+    const std::string path = std::string(output_dir) + "/surface.dat";
+    surf_file = fopen(path.c_str(), "w");
+    if (!surf_file) {
+      gvh_destroy(h);
+      return pfail(GVH_ERR_INVALID, "cannot open " + path);
+    }
+    // the reference's finder handles 3+1D and 2+1D lattices only (HydroPlugin.cpp:157-182)
+    if (L->numLatticePointsX > 1 && L->numLatticePointsY > 1) {
+      if ((rc = gvh_surface_create(h, e_fo, &surf)) || (rc = gvh_surface_set_lower(surf))) {
+        std::string msg = gvh_surface_last_error();
+        gvh_surface_destroy(surf);
+        fclose(surf_file);
+        gvh_destroy(h);
+        return pfail(rc, msg);
+      }
+    }
+  }
+
   const int nf = gvh_num_fields(h), nq = gvh_num_conserved(h);
   std::vector<std::vector<double>> fields;
   std::vector<double *> fp;
@@ -260,6 +308,34 @@ int gvh_run(const gvh_lattice_params *L, const gvh_ic_params *ic, const gvh_hydr
       gvh_write_field(output_dir, "ut", t, L, fp[base + 2]);
       for (int c = 4; c < nq; ++c) gvh_write_field(output_dir, qn[c], t, L, fp[c]);
     }
+    if (surf && n >= 2) {
+      const auto s0 = std::chrono::steady_clock::now();
+      const long long k = n - 2;  // slab between levels n-2 and n-1
+      double label, scale;
+      long long flush;
+      gvh_surface_slab_labels(k, t0, dt, &label, &scale, &flush);
+      long long nel = 0;
+      if ((rc = gvh_surface_find(surf, label, scale, &nel))) {
+        g_plugin_error = gvh_surface_last_error();
+        break;
+      }
+      const char *txt = nullptr;
+      long long len = 0;
+      gvh_surface_get_text(surf, &txt, &len);
+      chunk_text.append(txt, (size_t)len);
+      chunk_rows += nel;
+      if (flush == n) {
+        if (fwrite(chunk_text.data(), 1, chunk_text.size(), surf_file) != chunk_text.size()) {
+          rc = GVH_ERR_INVALID;
+          g_plugin_error = "writing surface.dat failed";
+          break;
+        }
+        surf_rows += chunk_rows;
+        chunk_text.clear();
+        chunk_rows = 0;
+      }
+      surf_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - s0).count();
+    }
     double emax = 0.0;
     if ((rc = gvh_max_energy_density(h, &emax))) break;
     if (emax <= e_fo) ++frozen;
@@ -282,9 +358,13 @@ int gvh_run(const gvh_lattice_params *L, const gvh_ic_params *ic, const gvh_hydr
     report->frozen_out = frozen >= kFreezeoutChecks;
     report->status = flags;
     report->freezeout_energy_density = e_fo;
+    report->surface_elements = surf_rows;
+    report->surface_seconds = surf_seconds;
   }
+  gvh_surface_destroy(surf);
+  if (surf_file) fclose(surf_file);
   gvh_destroy(h);
-  if (rc) return pfail(rc, gvh_last_error());
+  if (rc) return pfail(rc, g_plugin_error.empty() ? gvh_last_error() : g_plugin_error);
   return GVH_OK;
 }
 

@@ -2,7 +2,8 @@
 // HydroWrapper.cpp:17-87, flags of CommandLineArguments.cpp:17-24): -c <config dir> with
 // lattice/hydro/ic.properties, -o <output dir>; the initial state is read from
 // <cwd>/input/*.dat (initial-condition type 10). Extra flags select the reference's
-// compile-time switches: --conformal, --no-bulk, --ideal, --theta <v>, --mixed, --no-dump.
+// compile-time switches: --conformal, --no-bulk, --ideal, --theta <v>, --mixed; --no-dump and
+// --no-surface turn off the field dumps and <output dir>/surface.dat.
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -16,7 +17,7 @@ int main(int argc, char **argv) {
   std::string config = "rhic-conf", out = "output";
   gvh_options o;
   gvh_default_options(&o);
-  int dump = 1;
+  int outputs = GVH_RUN_FIELDS | GVH_RUN_SURFACE;
   for (int i = 1; i < argc; ++i) {
     std::string a = argv[i];
     if ((a == "-c" || a == "--config") && i + 1 < argc) config = argv[++i];
@@ -26,11 +27,12 @@ int main(int argc, char **argv) {
     else if (a == "--ideal") { o.bulk = 0; o.shear = 0; }
     else if (a == "--theta" && i + 1 < argc) o.theta = atof(argv[++i]);
     else if (a == "--mixed") o.precision = GVH_PRECISION_MIXED;
-    else if (a == "--no-dump") dump = 0;
+    else if (a == "--no-dump") outputs &= ~GVH_RUN_FIELDS;
+    else if (a == "--no-surface") outputs &= ~GVH_RUN_SURFACE;
     else if (a == "-h" || a == "-t") continue;  // the reference accepts these too
     else {
       fprintf(stderr, "usage: %s [-c config_dir] [-o output_dir] [--conformal] [--no-bulk] [--ideal] "
-                      "[--theta v] [--mixed] [--no-dump]\n", argv[0]);
+                      "[--theta v] [--mixed] [--no-dump] [--no-surface]\n", argv[0]);
       return 2;
     }
   }
@@ -48,7 +50,7 @@ int main(int argc, char **argv) {
   printf("spatial resolution = (%.3f, %.3f, %.3f)\n", L.latticeSpacingX, L.latticeSpacingY, L.latticeSpacingRapidity);
   printf("eta/s = %.6f\n", H.shearViscosityToEntropyDensity);
   gvh_run_report r;
-  int rc = gvh_run(&L, &ic, &H, cwd, out.c_str(), &o, dump, &r);
+  int rc = gvh_run(&L, &ic, &H, cwd, out.c_str(), &o, outputs, &r);
   if (rc) {
     fprintf(stderr, "gvh-run: %s\n", gvh_plugin_last_error());
     return 1;
@@ -56,5 +58,7 @@ int main(int argc, char **argv) {
   if (r.frozen_out) printf("\nAll cells have dropped below freezeout energy density\n");
   printf("Average time/step: %.3f ms\n", r.average_ms_per_step);
   printf("steps = %lld, tau = %.3f fm/c, status = %u\n", r.steps, r.tau_end, r.status);
+  if (outputs & GVH_RUN_SURFACE)
+    printf("surface elements = %lld (finder %.3f s)\n", r.surface_elements, r.surface_seconds);
   return 0;
 }

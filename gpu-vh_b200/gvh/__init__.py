@@ -396,3 +396,102 @@ class Batch:
         g = ctypes.c_int()
         _bcheck(self._L.gvh_batch_autotune(self._h, int(steps), ctypes.byref(g)), "gvh_batch_autotune")
         return g.value
+
+
+# ---- freeze-out hypersurface ------------------------------------------------------------
+
+SURFACE_COLUMNS = 20
+SURFACE_COLUMN_NAMES = ["tau", "x", "y", "eta", "dsigma_tau", "dsigma_x", "dsigma_y", "dsigma_eta", "ux", "uy",
+                        "un", "e", "T", "p", "pixx", "pixy", "pixn", "piyy", "piyn", "Pi"]
+
+
+class SurfaceInfo(ctypes.Structure):
+    _fields_ = [("slabs", ctypes.c_longlong), ("hypercubes_last", ctypes.c_longlong),
+                ("hypercubes_total", ctypes.c_longlong), ("points_last", ctypes.c_longlong),
+                ("elements_last", ctypes.c_longlong), ("elements_total", ctypes.c_longlong),
+                ("errors_total", ctypes.c_longlong), ("bytes_to_host_total", ctypes.c_double),
+                ("device_seconds_total", ctypes.c_double), ("host_seconds_total", ctypes.c_double)]
+
+
+def _bind_surface(L):
+    if getattr(L, "_surface_bound", False):
+        return L
+    vp, dp, ll = ctypes.c_void_p, ctypes.c_double, ctypes.c_longlong
+    L.gvh_surface_create.argtypes = [vp, dp, ctypes.POINTER(vp)]
+    L.gvh_surface_destroy.argtypes = [vp]
+    L.gvh_surface_set_threads.argtypes = [vp, ctypes.c_int]
+    L.gvh_surface_set_lower.argtypes = [vp]
+    L.gvh_surface_find.argtypes = [vp, dp, dp, ctypes.POINTER(ll)]
+    L.gvh_surface_get_rows.argtypes = [vp, ctypes.POINTER(dp), ll]
+    L.gvh_surface_get_text.argtypes = [vp, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ll)]
+    L.gvh_surface_get_info.argtypes = [vp, ctypes.POINTER(SurfaceInfo)]
+    L.gvh_surface_last_error.restype = ctypes.c_char_p
+    L.gvh_surface_slab_labels.argtypes = [ll, dp, dp, ctypes.POINTER(dp), ctypes.POINTER(dp), ctypes.POINTER(ll)]
+    L.gvh_surface_slab_labels.restype = None
+    L._surface_bound = True
+    return L
+
+
+def slab_labels(k, tau0, dtau):
+    """(tau_label, tau_scale, flush_iteration) the reference gives the slab (k, k+1)."""
+    L = _bind_surface(load())
+    a, b, f = ctypes.c_double(), ctypes.c_double(), ctypes.c_longlong()
+    L.gvh_surface_slab_labels(int(k), float(tau0), float(dtau), ctypes.byref(a), ctypes.byref(b), ctypes.byref(f))
+    return a.value, b.value, f.value
+
+
+class Surface:
+    """Freeze-out hypersurface of a Lattice's evolution (gvh_surface_*): device marking of the
+    crossed hypercubes, host cornelius, rows in the reference's surface.dat layout."""
+
+    def __init__(self, lattice, e_freezeout, threads=None):
+        self._L = _bind_surface(load())
+        self.lattice = lattice
+        h = ctypes.c_void_p()
+        rc = self._L.gvh_surface_create(lattice._h, float(e_freezeout), ctypes.byref(h))
+        if rc != 0:
+            raise GvhError(f"gvh_surface_create failed ({rc}): {self._L.gvh_surface_last_error().decode()}")
+        self._h = h
+        if threads:
+            self._L.gvh_surface_set_threads(h, int(threads))
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise GvhError(f"{what} failed ({rc}): {self._L.gvh_surface_last_error().decode()}")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.gvh_surface_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_lower(self):
+        self._check(self._L.gvh_surface_set_lower(self._h), "gvh_surface_set_lower")
+
+    def find(self, tau_label, tau_scale) -> int:
+        n = ctypes.c_longlong()
+        self._check(self._L.gvh_surface_find(self._h, float(tau_label), float(tau_scale), ctypes.byref(n)),
+                    "gvh_surface_find")
+        return n.value
+
+    def rows(self) -> np.ndarray:
+        n = self.info()["elements_last"]
+        out = np.zeros((n, SURFACE_COLUMNS))
+        self._check(self._L.gvh_surface_get_rows(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), n),
+                    "gvh_surface_get_rows")
+        return out
+
+    def text(self) -> str:
+        p, n = ctypes.c_char_p(), ctypes.c_longlong()
+        self._check(self._L.gvh_surface_get_text(self._h, ctypes.byref(p), ctypes.byref(n)), "gvh_surface_get_text")
+        return ctypes.string_at(p, n.value).decode() if n.value else ""
+
+    def info(self) -> dict:
+        inf = SurfaceInfo()
+        self._check(self._L.gvh_surface_get_info(self._h, ctypes.byref(inf)), "gvh_surface_get_info")
+        return {k: getattr(inf, k) for k, _ in SurfaceInfo._fields_}

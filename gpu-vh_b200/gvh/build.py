@@ -32,11 +32,30 @@ def needs_rebuild() -> bool:
 
 
 def build(verbose: bool = True, ptxas_info: bool = False) -> str:
+    """Compiles every source to an object in parallel (gpu-vh_b200/_build/), then links."""
+    from concurrent.futures import ThreadPoolExecutor
+
     nvcc = os.environ.get("NVCC", "nvcc")
-    cmd = [nvcc] + NVCC_FLAGS + (["-Xptxas", "-v"] if ptxas_info else []) + ["-o", LIB] + sources()
-    r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    obj_dir = os.path.join(PKG_ROOT, "_build")
+    os.makedirs(obj_dir, exist_ok=True)
+    compile_flags = [f for f in NVCC_FLAGS if f != "-shared"]
+
+    def compile_one(src):
+        obj = os.path.join(obj_dir, os.path.basename(src) + ".o")
+        cmd = [nvcc] + compile_flags + (["-Xptxas", "-v"] if ptxas_info else []) + ["-c", src, "-o", obj]
+        r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("libgvh build failed:\n" + r.stdout)
+        return obj, r.stdout
+
+    with ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 4)) as ex:
+        results = list(ex.map(compile_one, sources()))
+    objs = [o for o, _ in results]
+    log = "".join(out for _, out in results)
+    r = subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB] + objs,
+                       stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
     if r.returncode != 0:
-        raise RuntimeError("libgvh build failed:\n" + r.stdout)
+        raise RuntimeError("libgvh link failed:\n" + r.stdout)
     exe = [nvcc, "-O2", "-std=c++17", "-o", EXE, os.path.join(CSRC, "gvh_run_main.cpp"), "-L" + PKG_ROOT, "-lgvh",
            "-Xlinker", "-rpath=$ORIGIN"]
     r2 = subprocess.run(exe, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
@@ -44,4 +63,4 @@ def build(verbose: bool = True, ptxas_info: bool = False) -> str:
         raise RuntimeError("gvh-run build failed:\n" + r2.stdout)
     if verbose:
         print(f"[gvh] built {LIB} and {EXE}")
-    return r.stdout
+    return log

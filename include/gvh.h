@@ -246,7 +246,13 @@ typedef struct gvh_run_report {
 	int frozen_out;                   /* stopped by the freeze-out rule (else by numProperTimePoints) */
 	unsigned status;                  /* GVH_STATUS_* bits */
 	double freezeout_energy_density;  /* e(T_fo) in fm^-4 */
+	long long surface_elements;       /* rows written to surface.dat */
+	double surface_seconds;           /* wall time of the freeze-out surface finder */
 } gvh_run_report;
+
+/* gvh_run outputs (bit flags) */
+#define GVH_RUN_FIELDS 1  /* field dumps every 10 steps (FileIO.cpp:15-60) */
+#define GVH_RUN_SURFACE 2 /* <output_dir>/surface.dat, the reference's freeze-out surface */
 
 /* Positional .properties readers: readLatticeParameters (LatticeParameters.cpp:65-138),
  * readHydroParameters (HydroParameters.cpp:49-98), readInitialConditionParameters
@@ -267,12 +273,22 @@ int gvh_write_field(const char *output_dir, const char *name, double tau, const 
                     const double *field_ghosted);
 
 /* The run loop of run() (HydroPlugin.cpp:107-434) for initial-condition type 10: read the
- * input files, then for n = 1 .. numProperTimePoints+1: dump fields every 10 steps (if
- * dump_fields and output_dir), stop after 11 checks with every cell at or below e(T_fo),
- * take one RK2 step. Other initial-condition types return GVH_ERR_INVALID. */
+ * input files, then for n = 1 .. numProperTimePoints+1: dump fields every 10 steps
+ * (GVH_RUN_FIELDS), find the freeze-out surface of the last slab and write it to
+ * <output_dir>/surface.dat in chunks of 10 steps as the reference does (GVH_RUN_SURFACE;
+ * the reference writes output/surface.dat relative to its working directory), stop after 11
+ * checks with every cell at or below e(T_fo), take one RK2 step. Other initial-condition
+ * types return GVH_ERR_INVALID. */
 int gvh_run(const gvh_lattice_params *lattice, const gvh_ic_params *ic, const gvh_hydro_params *hydro,
-            const char *root_dir, const char *output_dir, const gvh_options *opts, int dump_fields,
+            const char *root_dir, const char *output_dir, const gvh_options *opts, int outputs,
             gvh_run_report *report);
+
+/* The reference's labels for the slab between time levels k and k+1 (HydroPlugin.cpp:262-314,
+ * FOFREQ = 10): its rows go to the file at loop iteration *flush_iteration (state = level
+ * flush_iteration - 1), with tau_label added to the centroid's tau and the normal multiplied by
+ * tau_scale. Slabs of a chunk whose flush iteration the loop does not reach are not written. */
+void gvh_surface_slab_labels(long long k, double tau0, double dtau, double *tau_label, double *tau_scale,
+                             long long *flush_iteration);
 const char *gvh_plugin_last_error(void);
 
 /* ---- Freeze-out hypersurface (surface.dat) ------------------------------------------------

@@ -208,6 +208,12 @@ class RefLattice(_Base):
             getattr(L, fn).restype = ctypes.c_double
         L.gvh_ref_inferred.argtypes = [ctypes.c_double, ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p]
         L.gvh_ref_set_threads.argtypes = [ctypes.c_int]
+        L.gvh_ref_surface_begin.argtypes = [ctypes.c_int] * 3 + [ctypes.c_double] * 6 + [ctypes.c_char_p]
+        L.gvh_ref_surface_begin.restype = ctypes.c_void_p
+        L.gvh_ref_surface_iteration.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double]
+        L.gvh_ref_surface_iteration.restype = ctypes.c_longlong
+        L.gvh_ref_surface_end.argtypes = [ctypes.c_void_p]
+        L.gvh_ref_surface_end.restype = ctypes.c_longlong
         self._L = L
         if threads:
             L.gvh_ref_set_threads(int(threads))
@@ -238,6 +244,23 @@ class RefLattice(_Base):
 
     def pressure(self, e):
         return self._L.gvh_ref_equilibrium_pressure(e)
+
+    # The freeze-out part of the reference's run loop (oracle/ref_surface.cpp).
+    def surface_begin(self, t0, e_fo, path):
+        p = self.params
+        h = self._L.gvh_ref_surface_begin(p["nx"], p["ny"], p["nz"], t0, p["dt"], p["dx"], p["dy"], p["dz"], e_fo,
+                                          str(path).encode())
+        if not h:
+            raise ValueError("the reference's surface finder needs nx, ny > 1")
+        self._surface = h
+
+    def surface_iteration(self, n, t):
+        return int(self._L.gvh_ref_surface_iteration(self._surface, n, t))
+
+    def surface_end(self):
+        rows = int(self._L.gvh_ref_surface_end(self._surface))
+        self._surface = None
+        return rows
 
     def temperature(self, e):
         return self._L.gvh_ref_effective_temperature(e)

@@ -98,6 +98,11 @@ def build_variant(name: str, flux_limiter: str) -> str:
     o = os.path.join(obj_dir, "ref_driver.o")
     _run(common + ["-c", os.path.join(HERE, "ref_driver.cpp"), "-o", o])
     objs.append(o)
+    # the freeze-out replay includes FreezeOut.cpp, Memory.cpp and cornelius.cpp from the
+    # reference's freezeout/ directory, as HydroPlugin.cpp does
+    o = os.path.join(obj_dir, "ref_surface.o")
+    _run(common + ["-I", os.path.join(REF_ROOT, "freezeout"), "-c", os.path.join(HERE, "ref_surface.cpp"), "-o", o])
+    objs.append(o)
     lib = lib_path(name)
     _run(["g++", "-shared", "-fopenmp", "-o", lib] + objs)
     return lib

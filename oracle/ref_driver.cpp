@@ -168,6 +168,13 @@ void regulate(PRECISION t, CONSERVED_VARIABLES *q, PRECISION *e, PRECISION *p, F
 
 } // namespace
 
+/* The current level's host state, for the freeze-out replay in ref_surface.cpp. */
+void gvh_ref_current(CONSERVED_VARIABLES **q, PRECISION **e, FLUID_VELOCITY **u) {
+	*q = g_cur;
+	*e = g_e.data();
+	*u = g_u;
+}
+
 extern "C" {
 
 int gvh_ref_nq(void) { return NQ; }
