@@ -237,6 +237,7 @@ int grow_pinned(T **buf, long long *cap, long long need) {
 
 struct gvh_surface {
   gvh_handle *h;
+  int device;        // the handle's device, kept so that destroying needs no handle
   Geometry g;
   double iso;
   int dim, nthreads;
@@ -272,6 +273,7 @@ int gvh_surface_create(gvh_handle *h, double e_freezeout, gvh_surface **out) {
   SF_CUDA(cudaSetDevice(h->device));
   gvh_surface *s = new gvh_surface();
   s->h = h;
+  s->device = h->device;
   s->iso = e_freezeout;
   s->dim = h->nz > 1 ? 4 : 3;
   Geometry &g = s->g;
@@ -313,8 +315,9 @@ int gvh_surface_create(gvh_handle *h, double e_freezeout, gvh_surface **out) {
 
 int gvh_surface_destroy(gvh_surface *s) {
   if (!s) return GVH_OK;
-  cudaSetDevice(s->h->device);
-  cudaStreamSynchronize(s->h->stream);
+  // touches nothing of the handle, which may be gone already; cudaFree waits for the
+  // device work that uses the buffers
+  cudaSetDevice(s->device);
   cudaFree(s->dev);
   cudaFreeHost(s->h_totals);
   if (s->h_cube_key) cudaFreeHost(s->h_cube_key);

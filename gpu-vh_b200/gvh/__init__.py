@@ -9,6 +9,7 @@ the library is missing this module raises instead of computing anything itself.
 from __future__ import annotations
 
 import ctypes
+import weakref
 import os
 
 import numpy as np
@@ -155,6 +156,10 @@ class Lattice:
         assert self._L.gvh_num_lattice_cells(h) == self.ng
 
     def close(self):
+        for dep in list(getattr(self, "_dependents", [])):  # surfaces bound to this lattice
+            d = dep()
+            if d is not None:
+                d.close()
         if getattr(self, "_h", None):
             self._L.gvh_destroy(self._h)
             self._h = None
@@ -452,6 +457,9 @@ class Surface:
         if rc != 0:
             raise GvhError(f"gvh_surface_create failed ({rc}): {self._L.gvh_surface_last_error().decode()}")
         self._h = h
+        if not hasattr(lattice, "_dependents"):
+            lattice._dependents = []
+        lattice._dependents.append(weakref.ref(self))
         if threads:
             self._L.gvh_surface_set_threads(h, int(threads))
 

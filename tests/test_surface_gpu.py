@@ -44,7 +44,7 @@ def test_same_states_same_surface_text(case, tmp_path):
     lat = CASES[case]
     t0, dt, iters = 0.5, lat["dt"], 31
     R = oracle.RefLattice(**lat)
-    R.set_primitive(rich_state(R, seed=4, e0=25.0, emin=0.3))
+    R.set_primitive(rich_state(R, seed=4, e0=25.0, emin=0.3, spacing=0.6))
     efo = e_freezeout(R)
     ref_path = tmp_path / "ref_surface.dat"
     R.surface_begin(t0, efo, ref_path)
@@ -77,7 +77,7 @@ def test_same_states_same_surface_text(case, tmp_path):
 def test_device_marking_counts():
     lat = CASES["qcd_bulk_3d"]
     R = oracle.RefLattice(**lat)
-    R.set_primitive(rich_state(R, seed=4, e0=25.0, emin=0.3))
+    R.set_primitive(rich_state(R, seed=4, e0=25.0, emin=0.3, spacing=0.6))
     efo = e_freezeout(R)
     G = gvh.Lattice(**lat)
     G.set_state(R.get_state())
@@ -134,7 +134,7 @@ def test_gvh_run_surface_matches_reference_run(tmp_path):
     open(cfg / "hydro.properties", "w").write("tau0=0.5\netas=0.2\nTfo=0.150\ninitPi=0\n")
     open(cfg / "ic.properties", "w").write("type=10\n")
     R = oracle.RefLattice(**lat)
-    prim = rich_state(R, seed=9, e0=25.0, emin=0.3)
+    prim = rich_state(R, seed=9, e0=25.0, emin=0.3, spacing=0.6)
     for k in prim:
         prim[k] = np.asarray(prim[k], np.float32).astype(np.float64)
     names = ["e", "ut", "ux", "uy", "un", "pitt", "pitx", "pity", "pitn", "pixx", "pixy", "pixn", "piyy", "piyn",
