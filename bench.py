@@ -50,6 +50,9 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-surface", dest="surface", action="store_false",
+                    help="skip the freeze-out surface extras (event to freeze-out with surface.dat, "
+                         "mixed-vs-FP64 report)")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the mixed-precision, event-to-freeze-out and serving measurements")
     ap.add_argument("--serving-seconds", type=float, default=45.0)
@@ -262,24 +265,39 @@ def time_steps(L, w, steps, warmup, stream):
     return e0.elapsed_time(e1) / steps
 
 
-def event_to_freezeout(w, prim, precision, device, max_steps=6000):
+def event_to_freezeout(w, prim, precision, device, max_steps=6000, surface_path=None):
     """One event on the single-lattice path, run the way the reference's loop runs it:
     before every step test max e against e(T_fo) (device reduction), stop after 11 all-frozen
-    checks (HydroPlugin.cpp:396-413). Returns steps, seconds, status."""
+    checks (HydroPlugin.cpp:396-413). With surface_path, the freeze-out surface of every slab
+    is found (device marking, host cornelius) and written in the reference's chunks of 10
+    steps, as gvh_run does. Returns steps, seconds, status (and the surface's figures)."""
     import gvh
 
     L = gvh.Lattice(device=device, precision=precision, **w.lattice_kwargs())
     L.set_primitive(prim)
-    # e(T_fo) of the QCD fit from a one-cell batch (the library computes it)
-    B = gvh.Batch(1 << 22, precision=precision, device=device)
-    eid = B.add_event(1, 1, 1, w.dx, w.dy, w.dz, w.dtau, w.etabar, {"e": np.ones(125)}, tau0=w.tau0,
-                      T_fo_GeV=w.T_fo_GeV)
-    e_fo = B.info(eid).freezeout_energy_density
-    B.close()
+    e_fo = gvh.energy_density_of_temperature(w.T_fo_GeV, conformal=w.conformal)
+    S, f, chunk = None, None, []
+    if surface_path:
+        S = gvh.Surface(L, e_fo)
+        S.set_lower()
+        f = open(surface_path, "w")
     L.synchronize()
     t0 = time.perf_counter()
     frozen, n, t = 0, 0, w.tau0
+    rows = 0
+    per_slab = []
     while n < max_steps:
+        it = n + 1  # loop iteration of the reference; the state is level n
+        if S is not None and it >= 2:
+            label, scale, flush = gvh.slab_labels(it - 2, w.tau0, w.dtau)
+            S.find(label, scale)
+            chunk.append(S.text())
+            per_slab.append(S.info()["hypercubes_last"])
+            if flush == it:
+                text = "".join(chunk)
+                f.write(text)
+                rows += text.count("\n")
+                chunk = []
         if L.max_energy_density() <= e_fo:
             frozen += 1
         if frozen >= 11:
@@ -290,8 +308,105 @@ def event_to_freezeout(w, prim, precision, device, max_steps=6000):
     L.synchronize()
     el = time.perf_counter() - t0
     st = L.status()
+    out = {"steps": n, "seconds": el, "frozen_out": frozen >= 11, "status": st, "tau_end": t}
+    if S is not None:
+        f.close()
+        inf = S.info()
+        ng = (w.nx + 4) * (w.ny + 4) * (w.nz + 4)
+        out["surface"] = {
+            "elements_written": rows,
+            "hypercubes_crossed_per_slab_mean": float(np.mean(per_slab)) if per_slab else 0.0,
+            "hypercubes_crossed_per_slab_max": int(np.max(per_slab)) if per_slab else 0,
+            "device_seconds": inf["device_seconds_total"],
+            "host_seconds": inf["host_seconds_total"],
+            "bytes_to_host_per_step": inf["bytes_to_host_total"] / max(1, inf["slabs"]),
+            # copyDeviceToHostMemory: 30 ghosted arrays every step (HydroPlugin.cpp:264,
+            # DynamicalVariables.cu copyDeviceToHostMemory)
+            "reference_bytes_to_host_per_step": 30 * ng * 8,
+            "host_threads": os.cpu_count(),
+        }
+        S.close()
     L.close()
-    return {"steps": n, "seconds": el, "frozen_out": frozen >= 11, "status": st, "tau_end": t}
+    return out
+
+
+def precision_report(device):
+    """Mixed precision against FP64 on the config-1 event (33x33x17, conformal, shear): the
+    L2 and Linf relative errors of e, u^mu and pi^{mu nu}/(e+p) at steps 100, 500 and at
+    freeze-out, and the total freeze-out sum of tau*dsigma_mu (surface.dat columns 5-8) of each
+    run. The FP64 path is the reference's FP64 build to 1e-12 (tests/test_parity_gpu.py)."""
+    import gvh
+
+    w = workloads.CONFIG1
+    prim = workloads.gaussian_profile(w)
+    e_fo = gvh.energy_density_of_temperature(w.T_fo_GeV, conformal=w.conformal)
+    runs = {}
+    for prec in ("fp64", "mixed"):
+        L = gvh.Lattice(device=device, precision=prec, **w.lattice_kwargs())
+        L.set_primitive(prim)
+        S = gvh.Surface(L, e_fo)
+        S.set_lower()
+        runs[prec] = {"L": L, "S": S, "dsigma": np.zeros(4), "frozen": 0, "done": False, "steps": 0}
+    snaps = {}
+    t, n = w.tau0, 0
+    pin = ["pixx", "pixy", "pixn", "piyy", "piyn", "pitt", "pitx", "pity", "pitn", "pinn"]
+
+    def snapshot(tag):
+        snaps[tag] = {}
+        for prec, r in runs.items():
+            st = r["L"].get_state()
+            g = {k: r["L"].interior(st[k]) for k in ["e", "p", "ut", "ux", "uy", "un"] + pin}
+            snaps[tag][prec] = g
+
+    while n < 3000 and not all(r["done"] for r in runs.values()):
+        it = n + 1
+        for r in runs.values():
+            if r["done"]:
+                continue
+            if it >= 2:
+                label, scale, flush = gvh.slab_labels(it - 2, w.tau0, w.dtau)
+                r["S"].find(label, scale)
+                rows = r["S"].rows()
+                r.setdefault("pending", []).append(rows[:, 4:8].sum(axis=0) if len(rows) else np.zeros(4))
+                if flush == it:
+                    r["dsigma"] += np.sum(r["pending"], axis=0)
+                    r["pending"] = []
+            if r["L"].max_energy_density() <= e_fo:
+                r["frozen"] += 1
+            if r["frozen"] >= 11:
+                r["done"], r["steps"] = True, n
+        if n in (100, 500):
+            snapshot(f"step_{n}")
+        if runs["fp64"]["done"] and "freezeout" not in snaps:
+            snapshot("freezeout")
+        for r in runs.values():
+            if not r["done"]:
+                r["L"].step(t, w.dtau)
+        n += 1
+        t = w.tau0 + n * w.dtau
+
+    def errs(a, b):
+        d = (a - b).ravel()
+        return {"l2": float(np.linalg.norm(d) / max(np.linalg.norm(b.ravel()), 1e-300)),
+                "linf": float(np.max(np.abs(d)) / max(np.max(np.abs(b)), 1e-300))}
+
+    report = {"workload": w.name, "fp64_freezeout_step": runs["fp64"]["steps"],
+              "mixed_freezeout_step": runs["mixed"]["steps"]}
+    for tag, sn in snaps.items():
+        a, b = sn["mixed"], sn["fp64"]
+        u_a = np.stack([a[k] for k in ("ut", "ux", "uy", "un")])
+        u_b = np.stack([b[k] for k in ("ut", "ux", "uy", "un")])
+        pa = np.stack([a[k] / (a["e"] + a["p"]) for k in pin])
+        pb = np.stack([b[k] / (b["e"] + b["p"]) for k in pin])
+        report[tag] = {"e": errs(a["e"], b["e"]), "u": errs(u_a, u_b), "pi_over_e_plus_p": errs(pa, pb)}
+    d64, dmx = runs["fp64"]["dsigma"], runs["mixed"]["dsigma"]
+    report["total_dsigma_fp64"] = d64.tolist()
+    report["total_dsigma_mixed"] = dmx.tolist()
+    report["total_dsigma_rel_err"] = float(np.max(np.abs(dmx - d64)) / max(np.max(np.abs(d64)), 1e-300))
+    for r in runs.values():
+        r["S"].close()
+        r["L"].close()
+    return report
 
 
 def serving_run(args, device):
@@ -430,6 +545,14 @@ def run_ours(args):
         ev = event_to_freezeout(w, prim, "fp64", local)
         ev["events_per_hour"] = 3600.0 / ev["seconds"] if ev["seconds"] > 0 else None
         extras["fp64_single_event_to_freezeout"] = ev
+        if args.surface:
+            import tempfile
+
+            with tempfile.TemporaryDirectory() as td:
+                evs = event_to_freezeout(w, prim, "fp64", local, surface_path=os.path.join(td, "surface.dat"))
+            evs["events_per_hour"] = 3600.0 / evs["seconds"] if evs["seconds"] > 0 else None
+            extras["fp64_single_event_to_freezeout_with_surface"] = evs
+            extras["mixed_vs_fp64_config1"] = precision_report(local)
         if args.serving_seconds > 0:
             # the plain FP64 single-event path on the serving mix: one event of each grid of
             # the mix run alone to freeze-out; the mix draws the grids uniformly

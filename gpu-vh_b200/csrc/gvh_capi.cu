@@ -330,6 +330,11 @@ int gvh_max_energy_density(gvh_handle *h, double *out) {
   return GVH_OK;
 }
 
+double gvh_energy_density_of_temperature(int eos, double T_GeV) {
+  const double T = T_GeV / 0.197326938;  // hbarc, HydroPlugin.cpp:132
+  return eos == GVH_EOS_CONFORMAL ? energy_density_of_T<EOS_CONFORMAL>(T) : energy_density_of_T<EOS_QCD>(T);
+}
+
 int gvh_synchronize(gvh_handle *h) {
   if (!h) return fail(GVH_ERR_INVALID, "null handle");
   GVH_CUDA(cudaSetDevice(h->device));

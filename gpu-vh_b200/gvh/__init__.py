@@ -437,6 +437,14 @@ def _bind_surface(L):
     return L
 
 
+def energy_density_of_temperature(T_GeV, conformal=False) -> float:
+    """e(T) of the library's EoS in fm^-4 (the freeze-out threshold e(T_fo))."""
+    L = load()
+    L.gvh_energy_density_of_temperature.argtypes = [ctypes.c_int, ctypes.c_double]
+    L.gvh_energy_density_of_temperature.restype = ctypes.c_double
+    return float(L.gvh_energy_density_of_temperature(GVH_EOS_CONFORMAL if conformal else GVH_EOS_QCD, T_GeV))
+
+
 def slab_labels(k, tau0, dtau):
     """(tau_label, tau_scale, flush_iteration) the reference gives the slab (k, k+1)."""
     L = _bind_surface(load())

@@ -160,6 +160,10 @@ const char *gvh_noalloc_last_error(void);
  * the lattice to the host. Synchronises the handle's stream. */
 int gvh_max_energy_density(gvh_handle *h, double *out);
 
+/* e(T) of the equation of state (equilibriumEnergyDensity, EquationOfState.cu:150-204) at
+ * T = T_GeV / hbarc, in fm^-4: the freeze-out threshold of HydroPlugin.cpp:131-135. */
+double gvh_energy_density_of_temperature(int eos, double T_GeV);
+
 /* Runs the handle's work on a caller-owned stream (a cudaStream_t passed as void*); NULL
  * returns to the handle's own stream. Waits for work already queued on the old stream. */
 int gvh_set_stream(gvh_handle *h, void *stream);
