@@ -265,39 +265,42 @@ def time_steps(L, w, steps, warmup, stream):
     return e0.elapsed_time(e1) / steps
 
 
-def event_to_freezeout(w, prim, precision, device, max_steps=6000, surface_path=None):
+def event_to_freezeout(w, prim, precision, device, max_steps=6000, surface_dir=None):
     """One event on the single-lattice path, run the way the reference's loop runs it:
     before every step test max e against e(T_fo) (device reduction), stop after 11 all-frozen
-    checks (HydroPlugin.cpp:396-413). With surface_path, the freeze-out surface of every slab
-    is found (device marking, host cornelius) and written in the reference's chunks of 10
-    steps, as gvh_run does. Returns steps, seconds, status (and the surface's figures)."""
+    checks (HydroPlugin.cpp:396-413). With surface_dir, the library's own run loop
+    (gvh_run_loop) also finds the freeze-out surface of every slab (device marking, host
+    cornelius) and writes surface.dat there in the reference's chunks of 10 steps.
+    Returns steps, seconds, status (and the surface's figures)."""
     import gvh
 
-    L = gvh.Lattice(device=device, precision=precision, **w.lattice_kwargs())
+    L = gvh.Lattice(device=device, precision=precision, tau0=w.tau0, T_fo_GeV=w.T_fo_GeV, **w.lattice_kwargs())
     L.set_primitive(prim)
-    e_fo = gvh.energy_density_of_temperature(w.T_fo_GeV, conformal=w.conformal)
-    S, f, chunk = None, None, []
-    if surface_path:
-        S = gvh.Surface(L, e_fo)
-        S.set_lower()
-        f = open(surface_path, "w")
     L.synchronize()
+    if surface_dir:
+        t0 = time.perf_counter()
+        rep = L.run_loop(max_steps, output_dir=surface_dir, surface=True)
+        el = time.perf_counter() - t0
+        ng = (w.nx + 4) * (w.ny + 4) * (w.nz + 4)
+        slabs = max(1, rep["steps"])
+        out = {"steps": rep["steps"], "seconds": el, "frozen_out": bool(rep["frozen_out"]), "status": rep["status"],
+               "tau_end": rep["tau_end"],
+               "surface": {"elements_written": rep["surface_elements"],
+                           "hypercubes_crossed_per_slab_mean": rep["surface_hypercubes"] / slabs,
+                           "finder_seconds": rep["surface_seconds"],
+                           "host_cornelius_seconds": rep["surface_host_seconds"],
+                           "bytes_to_host_per_step": rep["surface_bytes_to_host"] / slabs,
+                           # copyDeviceToHostMemory: 30 ghosted arrays every step
+                           # (HydroPlugin.cpp:264, DynamicalVariables.cu)
+                           "reference_bytes_to_host_per_step": 30 * ng * 8,
+                           "file_bytes": os.path.getsize(os.path.join(surface_dir, "surface.dat")),
+                           "host_threads": os.cpu_count()}}
+        L.close()
+        return out
+    e_fo = gvh.energy_density_of_temperature(w.T_fo_GeV, conformal=w.conformal)
     t0 = time.perf_counter()
     frozen, n, t = 0, 0, w.tau0
-    rows = 0
-    per_slab = []
     while n < max_steps:
-        it = n + 1  # loop iteration of the reference; the state is level n
-        if S is not None and it >= 2:
-            label, scale, flush = gvh.slab_labels(it - 2, w.tau0, w.dtau)
-            S.find(label, scale)
-            chunk.append(S.text())
-            per_slab.append(S.info()["hypercubes_last"])
-            if flush == it:
-                text = "".join(chunk)
-                f.write(text)
-                rows += text.count("\n")
-                chunk = []
         if L.max_energy_density() <= e_fo:
             frozen += 1
         if frozen >= 11:
@@ -308,26 +311,8 @@ def event_to_freezeout(w, prim, precision, device, max_steps=6000, surface_path=
     L.synchronize()
     el = time.perf_counter() - t0
     st = L.status()
-    out = {"steps": n, "seconds": el, "frozen_out": frozen >= 11, "status": st, "tau_end": t}
-    if S is not None:
-        f.close()
-        inf = S.info()
-        ng = (w.nx + 4) * (w.ny + 4) * (w.nz + 4)
-        out["surface"] = {
-            "elements_written": rows,
-            "hypercubes_crossed_per_slab_mean": float(np.mean(per_slab)) if per_slab else 0.0,
-            "hypercubes_crossed_per_slab_max": int(np.max(per_slab)) if per_slab else 0,
-            "device_seconds": inf["device_seconds_total"],
-            "host_seconds": inf["host_seconds_total"],
-            "bytes_to_host_per_step": inf["bytes_to_host_total"] / max(1, inf["slabs"]),
-            # copyDeviceToHostMemory: 30 ghosted arrays every step (HydroPlugin.cpp:264,
-            # DynamicalVariables.cu copyDeviceToHostMemory)
-            "reference_bytes_to_host_per_step": 30 * ng * 8,
-            "host_threads": os.cpu_count(),
-        }
-        S.close()
     L.close()
-    return out
+    return {"steps": n, "seconds": el, "frozen_out": frozen >= 11, "status": st, "tau_end": t}
 
 
 def precision_report(device):
@@ -549,7 +534,7 @@ def run_ours(args):
             import tempfile
 
             with tempfile.TemporaryDirectory() as td:
-                evs = event_to_freezeout(w, prim, "fp64", local, surface_path=os.path.join(td, "surface.dat"))
+                evs = event_to_freezeout(w, prim, "fp64", local, surface_dir=td)
             evs["events_per_hour"] = 3600.0 / evs["seconds"] if evs["seconds"] > 0 else None
             extras["fp64_single_event_to_freezeout_with_surface"] = evs
             extras["mixed_vs_fp64_config1"] = precision_report(local)

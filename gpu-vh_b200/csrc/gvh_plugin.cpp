@@ -28,6 +28,8 @@
 #include <vector>
 
 #include "../../include/gvh.h"
+#include "gvh_handle.h"
+#include "gvh_surface_internal.h"
 
 namespace {
 
@@ -203,8 +205,6 @@ void gvh_surface_slab_labels(long long k, double tau0, double dtau, double *tau_
 int gvh_run(const gvh_lattice_params *L, const gvh_ic_params *ic, const gvh_hydro_params *H, const char *root_dir,
             const char *output_dir, const gvh_options *opts, int outputs, gvh_run_report *report) {
   g_plugin_error.clear();
-  const bool dump_fields = (outputs & GVH_RUN_FIELDS) != 0;
-  const bool want_surface = (outputs & GVH_RUN_SURFACE) != 0 && output_dir;
   if (!L || !ic || !H || !root_dir) return pfail(GVH_ERR_INVALID, "null argument");
   if (ic->initialConditionType != 10)
     return pfail(GVH_ERR_INVALID, "gvh_run reads initial-condition type 10 (input/*.dat files); type " +
@@ -230,52 +230,46 @@ int gvh_run(const gvh_lattice_params *L, const gvh_ic_params *ic, const gvh_hydr
   }
   prim.clear();
 
+  rc = gvh_run_loop(h, L, H, output_dir, outputs, report);
+  gvh_destroy(h);
+  return rc;
+}
+
+int gvh_run_loop(gvh_handle *h, const gvh_lattice_params *L, const gvh_hydro_params *H, const char *output_dir,
+                 int outputs, gvh_run_report *report) {
+  if (!h || !L || !H) return pfail(GVH_ERR_INVALID, "gvh_run_loop: null argument");
+  if (L->numLatticePointsX != h->nx || L->numLatticePointsY != h->ny || L->numLatticePointsRapidity != h->nz)
+    return pfail(GVH_ERR_INVALID, "gvh_run_loop: lattice parameters do not match the handle");
+  g_plugin_error.clear();
+  const bool dump_fields = (outputs & GVH_RUN_FIELDS) != 0 && output_dir;
+  const bool want_surface = (outputs & GVH_RUN_SURFACE) != 0 && output_dir;
+  const int nx = L->numLatticePointsX, ny = L->numLatticePointsY, nz = L->numLatticePointsRapidity;
+  const long long ng = (long long)(nx + 4) * (ny + 4) * (nz + 4);
+  int rc = GVH_OK;
   const double t0 = H->initialProperTimePoint, dt = L->latticeSpacingProperTime;
   const double T_reg = H->regulationTemperatureGeV / kHbarc;
-  // e(T_fo) through a one-cell batch so the EoS is the library's (HydroPlugin.cpp:133-135)
-  double e_fo = 0.0;
-  {
-    gvh_batch *b = nullptr;
-    gvh_options ob = o;
-    ob.precision = GVH_PRECISION_FP64;
-    gvh_lattice_params one = *L;
-    one.numLatticePointsX = one.numLatticePointsY = one.numLatticePointsRapidity = 1;
-    std::vector<double> e1(125, 1.0), z1(125, 0.0);
-    std::vector<const double *> p1(n_prim, z1.data());
-    p1[0] = e1.data();
-    p1[1] = e1.data();
-    int id = -1;
-    gvh_event_info inf;
-    if (gvh_batch_create(&ob, 1 << 20, &b) || gvh_batch_add_event(b, &one, H, p1.data(), n_prim, &id) ||
-        gvh_batch_event_info(b, id, &inf)) {
-      gvh_batch_destroy(b);
-      gvh_destroy(h);
-      return pfail(GVH_ERR_CUDA, std::string("freeze-out threshold: ") + gvh_batch_last_error());
-    }
-    e_fo = inf.freezeout_energy_density;
-    gvh_batch_destroy(b);
-  }
+  // e(T_fo), HydroPlugin.cpp:131-135
+  const double e_fo = gvh_energy_density_of_temperature(h->eos, H->freezeoutTemperatureGeV);
 
   // freeze-out surface (HydroPlugin.cpp:155-211 set-up, 255-393 per iteration)
   gvh_surface *surf = nullptr;
   FILE *surf_file = nullptr;
-  std::string chunk_text;
+  std::vector<std::string> chunk_text;
   long long surf_rows = 0, chunk_rows = 0;
   double surf_seconds = 0.0;
   if (want_surface) {
     const std::string path = std::string(output_dir) + "/surface.dat";
     surf_file = fopen(path.c_str(), "w");
     if (!surf_file) {
-      gvh_destroy(h);
       return pfail(GVH_ERR_INVALID, "cannot open " + path);
     }
     // the reference's finder handles 3+1D and 2+1D lattices only (HydroPlugin.cpp:157-182)
     if (L->numLatticePointsX > 1 && L->numLatticePointsY > 1) {
-      if ((rc = gvh_surface_create(h, e_fo, &surf)) || (rc = gvh_surface_set_lower(surf))) {
+      if ((rc = gvh_surface_create(h, e_fo, &surf)) || (rc = gvh_surface_set_outputs(surf, GVH_SURFACE_TEXT)) ||
+          (rc = gvh_surface_set_lower(surf))) {
         std::string msg = gvh_surface_last_error();
         gvh_surface_destroy(surf);
         fclose(surf_file);
-        gvh_destroy(h);
         return pfail(rc, msg);
       }
     }
@@ -319,13 +313,13 @@ int gvh_run(const gvh_lattice_params *L, const gvh_ic_params *ic, const gvh_hydr
         g_plugin_error = gvh_surface_last_error();
         break;
       }
-      const char *txt = nullptr;
-      long long len = 0;
-      gvh_surface_get_text(surf, &txt, &len);
-      chunk_text.append(txt, (size_t)len);
+      gvh::surface::take_text(surf, chunk_text);
       chunk_rows += nel;
       if (flush == n) {
-        if (fwrite(chunk_text.data(), 1, chunk_text.size(), surf_file) != chunk_text.size()) {
+        bool ok = true;
+        for (const std::string &part : chunk_text)
+          ok = ok && fwrite(part.data(), 1, part.size(), surf_file) == part.size();
+        if (!ok) {
           rc = GVH_ERR_INVALID;
           g_plugin_error = "writing surface.dat failed";
           break;
@@ -360,10 +354,15 @@ int gvh_run(const gvh_lattice_params *L, const gvh_ic_params *ic, const gvh_hydr
     report->freezeout_energy_density = e_fo;
     report->surface_elements = surf_rows;
     report->surface_seconds = surf_seconds;
+    gvh_surface_info si;
+    memset(&si, 0, sizeof si);
+    if (surf) gvh_surface_get_info(surf, &si);
+    report->surface_hypercubes = si.hypercubes_total;
+    report->surface_bytes_to_host = si.bytes_to_host_total;
+    report->surface_host_seconds = si.host_seconds_total;
   }
   gvh_surface_destroy(surf);
   if (surf_file) fclose(surf_file);
-  gvh_destroy(h);
   if (rc) return pfail(rc, g_plugin_error.empty() ? gvh_last_error() : g_plugin_error);
   return GVH_OK;
 }

@@ -26,6 +26,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <memory>
 #include <string>
 #include <thread>
 #include <vector>
@@ -254,6 +255,8 @@ struct gvh_surface {
   double *h_point_vals;
   long long cap_cubes, cap_points, cap_vals;
   std::vector<int> c2p;
+  std::unique_ptr<gvh::surface::Pool> pool;
+  int outputs;       // gvh::surface::OUT_ROWS | OUT_TEXT
   gvh::surface::Result last;
   gvh_surface_info info;
 };
@@ -284,7 +287,8 @@ int gvh_surface_create(gvh_handle *h, double e_freezeout, gvh_surface **out) {
   g.ncubes = (long long)(g.nx - 1) * (g.ny - 1) * g.nzc;
   s->nbc = (int)((g.ncubes + kFoThreads - 1) / kFoThreads);
   s->nbp = (int)((g.ncells + kFoThreads - 1) / kFoThreads);
-  s->nthreads = (int)std::min(32u, std::max(1u, std::thread::hardware_concurrency()));
+  s->nthreads = (int)std::min(64u, std::max(1u, std::thread::hardware_concurrency()));
+  s->outputs = gvh::surface::OUT_ROWS | gvh::surface::OUT_TEXT;
   const long long n = g.ncells;
   auto al = [](long long b) { return (b + 255) / 256 * 256; };
   const long long bytes = 2 * al(kVars * n * 8) + al(g.ncubes) + al(n) + al(4 * (s->nbc + s->nbp + 2)) +
@@ -330,6 +334,15 @@ int gvh_surface_destroy(gvh_surface *s) {
 int gvh_surface_set_threads(gvh_surface *s, int nthreads) {
   if (!s || nthreads < 1) return sfail(GVH_ERR_INVALID, "gvh_surface_set_threads: bad argument");
   s->nthreads = nthreads;
+  s->pool.reset();
+  return GVH_OK;
+}
+
+int gvh_surface_set_outputs(gvh_surface *s, int outputs) {
+  if (!s || (outputs & ~(GVH_SURFACE_ROWS | GVH_SURFACE_TEXT)))
+    return sfail(GVH_ERR_INVALID, "gvh_surface_set_outputs: bad argument");
+  s->outputs = (outputs & GVH_SURFACE_ROWS ? gvh::surface::OUT_ROWS : 0) |
+               (outputs & GVH_SURFACE_TEXT ? gvh::surface::OUT_TEXT : 0);
   return GVH_OK;
 }
 
@@ -397,7 +410,9 @@ int gvh_surface_find(gvh_surface *s, double tau_label, double tau_scale, long lo
   slab.npoints = npoints;
   slab.point_cell = s->h_point_cell;
   slab.point_vals = s->h_point_vals;
-  gvh::surface::process_slab(slab, gvh::surface::Labels{tau_label, tau_scale}, s->nthreads, true, s->c2p, s->last);
+  if (!s->pool) s->pool.reset(new gvh::surface::Pool(s->nthreads));
+  gvh::surface::process_slab(slab, gvh::surface::Labels{tau_label, tau_scale}, *s->pool, s->outputs, s->c2p,
+                             s->last);
   const auto t2 = std::chrono::steady_clock::now();
   s->lower = upper;
   gvh_surface_info &in = s->info;
@@ -419,14 +434,20 @@ int gvh_surface_get_rows(gvh_surface *s, double *rows, long long max_rows) {
   if (!s || (!rows && max_rows > 0)) return sfail(GVH_ERR_INVALID, "gvh_surface_get_rows: bad argument");
   if (max_rows < s->last.elements)
     return sfail(GVH_ERR_INVALID, "gvh_surface_get_rows: %lld rows do not fit in %lld", s->last.elements, max_rows);
-  if (s->last.elements) memcpy(rows, s->last.rows.data(), s->last.rows.size() * sizeof(double));
+  if (s->last.elements && !(s->outputs & gvh::surface::OUT_ROWS))
+    return sfail(GVH_ERR_INVALID, "gvh_surface_get_rows: rows are not kept (gvh_surface_set_outputs)");
+  for (auto &p : s->last.parts) {
+    if (!p.rows.empty()) memcpy(rows, p.rows.data(), p.rows.size() * sizeof(double));
+    rows += p.rows.size();
+  }
   return GVH_OK;
 }
 
 int gvh_surface_get_text(gvh_surface *s, const char **text, long long *length) {
   if (!s || !text || !length) return sfail(GVH_ERR_INVALID, "gvh_surface_get_text: null argument");
-  *text = s->last.text.c_str();
-  *length = (long long)s->last.text.size();
+  const std::string &t = s->last.text();
+  *text = t.c_str();
+  *length = (long long)t.size();
   return GVH_OK;
 }
 
@@ -437,3 +458,16 @@ int gvh_surface_get_info(const gvh_surface *s, gvh_surface_info *info) {
 }
 
 }  // extern "C"
+
+namespace gvh {
+namespace surface {
+void take_text(gvh_surface *s, std::vector<std::string> &out) {
+  for (auto &p : s->last.parts) {
+    out.emplace_back(std::move(p.text));
+    p.text.clear();
+  }
+  s->last.joined.clear();
+  s->last.joined_valid = false;
+}
+}  // namespace surface
+}  // namespace gvh

@@ -7,6 +7,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <charconv>
 #include <thread>
 
 #include "../../include/gvh.h"
@@ -78,22 +79,28 @@ double interp3(double x0, double x1, double x2, const double a[2][2][2][2]) {
          (y0 * x1 * x2 * a[0][1][1][0]) + (x0 * x1 * x2 * a[1][1][1][0]);
 }
 
+// One row as the reference's ofstream writes it: default format (%g, 6 significant digits),
+// values separated by spaces, a newline after the last. std::to_chars with the general
+// format and precision 6 gives the same characters as printf's %g.
 void append_row_text(std::string &out, const double *row) {
-  char buf[20 * 32];
-  int n = 0;
-  for (int c = 0; c < kColumns; ++c)
-    n += snprintf(buf + n, sizeof buf - n, c + 1 < kColumns ? "%g " : "%g\n", row[c]);
-  out.append(buf, n);
+  char buf[kColumns * 32];
+  char *p = buf;
+  for (int c = 0; c < kColumns; ++c) {
+    p = std::to_chars(p, buf + sizeof buf, row[c], std::chars_format::general, 6).ptr;
+    *p++ = c + 1 < kColumns ? ' ' : '\n';
+  }
+  out.append(buf, p - buf);
 }
 
-struct Part {
-  std::vector<double> rows;
-  std::string text;
-  long long elements = 0, errors = 0;
-};
-
-void process_range(const Slab &s, const Labels &lab, bool want_text, const std::vector<int> &c2p, long long c0,
+void process_range(const Slab &s, const Labels &lab, int outputs, const std::vector<int> &c2p, long long c0,
                    long long c1, Part &part) {
+  const bool want_rows = outputs & OUT_ROWS, want_text = outputs & OUT_TEXT;
+  part.rows.clear();
+  part.text.clear();
+  part.elements = part.errors = 0;
+  const size_t expect = (size_t)((c1 - c0) * 5 / 4 + 8);  // about one element per hypercube
+  if (want_rows) part.rows.reserve(expect * kColumns);
+  if (want_text) part.text.reserve(expect * 240);
   const int nzc = s.dim == 4 ? s.nz - 1 : 1;
   const double dx4[4] = {s.dt, s.dx, s.dy, s.dim == 4 ? s.dz : 1.0};
   // cornelius is set up with the spacings of the dimensions in use (HydroPlugin.cpp:155-182);
@@ -172,7 +179,7 @@ void process_range(const Slab &s, const Labels &lab, bool want_text, const std::
       row[12] = eos_temperature(s.eos, val[3]);
       row[13] = eos_pressure(s.eos, val[3]);
       for (int q = 4; q < kVars; ++q) row[10 + q] = val[q];
-      part.rows.insert(part.rows.end(), row, row + kColumns);
+      if (want_rows) part.rows.insert(part.rows.end(), row, row + kColumns);
       if (want_text) append_row_text(part.text, row);
       ++part.elements;
     }
@@ -181,39 +188,77 @@ void process_range(const Slab &s, const Labels &lab, bool want_text, const std::
 
 }  // namespace
 
-void process_slab(const Slab &s, const Labels &lab, int nthreads, bool want_text, std::vector<int> &c2p,
-                  Result &out) {
-  out.rows.clear();
-  out.text.clear();
+Pool::Pool(int nthreads) {
+  for (int i = 1; i < nthreads; ++i) workers_.emplace_back([this] { loop(); });
+}
+
+Pool::~Pool() {
+  {
+    std::lock_guard<std::mutex> lock(mu_);
+    stop_ = true;
+  }
+  wake_.notify_all();
+  for (auto &t : workers_) t.join();
+}
+
+void Pool::loop() {
+  long long seen = 0;
+  std::unique_lock<std::mutex> lock(mu_);
+  for (;;) {
+    wake_.wait(lock, [&] { return stop_ || generation_ != seen; });
+    if (stop_) return;
+    seen = generation_;
+    while (next_ < njobs_) {
+      const int i = next_++;
+      const std::function<void(int)> *f = job_;
+      lock.unlock();
+      (*f)(i);
+      lock.lock();
+      if (--pending_ == 0) done_.notify_all();
+    }
+  }
+}
+
+void Pool::run(int n, const std::function<void(int)> &f) {
+  if (n <= 0) return;
+  std::unique_lock<std::mutex> lock(mu_);
+  job_ = &f;
+  njobs_ = n;
+  next_ = 0;
+  pending_ = n;
+  ++generation_;
+  wake_.notify_all();
+  while (next_ < njobs_) {  // the calling thread works too
+    const int i = next_++;
+    lock.unlock();
+    f(i);
+    lock.lock();
+    --pending_;
+  }
+  done_.wait(lock, [&] { return pending_ == 0; });
+  job_ = nullptr;
+}
+
+void process_slab(const Slab &s, const Labels &lab, Pool &pool, int outputs, std::vector<int> &c2p, Result &out) {
   out.elements = 0;
   out.errors = 0;
-  if (s.ncubes == 0) return;
+  out.joined_valid = false;
+  if (s.ncubes == 0) {
+    out.parts.clear();
+    return;
+  }
   const size_t ncells = (size_t)s.nx * s.ny * s.nz;
   if (c2p.size() < ncells) c2p.assign(ncells, 0);
   for (long long p = 0; p < s.npoints; ++p) c2p[s.point_cell[p]] = (int)p;
-  const long long per = 512;
-  int nt = (int)std::min<long long>(std::max(1, nthreads), (s.ncubes + per - 1) / per);
-  std::vector<Part> parts(nt);
-  if (nt == 1) {
-    process_range(s, lab, want_text, c2p, 0, s.ncubes, parts[0]);
-  } else {
-    std::vector<std::thread> pool;
-    for (int t = 0; t < nt; ++t) {
-      const long long c0 = s.ncubes * t / nt, c1 = s.ncubes * (t + 1) / nt;
-      pool.emplace_back([&, t, c0, c1] { process_range(s, lab, want_text, c2p, c0, c1, parts[t]); });
-    }
-    for (auto &th : pool) th.join();
-  }
-  size_t nrow = 0, ntext = 0;
-  for (auto &p : parts) {
-    nrow += p.rows.size();
-    ntext += p.text.size();
-  }
-  out.rows.reserve(nrow);
-  out.text.reserve(ntext);
-  for (auto &p : parts) {
-    out.rows.insert(out.rows.end(), p.rows.begin(), p.rows.end());
-    out.text += p.text;
+  // a few contiguous ranges per thread for balance; range i becomes part i, so order is kept
+  const long long min_range = 256;
+  const int nparts = (int)std::max<long long>(1, std::min<long long>(4ll * pool.size(), s.ncubes / min_range));
+  out.parts.resize(nparts);
+  pool.run(nparts, [&](int i) {
+    const long long c0 = s.ncubes * i / nparts, c1 = s.ncubes * (i + 1) / nparts;
+    process_range(s, lab, outputs, c2p, c0, c1, out.parts[i]);
+  });
+  for (auto &p : out.parts) {
     out.elements += p.elements;
     out.errors += p.errors;
   }

@@ -1,7 +1,11 @@
 // gvh_surface_internal.h -- what the device side of the freeze-out surface hands to the host.
 #pragma once
 
+#include <condition_variable>
+#include <functional>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace gvh {
@@ -32,17 +36,68 @@ struct Labels {
   double tau_scale;
 };
 
-struct Result {
+enum : int { OUT_ROWS = 1, OUT_TEXT = 2 };
+
+// One thread's share of a slab's rows, in order.
+struct Part {
   std::vector<double> rows;  // kColumns per element
   std::string text;          // the same rows formatted as the reference writes them
   long long elements = 0;
   long long errors = 0;      // hypercubes where the algorithm stops (the reference exits)
 };
 
-// Runs the surface finder on every crossed hypercube of the slab with nthreads host threads,
-// in order. cell_to_point is scratch of at least nx*ny*nz entries kept by the caller.
-void process_slab(const Slab &s, const Labels &lab, int nthreads, bool want_text, std::vector<int> &cell_to_point,
+struct Result {
+  std::vector<Part> parts;
+  long long elements = 0, errors = 0;
+  std::string joined;        // the parts' text in one piece, made on first request
+  bool joined_valid = false;
+  const std::string &text() {
+    if (!joined_valid) {
+      size_t n = 0;
+      for (auto &p : parts) n += p.text.size();
+      joined.clear();
+      joined.reserve(n);
+      for (auto &p : parts) joined += p.text;
+      joined_valid = true;
+    }
+    return joined;
+  }
+};
+
+// Persistent host worker threads: run(n, f) calls f(0..n-1) on the workers and waits.
+class Pool {
+ public:
+  explicit Pool(int nthreads);
+  ~Pool();
+  int size() const { return (int)workers_.size() + 1; }
+  void run(int n, const std::function<void(int)> &f);
+
+ private:
+  void loop();
+  std::vector<std::thread> workers_;
+  std::mutex mu_;
+  std::condition_variable wake_, done_;
+  const std::function<void(int)> *job_ = nullptr;
+  int njobs_ = 0, next_ = 0, pending_ = 0;
+  long long generation_ = 0;
+  bool stop_ = false;
+};
+
+// Runs the surface finder on every crossed hypercube of the slab on the pool, in order.
+// outputs: OUT_ROWS and/or OUT_TEXT. cell_to_point is scratch of at least nx*ny*nz entries
+// kept by the caller.
+void process_slab(const Slab &s, const Labels &lab, Pool &pool, int outputs, std::vector<int> &cell_to_point,
                   Result &out);
 
+}  // namespace surface
+}  // namespace gvh
+
+struct gvh_surface;
+
+namespace gvh {
+namespace surface {
+// Moves the last slab's text, part by part and in order, to the end of out (for writers that
+// keep a chunk of slabs before writing, as gvh_run does); the slab's text is empty afterwards.
+void take_text(gvh_surface *s, std::vector<std::string> &out);
 }  // namespace surface
 }  // namespace gvh

@@ -58,6 +58,18 @@ class HydroParams(ctypes.Structure):
                 ("regulationTemperatureGeV", ctypes.c_double)]
 
 
+class RunReport(ctypes.Structure):
+    _fields_ = [("steps", ctypes.c_longlong), ("tau_end", ctypes.c_double), ("average_ms_per_step", ctypes.c_double),
+                ("frozen_out", ctypes.c_int), ("status", ctypes.c_uint),
+                ("freezeout_energy_density", ctypes.c_double), ("surface_elements", ctypes.c_longlong),
+                ("surface_seconds", ctypes.c_double), ("surface_hypercubes", ctypes.c_longlong),
+                ("surface_bytes_to_host", ctypes.c_double), ("surface_host_seconds", ctypes.c_double)]
+
+
+GVH_RUN_FIELDS = 1
+GVH_RUN_SURFACE = 2
+
+
 class Options(ctypes.Structure):
     _fields_ = [("eos", ctypes.c_int), ("shear", ctypes.c_int), ("bulk", ctypes.c_int),
                 ("precision", ctypes.c_int), ("theta", ctypes.c_double), ("device", ctypes.c_int)]
@@ -204,6 +216,31 @@ class Lattice:
 
     def get_state_ptrs(self, ptrs):
         _check(self._L.gvh_get_state(self._h, _ptr_array(list(ptrs)), len(ptrs)), "gvh_get_state")
+
+    def run_loop(self, nt, output_dir=None, fields=False, surface=True, tau0=None, T_fo_GeV=None,
+                 T_reg_GeV=None) -> dict:
+        """The reference's run loop (gvh_run_loop) from the current state: up to nt+1
+        iterations, stop rule, field dumps and/or surface.dat in output_dir."""
+        lat = LatticeParams.from_buffer_copy(self.lattice)
+        lat.numProperTimePoints = int(nt)
+        hyd = HydroParams.from_buffer_copy(self.hydro)
+        if tau0 is not None:
+            hyd.initialProperTimePoint = float(tau0)
+        if T_fo_GeV is not None:
+            hyd.freezeoutTemperatureGeV = float(T_fo_GeV)
+        if T_reg_GeV is not None:
+            hyd.regulationTemperatureGeV = float(T_reg_GeV)
+        outputs = (GVH_RUN_FIELDS if fields else 0) | (GVH_RUN_SURFACE if surface else 0)
+        rep = RunReport()
+        L = self._L
+        L.gvh_run_loop.argtypes = [ctypes.c_void_p, ctypes.POINTER(LatticeParams), ctypes.POINTER(HydroParams),
+                                   ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(RunReport)]
+        L.gvh_plugin_last_error.restype = ctypes.c_char_p
+        rc = L.gvh_run_loop(self._h, ctypes.byref(lat), ctypes.byref(hyd),
+                            None if output_dir is None else str(output_dir).encode(), outputs, ctypes.byref(rep))
+        if rc != 0:
+            raise GvhError(f"gvh_run_loop failed ({rc}): {L.gvh_plugin_last_error().decode()}")
+        return {k: getattr(rep, k) for k, _ in RunReport._fields_}
 
     def interior(self, a):
         return np.asarray(a).reshape(self.ncz, self.ncy, self.ncx)[2:-2, 2:-2, 2:-2]

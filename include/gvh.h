@@ -252,6 +252,9 @@ typedef struct gvh_run_report {
 	double freezeout_energy_density;  /* e(T_fo) in fm^-4 */
 	long long surface_elements;       /* rows written to surface.dat */
 	double surface_seconds;           /* wall time of the freeze-out surface finder */
+	long long surface_hypercubes;     /* crossed hypercubes over all slabs */
+	double surface_bytes_to_host;     /* bytes the finder copied from the device */
+	double surface_host_seconds;      /* of surface_seconds: host cornelius and formatting */
 } gvh_run_report;
 
 /* gvh_run outputs (bit flags) */
@@ -286,6 +289,12 @@ int gvh_write_field(const char *output_dir, const char *name, double tau, const 
 int gvh_run(const gvh_lattice_params *lattice, const gvh_ic_params *ic, const gvh_hydro_params *hydro,
             const char *root_dir, const char *output_dir, const gvh_options *opts, int outputs,
             gvh_run_report *report);
+
+/* The same loop on a handle whose initial state the caller has set (gvh_set_primitive_state or
+ * gvh_set_state; an in-memory initial condition instead of input files): output_dir may be
+ * NULL for no output. The handle is left at the last level reached. */
+int gvh_run_loop(gvh_handle *h, const gvh_lattice_params *lattice, const gvh_hydro_params *hydro,
+                 const char *output_dir, int outputs, gvh_run_report *report);
 
 /* The reference's labels for the slab between time levels k and k+1 (HydroPlugin.cpp:262-314,
  * FOFREQ = 10): its rows go to the file at loop iteration *flush_iteration (state = level
@@ -331,7 +340,12 @@ typedef struct {
  * nothing else, HydroPlugin.cpp:157-182). The handle must outlive the surface. */
 int gvh_surface_create(gvh_handle *h, double e_freezeout, gvh_surface **out);
 int gvh_surface_destroy(gvh_surface *s);
+/* Host threads of the cornelius stage (default: the machine's hardware threads). */
 int gvh_surface_set_threads(gvh_surface *s, int nthreads);
+/* What gvh_surface_find keeps of each slab (default both): binary rows, text, or both. */
+#define GVH_SURFACE_ROWS 1
+#define GVH_SURFACE_TEXT 2
+int gvh_surface_set_outputs(gvh_surface *s, int outputs);
 /* Takes the handle's current state as the lower time level of the next slab. */
 int gvh_surface_set_lower(gvh_surface *s);
 /* Elements of the slab (lower level, handle's current level); then the current level becomes
