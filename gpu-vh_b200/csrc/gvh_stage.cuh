@@ -55,7 +55,10 @@ struct StageArgs {
   unsigned *status;       // or-ed STATUS_* bits
 };
 
-constexpr int kBlock = 128;  // threads per block of the stage kernel
+#ifndef GVH_BLOCK
+#define GVH_BLOCK 128
+#endif
+constexpr int kBlock = GVH_BLOCK;  // threads per block of the stage kernel
 
 template <bool SHEAR, bool BULK>
 struct NComp {
@@ -138,24 +141,12 @@ __device__ __forceinline__ int pi_spatial(int m, int a) {
 // with S_axis of SourceTerms.cu:443-567:
 //   S_0     = d(pi^{tt}) v - d(pi^{t a}) [- v d(Pi)]
 //   S_{m+1} = d(pi^{t m}) v - d(pi^{m a}) [- d(Pi), divided by tau^2 along eta, when m = a]
-template <int EOS, bool SHEAR, bool BULK, bool MIXED>
-__device__ __forceinline__ void axis_update(const StageArgs &a, int s, int axis, int idx, int n_axis, int stride,
-                                            double d, const GuessEos &g0, const double *uc, double *out,
-                                            unsigned &status) {
-  using R = typename std::conditional<MIXED, float, double>::type;
-  constexpr int NQ = NComp<SHEAR, BULK>::value;
-  const int o[5] = {(max(idx - 2, 0) - idx) * stride, (max(idx - 1, 0) - idx) * stride, 0,
-                    (min(idx + 1, n_axis - 1) - idx) * stride, (min(idx + 2, n_axis - 1) - idx) * stride};
-  const R inv_d = R(1.0 / d);
-  // Face states are recovered in FP64 on both paths (the mixed path rounds only the
-  // resulting speeds): an FP32 recovery was tried and let a 2+1D hotspot event run away
-  // to NaN that the FP64 recovery keeps finite.
-  const FaceSpeeds<double> fd = face_speeds<EOS, SHEAR, BULK>(a, s, axis, o, g0, status);
-  FaceSpeeds<R> f;
-  f.wRf = (R)fd.wRf; f.wLf = (R)fd.wLf; f.wRb = (R)fd.wRb; f.wLb = (R)fd.wLb;
-  f.af = (R)fd.af; f.ab = (R)fd.ab;
-
-  R Sa[4] = {R(0), R(0), R(0), R(0)};
+// Sa: the axis's pi and Pi derivative sources of T^{tau mu} (SourceTerms.cu:443-567), in the
+// working precision; zero without shear.
+template <bool SHEAR, bool BULK, class R>
+__device__ __forceinline__ void axis_pi_sources(const StageArgs &a, int s, int axis, const int (&o)[5], R inv_d,
+                                                const double *uc, R (&Sa)[4]) {
+  Sa[0] = Sa[1] = Sa[2] = Sa[3] = R(0);
   if (SHEAR) {
     const R fac = inv_d / R(2);
     auto der = [&](int c) {
@@ -175,6 +166,27 @@ __device__ __forceinline__ void axis_update(const StageArgs &a, int s, int axis,
       Sa[1 + m] = sm;
     }
   }
+}
+
+template <int EOS, bool SHEAR, bool BULK, bool MIXED>
+__device__ __forceinline__ void axis_update(const StageArgs &a, int s, int axis, int idx, int n_axis, int stride,
+                                            double d, const GuessEos &g0, const double *uc, double *out,
+                                            unsigned &status) {
+  using R = typename std::conditional<MIXED, float, double>::type;
+  constexpr int NQ = NComp<SHEAR, BULK>::value;
+  const int o[5] = {(max(idx - 2, 0) - idx) * stride, (max(idx - 1, 0) - idx) * stride, 0,
+                    (min(idx + 1, n_axis - 1) - idx) * stride, (min(idx + 2, n_axis - 1) - idx) * stride};
+  const R inv_d = R(1.0 / d);
+  // Face states are recovered in FP64 on both paths (the mixed path rounds only the
+  // resulting speeds): an FP32 recovery was tried and let a 2+1D hotspot event run away
+  // to NaN that the FP64 recovery keeps finite.
+  const FaceSpeeds<double> fd = face_speeds<EOS, SHEAR, BULK>(a, s, axis, o, g0, status);
+  FaceSpeeds<R> f;
+  f.wRf = (R)fd.wRf; f.wLf = (R)fd.wLf; f.wRb = (R)fd.wRb; f.wLb = (R)fd.wLb;
+  f.af = (R)fd.af; f.ab = (R)fd.ab;
+
+  R Sa[4];
+  axis_pi_sources<SHEAR, BULK, R>(a, s, axis, o, inv_d, uc, Sa);
   const R th = (R)a.theta;
 #pragma unroll 1
   for (int n = 0; n < NQ; ++n) {
@@ -194,118 +206,97 @@ __device__ __forceinline__ void axis_update(const StageArgs &a, int s, int axis,
 //
 // stage_cell does one cell (interior index id < a.ncells); it returns the cell's new energy
 // density so callers can reduce it (the batched engine tracks max e per event).
-template <int EOS, bool SHEAR, bool BULK, bool STAGE2, bool MIXED>
-__device__ __forceinline__ double stage_cell(const StageArgs &a, long long id) {
+// The source-term Euler step of one cell: out[n * OSTRIDE] = q_n + dt * S_n
+// (EulerStep.cu:946-1009, SourceTerms.cu:569-755).
+template <int EOS, bool SHEAR, bool BULK, bool MIXED, int OSTRIDE>
+__device__ __forceinline__ void stage_source(const StageArgs &a, long long s, int i, int j, int k, double ePrev,
+                                             const double (&uc)[4], double *out) {
   using R = typename std::conditional<MIXED, float, double>::type;
   constexpr int NQ = NComp<SHEAR, BULK>::value;
-  const int i = (int)(id % a.nx);
-  const int j = (int)((id / a.nx) % a.ny);
-  const int k = (int)(id / ((long long)a.nx * a.ny));
-  const long long s = i + a.sy * j + a.sz * k;
-  unsigned status = 0;
-
-  const double ePrev = a.e[s];
-  double uc[4];
+  R q[NQ];
 #pragma unroll
-  for (int m = 0; m < 4; ++m) uc[m] = __ldg(a.uin + m * a.cs + s);
-
-  // The running update of each component lives in shared memory (this thread's column of
-  // s_out): it is read-modified-written once per axis, and keeping it out of registers
-  // leaves them to the Newton solves and the source algebra.
-  __shared__ double s_out[NQ * kBlock];
-  double *out = s_out + threadIdx.x;
-
-  // ---- source term: out = q + dt * S (EulerStep.cu:946-1009, SourceTerms.cu:569-755) ---
-  {
-    R q[NQ];
+  for (int n = 0; n < NQ; ++n) q[n] = (R)__ldg(a.qin + n * a.cs + s);
+  const R pc = (R)__ldg(a.pin + s);
+  const long long xm = (i > 0) ? -1 : 0, xp = (i < a.nx - 1) ? 1 : 0;
+  const long long ym = (j > 0) ? -a.sy : 0, yp = (j < a.ny - 1) ? a.sy : 0;
+  const long long zm = (k > 0) ? -a.sz : 0, zp = (k < a.nz - 1) ? a.sz : 0;
+  // Derivatives of u and p: differences of nearly equal values, so they are formed in
+  // FP64 on both paths and only the results are rounded to the working precision.
+  CellFlowT<R> f;
+  R ucr[4];
 #pragma unroll
-    for (int n = 0; n < NQ; ++n) q[n] = (R)__ldg(a.qin + n * a.cs + s);
-    const R pc = (R)__ldg(a.pin + s);
-    const long long xm = (i > 0) ? -1 : 0, xp = (i < a.nx - 1) ? 1 : 0;
-    const long long ym = (j > 0) ? -a.sy : 0, yp = (j < a.ny - 1) ? a.sy : 0;
-    const long long zm = (k > 0) ? -a.sz : 0, zp = (k < a.nz - 1) ? a.sz : 0;
-    // Derivatives of u and p: differences of nearly equal values, so they are formed in
-    // FP64 on both paths and only the results are rounded to the working precision.
-    CellFlowT<R> f;
-    R ucr[4];
+  for (int m = 0; m < 4; ++m) ucr[m] = (R)uc[m];
+  f.ut = ucr[0]; f.ux = ucr[1]; f.uy = ucr[2]; f.un = ucr[3];
+  // d u^mu / d tau = (u - u^{n-1}) / dt (SourceTerms.cu:68-71)
+  f.dtut = (R)((uc[0] - a.uprev[s]) / a.dt);
+  f.dtux = (R)((uc[1] - a.uprev[a.cs + s]) / a.dt);
+  f.dtuy = (R)((uc[2] - a.uprev[2 * a.cs + s]) / a.dt);
+  f.dtun = (R)((uc[3] - a.uprev[3 * a.cs + s]) / a.dt);
+  const double thd = a.theta;
+  const double idxd = 1.0 / a.dx, idyd = 1.0 / a.dy, idzd = 1.0 / a.dz;
+  R du[3][4];
 #pragma unroll
-    for (int m = 0; m < 4; ++m) ucr[m] = (R)uc[m];
-    f.ut = ucr[0]; f.ux = ucr[1]; f.uy = ucr[2]; f.un = ucr[3];
-    // d u^mu / d tau = (u - u^{n-1}) / dt (SourceTerms.cu:68-71)
-    f.dtut = (R)((uc[0] - a.uprev[s]) / a.dt);
-    f.dtux = (R)((uc[1] - a.uprev[a.cs + s]) / a.dt);
-    f.dtuy = (R)((uc[2] - a.uprev[2 * a.cs + s]) / a.dt);
-    f.dtun = (R)((uc[3] - a.uprev[3 * a.cs + s]) / a.dt);
-    const double thd = a.theta;
-    const double idxd = 1.0 / a.dx, idyd = 1.0 / a.dy, idzd = 1.0 / a.dz;
-    R du[3][4];
-#pragma unroll
-    for (int m = 0; m < 4; ++m) {
-      const double *u = a.uin + m * a.cs + s;
-      du[0][m] = (R)(limited_slope(thd, __ldg(u + xm), uc[m], __ldg(u + xp)) * idxd);
-      du[1][m] = (R)(limited_slope(thd, __ldg(u + ym), uc[m], __ldg(u + yp)) * idyd);
-      du[2][m] = (R)(limited_slope(thd, __ldg(u + zm), uc[m], __ldg(u + zp)) * idzd);
-    }
-    f.dxut = du[0][0]; f.dyut = du[1][0]; f.dnut = du[2][0];
-    f.dxux = du[0][1]; f.dyux = du[1][1]; f.dnux = du[2][1];
-    f.dxuy = du[0][2]; f.dyuy = du[1][2]; f.dnuy = du[2][2];
-    f.dxun = du[0][3]; f.dyun = du[1][3]; f.dnun = du[2][3];
-    const double *p = a.pin + s;
-    const double pcd = __ldg(p);
-    const R dxp = (R)(limited_slope(thd, __ldg(p + xm), pcd, __ldg(p + xp)) * idxd);
-    const R dyp = (R)(limited_slope(thd, __ldg(p + ym), pcd, __ldg(p + yp)) * idyd);
-    const R dnp = (R)(limited_slope(thd, __ldg(p + zm), pcd, __ldg(p + zp)) * idzd);
-
-    const R t = (R)a.t_euler;
-    const R Pi = BULK ? q[NQ - 1] : R(0);
-    const R pitt = SHEAR ? q[4] : R(0), pitx = SHEAR ? q[5] : R(0), pity = SHEAR ? q[6] : R(0);
-    const R pitn = SHEAR ? q[7] : R(0), pinn = SHEAR ? q[13] : R(0);
-    const R ut = ucr[0], ux = ucr[1], uy = ucr[2], un = ucr[3];
-    const R iut = dv(R(1), ut), it = dv(R(1), t);
-    // Tnn (EnergyMomentumTensor.cu:205-207) with p + Pi
-    const R pP = pc + Pi;
-    const R er = (R)ePrev;
-    const R tnn = (er + pP) * un * un + pP * it * it + pinn;
-    const R vx = ux * iut, vy = uy * iut, vn = un * iut;
-    const R dxvx = (f.dxux - vx * f.dxut) * iut;
-    const R dyvy = (f.dyuy - vy * f.dyut) * iut;
-    const R dnvn = (f.dnun - vn * f.dnut) * iut;
-    const R dkvk = dxvx + dyvy + dnvn;
-    R S[NQ];
-    S[0] = -(q[0] * it + t * tnn) + dkvk * (pitt - pc - Pi) - vx * dxp - vy * dyp - vn * dnp;
-    S[1] = -q[1] * it - dxp + dkvk * pitx;
-    S[2] = -q[2] * it - dyp + dkvk * pity;
-    S[3] = R(-3) * q[3] * it - dnp * it * it + dkvk * pitn;
-    if (SHEAR) {
-      ShearT<R> pi{q[4], q[5], q[6], q[7], q[8], q[9], q[10], q[11], q[12], q[13]};
-      R rhs[11];
-      pimunu_rhs<EOS, BULK, R>(rhs, t, (R)a.etabar, er, pc, f, pi, Pi, dkvk);
-#pragma unroll
-      for (int n = 4; n < NQ; ++n) S[n] = rhs[n - 4];
-    }
-#pragma unroll
-    for (int n = 0; n < NQ; ++n) {
-      // the FP64 value of q is re-read for the accumulation (a no-op reload on the FP64 path)
-      const double qd = MIXED ? __ldg(a.qin + n * a.cs + s) : (double)q[n];
-      out[n * kBlock] = qd + a.dt * (double)S[n];
-    }
+  for (int m = 0; m < 4; ++m) {
+    const double *u = a.uin + m * a.cs + s;
+    du[0][m] = (R)(limited_slope(thd, __ldg(u + xm), uc[m], __ldg(u + xp)) * idxd);
+    du[1][m] = (R)(limited_slope(thd, __ldg(u + ym), uc[m], __ldg(u + yp)) * idyd);
+    du[2][m] = (R)(limited_slope(thd, __ldg(u + zm), uc[m], __ldg(u + zp)) * idzd);
   }
+  f.dxut = du[0][0]; f.dyut = du[1][0]; f.dnut = du[2][0];
+  f.dxux = du[0][1]; f.dyux = du[1][1]; f.dnux = du[2][1];
+  f.dxuy = du[0][2]; f.dyuy = du[1][2]; f.dnuy = du[2][2];
+  f.dxun = du[0][3]; f.dyun = du[1][3]; f.dnun = du[2][3];
+  const double *p = a.pin + s;
+  const double pcd = __ldg(p);
+  const R dxp = (R)(limited_slope(thd, __ldg(p + xm), pcd, __ldg(p + xp)) * idxd);
+  const R dyp = (R)(limited_slope(thd, __ldg(p + ym), pcd, __ldg(p + yp)) * idyd);
+  const R dnp = (R)(limited_slope(thd, __ldg(p + zm), pcd, __ldg(p + zp)) * idzd);
 
-  // ---- flux divergence along x, y, eta (EulerStep.cu:1011-1277) -------------------------
-  const GuessEos g0 = guess_eos<EOS>(ePrev);
-#pragma unroll 1
-  for (int axis = 0; axis < 3; ++axis) {
-    const int idx = axis == 0 ? i : axis == 1 ? j : k;
-    const int n_axis = axis == 0 ? a.nx : axis == 1 ? a.ny : a.nz;
-    const int stride = axis == 0 ? 1 : axis == 1 ? (int)a.sy : (int)a.sz;
-    const double d = axis == 0 ? a.dx : axis == 1 ? a.dy : a.dz;
-    axis_update<EOS, SHEAR, BULK, MIXED>(a, (int)s, axis, idx, n_axis, stride, d, g0, uc, out, status);
+  const R t = (R)a.t_euler;
+  const R Pi = BULK ? q[NQ - 1] : R(0);
+  const R pitt = SHEAR ? q[4] : R(0), pitx = SHEAR ? q[5] : R(0), pity = SHEAR ? q[6] : R(0);
+  const R pitn = SHEAR ? q[7] : R(0), pinn = SHEAR ? q[13] : R(0);
+  const R ut = ucr[0], ux = ucr[1], uy = ucr[2], un = ucr[3];
+  const R iut = dv(R(1), ut), it = dv(R(1), t);
+  // Tnn (EnergyMomentumTensor.cu:205-207) with p + Pi
+  const R pP = pc + Pi;
+  const R er = (R)ePrev;
+  const R tnn = (er + pP) * un * un + pP * it * it + pinn;
+  const R vx = ux * iut, vy = uy * iut, vn = un * iut;
+  const R dxvx = (f.dxux - vx * f.dxut) * iut;
+  const R dyvy = (f.dyuy - vy * f.dyut) * iut;
+  const R dnvn = (f.dnun - vn * f.dnut) * iut;
+  const R dkvk = dxvx + dyvy + dnvn;
+  R S[NQ];
+  S[0] = -(q[0] * it + t * tnn) + dkvk * (pitt - pc - Pi) - vx * dxp - vy * dyp - vn * dnp;
+  S[1] = -q[1] * it - dxp + dkvk * pitx;
+  S[2] = -q[2] * it - dyp + dkvk * pity;
+  S[3] = R(-3) * q[3] * it - dnp * it * it + dkvk * pitn;
+  if (SHEAR) {
+    ShearT<R> pi{q[4], q[5], q[6], q[7], q[8], q[9], q[10], q[11], q[12], q[13]};
+    R rhs[11];
+    pimunu_rhs<EOS, BULK, R>(rhs, t, (R)a.etabar, er, pc, f, pi, Pi, dkvk);
+#pragma unroll
+    for (int n = 4; n < NQ; ++n) S[n] = rhs[n - 4];
   }
+#pragma unroll
+  for (int n = 0; n < NQ; ++n) {
+    // the FP64 value of q is re-read for the accumulation (a no-op reload on the FP64 path)
+    const double qd = MIXED ? __ldg(a.qin + n * a.cs + s) : (double)q[n];
+    out[n * OSTRIDE] = qd + a.dt * (double)S[n];
+  }
+}
 
+// The rest of a stage for one cell once out holds its Euler update: the Heun combination
+// (stage 2), primitive recovery at the new time, regulation, and the writes. Returns e.
+template <int EOS, bool SHEAR, bool BULK, bool STAGE2, int OSTRIDE>
+__device__ __forceinline__ double stage_finish(const StageArgs &a, long long s, const double *out, const GuessEos &g0,
+                                               unsigned status) {
+  constexpr int NQ = NComp<SHEAR, BULK>::value;
   // ---- Heun combination Q = (Q + q^n)/2 (FullyDiscreteKurganovTadmorScheme.cu:60-104) ---
   double o[NQ];
 #pragma unroll
-  for (int n = 0; n < NQ; ++n) o[n] = out[n * kBlock];
+  for (int n = 0; n < NQ; ++n) o[n] = out[n * OSTRIDE];
   if (STAGE2) {
 #pragma unroll
     for (int n = 0; n < NQ; ++n) o[n] = (o[n] + a.qn[n * a.cs + s]) * 0.5;
@@ -352,6 +343,43 @@ __device__ __forceinline__ double stage_cell(const StageArgs &a, long long id) {
   a.uout[3 * a.cs + s] = pr.un;
   if (status) atomicOr(a.status, status);
   return pr.e;
+}
+
+template <int EOS, bool SHEAR, bool BULK, bool STAGE2, bool MIXED>
+__device__ __forceinline__ double stage_cell(const StageArgs &a, long long id) {
+  using R = typename std::conditional<MIXED, float, double>::type;
+  constexpr int NQ = NComp<SHEAR, BULK>::value;
+  const int i = (int)(id % a.nx);
+  const int j = (int)((id / a.nx) % a.ny);
+  const int k = (int)(id / ((long long)a.nx * a.ny));
+  const long long s = i + a.sy * j + a.sz * k;
+  unsigned status = 0;
+
+  const double ePrev = a.e[s];
+  double uc[4];
+#pragma unroll
+  for (int m = 0; m < 4; ++m) uc[m] = __ldg(a.uin + m * a.cs + s);
+
+  // The running update of each component lives in shared memory (this thread's column of
+  // s_out): it is read-modified-written once per axis, and keeping it out of registers
+  // leaves them to the Newton solves and the source algebra.
+  __shared__ double s_out[NQ * kBlock];
+  double *out = s_out + threadIdx.x;
+
+  stage_source<EOS, SHEAR, BULK, MIXED, kBlock>(a, s, i, j, k, ePrev, uc, out);
+
+  // ---- flux divergence along x, y, eta (EulerStep.cu:1011-1277) -------------------------
+  const GuessEos g0 = guess_eos<EOS>(ePrev);
+#pragma unroll 1
+  for (int axis = 0; axis < 3; ++axis) {
+    const int idx = axis == 0 ? i : axis == 1 ? j : k;
+    const int n_axis = axis == 0 ? a.nx : axis == 1 ? a.ny : a.nz;
+    const int stride = axis == 0 ? 1 : axis == 1 ? (int)a.sy : (int)a.sz;
+    const double d = axis == 0 ? a.dx : axis == 1 ? a.dy : a.dz;
+    axis_update<EOS, SHEAR, BULK, MIXED>(a, (int)s, axis, idx, n_axis, stride, d, g0, uc, out, status);
+  }
+
+  return stage_finish<EOS, SHEAR, BULK, STAGE2, kBlock>(a, s, out, g0, status);
 }
 
 // One RK substep over one lattice: one thread per interior cell.
