@@ -24,6 +24,7 @@
 #include "gvh_handle.h"
 #include "gvh_layout.cuh"
 #include "gvh_stage.cuh"
+#include "gvh_validity.cuh"
 
 using namespace gvh;
 
@@ -79,6 +80,32 @@ int dispatch_physics(const gvh_handle *h, const StageArgs &a, bool stage2) {
 int dispatch(const gvh_handle *h, const StageArgs &a, bool stage2) {
   if (h->eos == GVH_EOS_CONFORMAL) return dispatch_physics<EOS_CONFORMAL>(h, a, stage2);
   return dispatch_physics<EOS_QCD>(h, a, stage2);
+}
+
+// checkValidity after the step (FullyDiscreteKurganovTadmorScheme.cu:137): t + dt, the new
+// e, p and u, and u one step earlier.
+int launch_validity(const gvh_handle *h, double t_new, const double *u_new, const double *u_old) {
+  ValidityArgs v;
+  v.nx = h->nx; v.ny = h->ny; v.nz = h->nz;
+  v.sy = h->sy; v.sz = h->sz; v.cs = h->cs; v.ncells = h->ncells;
+  v.dx = h->dx; v.dy = h->dy; v.dz = h->dz; v.dt = h->dt_lattice; v.etabar = h->etabar;
+  v.t = t_new;
+  v.e = h->e; v.p = h->pA; v.u = u_new; v.up = u_old;
+  v.diag = h->diag;
+  const unsigned blocks = (unsigned)((h->ncells + 255) / 256);
+  const bool conf = h->eos == GVH_EOS_CONFORMAL;
+  if (!h->shear) {
+    if (conf) validity_kernel<EOS_CONFORMAL, false, false><<<blocks, 256, 0, h->stream>>>(v);
+    else validity_kernel<EOS_QCD, false, false><<<blocks, 256, 0, h->stream>>>(v);
+  } else if (!h->bulk) {
+    if (conf) validity_kernel<EOS_CONFORMAL, true, false><<<blocks, 256, 0, h->stream>>>(v);
+    else validity_kernel<EOS_QCD, true, false><<<blocks, 256, 0, h->stream>>>(v);
+  } else {
+    if (conf) validity_kernel<EOS_CONFORMAL, true, true><<<blocks, 256, 0, h->stream>>>(v);
+    else validity_kernel<EOS_QCD, true, true><<<blocks, 256, 0, h->stream>>>(v);
+  }
+  GVH_CUDA(cudaGetLastError());
+  return GVH_OK;
 }
 
 Pack make_pack(const gvh_handle *h) { return Pack{h->nx, h->ny, h->nz, h->sy, h->sz, h->ng}; }
@@ -193,6 +220,7 @@ int gvh_destroy(gvh_handle *h) {
   cudaStreamDestroy(h->own_stream);
   cudaFree(h->block);
   if (h->staging) cudaFree(h->staging);
+  if (h->diag) cudaFree(h->diag);
   delete h;
   return GVH_OK;
 }
@@ -301,9 +329,46 @@ int gvh_rk2_step(gvh_handle *h, double t, double dt, double T_reg) {
   a.qin = h->qB; a.qn = h->qA; a.qout = h->qA;
   a.pin = h->pB; a.pout = h->pA;
   a.uin = h->u[h->uprev]; a.uprev = h->u[h->ucur]; a.uout = h->u[h->ufree];
+  a.diag = h->validity_on ? h->diag : nullptr;
   if ((rc = dispatch(h, a, true))) return rc;
+  if (h->validity_on && (rc = launch_validity(h, t1, h->u[h->ufree], h->u[h->ucur]))) return rc;
   const int nc = h->ufree, np = h->ucur, nf = h->uprev;
   h->ucur = nc; h->uprev = np; h->ufree = nf;
+  return GVH_OK;
+}
+
+int gvh_enable_validity(gvh_handle *h, int on) {
+  if (!h) return fail(GVH_ERR_INVALID, "null handle");
+  int rc;
+  if ((rc = set_device(h))) return rc;
+  if (on && !h->diag) {
+    const size_t bytes = (size_t)(kValidityFields + kValiditySaved) * h->cs * sizeof(double);
+    if (cudaMalloc(&h->diag, bytes) != cudaSuccess) {
+      h->diag = nullptr;
+      return fail(GVH_ERR_NOMEM, "gvh_enable_validity: cannot allocate %zu bytes", bytes);
+    }
+    GVH_CUDA(cudaMemsetAsync(h->diag, 0, bytes, h->stream));
+  }
+  h->validity_on = on ? 1 : 0;
+  return GVH_OK;
+}
+
+int gvh_get_validity(gvh_handle *h, double *const *fields, int n_fields) {
+  if (!h || !fields) return fail(GVH_ERR_INVALID, "gvh_get_validity: null argument");
+  if (n_fields != kValidityFields) return fail(GVH_ERR_INVALID, "gvh_get_validity: expected %d fields", kValidityFields);
+  if (!h->diag) return fail(GVH_ERR_INVALID, "gvh_get_validity: diagnostics not enabled (gvh_enable_validity)");
+  int rc;
+  if ((rc = set_device(h)) || (rc = ensure_staging(h))) return rc;
+  double *src[kValidityFields];
+  for (int f = 0; f < kValidityFields; ++f) src[f] = fields[f] ? h->diag + (size_t)f * h->cs : nullptr;
+  double **table = staging_ptr_table(h);
+  GVH_CUDA(cudaMemcpyAsync(table, src, n_fields * sizeof(double *), cudaMemcpyHostToDevice, h->stream));
+  unpack_kernel<<<(unsigned)((h->ng + 255) / 256), 256, 0, h->stream>>>(make_pack(h), n_fields, table, h->staging);
+  GVH_CUDA(cudaGetLastError());
+  const size_t fb = h->ng * sizeof(double);
+  for (int f = 0; f < n_fields; ++f)
+    if (fields[f]) GVH_CUDA(cudaMemcpyAsync(fields[f], h->staging + f * h->ng, fb, cudaMemcpyDefault, h->stream));
+  GVH_CUDA(cudaStreamSynchronize(h->stream));
   return GVH_OK;
 }
 

@@ -17,6 +17,8 @@ struct gvh_handle {
   int ucur, uprev, ufree;
   unsigned *status;
   double *staging;          // reference-layout fields for set/get, allocated on first use
+  double *diag;             // validity diagnostics (allocated by gvh_enable_validity)
+  int validity_on;
 };
 
 // The current time level's fields in the handle's interior-only layout (cell

@@ -53,7 +53,14 @@ struct StageArgs {
   const double *uprev;    // u^mu of the previous time level, centre only (may alias uout)
   double *uout;
   unsigned *status;       // or-ed STATUS_* bits
+  double *diag;           // stage 2, optional: regulation factor (component 0) and the centre's
+                          // q^n pi^{mu nu}, Pi (components 13..23) for the validity diagnostics
 };
+
+// Components of the validity block (VALIDITY_DOMAIN, DynamicalVariables.cuh:82-98, in that
+// order), then the saved q^n dissipative currents the diagnostics read.
+constexpr int kValidityFields = 13;
+constexpr int kValiditySaved = 11;
 
 #ifndef GVH_BLOCK
 #define GVH_BLOCK 128
@@ -308,6 +315,7 @@ __device__ __forceinline__ double stage_finish(const StageArgs &a, long long s, 
                           SHEAR ? o[6] : 0.0, SHEAR ? o[7] : 0.0, BULK ? o[NQ - 1] : 0.0, g0, status);
 
   // ---- regulation (RegulateDissipativeCurrents.cu:15-134) ----------------------------------
+  double fac_reg = 1.0;
   if (SHEAR && pr.e <= a.e_reg) {
     const double pitt = o[4], pitx = o[5], pity = o[6], pitn = o[7], pixx = o[8], pixy = o[9];
     const double pixn = o[10], piyy = o[11], piyn = o[12], pinn = o[13];
@@ -330,6 +338,22 @@ __device__ __forceinline__ double stage_finish(const StageArgs &a, long long s, 
     // and the bulk factor is always 1 (RegulateDissipativeCurrents.cu:54-58, 106-109).
 #pragma unroll
     for (int n = 4; n < 14; ++n) o[n] *= facShear;
+    fac_reg = facShear;
+  }
+
+  // ---- validity diagnostics inputs (stage 2, when asked for) ------------------------------
+  // The reference's regulateDissipativeCurrents stores facShear (RegulateDissipativeCurrents
+  // .cu:132; the last of its calls in a step is on the corrected state), and its checkValidity
+  // reads pi^{mu nu} and Pi of d_q, the state before the step (FullyDiscreteKurganovTadmorScheme
+  // .cu:137); q^n is overwritten below, so its centre values are kept here.
+  if (STAGE2 && a.diag) {
+    a.diag[s] = fac_reg;
+#pragma unroll
+    for (int m = 0; m < kValiditySaved; ++m) {
+      const int c = 4 + m;
+      a.diag[(kValidityFields + m) * a.cs + s] =
+          (c < 14 ? SHEAR : BULK) ? a.qn[(c < 14 ? c : NQ - 1) * a.cs + s] : 0.0;
+    }
   }
 
   // ---- write ----------------------------------------------------------------------------

@@ -217,6 +217,23 @@ class Lattice:
     def get_state_ptrs(self, ptrs):
         _check(self._L.gvh_get_state(self._h, _ptr_array(list(ptrs)), len(ptrs)), "gvh_get_state")
 
+    VALIDITY_NAMES = ["regulations", "knudsenNumberTaupi", "knudsenNumberTauPi", "inverseReynoldsNumberPimunu",
+                      "inverseReynoldsNumber2Pimunu", "inverseReynoldsNumberTilde2Pimunu", "inverseReynoldsNumberPi",
+                      "inverseReynoldsNumber2Pi", "inverseReynoldsNumberTilde2Pi", "taupi", "dxux", "dyuy", "theta"]
+
+    def enable_validity(self, on=True):
+        """Compute the validity diagnostics (checkValidity) with every step from now on."""
+        self._L.gvh_enable_validity.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        _check(self._L.gvh_enable_validity(self._h, int(bool(on))), "gvh_enable_validity")
+
+    def get_validity(self) -> dict:
+        """The 13 VALIDITY_DOMAIN arrays of the last step (ghosted)."""
+        arrs = [np.zeros(self.ng) for _ in self.VALIDITY_NAMES]
+        self._L.gvh_get_validity.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+        _check(self._L.gvh_get_validity(self._h, _ptr_array([a.ctypes.data for a in arrs]), len(arrs)),
+               "gvh_get_validity")
+        return dict(zip(self.VALIDITY_NAMES, arrs))
+
     def run_loop(self, nt, output_dir=None, fields=False, surface=True, tau0=None, T_fo_GeV=None,
                  T_reg_GeV=None) -> dict:
         """The reference's run loop (gvh_run_loop) from the current state: up to nt+1

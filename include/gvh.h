@@ -160,6 +160,20 @@ const char *gvh_noalloc_last_error(void);
  * the lattice to the host. Synchronises the handle's stream. */
 int gvh_max_energy_density(gvh_handle *h, double *out);
 
+/* Validity diagnostics of the fluid-dynamic description (checkValidityKernel,
+ * HydrodynamicValidity.cu:18-226, and the regulation factor of RegulateDissipativeCurrents.cu:132):
+ * when enabled, every gvh_rk2_step also computes them for the new level, one extra kernel
+ * after the second stage (the reference runs them in every step). They are read back as the
+ * 13 members of the reference's VALIDITY_DOMAIN (DynamicalVariables.cuh:82-98), in its order:
+ * regulations, knudsenNumberTaupi, knudsenNumberTauPi, inverseReynoldsNumberPimunu,
+ * inverseReynoldsNumber2Pimunu (never written, 0), inverseReynoldsNumberTilde2Pimunu,
+ * inverseReynoldsNumberPi, inverseReynoldsNumber2Pi (never written, 0),
+ * inverseReynoldsNumberTilde2Pi, taupi, dxux, dyuy, theta; ghosted arrays like
+ * gvh_get_state's (a NULL entry skips a field). */
+#define GVH_VALIDITY_FIELDS 13
+int gvh_enable_validity(gvh_handle *h, int on);
+int gvh_get_validity(gvh_handle *h, double *const *fields, int n_fields);
+
 /* e(T) of the equation of state (equilibriumEnergyDensity, EquationOfState.cu:150-204) at
  * T = T_GeV / hbarc, in fm^-4: the freeze-out threshold of HydroPlugin.cpp:131-135. */
 double gvh_energy_density_of_temperature(int eos, double T_GeV);

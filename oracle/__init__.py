@@ -208,6 +208,7 @@ class RefLattice(_Base):
             getattr(L, fn).restype = ctypes.c_double
         L.gvh_ref_inferred.argtypes = [ctypes.c_double, ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p]
         L.gvh_ref_set_threads.argtypes = [ctypes.c_int]
+        L.gvh_ref_get_validity.argtypes = [ctypes.c_void_p]
         L.gvh_ref_surface_begin.argtypes = [ctypes.c_int] * 3 + [ctypes.c_double] * 6 + [ctypes.c_char_p]
         L.gvh_ref_surface_begin.restype = ctypes.c_void_p
         L.gvh_ref_surface_iteration.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double]
@@ -244,6 +245,16 @@ class RefLattice(_Base):
 
     def pressure(self, e):
         return self._L.gvh_ref_equilibrium_pressure(e)
+
+    VALIDITY_NAMES = ["regulations", "knudsenNumberTaupi", "knudsenNumberTauPi", "inverseReynoldsNumberPimunu",
+                      "inverseReynoldsNumber2Pimunu", "inverseReynoldsNumberTilde2Pimunu", "inverseReynoldsNumberPi",
+                      "inverseReynoldsNumber2Pi", "inverseReynoldsNumberTilde2Pi", "taupi", "dxux", "dyuy", "theta"]
+
+    def get_validity(self) -> dict:
+        """The reference's VALIDITY_DOMAIN arrays after the last step (ghosted)."""
+        arrs = [np.zeros(self.ng) for _ in self.VALIDITY_NAMES]
+        self._L.gvh_ref_get_validity(_ptrs(arrs))
+        return dict(zip(self.VALIDITY_NAMES, arrs))
 
     # The freeze-out part of the reference's run loop (oracle/ref_surface.cpp).
     def surface_begin(self, t0, e_fo, path):

@@ -6,10 +6,12 @@ the host shim in oracle/ref_shim, links them with oracle/ref_driver.cpp, and wri
 shared library per physics variant into oracle/_ref/ (git-ignored; it travels with the
 working tree to the GPU host like every other built .so).
 
-One file needs a generated overlay copy: FluxLimiter.cu hard-codes `#define THETA 2.0`
-(FluxLimiter.cu:15) after its includes, so no header can override it. The copy, written to
-oracle/_ref/overlay/, only turns THETA into a runtime double so one build serves both the
-shipped theta=2.0 and the theta=1.8 configuration. Every other source is compiled unchanged.
+Two files need a generated overlay copy, written to oracle/_ref/overlay/: FluxLimiter.cu
+hard-codes `#define THETA 2.0` (FluxLimiter.cu:15) after its includes, so no header can
+override it; the copy only turns THETA into a runtime double so one build serves both the
+shipped theta=2.0 and the theta=1.8 configuration. HydrodynamicValidity.cu ends with a
+<<<>>> launcher; its copy stops before that function. Every other source is compiled
+unchanged.
 
 Variants (compile-time switches the reference exposes as macros):
   precision  fp64 (PRECISION double + double intrinsics, via the shim) | fp32 (as shipped)
@@ -72,13 +74,31 @@ def _overlay_flux_limiter() -> str:
     return dst
 
 
+def _overlay_validity() -> str:
+    """HydrodynamicValidity.cu ends with its host launcher, a <<<>>> launch that g++ cannot
+    compile (HydrodynamicValidity.cu:231-235); the copy stops before it, the kernel itself is
+    unchanged (the driver launches it over the interior)."""
+    src = os.path.join(REF_ROOT, "rhic", "src", "HydrodynamicValidity.cu")
+    with open(src) as f:
+        text = f.read()
+    cut = text.find("void checkValidity(")
+    if cut < 0:
+        raise RuntimeError(f"{src}: launcher 'void checkValidity(' not found")
+    d = os.path.join(OUT, "overlay")
+    os.makedirs(d, exist_ok=True)
+    dst = os.path.join(d, "HydrodynamicValidity.cu")
+    with open(dst, "w") as f:
+        f.write(text[:cut])
+    return dst
+
+
 def _run(cmd):
     r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
     if r.returncode != 0:
         raise RuntimeError("command failed: " + " ".join(cmd) + "\n" + r.stdout)
 
 
-def build_variant(name: str, flux_limiter: str) -> str:
+def build_variant(name: str, flux_limiter: str, validity: str) -> str:
     prec, eos, phys = name.split("_")
     flags = PRECISIONS[prec] + EOS[eos] + PHYSICS[phys]
     obj_dir = os.path.join(OUT, "obj", name)
@@ -91,7 +111,7 @@ def build_variant(name: str, flux_limiter: str) -> str:
     ]
     common = ["g++", "-std=c++14", "-O2", "-fPIC", "-fopenmp", "-ffp-contract=off", "-w"] + inc + flags
     objs = []
-    for s in [os.path.join(src_dir, x) for x in SOURCES] + [flux_limiter]:
+    for s in [os.path.join(src_dir, x) for x in SOURCES] + [flux_limiter, validity]:
         o = os.path.join(obj_dir, os.path.basename(s) + ".o")
         _run(common + ["-x", "c++", "-c", s, "-o", o])
         objs.append(o)
@@ -127,9 +147,10 @@ def build(jobs: int | None = None, verbose: bool = True) -> list[str]:
         return []
     os.makedirs(OUT, exist_ok=True)
     fl = _overlay_flux_limiter()
+    va = _overlay_validity()
     names = variant_names()
     with ThreadPoolExecutor(max_workers=jobs or min(12, os.cpu_count() or 4)) as ex:
-        libs = list(ex.map(lambda n: build_variant(n, fl), names))
+        libs = list(ex.map(lambda n: build_variant(n, fl, va), names))
     libs.append(build_cornelius())
     shutil.rmtree(os.path.join(OUT, "obj"), ignore_errors=True)
     if verbose:

@@ -35,6 +35,7 @@
 #ifndef IDEAL
 #include "RegulateDissipativeCurrents.cuh"
 #endif
+#include "HydrodynamicValidity.cuh"
 
 thread_local dim3 threadIdx;
 thread_local dim3 blockIdx;
@@ -79,6 +80,7 @@ Velocity g_u0, g_u1, g_uS;
 FLUID_VELOCITY *g_u = nullptr, *g_up = nullptr;
 CONSERVED_VARIABLES *g_cur = nullptr, *g_next = nullptr;
 std::vector<PRECISION> g_e, g_p, g_reg;
+std::vector<PRECISION> g_vd[13];  /* the VALIDITY_DOMAIN arrays (regulations is g_vd[0]) */
 VALIDITY_DOMAIN g_validity;
 size_t g_ng = 0;
 int g_nx = 0, g_ny = 0, g_nz = 0;
@@ -205,7 +207,12 @@ int gvh_ref_init(int nx, int ny, int nz, double dx, double dy, double dz, double
 	g_u0.alloc(g_ng); g_u1.alloc(g_ng); g_uS.alloc(g_ng);
 	g_e.assign(g_ng, 0); g_p.assign(g_ng, 0); g_reg.assign(g_ng, 1);
 	memset(&g_validity, 0, sizeof(g_validity));
-	g_validity.regulations = g_reg.data();
+	for (int f = 1; f < 13; ++f) g_vd[f].assign(g_ng, 0);
+	{
+		PRECISION **vs = reinterpret_cast<PRECISION **>(&g_validity);
+		vs[0] = g_reg.data();
+		for (int f = 1; f < 13; ++f) vs[f] = g_vd[f].data();
+	}
 	g_cur = &g_q.view; g_next = &g_Q.view;
 	g_u = &g_u0.view; g_up = &g_u1.view;
 	return 0;
@@ -319,8 +326,31 @@ int gvh_ref_rk2_step(double t_in, double dt_in, double T_reg_in) {
 	launch(d_nElements, [&] { setInferredVariablesKernel(Q, e, p, g_u, t); });
 	regulate(t, Q, e, p, g_u, T_reg);
 	setGhostCells(Q, e, p, g_u);
+	/* checkValidity(t, d_validityDomain, d_q, d_e, d_p, d_u, d_up): the 3-D launch of
+	 * HydrodynamicValidity.cu:18-23 over the interior (line 137) */
+	{
+		const int nx = g_nx, ny = g_ny, nz = g_nz;
+#pragma omp parallel for collapse(2) schedule(static)
+		for (int kk = 0; kk < nz; ++kk)
+			for (int jj = 0; jj < ny; ++jj)
+				for (int ii = 0; ii < nx; ++ii) {
+					blockDim = dim3(1, 1, 1);
+					threadIdx = dim3(0, 0, 0);
+					blockIdx = dim3((unsigned)ii, (unsigned)jj, (unsigned)kk);
+					checkValidityKernel(t, &g_validity, q, e, p, g_u, g_up);
+				}
+	}
 
 	g_cur = Q; g_next = q;
+	return 0;
+}
+
+/* The VALIDITY_DOMAIN arrays after the last step (13 ghosted arrays, NULL entries skipped). */
+int gvh_ref_get_validity(double *const *fields) {
+	if (!g_ng) return -1;
+	PRECISION **vs = reinterpret_cast<PRECISION **>(&g_validity);
+	for (int f = 0; f < 13; ++f)
+		if (fields[f]) get(fields[f], vs[f]);
 	return 0;
 }
 
