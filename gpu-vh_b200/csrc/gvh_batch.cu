@@ -429,9 +429,9 @@ int gvh_batch_add_event(gvh_batch *b, const gvh_lattice_params *L, const gvh_hyd
   const unsigned blocks = (unsigned)((h.ncells + 255) / 256);
   pack_kernel<<<blocks, 256, 0, b->stream>>>(pk, n_prim, b->staging, b->d_ptrs);
   if (b->opts.eos == GVH_EOS_CONFORMAL)
-    init_conserved_kernel<EOS_CONFORMAL><<<blocks, 256, 0, b->stream>>>(h.ncells, b->nq, h.cs, qA, e, pA, u[0], u[1]);
+    init_conserved_kernel<EOS_CONFORMAL><<<blocks, 256, 0, b->stream>>>(h.ncells, b->nq, h.cs, qA, e, pA, u[0], u[1], 0);
   else
-    init_conserved_kernel<EOS_QCD><<<blocks, 256, 0, b->stream>>>(h.ncells, b->nq, h.cs, qA, e, pA, u[0], u[1]);
+    init_conserved_kernel<EOS_QCD><<<blocks, 256, 0, b->stream>>>(h.ncells, b->nq, h.cs, qA, e, pA, u[0], u[1], 0);
   BCUDA(cudaGetLastError());
   // initial freeze-out check (the reference tests the state before every step, the first
   // one included: HydroPlugin.cpp:396-408)

@@ -272,7 +272,7 @@ int gvh_get_state(gvh_handle *h, double *const *fields, int n_fields) {
   return GVH_OK;
 }
 
-int gvh_set_primitive_state(gvh_handle *h, const double *const *prim, int n_prim) {
+int gvh_set_primitive_state_p(gvh_handle *h, const double *const *prim, int n_prim, const double *p_ghosted) {
   if (!h || !prim) return fail(GVH_ERR_INVALID, "gvh_set_primitive_state: null argument");
   const int want = 5 + (h->nq - 4);
   if (n_prim != want) return fail(GVH_ERR_INVALID, "gvh_set_primitive_state: expected %d arrays", want);
@@ -283,24 +283,32 @@ int gvh_set_primitive_state(gvh_handle *h, const double *const *prim, int n_prim
   const size_t fb = h->ng * sizeof(double);
   for (int f = 0; f < n_prim; ++f)
     GVH_CUDA(cudaMemcpyAsync(h->staging + f * h->ng, prim[f], fb, cudaMemcpyDefault, h->stream));
+  if (p_ghosted)
+    GVH_CUDA(cudaMemcpyAsync(h->staging + n_prim * h->ng, p_ghosted, fb, cudaMemcpyDefault, h->stream));
   double *dst[32];
   dst[0] = h->e;
   for (int m = 0; m < 4; ++m) dst[1 + m] = h->u[h->ucur] + m * h->cs;
   for (int n = 4; n < h->nq; ++n) dst[5 + n - 4] = h->qA + n * h->cs;
+  dst[n_prim] = h->pA;
+  const int n_pack = n_prim + (p_ghosted ? 1 : 0);
   double **table = staging_ptr_table(h);
-  GVH_CUDA(cudaMemcpyAsync(table, dst, n_prim * sizeof(double *), cudaMemcpyHostToDevice, h->stream));
-  pack_kernel<<<(unsigned)((h->ncells + 255) / 256), 256, 0, h->stream>>>(make_pack(h), n_prim, h->staging, table);
+  GVH_CUDA(cudaMemcpyAsync(table, dst, n_pack * sizeof(double *), cudaMemcpyHostToDevice, h->stream));
+  pack_kernel<<<(unsigned)((h->ncells + 255) / 256), 256, 0, h->stream>>>(make_pack(h), n_pack, h->staging, table);
   GVH_CUDA(cudaGetLastError());
   const unsigned blocks = (unsigned)((h->ncells + 255) / 256);
   if (h->eos == GVH_EOS_CONFORMAL)
     init_conserved_kernel<EOS_CONFORMAL><<<blocks, 256, 0, h->stream>>>(h->ncells, h->nq, h->cs, h->qA, h->e, h->pA,
-                                                                        h->u[h->ucur], h->u[h->uprev]);
+                                                                        h->u[h->ucur], h->u[h->uprev], p_ghosted != nullptr);
   else
     init_conserved_kernel<EOS_QCD><<<blocks, 256, 0, h->stream>>>(h->ncells, h->nq, h->cs, h->qA, h->e, h->pA,
-                                                                  h->u[h->ucur], h->u[h->uprev]);
+                                                                  h->u[h->ucur], h->u[h->uprev], p_ghosted != nullptr);
   GVH_CUDA(cudaGetLastError());
   GVH_CUDA(cudaStreamSynchronize(h->stream));
   return GVH_OK;
+}
+
+int gvh_set_primitive_state(gvh_handle *h, const double *const *prim, int n_prim) {
+  return gvh_set_primitive_state_p(h, prim, n_prim, nullptr);
 }
 
 int gvh_rk2_step(gvh_handle *h, double t, double dt, double T_reg) {

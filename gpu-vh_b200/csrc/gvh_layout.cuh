@@ -48,12 +48,14 @@ __global__ void unpack_kernel(Pack p, int nf, const double *const *src, double *
 // T^{tau mu} from primitives (DynamicalVariables.cu:349-392 with EnergyMomentumTensor.cu
 // :159-177) and p = p(e) (InitialConditions.cpp:124-127), in the internal layout.
 template <int EOS>
+// p_given: the initial-condition reader supplied p (type 11, InitialConditions.cpp:29-97) and
+// p already holds it; otherwise p = p(e) of the EoS (type 10).
 __global__ void init_conserved_kernel(long long n, int nq, long long cs, double *q, double *e, double *p,
-                                      double *u, double *up) {
+                                      double *u, double *up, int p_given) {
   long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
   double es = e[s];
-  double ps = eq_pressure<EOS>(es);
+  double ps = p_given ? p[s] : eq_pressure<EOS>(es);
   p[s] = ps;
   double ut = u[s], ux = u[cs + s], uy = u[2 * cs + s], un = u[3 * cs + s];
   double pitt = 0, pitx = 0, pity = 0, pitn = 0, Pi = 0;

@@ -158,6 +158,47 @@ int gvh_read_ic_files(const char *root_dir, const gvh_lattice_params *L, int she
   return GVH_OK;
 }
 
+// setInitialTmunuFromFile (InitialConditions.cpp:29-97): one file <root>/input/Tmunu.dat, lines
+// "x y z e p ut ux uy un pitt pitx pity pitn pixx pixy pixn piyy piyn pinn Pi" scanned as floats,
+// i outermost and k innermost; e gets +1e-3; p is taken from the file; the dissipative
+// currents are kept when evolved.
+int gvh_read_ic_tmunu(const char *root_dir, const gvh_lattice_params *L, int shear, int bulk, double *const *prim,
+                      int n_prim, double *p_out) {
+  if (!root_dir || !L || !prim || !p_out) return pfail(GVH_ERR_INVALID, "null argument");
+  const int want = 5 + (shear ? 10 : 0) + (bulk ? 1 : 0);
+  if (n_prim != want) return pfail(GVH_ERR_INVALID, "wrong number of primitive arrays");
+  for (int f = 0; f < n_prim; ++f)
+    if (!prim[f]) return pfail(GVH_ERR_INVALID, "null primitive array");
+  const int nx = L->numLatticePointsX, ny = L->numLatticePointsY, nz = L->numLatticePointsRapidity;
+  const long long ng = (long long)(nx + 4) * (ny + 4) * (nz + 4);
+  for (int f = 0; f < n_prim; ++f) std::fill(prim[f], prim[f] + ng, 0.0);
+  std::fill(p_out, p_out + ng, 0.0);
+  const std::string path = std::string(root_dir) + "/input/Tmunu.dat";
+  FILE *fp = fopen(path.c_str(), "r");
+  if (!fp) return pfail(GVH_ERR_INVALID, "cannot open " + path);
+  for (int i = 2; i < nx + 2; ++i)
+    for (int j = 2; j < ny + 2; ++j)
+      for (int k = 2; k < nz + 2; ++k) {
+        float v[20];
+        int got = fscanf(fp, "%f %f %f %f %f %f %f %f %f %f %f %f %f %f %f %f %f %f %f %f", &v[0], &v[1], &v[2], &v[3],
+                         &v[4], &v[5], &v[6], &v[7], &v[8], &v[9], &v[10], &v[11], &v[12], &v[13], &v[14], &v[15],
+                         &v[16], &v[17], &v[18], &v[19]);
+        if (got != 20) {
+          fclose(fp);
+          return pfail(GVH_ERR_INVALID, "short or malformed file " + path);
+        }
+        const long long s = ghost_index(i, j, k, nx, ny);
+        prim[0][s] = (double)v[3] + 1.0e-3;
+        p_out[s] = (double)v[4];
+        for (int m = 0; m < 4; ++m) prim[1 + m][s] = (double)v[5 + m];
+        if (shear)
+          for (int m = 0; m < 10; ++m) prim[5 + m][s] = (double)v[9 + m];
+        if (bulk) prim[15][s] = (double)v[19];
+      }
+  fclose(fp);
+  return GVH_OK;
+}
+
 // FileIO.cpp:15-60: <dir>/<name>_<t %.3f>.dat, k outermost, "x y z value" lines.
 int gvh_write_field(const char *output_dir, const char *name, double t, const gvh_lattice_params *L,
                     const double *field) {
@@ -206,10 +247,11 @@ int gvh_run(const gvh_lattice_params *L, const gvh_ic_params *ic, const gvh_hydr
             const char *output_dir, const gvh_options *opts, int outputs, gvh_run_report *report) {
   g_plugin_error.clear();
   if (!L || !ic || !H || !root_dir) return pfail(GVH_ERR_INVALID, "null argument");
-  if (ic->initialConditionType != 10)
-    return pfail(GVH_ERR_INVALID, "gvh_run reads initial-condition type 10 (input/*.dat files); type " +
-                                      std::to_string(ic->initialConditionType) + " is generated by the reference's "
-                                      "own initial-condition code, which is outside this library");
+  const int ic_type = ic->initialConditionType;
+  if (ic_type != 10 && ic_type != 11)
+    return pfail(GVH_ERR_INVALID, "gvh_run reads initial-condition types 10 (input/*.dat files) and 11 "
+                                  "(input/Tmunu.dat); type " + std::to_string(ic_type) + " is generated by the "
+                                  "reference's own initial-condition code, which is outside this library");
   gvh_options o;
   if (opts) o = *opts; else gvh_default_options(&o);
   gvh_handle *h = nullptr;
@@ -221,8 +263,14 @@ int gvh_run(const gvh_lattice_params *L, const gvh_ic_params *ic, const gvh_hydr
   std::vector<std::vector<double>> prim(n_prim, std::vector<double>(ng));
   std::vector<double *> pp(n_prim);
   for (int f = 0; f < n_prim; ++f) pp[f] = prim[f].data();
-  rc = gvh_read_ic_files(root_dir, L, o.shear, o.bulk, pp.data(), n_prim);
-  if (!rc) rc = gvh_set_primitive_state(h, pp.data(), n_prim);
+  if (ic_type == 10) {
+    rc = gvh_read_ic_files(root_dir, L, o.shear, o.bulk, pp.data(), n_prim);
+    if (!rc) rc = gvh_set_primitive_state(h, pp.data(), n_prim);
+  } else {
+    std::vector<double> p_in(ng);
+    rc = gvh_read_ic_tmunu(root_dir, L, o.shear, o.bulk, pp.data(), n_prim, p_in.data());
+    if (!rc) rc = gvh_set_primitive_state_p(h, pp.data(), n_prim, p_in.data());
+  }
   if (rc) {
     std::string msg = g_plugin_error.empty() ? gvh_last_error() : g_plugin_error;
     gvh_destroy(h);

@@ -193,11 +193,20 @@ class Lattice:
         a = np.ascontiguousarray(np.broadcast_to(np.asarray(a, np.float64).reshape(-1), (self.ng,)))
         return a
 
-    def set_primitive(self, prim: dict):
+    def set_primitive(self, prim: dict, p=None):
+        """Initial state from primitives; p (ghosted) replaces p(e) of the EoS when given, as the
+        type-11 reader does."""
         order = ["e", "ut", "ux", "uy", "un"] + self.qnames[4:]
         arrs = [self._as_ghosted(prim.get(k, 0.0)) for k in order]
-        _check(self._L.gvh_set_primitive_state(self._h, _ptr_array([a.ctypes.data for a in arrs]), len(arrs)),
-               "gvh_set_primitive_state")
+        ptrs = _ptr_array([a.ctypes.data for a in arrs])
+        if p is None:
+            _check(self._L.gvh_set_primitive_state(self._h, ptrs, len(arrs)), "gvh_set_primitive_state")
+        else:
+            pa = self._as_ghosted(p)
+            self._L.gvh_set_primitive_state_p.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                                          ctypes.c_void_p]
+            _check(self._L.gvh_set_primitive_state_p(self._h, ptrs, len(arrs), pa.ctypes.data),
+                   "gvh_set_primitive_state_p")
 
     def set_state(self, state: dict):
         arrs = [None if state.get(k) is None else self._as_ghosted(state[k]) for k in self.field_names]

@@ -115,6 +115,10 @@ long long gvh_num_lattice_cells(const gvh_handle *h);
  * prim[1..4]=ut,ux,uy,un, then the evolved dissipative components (pitt..pinn, Pi).
  * Sets p = p(e), T^{tau mu} from (e, p, u, pi, Pi), u one step earlier = u. */
 int gvh_set_primitive_state(gvh_handle *h, const double *const *prim, int n_prim);
+/* The same with the pressure given (a ghosted array) instead of p(e) of the EoS, as the type-11
+ * reader sets it from its file (InitialConditions.cpp:60); T^{tau mu} is built with it
+ * (setConservedVariables, DynamicalVariables.cu:349-392). */
+int gvh_set_primitive_state_p(gvh_handle *h, const double *const *prim, int n_prim, const double *p_ghosted);
 int gvh_set_state(gvh_handle *h, const double *const *fields, int n_fields);
 /* Null entries are skipped. Ghost layers come back zero-gradient filled, edges and
  * corners included. Synchronises the handle's stream. */
@@ -289,17 +293,24 @@ int gvh_read_ic_parameters(const char *config_dir, gvh_ic_params *out);
 int gvh_read_ic_files(const char *root_dir, const gvh_lattice_params *lattice, int shear, int bulk,
                       double *const *prim, int n_prim);
 
+/* Initial-condition type 11 (setInitialTmunuFromFile, InitialConditions.cpp:29-97): reads
+ * <root>/input/Tmunu.dat (20 columns: x y z e p ut ux uy un pitt..pinn Pi) into ghosted arrays
+ * ordered as gvh_set_primitive_state takes them (e gets +1e-3) and the pressure into p_out;
+ * pass both to gvh_set_primitive_state_p. */
+int gvh_read_ic_tmunu(const char *root_dir, const gvh_lattice_params *lattice, int shear, int bulk,
+                      double *const *prim, int n_prim, double *p_out);
+
 /* One field dump in the reference's output format (output(), FileIO.cpp:15-60). */
 int gvh_write_field(const char *output_dir, const char *name, double tau, const gvh_lattice_params *lattice,
                     const double *field_ghosted);
 
-/* The run loop of run() (HydroPlugin.cpp:107-434) for initial-condition type 10: read the
+/* The run loop of run() (HydroPlugin.cpp:107-434) for initial-condition types 10 and 11: read the
  * input files, then for n = 1 .. numProperTimePoints+1: dump fields every 10 steps
  * (GVH_RUN_FIELDS), find the freeze-out surface of the last slab and write it to
  * <output_dir>/surface.dat in chunks of 10 steps as the reference does (GVH_RUN_SURFACE;
  * the reference writes output/surface.dat relative to its working directory), stop after 11
  * checks with every cell at or below e(T_fo), take one RK2 step. Other initial-condition
- * types return GVH_ERR_INVALID. */
+ * types (generated by the reference's own code) return GVH_ERR_INVALID. */
 int gvh_run(const gvh_lattice_params *lattice, const gvh_ic_params *ic, const gvh_hydro_params *hydro,
             const char *root_dir, const char *output_dir, const gvh_options *opts, int outputs,
             gvh_run_report *report);

@@ -202,6 +202,7 @@ class RefLattice(_Base):
         L.gvh_ref_rk2_step.argtypes = [ctypes.c_double] * 3
         for fn in ("gvh_ref_set_state", "gvh_ref_get_state", "gvh_ref_set_primitive_state"):
             getattr(L, fn).argtypes = [ctypes.c_void_p]
+        L.gvh_ref_set_primitive_state_p.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         for fn in ("gvh_ref_equilibrium_pressure", "gvh_ref_effective_temperature",
                    "gvh_ref_equilibrium_energy_density", "gvh_ref_speed_of_sound_squared"):
             getattr(L, fn).argtypes = [ctypes.c_double]
@@ -227,9 +228,14 @@ class RefLattice(_Base):
     def max_threads(self) -> int:
         return int(self._L.gvh_ref_max_threads())
 
-    def set_primitive(self, prim: dict):
+    def set_primitive(self, prim: dict, p=None):
+        """p: a ghosted pressure array to use instead of p(e) (the type-11 reader)."""
         arrs = self._prim_list(prim)  # keep the arrays alive across the call
-        self._L.gvh_ref_set_primitive_state(_ptrs(arrs))
+        if p is None:
+            self._L.gvh_ref_set_primitive_state(_ptrs(arrs))
+        else:
+            pa = np.ascontiguousarray(p, dtype=np.float64)
+            self._L.gvh_ref_set_primitive_state_p(_ptrs(arrs), pa.ctypes.data)
 
     def set_state(self, state: dict):
         arrs = self._field_list(state)

@@ -253,7 +253,14 @@ int gvh_ref_get_state(double *const *fields) {
  * p = equilibriumPressure(e) (InitialConditions.cpp type-10 reader), conserved T^{tau mu}
  * from setConservedVariables (DynamicalVariables.cu:349-392), up = u, then setGhostCells.
  * prim order: e, ut, ux, uy, un, then (if evolved) pitt..pinn, then (if evolved) Pi. */
-int gvh_ref_set_primitive_state(const double *const *prim) {
+static int set_primitive(const double *const *prim, const double *p_in);
+
+int gvh_ref_set_primitive_state(const double *const *prim) { return set_primitive(prim, nullptr); }
+
+/* Type 11 (setInitialTmunuFromFile, InitialConditions.cpp:29-97): p is read, not p(e). */
+int gvh_ref_set_primitive_state_p(const double *const *prim, const double *p_in) { return set_primitive(prim, p_in); }
+
+static int set_primitive(const double *const *prim, const double *p_in) {
 	if (!g_ng) return -1;
 	const int ncx = d_ncx, ncy = d_ncy;
 	PRECISION **c = slots(g_cur);
@@ -267,7 +274,7 @@ int gvh_ref_set_primitive_state(const double *const *prim) {
 			for (int i = 2; i < g_nx + 2; ++i) {
 				int s = columnMajorLinearIndex(i, j, k, ncx, ncy);
 				g_e[s] = (PRECISION)prim[0][s];
-				g_p[s] = equilibriumPressure(g_e[s]);
+				g_p[s] = p_in ? (PRECISION)p_in[s] : equilibriumPressure(g_e[s]);
 				g_u->ut[s] = (PRECISION)prim[1][s];
 				g_u->ux[s] = (PRECISION)prim[2][s];
 				g_u->uy[s] = (PRECISION)prim[3][s];
