@@ -175,6 +175,58 @@ __device__ __forceinline__ void qcd_p_cs2(double e, double &p, double &cs2) {
   cs2 = c / d;
 }
 
+// The four polynomials of the QCD fit, p = pa/pb and c_s^2 = ca/cb, without the divisions (the
+// Newton update below shares one reciprocal between them).
+__device__ __forceinline__ void qcd_poly(double e, double &pa, double &pb, double &ca, double &cb) {
+  double a = 1.9531729608963267e-11;
+  a = fma(a, e, 3.1188455176941583e-7); a = fma(a, e, 0.0009417586777847889); a = fma(a, e, 0.7158279081255019);
+  a = fma(a, e, 141.5073484468774); a = fma(a, e, 6340.448389300905); a = fma(a, e, 41913.439282708554);
+  a = fma(a, e, 334334.4309240126); a = fma(a, e, 1.6357487344679043e6); a = fma(a, e, 3.1729694865420084e6);
+  a = fma(a, e, 1.077580993288114e6); a = fma(a, e, 9737.845799644809); a = fma(a, e, -0.25181736420168666);
+  double b = 3.2581066229887368e-18;
+  b = fma(b, e, 5.928138360995685e-11); b = fma(b, e, 9.601103399348206e-7); b = fma(b, e, 0.002962497695527404);
+  b = fma(b, e, 2.3405487982094204); b = fma(b, e, 499.04919730607065); b = fma(b, e, 26452.34905933697);
+  b = fma(b, e, 278581.2989342773); b = fma(b, e, 1.7851642641834426e6); b = fma(b, e, 1.3512402226067686e7);
+  b = fma(b, e, 2.0931169138134286e7); b = fma(b, e, 4.0574329080826794e6); b = fma(b, e, 45829.44617893836);
+  double c = 8.189430244031285e-6;
+  c = fma(c, e, 0.03009027913262399); c = fma(c, e, 6.504847576502024); c = fma(c, e, 58.60283714484669);
+  c = fma(c, e, 275.0492627924299); c = fma(c, e, 1612.4245252438795); c = fma(c, e, 460.6487249985994);
+  c = fma(c, e, 15.382615282179595); c = fma(c, e, 0.02969737949090831); c = fma(c, e, 6.087136671592452e-6);
+  c = fma(c, e, 1.4170364808063119e-10); c = fma(c, e, 3.1955868410879504e-16);
+  c = fma(c, e, 4.123605749683891e-23); c = fma(c, e, 5.191934309650155e-32);
+  double d = 0.000024810902623582917;
+  d = fma(d, e, 0.09301685073435291); d = fma(d, e, 21.461303090563028); d = fma(d, e, 293.99144775704605);
+  d = fma(d, e, 590.2572000057821); d = fma(d, e, 15190.225535036281); d = fma(d, e, 1800.5461219450308);
+  d = fma(d, e, 60.85769171450653); d = fma(d, e, 0.13653226327408863); d = fma(d, e, 0.00003551782901018317);
+  d = fma(d, e, 1.1225580509306008e-9); d = fma(d, e, 3.5477700458515908e-15);
+  d = fma(d, e, 6.716598285341542e-22); d = fma(d, e, 1.4637868900982493e-30);
+  pa = a; pb = b; ca = c; cb = d;
+}
+
+// The Newton update of EnergyMomentumTensor.cu:22-40 at an iterate e0 where the fit's
+// polynomials are pa, pb (p = pa/pb) and ca, cb (c_s^2 = ca/cb). The reference's six
+// divisions (p, c_s^2, p/e0, D, f', f/f') become two: one reciprocal R = 1/(pa cb pb e0)
+// gives 1/pa, 1/cb and 1/(pb e0) by multiplication, and f/f' = f H / (H - X) with
+// X = g (...) pb / pa folds the division by p H into the last one. Equal to rounding.
+__device__ __forceinline__ double newton_update_poly(double e0, double pa, double pb, double ca, double cb, double M0,
+                                                     double M, double Pi, bool damped) {
+  const double be = pb * e0;
+  const double R = 1.0 / (pa * cb * be);
+  const double inv_pa = cb * be * R;
+  const double inv_be = pa * cb * R;
+  const double cst2 = pa * inv_be;        // p / e0
+  const double cs2 = ca * (pa * be * R);  // ca / cb
+  const double inv_e0 = pb * inv_be;
+  const double A = fma(M0, 1 - cst2, Pi);
+  const double B = fma(M0, M0 + Pi, -M);
+  const double H = sqrt(fabs(A * A + 4 * cst2 * B));
+  const double D = (A - H) * (0.5 * be * inv_pa);  // (A - H) / (2 cst2)
+  const double f = e0 + D;
+  const double g = cs2 - cst2;
+  const double X = (g * (B + D * H - (g * cst2 * D * M0) * inv_e0)) * (pb * inv_pa);  // f' = 1 - X / H
+  return e0 - ((damped ? 0.9 * f : f) * H) / (H - X);
+}
+
 // The QCD fit at the Newton guess. Every solve of one cell starts from the same guess (the
 // cell's energy density), so the first iteration's p and c_s^2 are computed once per cell.
 struct GuessEos {
@@ -240,9 +292,9 @@ __device__ __forceinline__ void energy_from_conserved_n(const GuessEos &g0, cons
 #pragma unroll
     for (int n = 0; n < N; ++n) {
       if (done[n]) continue;
-      double p, cs2;
-      qcd_p_cs2(e0[n], p, cs2);
-      double e = newton_update(e0[n], 1.0 / e0[n], p, cs2, M0[n], M[n], Pi[n], damped);
+      double pa, pb, ca, cb;
+      qcd_poly(e0[n], pa, pb, ca, cb);
+      double e = newton_update_poly(e0[n], pa, pb, ca, cb, M0[n], M[n], Pi[n], damped);
       done[n] = fabs(e - e0[n]) <= 0.001 * fabs(e);
       e0[n] = e;
       out[n] = e;
@@ -321,11 +373,11 @@ __device__ __forceinline__ void inferred_face_n(double t, int axis, const double
     double p = eq_pressure<EOS>(e[n]);
     double en = e[n];
     if (en < 1.e-7) { en = 1.e-7; p = 1.e-7; }
+    // u^axis/u^tau = M_axis E / ut^2 with ut^2 = |(M0 + P) E|, E = 1/(e + P)
+    // (EnergyMomentumTensor.cu:95-104 without the square root; equal to rounding)
     double P = p + Pi[n];
     double E = 1 / (en + P);
-    double ut = sqrt(fabs((M0[n] + P) * E));
-    double E2 = E / ut;
-    w[n] = (Mi[n] * E2) / ut;
+    w[n] = (Mi[n] * E) / fabs((M0[n] + P) * E);
   }
 }
 

@@ -204,7 +204,7 @@ __device__ __forceinline__ void axis_update(const StageArgs &a, int s, int axis,
 }
 
 #ifndef GVH_MIN_BLOCKS
-#define GVH_MIN_BLOCKS 3
+#define GVH_MIN_BLOCKS 4
 #endif
 // MIXED = false: plain FP64. MIXED = true: limiter, KT fluxes and source-term algebra in
 // FP32; the state, every primitive-variable recovery (face states and cell centre), the
