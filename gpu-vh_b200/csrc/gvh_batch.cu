@@ -22,6 +22,7 @@
 #include <string.h>
 
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -234,10 +235,11 @@ int launch_step_t(gvh_batch *b) {
   // cost; measured 2.3-2.5x faster than a persistent grid of 3 blocks per SM on 8-24
   // events); otherwise a persistent grid of that many blocks
   const int g = b->grid > 0 ? b->grid : (b->ntiles > 0 ? b->ntiles : 1);
-  batch_stage_kernel<EOS, SHEAR, BULK, false, MIXED><<<g, kBlock, 0, b->stream>>>(b->d_ev, b->d_tile_event,
-                                                                                  b->d_ntiles);
-  batch_stage_kernel<EOS, SHEAR, BULK, true, MIXED><<<g, kBlock, 0, b->stream>>>(b->d_ev, b->d_tile_event,
-                                                                                 b->d_ntiles);
+  const size_t smem = stage_smem_bytes<SHEAR, BULK>();
+  batch_stage_kernel<EOS, SHEAR, BULK, false, MIXED><<<g, kBlock, smem, b->stream>>>(b->d_ev, b->d_tile_event,
+                                                                                     b->d_ntiles);
+  batch_stage_kernel<EOS, SHEAR, BULK, true, MIXED><<<g, kBlock, smem, b->stream>>>(b->d_ev, b->d_tile_event,
+                                                                                    b->d_ntiles);
   batch_finish_kernel<<<(kMaxEvents + 127) / 128, 128, 0, b->stream>>>(b->d_ev, kMaxEvents);
   BCUDA(cudaGetLastError());
   return GVH_OK;
@@ -323,6 +325,28 @@ int gvh_batch_create(const gvh_options *opts, long long arena_bytes, gvh_batch *
   int dev = o.device;
   if (dev < 0) BCUDA(cudaGetDevice(&dev));
   BCUDA(cudaSetDevice(dev));
+  {
+    // the batched stage kernels' shared-memory limit, once per device, before any capture
+    static std::mutex mu;
+    static unsigned long long prepared = 0;
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev < 64 && !(prepared & (1ull << dev))) {
+      cudaError_t e = cudaSuccess;
+#define GVH_ALLOW_B(EOS_, SH, BU, MX)                                                                           \
+  if (e == cudaSuccess)                                                                                         \
+    e = allow_stage_smem(batch_stage_kernel<EOS_, SH, BU, false, MX>, stage_smem_bytes<SH, BU>());             \
+  if (e == cudaSuccess) e = allow_stage_smem(batch_stage_kernel<EOS_, SH, BU, true, MX>, stage_smem_bytes<SH, BU>());
+      GVH_ALLOW_B(EOS_QCD, false, false, false) GVH_ALLOW_B(EOS_QCD, true, false, false)
+      GVH_ALLOW_B(EOS_QCD, true, true, false) GVH_ALLOW_B(EOS_CONFORMAL, false, false, false)
+      GVH_ALLOW_B(EOS_CONFORMAL, true, false, false) GVH_ALLOW_B(EOS_CONFORMAL, true, true, false)
+      GVH_ALLOW_B(EOS_QCD, false, false, true) GVH_ALLOW_B(EOS_QCD, true, false, true)
+      GVH_ALLOW_B(EOS_QCD, true, true, true) GVH_ALLOW_B(EOS_CONFORMAL, false, false, true)
+      GVH_ALLOW_B(EOS_CONFORMAL, true, false, true) GVH_ALLOW_B(EOS_CONFORMAL, true, true, true)
+#undef GVH_ALLOW_B
+      if (e != cudaSuccess) return bfail(GVH_ERR_CUDA, "stage kernel set-up: %s", cudaGetErrorString(e));
+      prepared |= 1ull << dev;
+    }
+  }
   gvh_batch *b = new gvh_batch();
   b->opts = o;
   b->device = dev;

@@ -18,6 +18,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <mutex>
 #include <string>
 
 #include "../../include/gvh.h"
@@ -58,8 +59,9 @@ namespace {
 template <int EOS, bool SHEAR, bool BULK, bool MIXED>
 int launch_stage_p(const gvh_handle *h, const StageArgs &a, bool stage2) {
   const long long blocks = (h->ncells + kThreads - 1) / kThreads;
-  if (stage2) kt_stage_kernel<EOS, SHEAR, BULK, true, MIXED><<<(unsigned)blocks, kThreads, 0, h->stream>>>(a);
-  else kt_stage_kernel<EOS, SHEAR, BULK, false, MIXED><<<(unsigned)blocks, kThreads, 0, h->stream>>>(a);
+  const size_t smem = stage_smem_bytes<SHEAR, BULK>();
+  if (stage2) kt_stage_kernel<EOS, SHEAR, BULK, true, MIXED><<<(unsigned)blocks, kThreads, smem, h->stream>>>(a);
+  else kt_stage_kernel<EOS, SHEAR, BULK, false, MIXED><<<(unsigned)blocks, kThreads, smem, h->stream>>>(a);
   GVH_CUDA(cudaGetLastError());
   return GVH_OK;
 }
@@ -170,6 +172,16 @@ int gvh_create(const gvh_lattice_params *L, const gvh_hydro_params *H, const gvh
   int dev = o.device;
   if (dev < 0) GVH_CUDA(cudaGetDevice(&dev));
   GVH_CUDA(cudaSetDevice(dev));
+  {
+    // the stage kernels' shared-memory limit, once per device (kernel attributes are per device)
+    static std::mutex mu;
+    static unsigned long long prepared = 0;
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev < 64 && !(prepared & (1ull << dev))) {
+      GVH_CUDA(allow_all_stage_kernels());
+      prepared |= 1ull << dev;
+    }
+  }
 
   gvh_handle *h = new gvh_handle();
   memset(h, 0, sizeof(*h));

@@ -14,8 +14,9 @@
 // Rules of use:
 //  * the lattice must fit the array: (nq + 5) * 8 bytes per interior cell plus 256; larger
 //    lattices are rejected with GVH_ERR_INVALID and nothing runs;
-//  * the first call on a device looks up the array's device address (once per device, with
-//    that device current); make that first call before any stream capture;
+//  * the first call on a device looks up the array's device address and raises the stage
+//    kernels' shared-memory limit (once per device, with that device current); make that
+//    first call before any stream capture;
 //  * every call shares the one array and it keeps the last call's contents: the status word
 //    is cleared at the start of each call, and two calls whose work overlaps on the GPU
 //    (different streams, or host threads without ordering) race on it -- order them.
@@ -68,6 +69,10 @@ int scratch_address(int dev, unsigned char **out) {
       cudaError_t err = cudaGetSymbolAddress(reinterpret_cast<void **>(&p), g_noalloc_scratch);
       if (err != cudaSuccess)
         return nfail(GVH_ERR_CUDA, "cudaGetSymbolAddress(scratch) on device %d: %s", dev, cudaGetErrorString(err));
+      // the stage kernels' shared-memory limit, part of the same one-time set-up
+      err = allow_all_stage_kernels();
+      if (err != cudaSuccess)
+        return nfail(GVH_ERR_CUDA, "stage kernel set-up on device %d: %s", dev, cudaGetErrorString(err));
       g_scratch_ptr[dev].store(p, std::memory_order_release);
     }
   }
@@ -78,8 +83,9 @@ int scratch_address(int dev, unsigned char **out) {
 template <int EOS, bool SHEAR, bool BULK, bool MIXED>
 void launch_pair(const StageArgs &a1, const StageArgs &a2, long long n, cudaStream_t st) {
   const unsigned blocks = (unsigned)((n + kBlock - 1) / kBlock);
-  kt_stage_kernel<EOS, SHEAR, BULK, false, MIXED><<<blocks, kBlock, 0, st>>>(a1);
-  kt_stage_kernel<EOS, SHEAR, BULK, true, MIXED><<<blocks, kBlock, 0, st>>>(a2);
+  const size_t smem = stage_smem_bytes<SHEAR, BULK>();
+  kt_stage_kernel<EOS, SHEAR, BULK, false, MIXED><<<blocks, kBlock, smem, st>>>(a1);
+  kt_stage_kernel<EOS, SHEAR, BULK, true, MIXED><<<blocks, kBlock, smem, st>>>(a2);
 }
 
 template <int EOS, bool MIXED>

@@ -82,9 +82,11 @@ struct FaceSpeeds {
 // Phase A. Half-cell states (HalfSiteExtrapolation.cu:15-30) of the root-find components
 // at both faces, then primitive recovery of all four (SemiDiscreteKurganovTadmorScheme.cu
 // :41-44) with the cell's own energy density as guess.
+// The half-cell states also go to this thread's column of the shared-memory cache
+// (cache[(4 r + f) * kBlock]), from which phase B takes them instead of recomputing them.
 template <int EOS, bool SHEAR, bool BULK>
 __device__ __forceinline__ FaceSpeeds<double> face_speeds(const StageArgs &a, int s, int axis, const int (&o)[5],
-                                                       const GuessEos &g0, unsigned &status) {
+                                                       const GuessEos &g0, double *cache, unsigned &status) {
   // index 0: fwd R, 1: fwd L, 2: bwd R, 3: bwd L
   double st[9][4];
   constexpr int NR = 4 + (SHEAR ? 4 : 0) + (BULK ? 1 : 0);
@@ -100,6 +102,8 @@ __device__ __forceinline__ FaceSpeeds<double> face_speeds(const StageArgs &a, in
     st[r][1] = q2 + D0 / 2;   // fwd qL
     st[r][2] = q2 - D0 / 2;   // bwd qR
     st[r][3] = q1 + Dm / 2;   // bwd qL
+#pragma unroll
+    for (int f = 0; f < 4; ++f) cache[(4 * r + f) * kBlock] = st[r][f];
   }
 #pragma unroll
   for (int r = NR; r < 9; ++r)
@@ -121,6 +125,16 @@ __device__ __forceinline__ FaceSpeeds<double> face_speeds(const StageArgs &a, in
 __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
 
+// -H(i+1/2) + H(i-1/2) from the four half-cell states (fwd qR, fwd qL, bwd qR, bwd qL).
+template <class R>
+__device__ __forceinline__ R flux_from_states(R fR, R fL, R bR, R bL, const FaceSpeeds<R> &f) {
+  // F(qR) and F(qL) are rounded separately (no fused multiply-add across the pair), which
+  // keeps the scheme exactly mirror-symmetric.
+  const R Hf = (mul_rn(fR, f.wRf) + mul_rn(fL, f.wLf) - f.af * (fR - fL)) * R(0.5);
+  const R Hb = (mul_rn(bR, f.wRb) + mul_rn(bL, f.wLb) - f.ab * (bR - bL)) * R(0.5);
+  return -Hf + Hb;
+}
+
 template <class R>
 __device__ __forceinline__ R flux_difference(R theta, const double *q, const int (&o)[5], const FaceSpeeds<R> &f) {
   const R q0 = (R)__ldg(q + o[0]), q1 = (R)__ldg(q + o[1]), q2 = (R)__ldg(q), q3 = (R)__ldg(q + o[3]);
@@ -128,13 +142,7 @@ __device__ __forceinline__ R flux_difference(R theta, const double *q, const int
   const R Dm = limited_slope(theta, q0, q1, q2);
   const R D0 = limited_slope(theta, q1, q2, q3);
   const R Dp = limited_slope(theta, q2, q3, q4);
-  const R fR = q3 - Dp / R(2), fL = q2 + D0 / R(2);
-  const R bR = q2 - D0 / R(2), bL = q1 + Dm / R(2);
-  // F(qR) and F(qL) are rounded separately (no fused multiply-add across the pair), which
-  // keeps the scheme exactly mirror-symmetric.
-  const R Hf = (mul_rn(fR, f.wRf) + mul_rn(fL, f.wLf) - f.af * (fR - fL)) * R(0.5);
-  const R Hb = (mul_rn(bR, f.wRb) + mul_rn(bL, f.wLb) - f.ab * (bR - bL)) * R(0.5);
-  return -Hf + Hb;
+  return flux_from_states<R>(q3 - Dp / R(2), q2 + D0 / R(2), q2 - D0 / R(2), q1 + Dm / R(2), f);
 }
 
 // pi^{m a} component index for spatial m, a in {x, y, eta}.
@@ -178,7 +186,7 @@ __device__ __forceinline__ void axis_pi_sources(const StageArgs &a, int s, int a
 template <int EOS, bool SHEAR, bool BULK, bool MIXED>
 __device__ __forceinline__ void axis_update(const StageArgs &a, int s, int axis, int idx, int n_axis, int stride,
                                             double d, const GuessEos &g0, const double *uc, double *out,
-                                            unsigned &status) {
+                                            double *cache, unsigned &status) {
   using R = typename std::conditional<MIXED, float, double>::type;
   constexpr int NQ = NComp<SHEAR, BULK>::value;
   const int o[5] = {(max(idx - 2, 0) - idx) * stride, (max(idx - 1, 0) - idx) * stride, 0,
@@ -187,7 +195,7 @@ __device__ __forceinline__ void axis_update(const StageArgs &a, int s, int axis,
   // Face states are recovered in FP64 on both paths (the mixed path rounds only the
   // resulting speeds): an FP32 recovery was tried and let a 2+1D hotspot event run away
   // to NaN that the FP64 recovery keeps finite.
-  const FaceSpeeds<double> fd = face_speeds<EOS, SHEAR, BULK>(a, s, axis, o, g0, status);
+  const FaceSpeeds<double> fd = face_speeds<EOS, SHEAR, BULK>(a, s, axis, o, g0, cache, status);
   FaceSpeeds<R> f;
   f.wRf = (R)fd.wRf; f.wLf = (R)fd.wLf; f.wRb = (R)fd.wRb; f.wLb = (R)fd.wLb;
   f.af = (R)fd.af; f.ab = (R)fd.ab;
@@ -197,10 +205,26 @@ __device__ __forceinline__ void axis_update(const StageArgs &a, int s, int axis,
   const R th = (R)a.theta;
 #pragma unroll 1
   for (int n = 0; n < NQ; ++n) {
-    R r = flux_difference<R>(th, a.qin + (size_t)n * a.cs + s, o, f) * inv_d;
+    // T^{tau mu}, pi^{tau mu} and Pi: the states phase A cached; pi^{ij}: from the lattice
+    const int r_cached = n < 8 ? n : (BULK && n == NQ - 1) ? 8 : -1;
+    R r;
+    if (r_cached >= 0) {
+      const double *c = cache + 4 * r_cached * kBlock;
+      r = flux_from_states<R>((R)c[0], (R)c[kBlock], (R)c[2 * kBlock], (R)c[3 * kBlock], f);
+    } else {
+      r = flux_difference<R>(th, a.qin + (size_t)n * a.cs + s, o, f);
+    }
+    r = r * inv_d;
     if (SHEAR && n < 4) r += Sa[n];
     out[n * kBlock] += (double)r * a.dt;
   }
+}
+
+// Shared memory of one stage block: the running update (NQ per thread) and the half-cell
+// state cache (4 per root-find component per thread), in doubles.
+template <bool SHEAR, bool BULK>
+constexpr size_t stage_smem_bytes() {
+  return (size_t)(NComp<SHEAR, BULK>::value + 4 * (4 + (SHEAR ? 4 : 0) + (BULK ? 1 : 0))) * kBlock * sizeof(double);
 }
 
 #ifndef GVH_MIN_BLOCKS
@@ -384,11 +408,12 @@ __device__ __forceinline__ double stage_cell(const StageArgs &a, long long id) {
 #pragma unroll
   for (int m = 0; m < 4; ++m) uc[m] = __ldg(a.uin + m * a.cs + s);
 
-  // The running update of each component lives in shared memory (this thread's column of
-  // s_out): it is read-modified-written once per axis, and keeping it out of registers
-  // leaves them to the Newton solves and the source algebra.
-  __shared__ double s_out[NQ * kBlock];
-  double *out = s_out + threadIdx.x;
+  // The running update of each component lives in shared memory (this thread's column): it
+  // is read-modified-written once per axis, and keeping it out of registers leaves them to
+  // the Newton solves and the source algebra. The half-cell state cache follows it.
+  extern __shared__ double gvh_stage_smem[];
+  double *out = gvh_stage_smem + threadIdx.x;
+  double *cache = gvh_stage_smem + NQ * kBlock + threadIdx.x;
 
   stage_source<EOS, SHEAR, BULK, MIXED, kBlock>(a, s, i, j, k, ePrev, uc, out);
 
@@ -400,17 +425,43 @@ __device__ __forceinline__ double stage_cell(const StageArgs &a, long long id) {
     const int n_axis = axis == 0 ? a.nx : axis == 1 ? a.ny : a.nz;
     const int stride = axis == 0 ? 1 : axis == 1 ? (int)a.sy : (int)a.sz;
     const double d = axis == 0 ? a.dx : axis == 1 ? a.dy : a.dz;
-    axis_update<EOS, SHEAR, BULK, MIXED>(a, (int)s, axis, idx, n_axis, stride, d, g0, uc, out, status);
+    axis_update<EOS, SHEAR, BULK, MIXED>(a, (int)s, axis, idx, n_axis, stride, d, g0, uc, out, cache, status);
   }
 
   return stage_finish<EOS, SHEAR, BULK, STAGE2, kBlock>(a, s, out, g0, status);
 }
 
-// One RK substep over one lattice: one thread per interior cell.
+// One RK substep over one lattice: one thread per interior cell. Launch with
+// stage_smem_bytes<SHEAR, BULK>() of dynamic shared memory (above the 48 KB default: the
+// launcher raises the kernel's cudaFuncAttributeMaxDynamicSharedMemorySize first).
 template <int EOS, bool SHEAR, bool BULK, bool STAGE2, bool MIXED>
 __global__ void __launch_bounds__(kBlock, GVH_MIN_BLOCKS) kt_stage_kernel(const StageArgs a) {
   const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (id < a.ncells) stage_cell<EOS, SHEAR, BULK, STAGE2, MIXED>(a, id);
+}
+
+// Raises a stage kernel's dynamic shared-memory limit to what it is launched with. A kernel
+// template instantiated in several translation units has one copy in each, so each file that
+// launches one calls this for its own copies (host only; done once per device, before any
+// stream capture).
+template <class Kernel>
+inline cudaError_t allow_stage_smem(Kernel *kernel, size_t bytes) {
+  return cudaFuncSetAttribute(reinterpret_cast<const void *>(kernel), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)bytes);
+}
+
+// All 24 kt_stage_kernel instantiations of the calling translation unit.
+inline cudaError_t allow_all_stage_kernels() {
+  cudaError_t e = cudaSuccess;
+#define GVH_ALLOW(EOS_, SH, BU)                                                                                \
+  if (e == cudaSuccess) e = allow_stage_smem(kt_stage_kernel<EOS_, SH, BU, false, false>, stage_smem_bytes<SH, BU>()); \
+  if (e == cudaSuccess) e = allow_stage_smem(kt_stage_kernel<EOS_, SH, BU, true, false>, stage_smem_bytes<SH, BU>());  \
+  if (e == cudaSuccess) e = allow_stage_smem(kt_stage_kernel<EOS_, SH, BU, false, true>, stage_smem_bytes<SH, BU>());  \
+  if (e == cudaSuccess) e = allow_stage_smem(kt_stage_kernel<EOS_, SH, BU, true, true>, stage_smem_bytes<SH, BU>());
+  GVH_ALLOW(EOS_QCD, false, false) GVH_ALLOW(EOS_QCD, true, false) GVH_ALLOW(EOS_QCD, true, true)
+  GVH_ALLOW(EOS_CONFORMAL, false, false) GVH_ALLOW(EOS_CONFORMAL, true, false) GVH_ALLOW(EOS_CONFORMAL, true, true)
+#undef GVH_ALLOW
+  return e;
 }
 
 }  // namespace gvh
