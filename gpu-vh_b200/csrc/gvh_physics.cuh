@@ -203,6 +203,22 @@ __device__ __forceinline__ void qcd_poly(double e, double &pa, double &pb, doubl
   pa = a; pb = b; ca = c; cb = d;
 }
 
+// The two polynomials of p = pa/pb alone.
+__device__ __forceinline__ void qcd_poly_p(double e, double &pa, double &pb) {
+  double a = 1.9531729608963267e-11;
+  a = fma(a, e, 3.1188455176941583e-7); a = fma(a, e, 0.0009417586777847889); a = fma(a, e, 0.7158279081255019);
+  a = fma(a, e, 141.5073484468774); a = fma(a, e, 6340.448389300905); a = fma(a, e, 41913.439282708554);
+  a = fma(a, e, 334334.4309240126); a = fma(a, e, 1.6357487344679043e6); a = fma(a, e, 3.1729694865420084e6);
+  a = fma(a, e, 1.077580993288114e6); a = fma(a, e, 9737.845799644809); a = fma(a, e, -0.25181736420168666);
+  double b = 3.2581066229887368e-18;
+  b = fma(b, e, 5.928138360995685e-11); b = fma(b, e, 9.601103399348206e-7); b = fma(b, e, 0.002962497695527404);
+  b = fma(b, e, 2.3405487982094204); b = fma(b, e, 499.04919730607065); b = fma(b, e, 26452.34905933697);
+  b = fma(b, e, 278581.2989342773); b = fma(b, e, 1.7851642641834426e6); b = fma(b, e, 1.3512402226067686e7);
+  b = fma(b, e, 2.0931169138134286e7); b = fma(b, e, 4.0574329080826794e6); b = fma(b, e, 45829.44617893836);
+  pa = a;
+  pb = b;
+}
+
 // The Newton update of EnergyMomentumTensor.cu:22-40 at an iterate e0 where the fit's
 // polynomials are pa, pb (p = pa/pb) and ca, cb (c_s^2 = ca/cb). The reference's six
 // divisions (p, c_s^2, p/e0, D, f', f/f') become two: one reciprocal R = 1/(pa cb pb e0)
@@ -231,6 +247,7 @@ __device__ __forceinline__ double newton_update_poly(double e0, double pa, doubl
 // cell's energy density), so the first iteration's p and c_s^2 are computed once per cell.
 struct GuessEos {
   double e, inv_e, p, cs2;
+  double inv_p, half_inv_cst2;  // 1/p and 1/(2 p/e): the first update's divisions, per cell
 };
 template <int EOS>
 __device__ __forceinline__ GuessEos guess_eos(double ePrev) {
@@ -240,27 +257,37 @@ __device__ __forceinline__ GuessEos guess_eos(double ePrev) {
   if (EOS == EOS_CONFORMAL) {
     g.p = 0.0;
     g.cs2 = 0.0;
+    g.inv_p = 0.0;
+    g.half_inv_cst2 = 0.0;
   } else {
     qcd_p_cs2(ePrev, g.p, g.cs2);
+    g.inv_p = 1.0 / g.p;
+    g.half_inv_cst2 = 0.5 * ePrev * g.inv_p;
   }
   return g;
 }
 
-// One Newton update of EnergyMomentumTensor.cu:22-40 (divisions by e0 and by cst2*e0*H =
-// p*H taken through a shared reciprocal / the product p*H; equal to rounding). damped
-// selects e0 - 0.9 f/f' (EnergyMomentumTensor.cu:38) over e0 - f/f'.
-__device__ __forceinline__ double newton_update(double e0, double inv_e0, double p, double cs2, double M0, double M,
-                                                double Pi, bool damped = false) {
-  double cst2 = p * inv_e0;
-  double A = fma(M0, 1 - cst2, Pi);
-  double B = fma(M0, M0 + Pi, -M);
-  double H = sqrt(fabs(A * A + 4 * cst2 * B));
-  double D = (A - H) / (2 * cst2);
-  double f = e0 + D;
-  double g = cs2 - cst2;
-  double fp = 1 - (g * (B + D * H - (g * cst2 * D * M0) * inv_e0)) / (p * H);
-  return damped ? e0 - (0.9 * f) / fp : e0 - f / fp;
+// The first Newton update, at the guess (every solve of a cell starts there): the same
+// update as newton_update with the guess's reciprocals taken from GuessEos, leaving one
+// division (f/f' = f H / (H - X / p)).
+__device__ __forceinline__ double newton_update_guess(const GuessEos &g, double M0, double M, double Pi) {
+  const double e0 = g.e;
+  const double cst2 = g.p * g.inv_e;
+  const double A = fma(M0, 1 - cst2, Pi);
+  const double B = fma(M0, M0 + Pi, -M);
+  const double H = sqrt(fabs(A * A + 4 * cst2 * B));
+  const double D = (A - H) * g.half_inv_cst2;
+  const double f = e0 + D;
+  const double gg = g.cs2 - cst2;
+  const double X = (gg * (B + D * H - (gg * cst2 * D * M0) * g.inv_e)) * g.inv_p;
+  return e0 - (f * H) / (H - X);
 }
+
+// The reference's Newton update (EnergyMomentumTensor.cu:22-40) at an iterate e0 with
+// cst2 = p/e0, A = M0 (1 - cst2) + Pi, B = M0 (M0 + Pi) - M, H = sqrt|A^2 + 4 cst2 B|,
+// D = (A - H) / (2 cst2), f = e0 + D, g = c_s^2 - cst2,
+// f' = 1 - g (B + D H - g cst2 D M0 / e0) / (p H), e <- e0 - f/f' (or - 0.9 f/f' damped),
+// is computed by newton_update_guess (first update) and newton_update_poly (the others).
 
 // N independent Newton solves (EnergyMomentumTensor.cu:18-48) iterated together: each
 // follows its own sequence of iterates and stops at its own iteration (|de| <= 1e-3 |e|),
@@ -279,7 +306,7 @@ __device__ __forceinline__ void energy_from_conserved_n(const GuessEos &g0, cons
   bool all = true;
 #pragma unroll
   for (int n = 0; n < N; ++n) {
-    double e = newton_update(g0.e, g0.inv_e, g0.p, g0.cs2, M0[n], M[n], Pi[n]);
+    double e = newton_update_guess(g0, M0[n], M[n], Pi[n]);
     done[n] = fabs(e - g0.e) <= 0.001 * fabs(e);
     e0[n] = e;
     out[n] = e;
@@ -370,14 +397,23 @@ __device__ __forceinline__ void inferred_face_n(double t, int axis, const double
 #pragma unroll
   for (int n = 0; n < N; ++n) {
     if (isnan(e[n])) status |= STATUS_NAN;
-    double p = eq_pressure<EOS>(e[n]);
+    // u^axis/u^tau = M_axis E / ut^2 with E = 1/(e + P) and ut^2 = |(M0 + P) E|
+    // (EnergyMomentumTensor.cu:95-104), i.e. M_axis sign(e + P) / |M0 + P|: with the QCD fit
+    // p = pa/pb (pb > 0) that is one division, M_axis pb sign(...) / |pb (M0 + Pi) + pa|.
     double en = e[n];
-    if (en < 1.e-7) { en = 1.e-7; p = 1.e-7; }
-    // u^axis/u^tau = M_axis E / ut^2 with ut^2 = |(M0 + P) E|, E = 1/(e + P)
-    // (EnergyMomentumTensor.cu:95-104 without the square root; equal to rounding)
-    double P = p + Pi[n];
-    double E = 1 / (en + P);
-    w[n] = (Mi[n] * E) / fabs((M0[n] + P) * E);
+    double num, den, side;
+    if (en < 1.e-7) {
+      const double P = 1.e-7 + Pi[n];
+      num = Mi[n]; den = M0[n] + P; side = 1.e-7 + P;
+    } else if (EOS == EOS_CONFORMAL) {
+      const double P = en / 3 + Pi[n];
+      num = Mi[n]; den = M0[n] + P; side = en + P;
+    } else {
+      double pa, pb;
+      qcd_poly_p(en, pa, pb);
+      num = Mi[n] * pb; den = fma(pb, M0[n] + Pi[n], pa); side = fma(pb, en + Pi[n], pa);
+    }
+    w[n] = (side < 0 ? -num : num) / fabs(den);
   }
 }
 
