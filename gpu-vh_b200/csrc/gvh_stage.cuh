@@ -82,15 +82,16 @@ struct FaceSpeeds {
 // Phase A. Half-cell states (HalfSiteExtrapolation.cu:15-30) of the root-find components
 // at both faces, then primitive recovery of all four (SemiDiscreteKurganovTadmorScheme.cu
 // :41-44) with the cell's own energy density as guess.
-// The half-cell states also go to this thread's column of the shared-memory cache
+// The half-cell states go to this thread's column of the shared-memory cache
 // (cache[(4 r + f) * kBlock]), from which phase B takes them instead of recomputing them.
 template <int EOS, bool SHEAR, bool BULK>
 __device__ __forceinline__ FaceSpeeds<double> face_speeds(const StageArgs &a, int s, int axis, const int (&o)[5],
                                                        const GuessEos &g0, double *cache, unsigned &status) {
-  // index 0: fwd R, 1: fwd L, 2: bwd R, 3: bwd L
-  double st[9][4];
+  // index f: 0 fwd R, 1 fwd L, 2 bwd R, 3 bwd L. The states go to the cache first; the four
+  // recoveries then read them back one at a time (runtime loops keep the code small:
+  // instruction fetch, not arithmetic, is what the long straight-line variant waited on).
   constexpr int NR = 4 + (SHEAR ? 4 : 0) + (BULK ? 1 : 0);
-#pragma unroll
+#pragma unroll 1
   for (int r = 0; r < NR; ++r) {
     const int c = (r < 8) ? r : 14;
     const double *q = a.qin + (size_t)c * a.cs + s;
@@ -98,20 +99,26 @@ __device__ __forceinline__ FaceSpeeds<double> face_speeds(const StageArgs &a, in
     const double Dm = limited_slope(a.theta, q0, q1, q2);
     const double D0 = limited_slope(a.theta, q1, q2, q3);
     const double Dp = limited_slope(a.theta, q2, q3, q4);
-    st[r][0] = q3 - Dp / 2;   // fwd qR
-    st[r][1] = q2 + D0 / 2;   // fwd qL
-    st[r][2] = q2 - D0 / 2;   // bwd qR
-    st[r][3] = q1 + Dm / 2;   // bwd qL
-#pragma unroll
-    for (int f = 0; f < 4; ++f) cache[(4 * r + f) * kBlock] = st[r][f];
+    double *cr = cache + 4 * r * kBlock;
+    cr[0] = q3 - Dp / 2;           // fwd qR
+    cr[kBlock] = q2 + D0 / 2;      // fwd qL
+    cr[2 * kBlock] = q2 - D0 / 2;  // bwd qR
+    cr[3 * kBlock] = q1 + Dm / 2;  // bwd qL
   }
+  double w[4] = {0, 0, 0, 0};
+#pragma unroll 1
+  for (int h = 0; h < 4; ++h) {
+    double st[9][1];
 #pragma unroll
-  for (int r = NR; r < 9; ++r)
-#pragma unroll
-    for (int f = 0; f < 4; ++f) st[r][f] = 0.0;
-  double w[4];
-  inferred_face_n<EOS, 4>(a.t_euler, axis, st[0], st[1], st[2], st[3], st[4], st[5], st[6], st[7], st[8], g0, w,
-                          status);
+    for (int r = 0; r < 9; ++r) st[r][0] = r < NR ? cache[(4 * r + h) * kBlock] : 0.0;
+    double w1[1];
+    inferred_face_n<EOS, 1>(a.t_euler, axis, st[0], st[1], st[2], st[3], st[4], st[5], st[6], st[7], st[8], g0, w1,
+                            status);
+    w[0] = h == 0 ? w1[0] : w[0];
+    w[1] = h == 1 ? w1[0] : w[1];
+    w[2] = h == 2 ? w1[0] : w[2];
+    w[3] = h == 3 ? w1[0] : w[3];
+  }
   FaceSpeeds<double> f;
   f.wRf = w[0]; f.wLf = w[1]; f.wRb = w[2]; f.wLb = w[3];
   f.af = fmax(fabs(f.wLf), fabs(f.wRf));
