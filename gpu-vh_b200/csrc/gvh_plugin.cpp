@@ -331,6 +331,13 @@ int gvh_run_loop(gvh_handle *h, const gvh_lattice_params *L, const gvh_hydro_par
   int frozen = 0;
   double t = t0;
   const int nt = L->numProperTimePoints;
+  cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
+  cudaSetDevice(h->device);
+  if (cudaEventCreate(&ev_begin) != cudaSuccess || cudaEventCreate(&ev_end) != cudaSuccess) {
+    gvh_surface_destroy(surf);
+    if (surf_file) fclose(surf_file);
+    return pfail(GVH_ERR_CUDA, "gvh_run_loop: event creation failed");
+  }
   for (int n = 1; n <= nt + 1; ++n) {
     if (dump_fields && output_dir && (n - 1) % kFreq == 0) {
       if (fields.empty()) {
@@ -350,16 +357,31 @@ int gvh_run_loop(gvh_handle *h, const gvh_lattice_params *L, const gvh_hydro_par
       gvh_write_field(output_dir, "ut", t, L, fp[base + 2]);
       for (int c = 4; c < nq; ++c) gvh_write_field(output_dir, qn[c], t, L, fp[c]);
     }
+    // The slab (n-2, n-1) is marked and copied now; its host half runs while the GPU takes
+    // the next step (the copies are queued on the handle's stream before it).
+    bool surf_pending = false;
+    long long flush = -1;
     if (surf && n >= 2) {
       const auto s0 = std::chrono::steady_clock::now();
-      const long long k = n - 2;  // slab between levels n-2 and n-1
       double label, scale;
-      long long flush;
-      gvh_surface_slab_labels(k, t0, dt, &label, &scale, &flush);
-      long long nel = 0;
-      if ((rc = gvh_surface_find(surf, label, scale, &nel))) {
+      gvh_surface_slab_labels(n - 2, t0, dt, &label, &scale, &flush);
+      if ((rc = gvh_surface_find_begin(surf, label, scale))) {
         g_plugin_error = gvh_surface_last_error();
         break;
+      }
+      surf_pending = true;
+      surf_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - s0).count();
+    }
+    // the host half, and the chunk written at the reference's iteration (HydroPlugin.cpp:287)
+    auto finish_surface = [&]() -> int {
+      if (!surf_pending) return GVH_OK;
+      surf_pending = false;
+      const auto s0 = std::chrono::steady_clock::now();
+      long long nel = 0;
+      int r = gvh_surface_find_end(surf, &nel);
+      if (r) {
+        g_plugin_error = gvh_surface_last_error();
+        return r;
       }
       gvh::surface::take_text(surf, chunk_text);
       chunk_rows += nel;
@@ -368,29 +390,42 @@ int gvh_run_loop(gvh_handle *h, const gvh_lattice_params *L, const gvh_hydro_par
         for (const std::string &part : chunk_text)
           ok = ok && fwrite(part.data(), 1, part.size(), surf_file) == part.size();
         if (!ok) {
-          rc = GVH_ERR_INVALID;
           g_plugin_error = "writing surface.dat failed";
-          break;
+          return GVH_ERR_INVALID;
         }
         surf_rows += chunk_rows;
         chunk_text.clear();
         chunk_rows = 0;
       }
       surf_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - s0).count();
-    }
+      return GVH_OK;
+    };
     double emax = 0.0;
     if ((rc = gvh_max_energy_density(h, &emax))) break;
     if (emax <= e_fo) ++frozen;
-    if (frozen >= kFreezeoutChecks) break;
-    // wall time of one step, as the reference's Stopwatch brackets twoStepRungeKutta
-    // (HydroPlugin.cpp:414-420)
-    const auto c0 = std::chrono::steady_clock::now();
-    if ((rc = gvh_rk2_step(h, t, dt, T_reg))) break;
-    if ((rc = gvh_synchronize(h))) break;
-    total_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - c0).count();
+    if (frozen >= kFreezeoutChecks) {
+      rc = finish_surface();
+      break;
+    }
+    // device time of one step (the reference's Stopwatch brackets twoStepRungeKutta,
+    // HydroPlugin.cpp:414-420), taken with events so the host half of the slab overlaps it
+    if (cudaEventRecord(ev_begin, h->stream) != cudaSuccess || (rc = gvh_rk2_step(h, t, dt, T_reg)) ||
+        cudaEventRecord(ev_end, h->stream) != cudaSuccess) {
+      if (!rc) rc = GVH_ERR_CUDA;
+      break;
+    }
+    if ((rc = finish_surface())) break;
+    float ms = 0.f;
+    if (cudaEventSynchronize(ev_end) != cudaSuccess || cudaEventElapsedTime(&ms, ev_begin, ev_end) != cudaSuccess) {
+      rc = GVH_ERR_CUDA;
+      break;
+    }
+    total_ms += ms;
     ++steps;
     t = t0 + n * dt;
   }
+  cudaEventDestroy(ev_begin);
+  cudaEventDestroy(ev_end);
   unsigned flags = 0;
   gvh_status(h, &flags);
   if (report) {

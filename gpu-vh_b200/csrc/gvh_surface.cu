@@ -259,6 +259,13 @@ struct gvh_surface {
   int outputs;       // gvh::surface::OUT_ROWS | OUT_TEXT
   gvh::surface::Result last;
   gvh_surface_info info;
+  // a slab between gvh_surface_find_begin and _end: its copies to the pinned buffers are in
+  // flight on the handle's stream, ordered before whatever the caller queues next
+  bool pending;
+  long long p_ncubes, p_npoints;
+  double p_label, p_scale;
+  cudaEvent_t copied;
+  std::chrono::steady_clock::time_point p_t0;
 };
 
 extern "C" {
@@ -313,6 +320,12 @@ int gvh_surface_create(gvh_handle *h, double e_freezeout, gvh_surface **out) {
     return sfail(GVH_ERR_NOMEM, "gvh_surface_create: cannot pin host memory");
   }
   memset(&s->info, 0, sizeof s->info);
+  if (cudaEventCreateWithFlags(&s->copied, cudaEventDisableTiming) != cudaSuccess) {
+    cudaFreeHost(s->h_totals);
+    cudaFree(s->dev);
+    delete s;
+    return sfail(GVH_ERR_CUDA, "gvh_surface_create: event creation failed");
+  }
   *out = s;
   return GVH_OK;
 }
@@ -322,6 +335,8 @@ int gvh_surface_destroy(gvh_surface *s) {
   // touches nothing of the handle, which may be gone already; cudaFree waits for the
   // device work that uses the buffers
   cudaSetDevice(s->device);
+  cudaEventSynchronize(s->copied);
+  cudaEventDestroy(s->copied);
   cudaFree(s->dev);
   cudaFreeHost(s->h_totals);
   if (s->h_cube_key) cudaFreeHost(s->h_cube_key);
@@ -364,12 +379,13 @@ int gvh_surface_set_lower(gvh_surface *s) {
   return GVH_OK;
 }
 
-int gvh_surface_find(gvh_surface *s, double tau_label, double tau_scale, long long *n_elements) {
-  if (!s) return sfail(GVH_ERR_INVALID, "gvh_surface_find: null argument");
-  if (!s->have_lower) return sfail(GVH_ERR_INVALID, "gvh_surface_find: no lower time level (gvh_surface_set_lower)");
+int gvh_surface_find_begin(gvh_surface *s, double tau_label, double tau_scale) {
+  if (!s) return sfail(GVH_ERR_INVALID, "gvh_surface_find_begin: null argument");
+  if (!s->have_lower) return sfail(GVH_ERR_INVALID, "gvh_surface_find_begin: no lower time level (gvh_surface_set_lower)");
+  if (s->pending) return sfail(GVH_ERR_INVALID, "gvh_surface_find_begin: the previous slab has not been ended");
   gvh_handle *h = s->h;
   SF_CUDA(cudaSetDevice(h->device));
-  const auto t0 = std::chrono::steady_clock::now();
+  s->p_t0 = std::chrono::steady_clock::now();
   const int upper = 1 - s->lower;
   int rc = snapshot(s, upper);
   if (rc) return rc;
@@ -396,9 +412,27 @@ int gvh_surface_find(gvh_surface *s, double tau_label, double tau_scale, long lo
     SF_CUDA(cudaMemcpyAsync(s->h_point_cell, s->point_cell, npoints * sizeof(int), cudaMemcpyDeviceToHost, st));
     SF_CUDA(cudaMemcpyAsync(s->h_point_vals, s->point_vals, npoints * 2 * kVars * sizeof(double),
                             cudaMemcpyDeviceToHost, st));
-    SF_CUDA(cudaStreamSynchronize(st));
   }
+  SF_CUDA(cudaEventRecord(s->copied, st));
+  s->lower = upper;
+  s->pending = true;
+  s->p_ncubes = ncubes;
+  s->p_npoints = npoints;
+  s->p_label = tau_label;
+  s->p_scale = tau_scale;
+  return GVH_OK;
+}
+
+int gvh_surface_find_end(gvh_surface *s, long long *n_elements) {
+  if (!s) return sfail(GVH_ERR_INVALID, "gvh_surface_find_end: null argument");
+  if (!s->pending) return sfail(GVH_ERR_INVALID, "gvh_surface_find_end: no slab begun");
+  gvh_handle *h = s->h;
+  SF_CUDA(cudaSetDevice(h->device));
+  s->pending = false;
+  SF_CUDA(cudaEventSynchronize(s->copied));
   const auto t1 = std::chrono::steady_clock::now();
+  const Geometry &g = s->g;
+  const long long ncubes = s->p_ncubes, npoints = s->p_npoints;
   gvh::surface::Slab slab;
   slab.dim = s->dim;
   slab.nx = g.nx; slab.ny = g.ny; slab.nz = g.nz;
@@ -411,10 +445,9 @@ int gvh_surface_find(gvh_surface *s, double tau_label, double tau_scale, long lo
   slab.point_cell = s->h_point_cell;
   slab.point_vals = s->h_point_vals;
   if (!s->pool) s->pool.reset(new gvh::surface::Pool(s->nthreads));
-  gvh::surface::process_slab(slab, gvh::surface::Labels{tau_label, tau_scale}, *s->pool, s->outputs, s->c2p,
+  gvh::surface::process_slab(slab, gvh::surface::Labels{s->p_label, s->p_scale}, *s->pool, s->outputs, s->c2p,
                              s->last);
   const auto t2 = std::chrono::steady_clock::now();
-  s->lower = upper;
   gvh_surface_info &in = s->info;
   in.slabs += 1;
   in.hypercubes_last = ncubes;
@@ -424,10 +457,16 @@ int gvh_surface_find(gvh_surface *s, double tau_label, double tau_scale, long lo
   in.elements_total += s->last.elements;
   in.errors_total += s->last.errors;
   in.bytes_to_host_total += (double)ncubes * 4 + (double)npoints * (4 + 2 * kVars * 8) + 8;
-  in.device_seconds_total += std::chrono::duration<double>(t1 - t0).count();
+  in.device_seconds_total += std::chrono::duration<double>(t1 - s->p_t0).count();
   in.host_seconds_total += std::chrono::duration<double>(t2 - t1).count();
   if (n_elements) *n_elements = s->last.elements;
   return GVH_OK;
+}
+
+int gvh_surface_find(gvh_surface *s, double tau_label, double tau_scale, long long *n_elements) {
+  int rc = gvh_surface_find_begin(s, tau_label, tau_scale);
+  if (rc) return rc;
+  return gvh_surface_find_end(s, n_elements);
 }
 
 int gvh_surface_get_rows(gvh_surface *s, double *rows, long long max_rows) {

@@ -377,6 +377,13 @@ int gvh_surface_set_lower(gvh_surface *s);
  * the lower one. tau_label is added to each element's centroid tau and tau_scale multiplies
  * its normal, as the reference labels its rows (HydroPlugin.cpp:298-314). */
 int gvh_surface_find(gvh_surface *s, double tau_label, double tau_scale, long long *n_elements);
+/* gvh_surface_find in two halves, so that the host half of one slab overlaps the device's
+ * next steps: _begin marks and compacts the slab on the device and queues the copies to the
+ * host on the handle's stream (later work the caller queues there, such as gvh_rk2_step,
+ * runs after them); _end waits for those copies and runs the host half. One slab at a time:
+ * _begin again before _end is an error. */
+int gvh_surface_find_begin(gvh_surface *s, double tau_label, double tau_scale);
+int gvh_surface_find_end(gvh_surface *s, long long *n_elements);
 /* The last slab's rows: n_elements x GVH_SURFACE_COLUMNS doubles, or as the text the
  * reference writes (ostream default format, space separated, one row per line). The text
  * stays valid until the next gvh_surface_find. */
