@@ -50,6 +50,9 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serving-sweep", default="1,16,50",
+                    help="offered request rates (req/s) of the serving sweep; empty to skip")
+    ap.add_argument("--serving-sweep-seconds", type=float, default=20.0)
     ap.add_argument("--no-surface", dest="surface", action="store_false",
                     help="skip the freeze-out surface extras (event to freeze-out with surface.dat, "
                          "mixed-vs-FP64 report)")
@@ -394,17 +397,19 @@ def precision_report(device):
     return report
 
 
-def serving_run(args, device):
+def serving_run(args, device, rate=None, seconds=None):
     from gvh import serve
 
+    rate = args.serving_rate if rate is None else rate
+    seconds = args.serving_seconds if seconds is None else seconds
     rng = np.random.default_rng(2024)
-    n_req = max(8, int(args.serving_rate * args.serving_seconds))
-    arrivals = serve.poisson_arrivals(args.serving_rate, n_req, rng)
+    n_req = max(8, int(rate * seconds))
+    arrivals = serve.poisson_arrivals(rate, n_req, rng)
     reqs = [serve.make_request(i, a, rng) for i, a in enumerate(arrivals)]
     srv = serve.Server(int(60 * (1 << 30)), precision="mixed", steps_per_round=10, device=device)
-    out = srv.run(reqs, time_limit=args.serving_seconds)
+    out = srv.run(reqs, time_limit=seconds)
     out.pop("steps", None)
-    out.update({"rate_per_s": args.serving_rate, "requests_offered": n_req, "precision": "mixed",
+    out.update({"rate_per_s": rate, "requests_offered": n_req, "precision": "mixed",
                 "mix": "grids {61x61x1 @0.2 fm, 101x101x31 @0.15, 131x131x61 @0.1}, b~U(0,12), eta/s~U(0.08,0.24)"})
     return out
 
@@ -559,6 +564,15 @@ def run_ours(args):
             sv = serving_run(args, local)
             sv["events_per_hour_vs_fp64_single_path"] = sv["events_per_hour"] / fp64_mix["events_per_hour"]
             extras["batched_mixed_serving"] = sv
+            # the offered-rate sweep of the serving configuration (1-50 req/s), shorter windows
+            sweep = []
+            for rate in [float(r) for r in args.serving_sweep.split(",") if r.strip()]:
+                r = serving_run(args, local, rate=rate, seconds=args.serving_sweep_seconds)
+                sweep.append({k: r.get(k) for k in ("rate_per_s", "requests_offered", "completed", "frozen_out",
+                                                    "elapsed_s", "events_per_hour", "p50_latency_s",
+                                                    "p99_latency_s", "cell_updates_per_s", "gpu_busy_fraction")})
+            if sweep:
+                extras["serving_rate_sweep"] = sweep
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
