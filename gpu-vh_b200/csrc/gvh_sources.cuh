@@ -42,6 +42,9 @@ __device__ __forceinline__ void pimunu_rhs(R *rhs, R t, R etabar, R e, R p, cons
   R beta_pi = R(kF02) * (e + p);
 
   R ut2 = ut * ut, un2 = un * un, t2 = t * t, t3 = t * t2;
+  // reciprocals of the divisors used below (the reference divides each time; equal to rounding)
+  const R it = dv(R(1), t), iut = dv(R(1), ut);
+  const R it2 = it * it, it3 = it2 * it;
   const R dtut = f.dtut, dtux = f.dtux, dtuy = f.dtuy, dtun = f.dtun;
 
   R Dut = ut * dtut + ux * dxut + uy * dyut + un * dnut + t * un * un;
@@ -53,21 +56,21 @@ __device__ __forceinline__ void pimunu_rhs(R *rhs, R t, R etabar, R e, R p, cons
   R dun = ut * dtun + ux * dxun + uy * dyun + un * dnun;
   R Dun = -t2 * dun - R(2.0) * t * ut * un;
 
-  R theta = dv(ut, t) + dtut + dxux + dyuy + dnun;
-  R theta3 = dv(theta, R(3.0));
+  R theta = (ut) * it + dtut + dxux + dyuy + dnun;
+  R theta3 = theta * R(1.0 / 3.0);
 
   // shear tensor sigma^{mu nu}
   R stt = -t * ut * un2 + (dtut - ut * dut) + (ut2 - R(1.0)) * theta3;
   R stx = -(t * un2 * ux) / R(2.0) + (dtux - dxut) / R(2.0) - (ux * dut + ut * dux) / R(2.0) + ut * ux * theta3;
   R sty = -(t * un2 * uy) / R(2.0) + (dtuy - dyut) / R(2.0) - (uy * dut + ut * duy) / R(2.0) + ut * uy * theta3;
-  R stn = dv(-un * (R(2.0) * ut2 + t2 * un2), R(2.0) * t) + (dtun - dv(dnut, t2)) / R(2.0) - (un * dut + ut * dun) / R(2.0)
+  R stn = (-un * (R(2.0) * ut2 + t2 * un2)) * (R(0.5) * it) + (dtun - dnut * it2) / R(2.0) - (un * dut + ut * dun) / R(2.0)
                + ut * un * theta3;
   R sxx = -(dxux + ux * dux) + (R(1.0) + ux * ux) * theta3;
   R sxy = -(dxuy + dyux) / R(2.0) - (uy * dux + ux * duy) / R(2.0) + ux * uy * theta3;
-  R sxn = dv(-ut * ux * un, t) - (dxun + dv(dnux, t2)) / R(2.0) - (un * dux + ux * dun) / R(2.0) + ux * un * theta3;
+  R sxn = (-ut * ux * un) * it - (dxun + dnux * it2) / R(2.0) - (un * dux + ux * dun) / R(2.0) + ux * un * theta3;
   R syy = -(dyuy + uy * duy) + (R(1.0) + uy * uy) * theta3;
-  R syn = dv(-ut * uy * un, t) - (dyun + dv(dnuy, t2)) / R(2.0) - (un * duy + uy * dun) / R(2.0) + uy * un * theta3;
-  R snn = dv(-ut * (R(1.0) + R(2.0) * t2 * un2), t3) - dv(dnun, t2) - un * dun + (dv(R(1.0), t2) + un2) * theta3;
+  R syn = (-ut * uy * un) * it - (dyun + dnuy * it2) / R(2.0) - (un * duy + uy * dun) / R(2.0) + uy * un * theta3;
+  R snn = (-ut * (R(1.0) + R(2.0) * t2 * un2)) * it3 - dnun * it2 - un * dun + (it2 + un2) * theta3;
 
   // vorticity (SourceTerms.cu:122-136)
   R wtx = (-dtux - dxut + ut * dux - ux * dut - t * un2 * ux) / R(2.0);
@@ -76,7 +79,7 @@ __device__ __forceinline__ void pimunu_rhs(R *rhs, R t, R etabar, R e, R p, cons
   R wxy = (dxuy - dyux + ux * duy - uy * dux) / R(2.0);
   R wxn = (t2 * dxun - dnux - ux * Dun - t2 * un * dux) / R(2.0);
   R wyn = (t2 * dyun - dnuy - uy * Dun - t2 * un * duy) / R(2.0);
-  R wxt = wtx, wyt = wty, wnt = dv(wtn, t2), wyx = -wxy, wnx = dv(-wxn, t2), wny = dv(-wyn, t2);
+  R wxt = wtx, wyt = wty, wnt = wtn * it2, wyx = -wxy, wnx = -wxn * it2, wny = -wyn * it2;
 
   // I1 (SourceTerms.cu:141-150)
   R I1tt = R(2.0) * ut * (pitt * Dut + pitx * Dux + pity * Duy + pitn * Dun);
@@ -112,7 +115,7 @@ __device__ __forceinline__ void pimunu_rhs(R *rhs, R t, R etabar, R e, R p, cons
   R ux2 = ux * ux, uy2 = uy * uy;
   R ps = pitt * stt - R(2.0) * pitx * stx - R(2.0) * pity * sty + pixx * sxx + R(2.0) * pixy * sxy + piyy * syy
               - R(2.0) * pitn * stn * t2 + R(2.0) * pixn * sxn * t2 + R(2.0) * piyn * syn * t2 + pinn * snn * t2 * t2;
-  R ps3 = dv(ps, R(3.0));
+  R ps3 = ps * R(1.0 / 3.0);
   R I4tt = (pitt * stt - pitx * stx - pity * sty - t2 * pitn * stn) - (1 - ut2) * ps3;
   R I4tx = (pitt * stx + pitx * stt) / R(2.0) - (pitx * sxx + pixx * stx) / R(2.0) - (pity * sxy + pixy * sty) / R(2.0)
                 - t2 * (pitn * sxn + pixn * stn) / R(2.0) + (ut * ux) * ps3;
@@ -128,7 +131,7 @@ __device__ __forceinline__ void pimunu_rhs(R *rhs, R t, R etabar, R e, R p, cons
   R I4yy = (pity * sty - pixy * sxy - piyy * syy - t2 * piyn * syn) + (R(1.0) + uy2) * ps3;
   R I4yn = (pity * stn + pitn * sty) / R(2.0) - (pixy * sxn + pixn * sxy) / R(2.0) - (piyy * syn + piyn * syy) / R(2.0)
                 - t2 * (piyn * snn + pinn * syn) / R(2.0) + (uy * un) * ps3;
-  R I4nn = (pitn * stn - pixn * sxn - piyn * syn - t2 * pinn * snn) + (dv(R(1.0), t2) + un2) * ps3;
+  R I4nn = (pitn * stn - pixn * sxn - piyn * syn - t2 * pinn * snn) + (it2 + un2) * ps3;
 
   // I = I1 + delta I2 - I3 + tau I4 - lambda Pi sigma (SourceTerms.cu:209-218); I2 = theta pi
   R Itt = I1tt + R(kDeltaPiPi) * (theta * pitt) - I3tt + R(kTauPiPi) * I4tt - R(kLambdaPiBulk) * Pi * stt;
@@ -146,24 +149,24 @@ __device__ __forceinline__ void pimunu_rhs(R *rhs, R t, R etabar, R e, R p, cons
   R dpitt = R(2.0) * beta_pi * stt - pitt * taupiInv - Itt - R(2.0) * un * t * pitn;
   R dpitx = R(2.0) * beta_pi * stx - pitx * taupiInv - Itx - un * t * pixn;
   R dpity = R(2.0) * beta_pi * sty - pity * taupiInv - Ity - un * t * piyn;
-  R dpitn = R(2.0) * beta_pi * stn - pitn * taupiInv - Itn - un * t * pinn - dv(ut * pitn + un * pitt, t);
+  R dpitn = R(2.0) * beta_pi * stn - pitn * taupiInv - Itn - un * t * pinn - (ut * pitn + un * pitt) * it;
   R dpixx = R(2.0) * beta_pi * sxx - pixx * taupiInv - Ixx;
   R dpixy = R(2.0) * beta_pi * sxy - pixy * taupiInv - Ixy;
-  R dpixn = R(2.0) * beta_pi * sxn - pixn * taupiInv - Ixn - dv(ut * pixn + un * pitx, t);
+  R dpixn = R(2.0) * beta_pi * sxn - pixn * taupiInv - Ixn - (ut * pixn + un * pitx) * it;
   R dpiyy = R(2.0) * beta_pi * syy - piyy * taupiInv - Iyy;
-  R dpiyn = R(2.0) * beta_pi * syn - piyn * taupiInv - Iyn - dv(ut * piyn + un * pity, t);
-  R dpinn = R(2.0) * beta_pi * snn - pinn * taupiInv - Inn - dv(R(2.0) * (ut * pinn + un * pitn), t);
+  R dpiyn = R(2.0) * beta_pi * syn - piyn * taupiInv - Iyn - (ut * piyn + un * pity) * it;
+  R dpinn = R(2.0) * beta_pi * snn - pinn * taupiInv - Inn - (R(2.0) * (ut * pinn + un * pitn)) * it;
 
-  rhs[0] = dv(dpitt, ut) + pitt * dkvk;
-  rhs[1] = dv(dpitx, ut) + pitx * dkvk;
-  rhs[2] = dv(dpity, ut) + pity * dkvk;
-  rhs[3] = dv(dpitn, ut) + pitn * dkvk;
-  rhs[4] = dv(dpixx, ut) + pixx * dkvk;
-  rhs[5] = dv(dpixy, ut) + pixy * dkvk;
-  rhs[6] = dv(dpixn, ut) + pixn * dkvk;
-  rhs[7] = dv(dpiyy, ut) + piyy * dkvk;
-  rhs[8] = dv(dpiyn, ut) + piyn * dkvk;
-  rhs[9] = dv(dpinn, ut) + pinn * dkvk;
+  rhs[0] = dpitt * iut + pitt * dkvk;
+  rhs[1] = dpitx * iut + pitx * dkvk;
+  rhs[2] = dpity * iut + pity * dkvk;
+  rhs[3] = dpitn * iut + pitn * dkvk;
+  rhs[4] = dpixx * iut + pixx * dkvk;
+  rhs[5] = dpixy * iut + pixy * dkvk;
+  rhs[6] = dpixn * iut + pixn * dkvk;
+  rhs[7] = dpiyy * iut + piyy * dkvk;
+  rhs[8] = dpiyn * iut + piyn * dkvk;
+  rhs[9] = dpinn * iut + pinn * dkvk;
   if (BULK) {
     // bulk coefficients (SourceTerms.cu:53-60, 238, 254)
     R cs2 = sound_speed2<EOS>(e);
@@ -174,7 +177,7 @@ __device__ __forceinline__ void pimunu_rhs(R *rhs, R t, R etabar, R e, R p, cons
     R zetabar = bulk_zeta_over_s(T);
     R tauPiInv = R(15) * a2 * dv(T, zetabar);
     R dPi = -beta_Pi * theta - Pi * tauPiInv - R(kDeltaBulk) * Pi * theta + lambda_Pipi * ps;
-    rhs[10] = dv(dPi, ut) + Pi * dkvk;
+    rhs[10] = dPi * iut + Pi * dkvk;
   }
 }
 

@@ -266,10 +266,11 @@ __device__ __forceinline__ void stage_source(const StageArgs &a, long long s, in
   for (int m = 0; m < 4; ++m) ucr[m] = (R)uc[m];
   f.ut = ucr[0]; f.ux = ucr[1]; f.uy = ucr[2]; f.un = ucr[3];
   // d u^mu / d tau = (u - u^{n-1}) / dt (SourceTerms.cu:68-71)
-  f.dtut = (R)((uc[0] - a.uprev[s]) / a.dt);
-  f.dtux = (R)((uc[1] - a.uprev[a.cs + s]) / a.dt);
-  f.dtuy = (R)((uc[2] - a.uprev[2 * a.cs + s]) / a.dt);
-  f.dtun = (R)((uc[3] - a.uprev[3 * a.cs + s]) / a.dt);
+  const double inv_dt = 1.0 / a.dt;
+  f.dtut = (R)((uc[0] - a.uprev[s]) * inv_dt);
+  f.dtux = (R)((uc[1] - a.uprev[a.cs + s]) * inv_dt);
+  f.dtuy = (R)((uc[2] - a.uprev[2 * a.cs + s]) * inv_dt);
+  f.dtun = (R)((uc[3] - a.uprev[3 * a.cs + s]) * inv_dt);
   const double thd = a.theta;
   const double idxd = 1.0 / a.dx, idyd = 1.0 / a.dy, idzd = 1.0 / a.dz;
   R du[3][4];
