@@ -61,6 +61,7 @@ struct EventDev {
   int nx, ny, nz, active;
   long long sy, sz, cs, ncells;
   double dx, dy, dz, dt, etabar, theta, e_reg, e_fo;
+  double inv_dx, inv_dy, inv_dz, inv_dt;  // reciprocals, computed on the host at admission
   double t0;            // initial proper time; the step from t0 + n dt is step n + 1
   long long step;       // completed steps
   double *qA, *qB, *e, *pA, *pB, *u[3];
@@ -76,6 +77,7 @@ __device__ __forceinline__ StageArgs make_args(EventDev &E, bool stage2) {
   a.nx = E.nx; a.ny = E.ny; a.nz = E.nz;
   a.sy = E.sy; a.sz = E.sz; a.cs = E.cs; a.ncells = E.ncells;
   a.dx = E.dx; a.dy = E.dy; a.dz = E.dz; a.dt = E.dt;
+  a.inv_dx = E.inv_dx; a.inv_dy = E.inv_dy; a.inv_dz = E.inv_dz; a.inv_dt = E.inv_dt;
   a.etabar = E.etabar; a.theta = E.theta; a.e_reg = E.e_reg;
   a.status = &E.status;
   a.diag = nullptr;  // validity diagnostics are a single-lattice option
@@ -473,6 +475,7 @@ int gvh_batch_add_event(gvh_batch *b, const gvh_lattice_params *L, const gvh_hyd
   E.sy = h.nx; E.sz = (long long)h.nx * h.ny; E.cs = h.cs; E.ncells = h.ncells;
   E.dx = L->latticeSpacingX; E.dy = L->latticeSpacingY; E.dz = L->latticeSpacingRapidity;
   E.dt = L->latticeSpacingProperTime;
+  E.inv_dx = 1.0 / E.dx; E.inv_dy = 1.0 / E.dy; E.inv_dz = 1.0 / E.dz; E.inv_dt = 1.0 / E.dt;
   E.etabar = H->shearViscosityToEntropyDensity;
   E.theta = b->opts.theta;
   const double T_reg = H->regulationTemperatureGeV / kHbarc;

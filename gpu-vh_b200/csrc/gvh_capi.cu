@@ -332,6 +332,7 @@ int gvh_rk2_step(gvh_handle *h, double t, double dt, double T_reg) {
   a.nx = h->nx; a.ny = h->ny; a.nz = h->nz;
   a.sy = h->sy; a.sz = h->sz; a.cs = h->cs; a.ncells = h->ncells;
   a.dx = h->dx; a.dy = h->dy; a.dz = h->dz; a.dt = h->dt_lattice;
+  set_inverse_spacings(a);
   a.etabar = h->etabar; a.theta = h->theta;
   a.e_reg = (h->eos == GVH_EOS_CONFORMAL) ? energy_density_of_T<EOS_CONFORMAL>(T_reg)
                                           : energy_density_of_T<EOS_QCD>(T_reg);

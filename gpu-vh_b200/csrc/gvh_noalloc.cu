@@ -155,6 +155,7 @@ int gvh_rk2_step_noalloc(const gvh_lattice_params *L, const gvh_hydro_params *H,
   a.sy = nx; a.sz = (long long)nx * ny; a.cs = n; a.ncells = n;
   a.dx = L->latticeSpacingX; a.dy = L->latticeSpacingY; a.dz = L->latticeSpacingRapidity;
   a.dt = L->latticeSpacingProperTime;
+  set_inverse_spacings(a);
   a.etabar = H->shearViscosityToEntropyDensity;
   a.theta = o.theta;
   a.e_reg = (o.eos == GVH_EOS_CONFORMAL) ? energy_density_of_T<EOS_CONFORMAL>(T_reg) : energy_density_of_T<EOS_QCD>(T_reg);

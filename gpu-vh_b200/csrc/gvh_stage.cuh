@@ -39,6 +39,7 @@ struct StageArgs {
   long long ncells;       // nx*ny*nz
   double dx, dy, dz;      // lattice spacings
   double dt;              // lattice time step (d_dt) used in the Euler update
+  double inv_dx, inv_dy, inv_dz, inv_dt;  // 1/dx, 1/dy, 1/dz, 1/dt (set_inverse_spacings)
   double etabar, theta;
   double t_euler;         // time passed to the Euler step
   double t_after;         // time passed to primitive recovery and regulation
@@ -66,6 +67,14 @@ constexpr int kValiditySaved = 11;
 #define GVH_BLOCK 128
 #endif
 constexpr int kBlock = GVH_BLOCK;  // threads per block of the stage kernel
+
+// The reciprocal spacings, computed once by whoever fills the arguments.
+__host__ __device__ inline void set_inverse_spacings(StageArgs &a) {
+  a.inv_dx = 1.0 / a.dx;
+  a.inv_dy = 1.0 / a.dy;
+  a.inv_dz = 1.0 / a.dz;
+  a.inv_dt = 1.0 / a.dt;
+}
 
 template <bool SHEAR, bool BULK>
 struct NComp {
@@ -192,13 +201,13 @@ __device__ __forceinline__ void axis_pi_sources(const StageArgs &a, int s, int a
 
 template <int EOS, bool SHEAR, bool BULK, bool MIXED>
 __device__ __forceinline__ void axis_update(const StageArgs &a, int s, int axis, int idx, int n_axis, int stride,
-                                            double d, const GuessEos &g0, const double *uc, double *out,
+                                            double inv_spacing, const GuessEos &g0, const double *uc, double *out,
                                             double *cache, unsigned &status) {
   using R = typename std::conditional<MIXED, float, double>::type;
   constexpr int NQ = NComp<SHEAR, BULK>::value;
   const int o[5] = {(max(idx - 2, 0) - idx) * stride, (max(idx - 1, 0) - idx) * stride, 0,
                     (min(idx + 1, n_axis - 1) - idx) * stride, (min(idx + 2, n_axis - 1) - idx) * stride};
-  const R inv_d = R(1.0 / d);
+  const R inv_d = R(inv_spacing);
   // Face states are recovered in FP64 on both paths (the mixed path rounds only the
   // resulting speeds): an FP32 recovery was tried and let a 2+1D hotspot event run away
   // to NaN that the FP64 recovery keeps finite.
@@ -266,13 +275,13 @@ __device__ __forceinline__ void stage_source(const StageArgs &a, long long s, in
   for (int m = 0; m < 4; ++m) ucr[m] = (R)uc[m];
   f.ut = ucr[0]; f.ux = ucr[1]; f.uy = ucr[2]; f.un = ucr[3];
   // d u^mu / d tau = (u - u^{n-1}) / dt (SourceTerms.cu:68-71)
-  const double inv_dt = 1.0 / a.dt;
+  const double inv_dt = a.inv_dt;
   f.dtut = (R)((uc[0] - a.uprev[s]) * inv_dt);
   f.dtux = (R)((uc[1] - a.uprev[a.cs + s]) * inv_dt);
   f.dtuy = (R)((uc[2] - a.uprev[2 * a.cs + s]) * inv_dt);
   f.dtun = (R)((uc[3] - a.uprev[3 * a.cs + s]) * inv_dt);
   const double thd = a.theta;
-  const double idxd = 1.0 / a.dx, idyd = 1.0 / a.dy, idzd = 1.0 / a.dz;
+  const double idxd = a.inv_dx, idyd = a.inv_dy, idzd = a.inv_dz;
   R du[3][4];
 #pragma unroll
   for (int m = 0; m < 4; ++m) {
@@ -362,8 +371,9 @@ __device__ __forceinline__ double stage_finish(const StageArgs &a, long long s, 
     double piu2 = -piyn * t2 * pr.un + pity * pr.ut - pixy * pr.ux - piyy * pr.uy;
     double piu3 = -pinn * t2 * pr.un + pitn * pr.ut - pixn * pr.ux - piyn * pr.uy;
     double a1 = (spipi / rhomax) * (1.0 / sqrt(pr.e * pr.e + 3 * pr.p * pr.p));
-    double den = xi0 * rhomax * spipi;
-    double rho = fmax(a1, fmax(pimumu / den, fmax(piu0 / den, fmax(piu1 / den, fmax(piu2 / den, piu3 / den)))));
+    double inv_den = 1.0 / (xi0 * rhomax * spipi);  // one reciprocal for the five quotients
+    double rho = fmax(a1, fmax(pimumu * inv_den,
+                               fmax(piu0 * inv_den, fmax(piu1 * inv_den, fmax(piu2 * inv_den, piu3 * inv_den)))));
     double facShear = tanh(rho) / rho;
     if (fabs(rho) < 1.e-7) facShear = 1.0;
     // The reference reads Pi as 0 here (its `#ifdef Pi` is never true), so rho_bulk = 0
@@ -432,8 +442,9 @@ __device__ __forceinline__ double stage_cell(const StageArgs &a, long long id) {
     const int idx = axis == 0 ? i : axis == 1 ? j : k;
     const int n_axis = axis == 0 ? a.nx : axis == 1 ? a.ny : a.nz;
     const int stride = axis == 0 ? 1 : axis == 1 ? (int)a.sy : (int)a.sz;
-    const double d = axis == 0 ? a.dx : axis == 1 ? a.dy : a.dz;
-    axis_update<EOS, SHEAR, BULK, MIXED>(a, (int)s, axis, idx, n_axis, stride, d, g0, uc, out, cache, status);
+    const double inv_spacing = axis == 0 ? a.inv_dx : axis == 1 ? a.inv_dy : a.inv_dz;
+    axis_update<EOS, SHEAR, BULK, MIXED>(a, (int)s, axis, idx, n_axis, stride, inv_spacing, g0, uc, out, cache,
+                                         status);
   }
 
   return stage_finish<EOS, SHEAR, BULK, STAGE2, kBlock>(a, s, out, g0, status);
