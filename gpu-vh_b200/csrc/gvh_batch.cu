@@ -158,7 +158,6 @@ struct gvh_batch {
   int tile_capacity = 0;
   double *staging = nullptr;
   size_t staging_bytes = 0;
-  double **d_ptrs = nullptr;
   unsigned long long *d_scratch = nullptr;
   cudaGraphExec_t graph = nullptr;
   int grid = 0;                          // persistent grid (blocks); 0 = one block per tile
@@ -360,7 +359,6 @@ int gvh_batch_create(const gvh_options *opts, long long arena_bytes, gvh_batch *
   ok = ok && cudaMalloc(&b->d_ev, kMaxEvents * sizeof(EventDev)) == cudaSuccess;
   ok = ok && cudaMalloc(&b->d_tile_event, (size_t)b->tile_capacity * sizeof(int)) == cudaSuccess;
   ok = ok && cudaMalloc(&b->d_ntiles, sizeof(int)) == cudaSuccess;
-  ok = ok && cudaMalloc(&b->d_ptrs, 64 * sizeof(double *)) == cudaSuccess;
   ok = ok && cudaMalloc(&b->d_scratch, sizeof(unsigned long long)) == cudaSuccess;
   ok = ok && cudaStreamCreateWithFlags(&b->own_stream, cudaStreamNonBlocking) == cudaSuccess;
   if (!ok) {
@@ -390,7 +388,6 @@ int gvh_batch_destroy(gvh_batch *b) {
   cudaFree(b->d_ev);
   cudaFree(b->d_tile_event);
   cudaFree(b->d_ntiles);
-  cudaFree(b->d_ptrs);
   cudaFree(b->d_scratch);
   if (b->staging) cudaFree(b->staging);
   if (b->own_stream) cudaStreamDestroy(b->own_stream);
@@ -446,14 +443,13 @@ int gvh_batch_add_event(gvh_batch *b, const gvh_lattice_params *L, const gvh_hyd
   const size_t fb = h.ng * sizeof(double);
   for (int f = 0; f < n_prim; ++f)
     BCUDA(cudaMemcpyAsync(b->staging + f * h.ng, prim[f], fb, cudaMemcpyDefault, b->stream));
-  double *dst[32];
-  dst[0] = e;
-  for (int m = 0; m < 4; ++m) dst[1 + m] = u[0] + m * h.cs;
-  for (int n = 4; n < b->nq; ++n) dst[5 + n - 4] = qA + n * h.cs;
-  BCUDA(cudaMemcpyAsync(b->d_ptrs, dst, n_prim * sizeof(double *), cudaMemcpyHostToDevice, b->stream));
+  FieldTable dst = {};
+  dst.p[0] = e;
+  for (int m = 0; m < 4; ++m) dst.p[1 + m] = u[0] + m * h.cs;
+  for (int n = 4; n < b->nq; ++n) dst.p[5 + n - 4] = qA + n * h.cs;
   Pack pk{h.nx, h.ny, h.nz, (long long)h.nx, (long long)h.nx * h.ny, h.ng};
   const unsigned blocks = (unsigned)((h.ncells + 255) / 256);
-  pack_kernel<<<blocks, 256, 0, b->stream>>>(pk, n_prim, b->staging, b->d_ptrs);
+  pack_kernel<<<blocks, 256, 0, b->stream>>>(pk, n_prim, b->staging, dst);
   if (b->opts.eos == GVH_EOS_CONFORMAL)
     init_conserved_kernel<EOS_CONFORMAL><<<blocks, 256, 0, b->stream>>>(h.ncells, b->nq, h.cs, qA, e, pA, u[0], u[1], 0);
   else
@@ -576,15 +572,14 @@ int gvh_batch_get_state(gvh_batch *b, int id, double *const *fields, int n_field
   EventDev E;
   BCUDA(cudaMemcpyAsync(&E, b->d_ev + id, sizeof E, cudaMemcpyDeviceToHost, b->stream));
   BCUDA(cudaStreamSynchronize(b->stream));
-  double *src[32];
-  for (int n = 0; n < b->nq; ++n) src[n] = fields[n] ? E.qA + n * h.cs : nullptr;
-  src[b->nq] = fields[b->nq] ? E.e : nullptr;
-  src[b->nq + 1] = fields[b->nq + 1] ? E.pA : nullptr;
-  for (int m = 0; m < 4; ++m) src[b->nq + 2 + m] = fields[b->nq + 2 + m] ? E.u[E.ucur] + m * h.cs : nullptr;
-  for (int m = 0; m < 4; ++m) src[b->nq + 6 + m] = fields[b->nq + 6 + m] ? E.u[E.uprev] + m * h.cs : nullptr;
-  BCUDA(cudaMemcpyAsync(b->d_ptrs, src, n_fields * sizeof(double *), cudaMemcpyHostToDevice, b->stream));
+  FieldTable src = {};
+  for (int n = 0; n < b->nq; ++n) src.p[n] = fields[n] ? E.qA + n * h.cs : nullptr;
+  src.p[b->nq] = fields[b->nq] ? E.e : nullptr;
+  src.p[b->nq + 1] = fields[b->nq + 1] ? E.pA : nullptr;
+  for (int m = 0; m < 4; ++m) src.p[b->nq + 2 + m] = fields[b->nq + 2 + m] ? E.u[E.ucur] + m * h.cs : nullptr;
+  for (int m = 0; m < 4; ++m) src.p[b->nq + 6 + m] = fields[b->nq + 6 + m] ? E.u[E.uprev] + m * h.cs : nullptr;
   Pack pk{h.nx, h.ny, h.nz, (long long)h.nx, (long long)h.nx * h.ny, h.ng};
-  unpack_kernel<<<(unsigned)((h.ng + 255) / 256), 256, 0, b->stream>>>(pk, n_fields, b->d_ptrs, b->staging);
+  unpack_kernel<<<(unsigned)((h.ng + 255) / 256), 256, 0, b->stream>>>(pk, n_fields, src, b->staging);
   BCUDA(cudaGetLastError());
   const size_t fb = h.ng * sizeof(double);
   for (int f = 0; f < n_fields; ++f)

@@ -114,14 +114,32 @@ Pack make_pack(const gvh_handle *h) { return Pack{h->nx, h->ny, h->nz, h->sy, h-
 
 int ensure_staging(gvh_handle *h) {
   if (h->staging) return GVH_OK;
-  size_t bytes = (size_t)(h->nq + 10) * h->ng * sizeof(double) + 64 * sizeof(double *);
+  size_t bytes = (size_t)(h->nq + 10) * h->ng * sizeof(double);
   if (cudaMalloc(&h->staging, bytes) != cudaSuccess) return fail(GVH_ERR_NOMEM, "staging allocation failed");
   return GVH_OK;
 }
 
-// device array of field pointers lives after the staging fields
-double **staging_ptr_table(gvh_handle *h) {
-  return reinterpret_cast<double **>(h->staging + (size_t)(h->nq + 10) * h->ng);
+int ensure_async(gvh_handle *h) {
+  if (h->async_ready) return GVH_OK;
+  const size_t bytes = (size_t)(h->nq + 10) * h->ng * sizeof(double);
+  if (cudaMalloc(&h->staging_in, bytes) != cudaSuccess) return fail(GVH_ERR_NOMEM, "async staging allocation failed");
+  if (cudaMalloc(&h->staging_out, bytes) != cudaSuccess) {
+    cudaFree(h->staging_in);
+    return fail(GVH_ERR_NOMEM, "async staging allocation failed");
+  }
+  GVH_CUDA(cudaStreamCreateWithFlags(&h->s_h2d, cudaStreamNonBlocking));
+  GVH_CUDA(cudaStreamCreateWithFlags(&h->s_d2h, cudaStreamNonBlocking));
+  GVH_CUDA(cudaEventCreateWithFlags(&h->ev_in_ready, cudaEventDisableTiming));
+  GVH_CUDA(cudaEventCreateWithFlags(&h->ev_in_free, cudaEventDisableTiming));
+  GVH_CUDA(cudaEventCreateWithFlags(&h->ev_out_ready, cudaEventDisableTiming));
+  GVH_CUDA(cudaEventCreateWithFlags(&h->ev_out_free, cudaEventDisableTiming));
+  GVH_CUDA(cudaEventCreateWithFlags(&h->ev_fence, cudaEventDisableTiming));
+  // the events start recorded (complete), so the first waits pass
+  GVH_CUDA(cudaEventRecord(h->ev_in_free, h->stream));
+  GVH_CUDA(cudaEventRecord(h->ev_out_free, h->stream));
+  GVH_CUDA(cudaEventRecord(h->ev_in_ready, h->stream));
+  h->async_ready = 1;
+  return GVH_OK;
 }
 
 void internal_fields(const gvh_handle *h, double **f) {
@@ -233,6 +251,19 @@ int gvh_destroy(gvh_handle *h) {
   cudaFree(h->block);
   if (h->staging) cudaFree(h->staging);
   if (h->diag) cudaFree(h->diag);
+  if (h->async_ready) {
+    cudaStreamSynchronize(h->s_h2d);
+    cudaStreamSynchronize(h->s_d2h);
+    cudaFree(h->staging_in);
+    cudaFree(h->staging_out);
+    cudaStreamDestroy(h->s_h2d);
+    cudaStreamDestroy(h->s_d2h);
+    cudaEventDestroy(h->ev_in_ready);
+    cudaEventDestroy(h->ev_in_free);
+    cudaEventDestroy(h->ev_out_ready);
+    cudaEventDestroy(h->ev_out_free);
+    cudaEventDestroy(h->ev_fence);
+  }
   delete h;
   return GVH_OK;
 }
@@ -254,13 +285,11 @@ int gvh_set_state(gvh_handle *h, const double *const *fields, int n_fields) {
     if (!src) return fail(GVH_ERR_INVALID, "gvh_set_state: field %d is null", f);
     GVH_CUDA(cudaMemcpyAsync(h->staging + f * h->ng, src, fb, cudaMemcpyDefault, h->stream));
   }
-  double *dst[32];
-  internal_fields(h, dst);
-  double **table = staging_ptr_table(h);
-  GVH_CUDA(cudaMemcpyAsync(table, dst, n_fields * sizeof(double *), cudaMemcpyHostToDevice, h->stream));
-  pack_kernel<<<(unsigned)((h->ncells + 255) / 256), 256, 0, h->stream>>>(make_pack(h), n_fields, h->staging, table);
+  FieldTable dst = {};
+  internal_fields(h, dst.p);
+  pack_kernel<<<(unsigned)((h->ncells + 255) / 256), 256, 0, h->stream>>>(make_pack(h), n_fields, h->staging, dst);
   GVH_CUDA(cudaGetLastError());
-  GVH_CUDA(cudaStreamSynchronize(h->stream));  // the host pointer table above is on the stack
+  GVH_CUDA(cudaStreamSynchronize(h->stream));  // the caller may reuse its arrays on return
   return GVH_OK;
 }
 
@@ -269,13 +298,11 @@ int gvh_get_state(gvh_handle *h, double *const *fields, int n_fields) {
   if (n_fields != h->nq + 10) return fail(GVH_ERR_INVALID, "gvh_get_state: expected %d fields", h->nq + 10);
   int rc;
   if ((rc = set_device(h)) || (rc = ensure_staging(h))) return rc;
-  double *src[32];
-  internal_fields(h, src);
+  FieldTable src = {};
+  internal_fields(h, src.p);
   for (int f = 0; f < n_fields; ++f)
-    if (!fields[f]) src[f] = nullptr;
-  double **table = staging_ptr_table(h);
-  GVH_CUDA(cudaMemcpyAsync(table, src, n_fields * sizeof(double *), cudaMemcpyHostToDevice, h->stream));
-  unpack_kernel<<<(unsigned)((h->ng + 255) / 256), 256, 0, h->stream>>>(make_pack(h), n_fields, table, h->staging);
+    if (!fields[f]) src.p[f] = nullptr;
+  unpack_kernel<<<(unsigned)((h->ng + 255) / 256), 256, 0, h->stream>>>(make_pack(h), n_fields, src, h->staging);
   GVH_CUDA(cudaGetLastError());
   const size_t fb = h->ng * sizeof(double);
   for (int f = 0; f < n_fields; ++f)
@@ -297,15 +324,13 @@ int gvh_set_primitive_state_p(gvh_handle *h, const double *const *prim, int n_pr
     GVH_CUDA(cudaMemcpyAsync(h->staging + f * h->ng, prim[f], fb, cudaMemcpyDefault, h->stream));
   if (p_ghosted)
     GVH_CUDA(cudaMemcpyAsync(h->staging + n_prim * h->ng, p_ghosted, fb, cudaMemcpyDefault, h->stream));
-  double *dst[32];
-  dst[0] = h->e;
-  for (int m = 0; m < 4; ++m) dst[1 + m] = h->u[h->ucur] + m * h->cs;
-  for (int n = 4; n < h->nq; ++n) dst[5 + n - 4] = h->qA + n * h->cs;
-  dst[n_prim] = h->pA;
+  FieldTable dst = {};
+  dst.p[0] = h->e;
+  for (int m = 0; m < 4; ++m) dst.p[1 + m] = h->u[h->ucur] + m * h->cs;
+  for (int n = 4; n < h->nq; ++n) dst.p[5 + n - 4] = h->qA + n * h->cs;
+  dst.p[n_prim] = h->pA;
   const int n_pack = n_prim + (p_ghosted ? 1 : 0);
-  double **table = staging_ptr_table(h);
-  GVH_CUDA(cudaMemcpyAsync(table, dst, n_pack * sizeof(double *), cudaMemcpyHostToDevice, h->stream));
-  pack_kernel<<<(unsigned)((h->ncells + 255) / 256), 256, 0, h->stream>>>(make_pack(h), n_pack, h->staging, table);
+  pack_kernel<<<(unsigned)((h->ncells + 255) / 256), 256, 0, h->stream>>>(make_pack(h), n_pack, h->staging, dst);
   GVH_CUDA(cudaGetLastError());
   const unsigned blocks = (unsigned)((h->ncells + 255) / 256);
   if (h->eos == GVH_EOS_CONFORMAL)
@@ -380,11 +405,9 @@ int gvh_get_validity(gvh_handle *h, double *const *fields, int n_fields) {
   if (!h->diag) return fail(GVH_ERR_INVALID, "gvh_get_validity: diagnostics not enabled (gvh_enable_validity)");
   int rc;
   if ((rc = set_device(h)) || (rc = ensure_staging(h))) return rc;
-  double *src[kValidityFields];
-  for (int f = 0; f < kValidityFields; ++f) src[f] = fields[f] ? h->diag + (size_t)f * h->cs : nullptr;
-  double **table = staging_ptr_table(h);
-  GVH_CUDA(cudaMemcpyAsync(table, src, n_fields * sizeof(double *), cudaMemcpyHostToDevice, h->stream));
-  unpack_kernel<<<(unsigned)((h->ng + 255) / 256), 256, 0, h->stream>>>(make_pack(h), n_fields, table, h->staging);
+  FieldTable src = {};
+  for (int f = 0; f < kValidityFields; ++f) src.p[f] = fields[f] ? h->diag + (size_t)f * h->cs : nullptr;
+  unpack_kernel<<<(unsigned)((h->ng + 255) / 256), 256, 0, h->stream>>>(make_pack(h), n_fields, src, h->staging);
   GVH_CUDA(cudaGetLastError());
   const size_t fb = h->ng * sizeof(double);
   for (int f = 0; f < n_fields; ++f)
@@ -425,6 +448,73 @@ int gvh_synchronize(gvh_handle *h) {
   if (!h) return fail(GVH_ERR_INVALID, "null handle");
   GVH_CUDA(cudaSetDevice(h->device));
   GVH_CUDA(cudaStreamSynchronize(h->stream));
+  if (h->async_ready) {
+    GVH_CUDA(cudaStreamSynchronize(h->s_h2d));
+    GVH_CUDA(cudaStreamSynchronize(h->s_d2h));
+  }
+  return GVH_OK;
+}
+
+int gvh_set_state_async(gvh_handle *h, const double *const *fields, int n_fields) {
+  if (!h || !fields) return fail(GVH_ERR_INVALID, "gvh_set_state_async: null argument");
+  if (n_fields != h->nq + 10) return fail(GVH_ERR_INVALID, "gvh_set_state_async: expected %d fields", h->nq + 10);
+  int rc;
+  if ((rc = set_device(h)) || (rc = ensure_async(h))) return rc;
+  FieldTable dst = {};
+  internal_fields(h, dst.p);
+  const size_t fb = h->ng * sizeof(double);
+  // the input staging is free once the previous pack has read it
+  GVH_CUDA(cudaStreamWaitEvent(h->s_h2d, h->ev_in_free, 0));
+  for (int f = 0; f < n_fields; ++f) {
+    const double *src = fields[f];
+    if (!src && f >= h->nq + 6) src = fields[f - 4];  // up defaults to u
+    if (!src) return fail(GVH_ERR_INVALID, "gvh_set_state_async: field %d is null", f);
+    GVH_CUDA(cudaMemcpyAsync(h->staging_in + f * h->ng, src, fb, cudaMemcpyDefault, h->s_h2d));
+  }
+  GVH_CUDA(cudaEventRecord(h->ev_in_ready, h->s_h2d));
+  GVH_CUDA(cudaStreamWaitEvent(h->stream, h->ev_in_ready, 0));
+  pack_kernel<<<(unsigned)((h->ncells + 255) / 256), 256, 0, h->stream>>>(make_pack(h), n_fields, h->staging_in,
+                                                                            dst);
+  GVH_CUDA(cudaGetLastError());
+  GVH_CUDA(cudaEventRecord(h->ev_in_free, h->stream));
+  return GVH_OK;
+}
+
+int gvh_get_state_async(gvh_handle *h, double *const *fields, int n_fields) {
+  if (!h || !fields) return fail(GVH_ERR_INVALID, "gvh_get_state_async: null argument");
+  if (n_fields != h->nq + 10) return fail(GVH_ERR_INVALID, "gvh_get_state_async: expected %d fields", h->nq + 10);
+  int rc;
+  if ((rc = set_device(h)) || (rc = ensure_async(h))) return rc;
+  FieldTable src = {};
+  internal_fields(h, src.p);
+  for (int f = 0; f < n_fields; ++f)
+    if (!fields[f]) src.p[f] = nullptr;
+  // the output staging is free once the previous copy to the host has read it
+  GVH_CUDA(cudaStreamWaitEvent(h->stream, h->ev_out_free, 0));
+  unpack_kernel<<<(unsigned)((h->ng + 255) / 256), 256, 0, h->stream>>>(make_pack(h), n_fields, src,
+                                                                          h->staging_out);
+  GVH_CUDA(cudaGetLastError());
+  GVH_CUDA(cudaEventRecord(h->ev_out_ready, h->stream));
+  GVH_CUDA(cudaStreamWaitEvent(h->s_d2h, h->ev_out_ready, 0));
+  const size_t fb = h->ng * sizeof(double);
+  for (int f = 0; f < n_fields; ++f)
+    if (fields[f])
+      GVH_CUDA(cudaMemcpyAsync(fields[f], h->staging_out + f * h->ng, fb, cudaMemcpyDefault, h->s_d2h));
+  GVH_CUDA(cudaEventRecord(h->ev_out_free, h->s_d2h));
+  return GVH_OK;
+}
+
+int gvh_join_async(gvh_handle *h) {
+  if (!h) return fail(GVH_ERR_INVALID, "null handle");
+  if (!h->async_ready) return GVH_OK;
+  GVH_CUDA(cudaSetDevice(h->device));
+  // the handle's stream waits for every queued copy, then the copy streams wait for
+  // everything queued on the handle's stream up to here
+  GVH_CUDA(cudaStreamWaitEvent(h->stream, h->ev_in_ready, 0));
+  GVH_CUDA(cudaStreamWaitEvent(h->stream, h->ev_out_free, 0));
+  GVH_CUDA(cudaEventRecord(h->ev_fence, h->stream));
+  GVH_CUDA(cudaStreamWaitEvent(h->s_h2d, h->ev_fence, 0));
+  GVH_CUDA(cudaStreamWaitEvent(h->s_d2h, h->ev_fence, 0));
   return GVH_OK;
 }
 

@@ -19,6 +19,12 @@ struct gvh_handle {
   double *staging;          // reference-layout fields for set/get, allocated on first use
   double *diag;             // validity diagnostics (allocated by gvh_enable_validity)
   int validity_on;
+  // asynchronous set/get (allocated on first use): separate input and output staging, one
+  // copy stream each way, events that order them with the handle's stream
+  double *staging_in, *staging_out;
+  cudaStream_t s_h2d, s_d2h;
+  cudaEvent_t ev_in_ready, ev_in_free, ev_out_ready, ev_out_free, ev_fence;
+  int async_ready;
 };
 
 // The current time level's fields in the handle's interior-only layout (cell

@@ -21,20 +21,27 @@ __device__ __forceinline__ long long ref_index(const Pack &p, int i, int j, int 
   return (long long)(i + 2) + (long long)(p.nx + 4) * ((j + 2) + (long long)(p.ny + 4) * (k + 2));
 }
 
-// staging (nf fields, ghosted) -> internal fields dst[f] (interior)
-__global__ void pack_kernel(Pack p, int nf, const double *__restrict__ staging, double *const *dst) {
+// Field pointers passed by value: no table has to reach the device before a launch, so the
+// conversions can be queued without waiting (the asynchronous set/get of the C ABI).
+struct FieldTable {
+  double *p[32];
+};
+
+// staging (nf fields, ghosted) -> internal fields dst.p[f] (interior); null entries are skipped
+__global__ void pack_kernel(Pack p, int nf, const double *__restrict__ staging, FieldTable dst) {
   long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   long long n = (long long)p.nx * p.ny * p.nz;
   if (id >= n) return;
   int i = id % p.nx, j = (id / p.nx) % p.ny, k = id / ((long long)p.nx * p.ny);
   long long r = ref_index(p, i, j, k), s = i + p.sy * j + p.sz * k;
   for (int f = 0; f < nf; ++f)
-    if (dst[f]) dst[f][s] = staging[f * p.ng + r];
+    if (dst.p[f]) dst.p[f][s] = staging[f * p.ng + r];
 }
 
-// internal fields src[f] -> staging (ghosted, every ghost cell filled from the nearest
-// interior cell: the reference's zero-gradient faces, edges and corners alike)
-__global__ void unpack_kernel(Pack p, int nf, const double *const *src, double *__restrict__ staging) {
+// internal fields src.p[f] -> staging (ghosted, every ghost cell filled from the nearest
+// interior cell: the reference's zero-gradient faces, edges and corners alike); null entries
+// are skipped
+__global__ void unpack_kernel(Pack p, int nf, FieldTable src, double *__restrict__ staging) {
   long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   long long n = p.ng;
   if (id >= n) return;
@@ -42,7 +49,7 @@ __global__ void unpack_kernel(Pack p, int nf, const double *const *src, double *
   int i = min(max(gi - 2, 0), p.nx - 1), j = min(max(gj - 2, 0), p.ny - 1), k = min(max(gk - 2, 0), p.nz - 1);
   long long s = i + p.sy * j + p.sz * k;
   for (int f = 0; f < nf; ++f)
-    if (src[f]) staging[f * p.ng + id] = src[f][s];
+    if (src.p[f]) staging[f * p.ng + id] = src.p[f][s];
 }
 
 // T^{tau mu} from primitives (DynamicalVariables.cu:349-392 with EnergyMomentumTensor.cu

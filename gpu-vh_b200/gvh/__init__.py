@@ -81,7 +81,7 @@ EXPORTS = [
     "gvh_default_options", "gvh_create", "gvh_destroy", "gvh_num_conserved", "gvh_num_fields",
     "gvh_num_lattice_cells", "gvh_set_primitive_state", "gvh_set_state", "gvh_get_state", "gvh_rk2_step",
     "gvh_status", "gvh_clear_status", "gvh_synchronize", "gvh_launches_per_step", "gvh_last_error",
-    "gvh_set_stream", "gvh_max_energy_density",
+    "gvh_set_stream", "gvh_max_energy_density", "gvh_set_state_async", "gvh_get_state_async", "gvh_join_async",
 ]
 
 
@@ -107,6 +107,9 @@ def load(path: str | None = None):
     L.gvh_set_primitive_state.argtypes = [vp, vp, ip]
     L.gvh_set_state.argtypes = [vp, vp, ip]
     L.gvh_get_state.argtypes = [vp, vp, ip]
+    L.gvh_set_state_async.argtypes = [vp, vp, ip]
+    L.gvh_get_state_async.argtypes = [vp, vp, ip]
+    L.gvh_join_async.argtypes = [vp]
     L.gvh_rk2_step.argtypes = [vp, dp, dp, dp]
     L.gvh_status.argtypes = [vp, ctypes.POINTER(ctypes.c_uint)]
     L.gvh_clear_status.argtypes = [vp]
@@ -225,6 +228,20 @@ class Lattice:
 
     def get_state_ptrs(self, ptrs):
         _check(self._L.gvh_get_state(self._h, _ptr_array(list(ptrs)), len(ptrs)), "gvh_get_state")
+
+    # Pipelined copies (gvh_set_state_async / gvh_get_state_async): queued on the handle's copy
+    # streams and returned from at once; the host arrays (pinned, for overlap) must stay
+    # untouched until synchronize(). join_async() orders the handle's stream and its copy
+    # streams both ways: later stream work after every queued copy, later copies after every
+    # queued stream work.
+    def set_state_async_ptrs(self, ptrs):
+        _check(self._L.gvh_set_state_async(self._h, _ptr_array(list(ptrs)), len(ptrs)), "gvh_set_state_async")
+
+    def get_state_async_ptrs(self, ptrs):
+        _check(self._L.gvh_get_state_async(self._h, _ptr_array(list(ptrs)), len(ptrs)), "gvh_get_state_async")
+
+    def join_async(self):
+        _check(self._L.gvh_join_async(self._h), "gvh_join_async")
 
     VALIDITY_NAMES = ["regulations", "knudsenNumberTaupi", "knudsenNumberTauPi", "inverseReynoldsNumberPimunu",
                       "inverseReynoldsNumber2Pimunu", "inverseReynoldsNumberTilde2Pimunu", "inverseReynoldsNumberPi",

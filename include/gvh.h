@@ -123,6 +123,20 @@ int gvh_set_state(gvh_handle *h, const double *const *fields, int n_fields);
 /* Null entries are skipped. Ghost layers come back zero-gradient filled, edges and
  * corners included. Synchronises the handle's stream. */
 int gvh_get_state(gvh_handle *h, double *const *fields, int n_fields);
+/* Pipelined set/get for a caller that streams states through the handle (a new state in,
+ * one or more steps, the result out, again and again): the copies go on the handle's own
+ * copy streams, one each way, with separate device staging for inputs and outputs, and are
+ * ordered with the handle's stream by events, so the next state's copy in, the step and the
+ * last result's copy out overlap. The calls return without waiting. Host arrays should be
+ * pinned (pageable memory still works but the copies then serialise) and must not be
+ * touched until gvh_synchronize(h) returns. gvh_join_async(h) joins the handle's stream
+ * and its copy streams both ways: work queued on the handle's stream afterwards waits for
+ * every copy queued so far, and copies queued afterwards wait for the work queued on the
+ * handle's stream so far (so that events recorded on the handle's stream on either side of
+ * a join bracket the copies too). */
+int gvh_set_state_async(gvh_handle *h, const double *const *fields, int n_fields);
+int gvh_get_state_async(gvh_handle *h, double *const *fields, int n_fields);
+int gvh_join_async(gvh_handle *h);
 
 /* One Heun RK2 step from time t (t and dt as twoStepRungeKutta takes them). Cells with
  * e <= e(T_reg) have pi^{mu nu} regulated; T_reg is in fm^-1 and 0 (the reference's default
