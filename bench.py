@@ -19,7 +19,9 @@ next state's copy in and the last state's copy out overlap the step. The blockin
 gvh_set_state / gvh_get_state loop is reported beside it (`serial_ms_per_step`).
 
 --impl reference times the reference's own KT step (its rhic/src sources compiled for the
-CPU by oracle/build_ref.py, OpenMP over the launch grid) on the host cores.
+CPU by oracle/build_ref.py, OpenMP over the launch grid) on the host cores; beside it
+(`reference_gpu`) the reference's own CUDA build, as shipped in FP32 and in FP64, on the
+full event on this GPU.
 """
 from __future__ import annotations
 
@@ -247,8 +249,43 @@ def run_reference(args):
                                    f"on the central {nz_s} of {w.nz} rapidity planes of the event"},
         "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    gpu = reference_gpu_timings(args, w, prim)
+    if gpu:
+        line["reference_gpu"] = gpu
     print(json.dumps(line))
     return 0
+
+
+def reference_gpu_timings(args, w, prim):
+    """The reference's own CUDA build (oracle/ref_gpu_driver.cu: its allocation, set-up and
+    twoStepRungeKutta, compiled with nvcc for sm_100a) on the full event on this GPU, as
+    shipped (FP32) and with the PRECISION double overlay: W warm-up steps, then K steps timed
+    with CUDA events. Reported beside the CPU arm; {} without a GPU or the builds."""
+    import oracle
+
+    try:
+        import torch
+
+        if not torch.cuda.is_available():
+            return {}
+    except ImportError:
+        return {}
+    out = {}
+    kw = w.lattice_kwargs()
+    cells = w.nx * w.ny * w.nz
+    for prec in ("fp32", "fp64"):
+        variant = oracle.ref_gpu_variant(prec, w.conformal, w.shear, w.bulk, w.theta)
+        if not oracle.ref_gpu_available(variant):
+            continue
+        R = oracle.RefGpuLattice(precision=prec, **kw)
+        R.set_primitive(prim)
+        if args.warmup:
+            R.time_steps(args.warmup, w.tau0, w.dtau)
+        ms = R.time_steps(args.steps, w.tau0 + args.warmup * w.dtau, w.dtau)
+        out[prec] = {"ms_per_step": ms / args.steps, "cell_updates_per_s": cells * args.steps / (ms / 1e3),
+                     "build": f"reference rhic/src, nvcc sm_100a, PRECISION {'double' if prec == 'fp64' else 'float'}",
+                     "timing": "CUDA events around the reference's own twoStepRungeKutta loop (legacy stream)"}
+    return out
 
 
 def time_steps(L, w, steps, warmup, stream):

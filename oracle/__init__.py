@@ -9,6 +9,10 @@ SoA layout):
   (oracle/build_ref.py -> oracle/_ref/), used to pin the restatement and as the
   benchmark's reference arm. Each variant library holds one lattice (the reference keeps
   its state in globals).
+* ``RefGpuLattice`` -- the reference's own CUDA build (as shipped in FP32, and with the
+  PRECISION double overlay) driven by oracle/ref_gpu_driver.cu: the reference's step timed
+  on the same GPU, and its FP64 CUDA build as an oracle. Needs a GPU; one lattice per
+  process and variant library.
 
 Only tests/, the smoke check and the CPU-baseline/reference legs of bench.py use this
 package; the product never imports it.
@@ -291,3 +295,74 @@ class RefLattice(_Base):
         out = np.zeros(6)
         self._L.gvh_ref_inferred(t, qa.ctypes.data, e_prev, out.ctypes.data)
         return list(out)
+
+
+def ref_gpu_variant(precision: str, conformal: bool, shear: bool, bulk: bool, theta: float) -> str:
+    phys = "bulk" if bulk else ("shear" if shear else "ideal")
+    return f"{precision}_{'conf' if conformal else 'qcd'}_{phys}_th{theta:.1f}"
+
+
+def ref_gpu_available(variant: str) -> bool:
+    return os.path.exists(os.path.join(REF_DIR, f"libref_gpu_{variant}.so"))
+
+
+class RefGpuLattice(_Base):
+    """The reference's own CUDA build (oracle/ref_gpu_driver.cu): its allocation, launch
+    set-up, initial-state path and twoStepRungeKutta, on the current GPU. The reference keeps
+    one lattice in globals, so a process holds at most one lattice per variant library (a
+    second instance must have the same sizes and reuses the buffers)."""
+
+    def __init__(self, precision="fp64", **kw):
+        super().__init__(**kw)
+        self.variant = ref_gpu_variant(precision, self.conformal, self.shear, self.bulk, kw["theta"])
+        path = os.path.join(REF_DIR, f"libref_gpu_{self.variant}.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        L = ctypes.CDLL(path)
+        L.gvh_ref_init.argtypes = [ctypes.c_int] * 3 + [ctypes.c_double] * 6
+        L.gvh_ref_rk2_step.argtypes = [ctypes.c_double] * 3
+        L.gvh_ref_time_steps.argtypes = [ctypes.c_int] + [ctypes.c_double] * 3 + [ctypes.POINTER(ctypes.c_double)]
+        for fn in ("gvh_ref_set_state", "gvh_ref_get_state", "gvh_ref_set_primitive_state"):
+            getattr(L, fn).argtypes = [ctypes.c_void_p]
+        L.gvh_ref_set_primitive_state_p.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.gvh_ref_equilibrium_pressure.argtypes = [ctypes.c_double]
+        L.gvh_ref_equilibrium_pressure.restype = ctypes.c_double
+        self._L = L
+        assert L.gvh_ref_nq() == self.nq, (L.gvh_ref_nq(), self.nq)
+        assert L.gvh_ref_precision_bytes() == (8 if precision == "fp64" else 4)
+        p = self.params
+        if L.gvh_ref_init(p["nx"], p["ny"], p["nz"], p["dx"], p["dy"], p["dz"], p["dt"], p["etabar"], p["theta"]):
+            raise ValueError("gvh_ref_init failed (sizes differ from this process's first lattice?)")
+
+    def _ok(self, rc, what):
+        if rc != 0:
+            raise RuntimeError(f"reference CUDA build: {what} failed ({rc})")
+
+    def set_primitive(self, prim: dict, p=None):
+        arrs = self._prim_list(prim)
+        if p is None:
+            self._ok(self._L.gvh_ref_set_primitive_state(_ptrs(arrs)), "set_primitive_state")
+        else:
+            pa = np.ascontiguousarray(p, dtype=np.float64)
+            self._ok(self._L.gvh_ref_set_primitive_state_p(_ptrs(arrs), pa.ctypes.data), "set_primitive_state_p")
+
+    def set_state(self, state: dict):
+        arrs = self._field_list(state)
+        self._ok(self._L.gvh_ref_set_state(_ptrs(arrs)), "set_state")
+
+    def get_state(self) -> dict:
+        arrs = [np.zeros(self.ng) for _ in self.field_names]
+        self._ok(self._L.gvh_ref_get_state(_ptrs(arrs)), "get_state")
+        return dict(zip(self.field_names, arrs))
+
+    def step(self, t, dt, T_reg=0.0):
+        self._ok(self._L.gvh_ref_rk2_step(t, dt, T_reg), "rk2_step")
+
+    def time_steps(self, n, t0, dt, T_reg=0.0) -> float:
+        """n steps of the reference's loop from t0; returns the CUDA-event time in ms."""
+        ms = ctypes.c_double()
+        self._ok(self._L.gvh_ref_time_steps(int(n), t0, dt, T_reg, ctypes.byref(ms)), "time_steps")
+        return ms.value
+
+    def pressure(self, e):
+        return self._L.gvh_ref_equilibrium_pressure(e)

@@ -1,4 +1,5 @@
-"""Build recipe for oracle/_ref: the reference's own hot-path sources compiled for the CPU.
+"""Build recipe for oracle/_ref: the reference's own hot-path sources compiled for the CPU
+(and, further down, with nvcc for the GPU, as shipped and in FP64).
 
 Test infrastructure only (the pinning oracle and the benchmark's reference arm). It
 compiles gpu-vh's rhic/src/*.cu files IN PLACE from the reference tree with g++ through
@@ -138,6 +139,86 @@ def build_cornelius() -> str:
     return lib
 
 
+# ---- the reference's own CUDA build (nvcc, sm_100a) -------------------------------------
+# The same hot-path sources plus the files that hold its launches and device state, compiled
+# with relocatable device code and linked with oracle/ref_gpu_driver.cu into one shared
+# library per variant (oracle/_ref/libref_gpu_<variant>.so). "fp32" is the build as shipped;
+# "fp64" adds the PRECISION double overlay (oracle/ref_gpu_shim). The limiter slope is a
+# literal in FluxLimiter.cu:15 (THETA 2.0): the 2.0 variants compile that file unchanged,
+# the 1.8 variants compile a generated overlay copy whose only change is the literal.
+GPU_SOURCES = SOURCES + [
+    "HydrodynamicValidity.cu",
+    "FullyDiscreteKurganovTadmorScheme.cu",
+    "GhostCells.cu",
+    "DynamicalVariables.cu",
+    "CudaConfiguration.cu",
+]
+# (precision, eos, physics, theta): the benchmark event's physics as shipped and in FP64,
+# and the 33x33x17 conformal configuration (theta 1.8) in both precisions
+GPU_VARIANTS = [
+    ("fp32", "qcd", "bulk", "2.0"),
+    ("fp64", "qcd", "bulk", "2.0"),
+    ("fp32", "conf", "shear", "1.8"),
+    ("fp64", "conf", "shear", "1.8"),
+]
+NVCC_ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def gpu_variant_name(prec: str, eos: str, phys: str, theta: str) -> str:
+    return f"{prec}_{eos}_{phys}_th{theta}"
+
+
+def gpu_lib_path(name: str) -> str:
+    return os.path.join(OUT, f"libref_gpu_{name}.so")
+
+
+def _overlay_flux_limiter_theta(theta: str) -> str:
+    src = os.path.join(REF_ROOT, "rhic", "src", "FluxLimiter.cu")
+    with open(src) as f:
+        text = f.read()
+    needle = "#define THETA 2.0"
+    if needle not in text:
+        raise RuntimeError(f"{src}: expected '{needle}' not found")
+    d = os.path.join(OUT, "overlay", f"theta{theta}")
+    os.makedirs(d, exist_ok=True)
+    dst = os.path.join(d, "FluxLimiter.cu")
+    with open(dst, "w") as f:
+        f.write(text.replace(needle, f"#define THETA {theta}"))
+    return dst
+
+
+def build_gpu_variant(prec: str, eos: str, phys: str, theta: str) -> str:
+    name = gpu_variant_name(prec, eos, phys, theta)
+    flags = PRECISIONS[prec] + EOS[eos] + PHYSICS[phys] + [f"-DGVH_REF_THETA={theta}"]
+    obj_dir = os.path.join(OUT, "obj", "gpu_" + name)
+    os.makedirs(obj_dir, exist_ok=True)
+    src_dir = os.path.join(REF_ROOT, "rhic", "src")
+    inc = ["-I", os.path.join(HERE, "ref_gpu_shim"), "-I", os.path.join(REF_ROOT, "rhic", "include"), "-I", src_dir]
+    common = ["nvcc"] + NVCC_ARCH + ["-O3", "-rdc=true", "-Xcompiler", "-fPIC", "-w", "-std=c++14"] + inc + flags
+    flux = os.path.join(src_dir, "FluxLimiter.cu") if theta == "2.0" else _overlay_flux_limiter_theta(theta)
+    objs = []
+    for s in [os.path.join(src_dir, x) for x in GPU_SOURCES] + [flux, os.path.join(HERE, "ref_gpu_driver.cu")]:
+        o = os.path.join(obj_dir, os.path.basename(s) + ".o")
+        _run(common + ["-x", "cu", "-c", s, "-o", o])
+        objs.append(o)
+    lib = gpu_lib_path(name)
+    _run(["nvcc"] + NVCC_ARCH + ["-shared", "-rdc=true", "-Xcompiler", "-fPIC", "-o", lib] + objs)
+    return lib
+
+
+def build_gpu(jobs: int | None = None, verbose: bool = True) -> list[str]:
+    """Build the reference's CUDA variants (nvcc cross-compiles without a GPU). Skips
+    (returns []) when the reference tree is not present."""
+    if not os.path.isdir(os.path.join(REF_ROOT, "rhic", "src")):
+        return []
+    os.makedirs(OUT, exist_ok=True)
+    with ThreadPoolExecutor(max_workers=jobs or min(4, os.cpu_count() or 4)) as ex:
+        libs = list(ex.map(lambda v: build_gpu_variant(*v), GPU_VARIANTS))
+    if verbose:
+        print(f"[oracle/_ref] built {len(libs)} CUDA variants of the reference into {OUT}")
+    return libs
+
+
 def build(jobs: int | None = None, verbose: bool = True) -> list[str]:
     """Build every variant; returns the library paths. Skips (returns []) when the
     reference tree is not present, e.g. on a host that only runs prebuilt files."""
@@ -152,6 +233,7 @@ def build(jobs: int | None = None, verbose: bool = True) -> list[str]:
     with ThreadPoolExecutor(max_workers=jobs or min(12, os.cpu_count() or 4)) as ex:
         libs = list(ex.map(lambda n: build_variant(n, fl, va), names))
     libs.append(build_cornelius())
+    libs += build_gpu(jobs=4, verbose=verbose)
     shutil.rmtree(os.path.join(OUT, "obj"), ignore_errors=True)
     if verbose:
         print(f"[oracle/_ref] built {len(libs)} variants into {OUT}")

@@ -54,41 +54,5 @@ static inline double gvh_ref_rsqrt(double x) { return 1.0 / sqrt(x); }
 
 #endif /* GVH_REF_SHIM_TYPES_ */
 
-/* ---- overlays: evaluated at every inclusion ---------------------------------------- */
-#ifdef GVH_REF_FP64
-#undef PRECISION
-#define PRECISION double
-#undef fminf
-#define fminf fmin
-#undef fmaxf
-#define fmaxf fmax
-#undef fabsf
-#define fabsf fabs
-#undef sqrtf
-#define sqrtf sqrt
-#undef fmaf
-#define fmaf fma
-#undef tanhf
-#define tanhf tanh
-#undef powf
-#define powf pow
-#undef rsqrtf
-#define rsqrtf gvh_ref_rsqrt
-#undef fdividef
-#define fdividef(a, b) ((a) / (b))
-#endif
-
-#if defined(GVH_REF_NO_BULK) || defined(GVH_REF_IDEAL)
-#undef PI
-#undef NUMBER_PI_COMPONENTS
-#define NUMBER_PI_COMPONENTS 0
-#endif
-
-#ifdef GVH_REF_IDEAL
-#undef PIMUNU
-#undef NUMBER_PROPAGATED_PIMUNU_COMPONENTS
-#define NUMBER_PROPAGATED_PIMUNU_COMPONENTS 0
-#ifndef IDEAL
-#define IDEAL
-#endif
-#endif
+/* ---- overlays: evaluated at every inclusion (shared with the nvcc build) ---------- */
+#include "gvh_ref_overlays.h"
