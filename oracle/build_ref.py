@@ -199,7 +199,15 @@ def build_gpu_variant(prec: str, eos: str, phys: str, theta: str) -> str:
     objs = []
     for s in [os.path.join(src_dir, x) for x in GPU_SOURCES] + [flux, os.path.join(HERE, "ref_gpu_driver.cu")]:
         o = os.path.join(obj_dir, os.path.basename(s) + ".o")
-        _run(common + ["-x", "cu", "-c", s, "-o", o])
+        extra = []
+        if prec == "fp64" and os.path.basename(s) == "HydrodynamicValidity.cu":
+            # checkValidityKernel is launched with a fixed 16x16x2 = 512-thread block
+            # (HydrodynamicValidity.cu:233, CudaConfiguration.cuh:36-38), which fits an SM's
+            # 65536 registers only at <= 128 per thread; in double precision nvcc gives it 134
+            # and the launch fails (the reference ignores the error). The as-shipped FP32
+            # build needs 79 and is compiled unchanged.
+            extra = ["-maxrregcount=128"]
+        _run(common + extra + ["-x", "cu", "-c", s, "-o", o])
         objs.append(o)
     lib = gpu_lib_path(name)
     _run(["nvcc"] + NVCC_ARCH + ["-shared", "-rdc=true", "-Xcompiler", "-fPIC", "-o", lib] + objs)
