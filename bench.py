@@ -252,6 +252,23 @@ def run_reference(args):
     gpu = reference_gpu_timings(args, w, prim)
     if gpu:
         line["reference_gpu"] = gpu
+    # the 33x33x17 conformal configuration: its 100 steps, on the host cores and on this GPU
+    w1 = workloads.CONFIG1
+    prim1 = workloads.gaussian_profile(w1)
+    if oracle.ref_available("fp64_conf_shear"):
+        R1 = oracle.RefLattice(threads=threads, **w1.lattice_kwargs())
+        R1.set_primitive(prim1)
+        t0 = time.perf_counter()
+        t = w1.tau0
+        for n in range(w1.steps):
+            R1.step(t, w1.dtau)
+            t = w1.tau0 + (n + 1) * w1.dtau
+        el1 = time.perf_counter() - t0
+        c1 = w1.nx * w1.ny * w1.nz
+        line["config1"] = {"workload": w1.name, "steps": w1.steps,
+                           "cpu": {"ms_per_step": el1 / w1.steps * 1e3, "cell_updates_per_s": c1 * w1.steps / el1,
+                                   "cores": threads},
+                           "gpu": reference_gpu_timings(argparse.Namespace(steps=w1.steps, warmup=5), w1, prim1)}
     print(json.dumps(line))
     return 0
 
@@ -588,6 +605,15 @@ def run_ours(args):
         Lm.close()
         extras["mixed_cell_updates_per_s"] = cells / (ms_mixed / 1e3)
         extras["mixed_ms_per_step"] = ms_mixed
+        # the 33x33x17 conformal configuration (its 100 steps, after 5 warm-up steps)
+        w1 = workloads.CONFIG1
+        L1 = _g.Lattice(device=local, **w1.lattice_kwargs())
+        L1.set_primitive(workloads.gaussian_profile(w1))
+        L1.set_stream(stream.cuda_stream)
+        ms1 = time_steps(L1, w1, w1.steps, 5, stream)
+        L1.close()
+        extras["config1_fp64"] = {"workload": w1.name, "ms_per_step": ms1,
+                                  "cell_updates_per_s": w1.nx * w1.ny * w1.nz / (ms1 / 1e3), "steps": w1.steps}
         ev = event_to_freezeout(w, prim, "fp64", local)
         ev["events_per_hour"] = 3600.0 / ev["seconds"] if ev["seconds"] > 0 else None
         extras["fp64_single_event_to_freezeout"] = ev
