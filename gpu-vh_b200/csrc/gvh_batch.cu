@@ -81,7 +81,6 @@ __device__ __forceinline__ StageArgs make_args(EventDev &E, bool stage2) {
   a.etabar = E.etabar; a.theta = E.theta; a.e_reg = E.e_reg;
   a.status = &E.status;
   a.diag = nullptr;  // validity diagnostics are a single-lattice option
-  a.wface = nullptr;  // the batched engine runs the fused stage kernel
   a.e = E.e;
   // twoStepRungeKutta receives t = t0 + n dt (HydroPlugin.cpp:424) and advances it by dt
   const double t = E.t0 + (double)E.step * E.dt;

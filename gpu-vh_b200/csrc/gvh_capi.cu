@@ -51,10 +51,6 @@ int fail(int code, const char *fmt, ...) {
 
 constexpr int kThreads = gvh::kBlock;
 
-#ifndef GVH_USE_SPLIT
-#define GVH_USE_SPLIT 1
-#endif
-
 }  // namespace
 
 
@@ -63,16 +59,6 @@ namespace {
 template <int EOS, bool SHEAR, bool BULK, bool MIXED>
 int launch_stage_p(const gvh_handle *h, const StageArgs &a, bool stage2) {
   const long long blocks = (h->ncells + kThreads - 1) / kThreads;
-  if (a.wface) {
-    // split form: the face recoveries, then the rest of the stage
-    const long long fblocks = (h->ncells + kFaceBlock - 1) / kFaceBlock;
-    kt_face_kernel<EOS, SHEAR, BULK><<<(unsigned)fblocks, kFaceBlock, 0, h->stream>>>(a);
-    const size_t ssmem = stage_split_smem_bytes<SHEAR, BULK>();
-    if (stage2) kt_stage_split_kernel<EOS, SHEAR, BULK, true, MIXED><<<(unsigned)blocks, kThreads, ssmem, h->stream>>>(a);
-    else kt_stage_split_kernel<EOS, SHEAR, BULK, false, MIXED><<<(unsigned)blocks, kThreads, ssmem, h->stream>>>(a);
-    GVH_CUDA(cudaGetLastError());
-    return GVH_OK;
-  }
   const size_t smem = stage_smem_bytes<SHEAR, BULK>();
   if (stage2) kt_stage_kernel<EOS, SHEAR, BULK, true, MIXED><<<(unsigned)blocks, kThreads, smem, h->stream>>>(a);
   else kt_stage_kernel<EOS, SHEAR, BULK, false, MIXED><<<(unsigned)blocks, kThreads, smem, h->stream>>>(a);
@@ -231,10 +217,7 @@ int gvh_create(const gvh_lattice_params *L, const gvh_hydro_params *H, const gvh
   h->eos = o.eos; h->shear = o.shear; h->bulk = o.bulk; h->precision = o.precision; h->device = dev;
   h->ucur = 0; h->uprev = 1; h->ufree = 2;
 
-  // The QCD equation of state is solved by Newton's method at every face: those solves run
-  // in a kernel of their own (split form), which needs room for their results.
-  const bool split = GVH_USE_SPLIT && o.eos == GVH_EOS_QCD;
-  size_t nbuf = 2 * (size_t)h->nq + 3 + 12 + (split ? kFaceFields : 0);
+  size_t nbuf = 2 * (size_t)h->nq + 3 + 12;
   size_t bytes = nbuf * h->cs * sizeof(double) + 256;
   if (cudaMalloc(&h->block, bytes) != cudaSuccess) {
     delete h;
@@ -248,7 +231,6 @@ int gvh_create(const gvh_lattice_params *L, const gvh_hydro_params *H, const gvh
   h->pA = b; b += h->cs;
   h->pB = b; b += h->cs;
   for (int m = 0; m < 3; ++m) { h->u[m] = b; b += 4 * h->cs; }
-  if (split) { h->wface = b; b += kFaceFields * h->cs; }
   h->status = reinterpret_cast<unsigned *>(b);
   if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
     cudaFree(h->block);
@@ -289,7 +271,7 @@ int gvh_destroy(gvh_handle *h) {
 int gvh_num_conserved(const gvh_handle *h) { return h ? h->nq : GVH_ERR_INVALID; }
 int gvh_num_fields(const gvh_handle *h) { return h ? h->nq + 10 : GVH_ERR_INVALID; }
 long long gvh_num_lattice_cells(const gvh_handle *h) { return h ? h->ng : GVH_ERR_INVALID; }
-int gvh_launches_per_step(const gvh_handle *h) { return h ? (h->wface ? 4 : 2) : GVH_ERR_INVALID; }
+int gvh_launches_per_step(const gvh_handle *h) { return h ? 2 : GVH_ERR_INVALID; }
 
 int gvh_set_state(gvh_handle *h, const double *const *fields, int n_fields) {
   if (!h || !fields) return fail(GVH_ERR_INVALID, "gvh_set_state: null argument");
@@ -381,7 +363,6 @@ int gvh_rk2_step(gvh_handle *h, double t, double dt, double T_reg) {
                                           : energy_density_of_T<EOS_QCD>(T_reg);
   a.status = h->status;
   a.e = h->e;
-  a.wface = h->wface;
   const double t1 = t + dt;
   // stage 1 (predictor)
   a.t_euler = t; a.t_after = t1;

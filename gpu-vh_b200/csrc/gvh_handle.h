@@ -13,7 +13,6 @@ struct gvh_handle {
   cudaStream_t stream;      // where work is queued (own_stream unless the caller set one)
   cudaStream_t own_stream;
   double *block;
-  double *wface;            // split form (QCD): face velocity ratios between the two kernels
   double *qA, *qB, *e, *pA, *pB, *u[3];
   int ucur, uprev, ufree;
   unsigned *status;

@@ -56,8 +56,6 @@ struct StageArgs {
   unsigned *status;       // or-ed STATUS_* bits
   double *diag;           // stage 2, optional: regulation factor (component 0) and the centre's
                           // q^n pi^{mu nu}, Pi (components 13..23) for the validity diagnostics
-  double *wface;          // split form: the face velocity ratios of kt_face_kernel (kFaceFields
-                          // components of stride cs), written by it and read by the stage kernel
 };
 
 // Components of the validity block (VALIDITY_DOMAIN, DynamicalVariables.cuh:82-98, in that
@@ -201,7 +199,7 @@ __device__ __forceinline__ void axis_pi_sources(const StageArgs &a, int s, int a
   }
 }
 
-template <int EOS, bool SHEAR, bool BULK, bool MIXED, bool SPLIT = false>
+template <int EOS, bool SHEAR, bool BULK, bool MIXED>
 __device__ __forceinline__ void axis_update(const StageArgs &a, int s, int axis, int idx, int n_axis, int stride,
                                             double inv_spacing, const GuessEos &g0, const double *uc, double *out,
                                             double *cache, unsigned &status) {
@@ -212,17 +210,8 @@ __device__ __forceinline__ void axis_update(const StageArgs &a, int s, int axis,
   const R inv_d = R(inv_spacing);
   // Face states are recovered in FP64 on both paths (the mixed path rounds only the
   // resulting speeds): an FP32 recovery was tried and let a 2+1D hotspot event run away
-  // to NaN that the FP64 recovery keeps finite. The split form reads the four ratios that
-  // kt_face_kernel stored for this cell and axis.
-  FaceSpeeds<double> fd;
-  if (SPLIT) {
-    const double *w = a.wface + (size_t)(4 * axis) * a.cs + s;
-    fd.wRf = w[0]; fd.wLf = w[a.cs]; fd.wRb = w[2 * a.cs]; fd.wLb = w[3 * a.cs];
-    fd.af = fmax(fabs(fd.wLf), fabs(fd.wRf));
-    fd.ab = fmax(fabs(fd.wLb), fabs(fd.wRb));
-  } else {
-    fd = face_speeds<EOS, SHEAR, BULK>(a, s, axis, o, g0, cache, status);
-  }
+  // to NaN that the FP64 recovery keeps finite.
+  const FaceSpeeds<double> fd = face_speeds<EOS, SHEAR, BULK>(a, s, axis, o, g0, cache, status);
   FaceSpeeds<R> f;
   f.wRf = (R)fd.wRf; f.wLf = (R)fd.wLf; f.wRb = (R)fd.wRb; f.wLb = (R)fd.wLb;
   f.af = (R)fd.af; f.ab = (R)fd.ab;
@@ -235,16 +224,7 @@ __device__ __forceinline__ void axis_update(const StageArgs &a, int s, int axis,
     // T^{tau mu}, pi^{tau mu} and Pi: the states phase A cached; pi^{ij}: from the lattice
     const int r_cached = n < 8 ? n : (BULK && n == NQ - 1) ? 8 : -1;
     R r;
-    if (SPLIT && r_cached >= 0) {
-      // the root-find components' states in FP64, as phase A forms them, then rounded
-      const double *q = a.qin + (size_t)n * a.cs + s;
-      const double q0 = __ldg(q + o[0]), q1 = __ldg(q + o[1]), q2 = __ldg(q), q3 = __ldg(q + o[3]);
-      const double q4 = __ldg(q + o[4]);
-      const double Dm = limited_slope(a.theta, q0, q1, q2);
-      const double D0 = limited_slope(a.theta, q1, q2, q3);
-      const double Dp = limited_slope(a.theta, q2, q3, q4);
-      r = flux_from_states<R>((R)(q3 - Dp / 2), (R)(q2 + D0 / 2), (R)(q2 - D0 / 2), (R)(q1 + Dm / 2), f);
-    } else if (r_cached >= 0) {
+    if (r_cached >= 0) {
       const double *c = cache + 4 * r_cached * kBlock;
       r = flux_from_states<R>((R)c[0], (R)c[kBlock], (R)c[2 * kBlock], (R)c[3 * kBlock], f);
     } else {
@@ -261,12 +241,6 @@ __device__ __forceinline__ void axis_update(const StageArgs &a, int s, int axis,
 template <bool SHEAR, bool BULK>
 constexpr size_t stage_smem_bytes() {
   return (size_t)(NComp<SHEAR, BULK>::value + 4 * (4 + (SHEAR ? 4 : 0) + (BULK ? 1 : 0))) * kBlock * sizeof(double);
-}
-
-// The split form keeps only the running update in shared memory.
-template <bool SHEAR, bool BULK>
-constexpr size_t stage_split_smem_bytes() {
-  return (size_t)NComp<SHEAR, BULK>::value * kBlock * sizeof(double);
 }
 
 #ifndef GVH_MIN_BLOCKS
@@ -437,7 +411,7 @@ __device__ __forceinline__ double stage_finish(const StageArgs &a, long long s, 
   return pr.e;
 }
 
-template <int EOS, bool SHEAR, bool BULK, bool STAGE2, bool MIXED, bool SPLIT = false>
+template <int EOS, bool SHEAR, bool BULK, bool STAGE2, bool MIXED>
 __device__ __forceinline__ double stage_cell(const StageArgs &a, long long id) {
   using R = typename std::conditional<MIXED, float, double>::type;
   constexpr int NQ = NComp<SHEAR, BULK>::value;
@@ -469,8 +443,8 @@ __device__ __forceinline__ double stage_cell(const StageArgs &a, long long id) {
     const int n_axis = axis == 0 ? a.nx : axis == 1 ? a.ny : a.nz;
     const int stride = axis == 0 ? 1 : axis == 1 ? (int)a.sy : (int)a.sz;
     const double inv_spacing = axis == 0 ? a.inv_dx : axis == 1 ? a.inv_dy : a.inv_dz;
-    axis_update<EOS, SHEAR, BULK, MIXED, SPLIT>(a, (int)s, axis, idx, n_axis, stride, inv_spacing, g0, uc, out,
-                                                cache, status);
+    axis_update<EOS, SHEAR, BULK, MIXED>(a, (int)s, axis, idx, n_axis, stride, inv_spacing, g0, uc, out, cache,
+                                         status);
   }
 
   return stage_finish<EOS, SHEAR, BULK, STAGE2, kBlock>(a, s, out, g0, status);
@@ -483,84 +457,6 @@ template <int EOS, bool SHEAR, bool BULK, bool STAGE2, bool MIXED>
 __global__ void __launch_bounds__(kBlock, GVH_MIN_BLOCKS) kt_stage_kernel(const StageArgs a) {
   const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (id < a.ncells) stage_cell<EOS, SHEAR, BULK, STAGE2, MIXED>(a, id);
-}
-
-// ---- split form: the face recoveries as a kernel of their own ------------------------------
-// kt_face_kernel does, for every interior cell, the 12 face recoveries of one stage (both
-// sides of both faces of each axis, each with the cell's own energy density as the guess,
-// EulerStep.cu:1054-1062) and stores u^axis/u^tau of each in wface[(4 axis + h) cs + s]
-// (h: 0 fwd R, 1 fwd L, 2 bwd R, 3 bwd L). Without the flux and source-term code around them
-// the solves need few registers, so many more warps per SM hide their FP64 latency;
-// kt_stage_split_kernel then does the rest of the stage with the stored ratios. The
-// arithmetic of every recovery and every flux is the fused kernel's.
-#ifndef GVH_FACE_BLOCK
-#define GVH_FACE_BLOCK 128
-#endif
-#ifndef GVH_FACE_MIN_BLOCKS
-#define GVH_FACE_MIN_BLOCKS 8
-#endif
-#ifndef GVH_SPLIT_MIN_BLOCKS
-#define GVH_SPLIT_MIN_BLOCKS 4
-#endif
-constexpr int kFaceBlock = GVH_FACE_BLOCK;
-constexpr int kFaceFields = 12;
-
-template <int EOS, bool SHEAR, bool BULK>
-__device__ __forceinline__ void face_cell(const StageArgs &a, long long id) {
-  constexpr int NR = 4 + (SHEAR ? 4 : 0) + (BULK ? 1 : 0);
-  const int i = (int)(id % a.nx);
-  const int j = (int)((id / a.nx) % a.ny);
-  const int k = (int)(id / ((long long)a.nx * a.ny));
-  const long long s = i + a.sy * j + a.sz * k;
-  unsigned status = 0;
-  const GuessEos g0 = guess_eos<EOS>(a.e[s]);
-#pragma unroll 1
-  for (int axis = 0; axis < 3; ++axis) {
-    const int idx = axis == 0 ? i : axis == 1 ? j : k;
-    const int n_axis = axis == 0 ? a.nx : axis == 1 ? a.ny : a.nz;
-    const int stride = axis == 0 ? 1 : axis == 1 ? (int)a.sy : (int)a.sz;
-#pragma unroll 1
-    for (int h = 0; h < 4; ++h) {
-      // the three-point window of the limited slope this state needs (HalfSiteExtrapolation.cu
-      // :15-30): fwd qR = q(i+1) - D(i+1)/2, fwd qL = q(i) + D(i)/2, bwd qR = q(i) - D(i)/2,
-      // bwd qL = q(i-1) + D(i-1)/2, the window centred on the cell named
-      const int c0 = idx + (h == 0 ? 1 : h == 3 ? -1 : 0);
-      const int om = (min(max(c0 - 1, 0), n_axis - 1) - idx) * stride;
-      const int oc = (min(max(c0, 0), n_axis - 1) - idx) * stride;
-      const int op = (min(max(c0 + 1, 0), n_axis - 1) - idx) * stride;
-      double st[9][1];
-#pragma unroll
-      for (int r = 0; r < 9; ++r) {
-        if (r < NR) {
-          const double *q = a.qin + (size_t)(r < 8 ? r : 14) * a.cs + s;
-          const double x = __ldg(q + om), y = __ldg(q + oc), z = __ldg(q + op);
-          const double D = limited_slope(a.theta, x, y, z);
-          st[r][0] = (h & 1) ? y + D / 2 : y - D / 2;
-        } else {
-          st[r][0] = 0.0;
-        }
-      }
-      double w1[1];
-      inferred_face_n<EOS, 1>(a.t_euler, axis, st[0], st[1], st[2], st[3], st[4], st[5], st[6], st[7], st[8], g0,
-                              w1, status);
-      a.wface[(size_t)(4 * axis + h) * a.cs + s] = w1[0];
-    }
-  }
-  if (status) atomicOr(a.status, status);
-}
-
-template <int EOS, bool SHEAR, bool BULK>
-__global__ void __launch_bounds__(kFaceBlock, GVH_FACE_MIN_BLOCKS) kt_face_kernel(const StageArgs a) {
-  const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (id < a.ncells) face_cell<EOS, SHEAR, BULK>(a, id);
-}
-
-// The stage with the face ratios of kt_face_kernel (a.wface). Launch with
-// stage_split_smem_bytes<SHEAR, BULK>() of dynamic shared memory.
-template <int EOS, bool SHEAR, bool BULK, bool STAGE2, bool MIXED>
-__global__ void __launch_bounds__(kBlock, GVH_SPLIT_MIN_BLOCKS) kt_stage_split_kernel(const StageArgs a) {
-  const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (id < a.ncells) stage_cell<EOS, SHEAR, BULK, STAGE2, MIXED, true>(a, id);
 }
 
 // Raises a stage kernel's dynamic shared-memory limit to what it is launched with. A kernel
