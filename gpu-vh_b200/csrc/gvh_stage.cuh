@@ -146,9 +146,11 @@ template <class R>
 __device__ __forceinline__ R flux_from_states(R fR, R fL, R bR, R bL, const FaceSpeeds<R> &f) {
   // F(qR) and F(qL) are rounded separately (no fused multiply-add across the pair), which
   // keeps the scheme exactly mirror-symmetric.
-  const R Hf = (mul_rn(fR, f.wRf) + mul_rn(fL, f.wLf) - f.af * (fR - fL)) * R(0.5);
-  const R Hb = (mul_rn(bR, f.wRb) + mul_rn(bL, f.wLb) - f.ab * (bR - bL)) * R(0.5);
-  return -Hf + Hb;
+  // The halving of both fluxes is applied once to their difference: a power-of-two scaling
+  // commutes with rounding, so the value is the same.
+  const R Hf = mul_rn(fR, f.wRf) + mul_rn(fL, f.wLf) - f.af * (fR - fL);
+  const R Hb = mul_rn(bR, f.wRb) + mul_rn(bL, f.wLb) - f.ab * (bR - bL);
+  return (-Hf + Hb) * R(0.5);
 }
 
 template <class R>
