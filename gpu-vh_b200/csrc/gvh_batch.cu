@@ -323,6 +323,7 @@ int gvh_batch_create(const gvh_options *opts, long long arena_bytes, gvh_batch *
   if (o.precision != GVH_PRECISION_FP64 && o.precision != GVH_PRECISION_MIXED)
     return bfail(GVH_ERR_INVALID, "unknown precision");
   if (arena_bytes <= 0) return bfail(GVH_ERR_INVALID, "arena_bytes must be > 0");
+  if (!(o.theta > 0)) return bfail(GVH_ERR_INVALID, "the limiter's theta must be > 0");
   int dev = o.device;
   if (dev < 0) BCUDA(cudaGetDevice(&dev));
   BCUDA(cudaSetDevice(dev));

@@ -187,6 +187,7 @@ int gvh_create(const gvh_lattice_params *L, const gvh_hydro_params *H, const gvh
     return fail(GVH_ERR_INVALID, "gvh_create: unknown precision mode %d", o.precision);
   if (o.shear && !(H->shearViscosityToEntropyDensity > 0))
     return fail(GVH_ERR_INVALID, "gvh_create: eta/s must be > 0 with shear");
+  if (!(o.theta > 0)) return fail(GVH_ERR_INVALID, "gvh_create: the limiter's theta must be > 0");
   int dev = o.device;
   if (dev < 0) GVH_CUDA(cudaGetDevice(&dev));
   GVH_CUDA(cudaSetDevice(dev));

@@ -120,6 +120,7 @@ int gvh_rk2_step_noalloc(const gvh_lattice_params *L, const gvh_hydro_params *H,
     return nfail(GVH_ERR_INVALID, "gvh_rk2_step_noalloc: unknown eos");
   if (o.precision != GVH_PRECISION_FP64 && o.precision != GVH_PRECISION_MIXED)
     return nfail(GVH_ERR_INVALID, "gvh_rk2_step_noalloc: unknown precision");
+  if (!(o.theta > 0)) return nfail(GVH_ERR_INVALID, "gvh_rk2_step_noalloc: the limiter's theta must be > 0");
   if (u_next == u || u_next == u_prev)
     return nfail(GVH_ERR_INVALID, "gvh_rk2_step_noalloc: u_next must not alias u or u_prev");
   const int nq = 4 + (o.shear ? 10 : 0) + (o.bulk ? 1 : 0);

@@ -435,14 +435,15 @@ __device__ __forceinline__ double with_sign_of(double m, double s) {
 __device__ __forceinline__ float with_sign_of(float m, float s) {
   return __int_as_float(__float_as_int(m) | (__float_as_int(s) & (int)0x80000000));
 }
+// With theta > 0 (the C ABI rejects anything else) the slopes theta (y - x) and theta (z - y)
+// have the signs of the differences, and rounding is monotonic, so
+// min(|theta a|, |theta b|) = theta min(|a|, |b|) exactly: one multiplication by theta.
 template <class R>
 __device__ __forceinline__ R limited_slope(R theta, R x, R y, R z) {
-  const R left = theta * (y - x);
-  const R ctr = (z - x) / R(2);
-  const R right = theta * (z - y);
-  const unsigned sl = sign_bit(left);
-  const R m = fmin(fabs(left), fmin(fabs(ctr), fabs(right)));
-  return ((sl ^ sign_bit(ctr)) | (sl ^ sign_bit(right))) ? R(0) : with_sign_of(m, left);
+  const R dl = y - x, dc = z - x, dr = z - y;
+  const unsigned sl = sign_bit(dl);
+  const R m = fmin(theta * fmin(fabs(dl), fabs(dr)), fabs(dc) / R(2));
+  return ((sl ^ sign_bit(dc)) | (sl ^ sign_bit(dr))) ? R(0) : with_sign_of(m, dl);
 }
 
 }  // namespace gvh

@@ -141,16 +141,16 @@ __device__ __forceinline__ FaceSpeeds<double> face_speeds(const StageArgs &a, in
 __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
 
-// -H(i+1/2) + H(i-1/2) from the four half-cell states (fwd qR, fwd qL, bwd qR, bwd qL).
+// 2 (-H(i+1/2) + H(i-1/2)) from the four half-cell states (fwd qR, fwd qL, bwd qR, bwd qL).
 template <class R>
 __device__ __forceinline__ R flux_from_states(R fR, R fL, R bR, R bL, const FaceSpeeds<R> &f) {
   // F(qR) and F(qL) are rounded separately (no fused multiply-add across the pair), which
   // keeps the scheme exactly mirror-symmetric.
-  // The halving of both fluxes is applied once to their difference: a power-of-two scaling
-  // commutes with rounding, so the value is the same.
+  // Returned doubled: the halving of both fluxes is folded into the caller's 1/(2 d), a
+  // power-of-two scaling that commutes with rounding, so the value is the same.
   const R Hf = mul_rn(fR, f.wRf) + mul_rn(fL, f.wLf) - f.af * (fR - fL);
   const R Hb = mul_rn(bR, f.wRb) + mul_rn(bL, f.wLb) - f.ab * (bR - bL);
-  return (-Hf + Hb) * R(0.5);
+  return -Hf + Hb;
 }
 
 template <class R>
@@ -210,6 +210,7 @@ __device__ __forceinline__ void axis_update(const StageArgs &a, int s, int axis,
   const int o[5] = {(max(idx - 2, 0) - idx) * stride, (max(idx - 1, 0) - idx) * stride, 0,
                     (min(idx + 1, n_axis - 1) - idx) * stride, (min(idx + 2, n_axis - 1) - idx) * stride};
   const R inv_d = R(inv_spacing);
+  const R half_inv_d = R(0.5) * inv_d;  // the fluxes come doubled from flux_from_states
   // Face states are recovered in FP64 on both paths (the mixed path rounds only the
   // resulting speeds): an FP32 recovery was tried and let a 2+1D hotspot event run away
   // to NaN that the FP64 recovery keeps finite.
@@ -232,7 +233,7 @@ __device__ __forceinline__ void axis_update(const StageArgs &a, int s, int axis,
     } else {
       r = flux_difference<R>(th, a.qin + (size_t)n * a.cs + s, o, f);
     }
-    r = r * inv_d;
+    r = r * half_inv_d;
     if (SHEAR && n < 4) r += Sa[n];
     out[n * kBlock] += (double)r * a.dt;
   }

@@ -91,7 +91,7 @@ typedef struct gvh_options {
 	int shear;      /* evolve pi^{mu nu} (reference: PIMUNU macro, DynamicalVariables.cuh:13) */
 	int bulk;       /* evolve Pi, needs shear (reference: PI macro, DynamicalVariables.cuh:14) */
 	int precision;  /* GVH_PRECISION_* (reference: PRECISION macro, DynamicalVariables.cuh:44) */
-	double theta;   /* minmod limiter slope (reference: THETA 2.0, FluxLimiter.cu:15) */
+	double theta;   /* minmod limiter slope, > 0 (reference: THETA 2.0, FluxLimiter.cu:15) */
 	int device;     /* CUDA device ordinal; -1 = current device */
 } gvh_options;
 

@@ -61,3 +61,9 @@ def test_create_rejects_bad_lattice_without_gpu(lib):
     o.shear, o.bulk = 0, 1
     assert L.gvh_create(ctypes.byref(lat), ctypes.byref(hyd), ctypes.byref(o), ctypes.byref(h)) == -1
     assert b"bulk" in L.gvh_last_error()
+    # the limiter's closed form takes theta > 0 (minmod of theta-scaled differences)
+    o.shear, o.bulk = 1, 1
+    for bad in (0.0, -1.8, float("nan")):
+        o.theta = bad
+        assert L.gvh_create(ctypes.byref(lat), ctypes.byref(hyd), ctypes.byref(o), ctypes.byref(h)) == -1
+        assert b"theta" in L.gvh_last_error()
