@@ -438,11 +438,15 @@ __device__ __forceinline__ float with_sign_of(float m, float s) {
 // With theta > 0 (the C ABI rejects anything else) the slopes theta (y - x) and theta (z - y)
 // have the signs of the differences, and rounding is monotonic, so
 // min(|theta a|, |theta b|) = theta min(|a|, |b|) exactly: one multiplication by theta.
+// limited_slope2 returns twice the slope, from theta2 = 2 theta: the centred slope (z - x)/2
+// then needs no halving, and callers fold the 1/2 into a factor they apply anyway (the
+// half-cell states q +- D/2 become q +- D2/4, a derivative D/dx becomes D2 (1/(2 dx))).
+// Power-of-two scalings commute with rounding, so every value is the same.
 template <class R>
-__device__ __forceinline__ R limited_slope(R theta, R x, R y, R z) {
+__device__ __forceinline__ R limited_slope2(R theta2, R x, R y, R z) {
   const R dl = y - x, dc = z - x, dr = z - y;
   const unsigned sl = sign_bit(dl);
-  const R m = fmin(theta * fmin(fabs(dl), fabs(dr)), fabs(dc) / R(2));
+  const R m = fmin(theta2 * fmin(fabs(dl), fabs(dr)), fabs(dc));
   return ((sl ^ sign_bit(dc)) | (sl ^ sign_bit(dr))) ? R(0) : with_sign_of(m, dl);
 }
 

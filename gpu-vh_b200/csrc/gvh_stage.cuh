@@ -105,14 +105,15 @@ __device__ __forceinline__ FaceSpeeds<double> face_speeds(const StageArgs &a, in
     const int c = (r < 8) ? r : 14;
     const double *q = a.qin + (size_t)c * a.cs + s;
     const double q0 = __ldg(q + o[0]), q1 = __ldg(q + o[1]), q2 = __ldg(q), q3 = __ldg(q + o[3]), q4 = __ldg(q + o[4]);
-    const double Dm = limited_slope(a.theta, q0, q1, q2);
-    const double D0 = limited_slope(a.theta, q1, q2, q3);
-    const double Dp = limited_slope(a.theta, q2, q3, q4);
+    const double theta2 = 2 * a.theta;  // the slopes come doubled: q -+ D/2 = q -+ D2/4
+    const double Dm = limited_slope2(theta2, q0, q1, q2);
+    const double D0 = limited_slope2(theta2, q1, q2, q3);
+    const double Dp = limited_slope2(theta2, q2, q3, q4);
     double *cr = cache + 4 * r * kBlock;
-    cr[0] = q3 - Dp / 2;           // fwd qR
-    cr[kBlock] = q2 + D0 / 2;      // fwd qL
-    cr[2 * kBlock] = q2 - D0 / 2;  // bwd qR
-    cr[3 * kBlock] = q1 + Dm / 2;  // bwd qL
+    cr[0] = q3 - Dp * 0.25;           // fwd qR
+    cr[kBlock] = q2 + D0 * 0.25;      // fwd qL
+    cr[2 * kBlock] = q2 - D0 * 0.25;  // bwd qR
+    cr[3 * kBlock] = q1 + Dm * 0.25;  // bwd qL
   }
   double w[4] = {0, 0, 0, 0};
 #pragma unroll 1
@@ -157,10 +158,12 @@ template <class R>
 __device__ __forceinline__ R flux_difference(R theta, const double *q, const int (&o)[5], const FaceSpeeds<R> &f) {
   const R q0 = (R)__ldg(q + o[0]), q1 = (R)__ldg(q + o[1]), q2 = (R)__ldg(q), q3 = (R)__ldg(q + o[3]);
   const R q4 = (R)__ldg(q + o[4]);
-  const R Dm = limited_slope(theta, q0, q1, q2);
-  const R D0 = limited_slope(theta, q1, q2, q3);
-  const R Dp = limited_slope(theta, q2, q3, q4);
-  return flux_from_states<R>(q3 - Dp / R(2), q2 + D0 / R(2), q2 - D0 / R(2), q1 + Dm / R(2), f);
+  const R theta2 = R(2) * theta;  // doubled slopes: q -+ D/2 = q -+ D2/4
+  const R Dm = limited_slope2(theta2, q0, q1, q2);
+  const R D0 = limited_slope2(theta2, q1, q2, q3);
+  const R Dp = limited_slope2(theta2, q2, q3, q4);
+  const R qu = R(0.25);
+  return flux_from_states<R>(q3 - Dp * qu, q2 + D0 * qu, q2 - D0 * qu, q1 + Dm * qu, f);
 }
 
 // pi^{m a} component index for spatial m, a in {x, y, eta}.
@@ -283,15 +286,17 @@ __device__ __forceinline__ void stage_source(const StageArgs &a, long long s, in
   f.dtux = (R)((uc[1] - a.uprev[a.cs + s]) * inv_dt);
   f.dtuy = (R)((uc[2] - a.uprev[2 * a.cs + s]) * inv_dt);
   f.dtun = (R)((uc[3] - a.uprev[3 * a.cs + s]) * inv_dt);
-  const double thd = a.theta;
-  const double idxd = a.inv_dx, idyd = a.inv_dy, idzd = a.inv_dz;
+  // doubled slopes (limited_slope2) times 1/(2 dx): the limited derivatives of
+  // SourceTerms.cu:659-720
+  const double thd = 2 * a.theta;
+  const double idxd = 0.5 * a.inv_dx, idyd = 0.5 * a.inv_dy, idzd = 0.5 * a.inv_dz;
   R du[3][4];
 #pragma unroll
   for (int m = 0; m < 4; ++m) {
     const double *u = a.uin + m * a.cs + s;
-    du[0][m] = (R)(limited_slope(thd, __ldg(u + xm), uc[m], __ldg(u + xp)) * idxd);
-    du[1][m] = (R)(limited_slope(thd, __ldg(u + ym), uc[m], __ldg(u + yp)) * idyd);
-    du[2][m] = (R)(limited_slope(thd, __ldg(u + zm), uc[m], __ldg(u + zp)) * idzd);
+    du[0][m] = (R)(limited_slope2(thd, __ldg(u + xm), uc[m], __ldg(u + xp)) * idxd);
+    du[1][m] = (R)(limited_slope2(thd, __ldg(u + ym), uc[m], __ldg(u + yp)) * idyd);
+    du[2][m] = (R)(limited_slope2(thd, __ldg(u + zm), uc[m], __ldg(u + zp)) * idzd);
   }
   f.dxut = du[0][0]; f.dyut = du[1][0]; f.dnut = du[2][0];
   f.dxux = du[0][1]; f.dyux = du[1][1]; f.dnux = du[2][1];
@@ -299,9 +304,9 @@ __device__ __forceinline__ void stage_source(const StageArgs &a, long long s, in
   f.dxun = du[0][3]; f.dyun = du[1][3]; f.dnun = du[2][3];
   const double *p = a.pin + s;
   const double pcd = __ldg(p);
-  const R dxp = (R)(limited_slope(thd, __ldg(p + xm), pcd, __ldg(p + xp)) * idxd);
-  const R dyp = (R)(limited_slope(thd, __ldg(p + ym), pcd, __ldg(p + yp)) * idyd);
-  const R dnp = (R)(limited_slope(thd, __ldg(p + zm), pcd, __ldg(p + zp)) * idzd);
+  const R dxp = (R)(limited_slope2(thd, __ldg(p + xm), pcd, __ldg(p + xp)) * idxd);
+  const R dyp = (R)(limited_slope2(thd, __ldg(p + ym), pcd, __ldg(p + yp)) * idyd);
+  const R dnp = (R)(limited_slope2(thd, __ldg(p + zm), pcd, __ldg(p + zp)) * idzd);
 
   const R t = (R)a.t_euler;
   const R Pi = BULK ? q[NQ - 1] : R(0);
