@@ -466,11 +466,21 @@ int gvh_set_state_async(gvh_handle *h, const double *const *fields, int n_fields
   const size_t fb = h->ng * sizeof(double);
   // the input staging is free once the previous pack has read it
   GVH_CUDA(cudaStreamWaitEvent(h->s_h2d, h->ev_in_free, 0));
+  const double *srcs[32];
   for (int f = 0; f < n_fields; ++f) {
     const double *src = fields[f];
     if (!src && f >= h->nq + 6) src = fields[f - 4];  // up defaults to u
     if (!src) return fail(GVH_ERR_INVALID, "gvh_set_state_async: field %d is null", f);
-    GVH_CUDA(cudaMemcpyAsync(h->staging_in + f * h->ng, src, fb, cudaMemcpyDefault, h->s_h2d));
+    srcs[f] = src;
+  }
+  // one copy per run of fields that follow each other in host memory (a caller's
+  // [n_fields][ng] block is one copy): fewer, larger transfers share the link better with the
+  // copies going the other way
+  for (int f = 0; f < n_fields;) {
+    int g = f + 1;
+    while (g < n_fields && srcs[g] == srcs[f] + (size_t)(g - f) * h->ng) ++g;
+    GVH_CUDA(cudaMemcpyAsync(h->staging_in + f * h->ng, srcs[f], (g - f) * fb, cudaMemcpyDefault, h->s_h2d));
+    f = g;
   }
   GVH_CUDA(cudaEventRecord(h->ev_in_ready, h->s_h2d));
   GVH_CUDA(cudaStreamWaitEvent(h->stream, h->ev_in_ready, 0));
@@ -498,9 +508,13 @@ int gvh_get_state_async(gvh_handle *h, double *const *fields, int n_fields) {
   GVH_CUDA(cudaEventRecord(h->ev_out_ready, h->stream));
   GVH_CUDA(cudaStreamWaitEvent(h->s_d2h, h->ev_out_ready, 0));
   const size_t fb = h->ng * sizeof(double);
-  for (int f = 0; f < n_fields; ++f)
-    if (fields[f])
-      GVH_CUDA(cudaMemcpyAsync(fields[f], h->staging_out + f * h->ng, fb, cudaMemcpyDefault, h->s_d2h));
+  for (int f = 0; f < n_fields;) {  // runs of adjacent host fields, as in gvh_set_state_async
+    if (!fields[f]) { ++f; continue; }
+    int g = f + 1;
+    while (g < n_fields && fields[g] && fields[g] == fields[f] + (size_t)(g - f) * h->ng) ++g;
+    GVH_CUDA(cudaMemcpyAsync(fields[f], h->staging_out + f * h->ng, (g - f) * fb, cudaMemcpyDefault, h->s_d2h));
+    f = g;
+  }
   GVH_CUDA(cudaEventRecord(h->ev_out_free, h->s_d2h));
   return GVH_OK;
 }
