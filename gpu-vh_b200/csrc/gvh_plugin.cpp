@@ -23,8 +23,13 @@
 #include <algorithm>
 #include <cctype>
 #include <chrono>
+#include <condition_variable>
+#include <deque>
 #include <fstream>
+#include <memory>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/gvh.h"
@@ -283,6 +288,65 @@ int gvh_run(const gvh_lattice_params *L, const gvh_ic_params *ic, const gvh_hydr
   return rc;
 }
 
+namespace {
+
+// Writes surface.dat chunks on a thread of its own, in the order they are handed over, so
+// that the file writes overlap the host half of the next slabs. At most two chunks wait.
+class ChunkWriter {
+ public:
+  explicit ChunkWriter(FILE *fp) : fp_(fp) { th_ = std::thread([this] { loop(); }); }
+  ~ChunkWriter() { finish(); }
+  // false once a write has failed
+  bool push(std::vector<std::string> &&chunk) {
+    std::unique_lock<std::mutex> lock(mu_);
+    space_.wait(lock, [&] { return q_.size() < kMaxQueued || failed_; });
+    if (failed_) return false;
+    q_.push_back(std::move(chunk));
+    ready_.notify_one();
+    return true;
+  }
+  // waits until every chunk handed over is written; false if a write failed
+  bool finish() {
+    {
+      std::lock_guard<std::mutex> lock(mu_);
+      stop_ = true;
+    }
+    ready_.notify_one();
+    if (th_.joinable()) th_.join();
+    return !failed_;
+  }
+
+ private:
+  void loop() {
+    std::unique_lock<std::mutex> lock(mu_);
+    for (;;) {
+      ready_.wait(lock, [&] { return stop_ || !q_.empty(); });
+      if (q_.empty()) return;
+      std::vector<std::string> chunk = std::move(q_.front());
+      q_.pop_front();
+      space_.notify_one();
+      lock.unlock();
+      bool ok = true;
+      for (const std::string &part : chunk) ok = ok && fwrite(part.data(), 1, part.size(), fp_) == part.size();
+      chunk.clear();
+      lock.lock();
+      if (!ok) {
+        failed_ = true;
+        space_.notify_all();
+      }
+    }
+  }
+  static constexpr size_t kMaxQueued = 2;
+  FILE *fp_;
+  std::mutex mu_;
+  std::condition_variable ready_, space_;
+  std::deque<std::vector<std::string>> q_;
+  bool stop_ = false, failed_ = false;
+  std::thread th_;
+};
+
+}  // namespace
+
 int gvh_run_loop(gvh_handle *h, const gvh_lattice_params *L, const gvh_hydro_params *H, const char *output_dir,
                  int outputs, gvh_run_report *report) {
   if (!h || !L || !H) return pfail(GVH_ERR_INVALID, "gvh_run_loop: null argument");
@@ -322,6 +386,9 @@ int gvh_run_loop(gvh_handle *h, const gvh_lattice_params *L, const gvh_hydro_par
       }
     }
   }
+
+  std::unique_ptr<ChunkWriter> writer;
+  if (surf_file) writer.reset(new ChunkWriter(surf_file));
 
   const int nf = gvh_num_fields(h), nq = gvh_num_conserved(h);
   std::vector<std::vector<double>> fields;
@@ -386,10 +453,7 @@ int gvh_run_loop(gvh_handle *h, const gvh_lattice_params *L, const gvh_hydro_par
       gvh::surface::take_text(surf, chunk_text);
       chunk_rows += nel;
       if (flush == n) {
-        bool ok = true;
-        for (const std::string &part : chunk_text)
-          ok = ok && fwrite(part.data(), 1, part.size(), surf_file) == part.size();
-        if (!ok) {
+        if (!writer->push(std::move(chunk_text))) {
           g_plugin_error = "writing surface.dat failed";
           return GVH_ERR_INVALID;
         }
@@ -444,6 +508,11 @@ int gvh_run_loop(gvh_handle *h, const gvh_lattice_params *L, const gvh_hydro_par
     report->surface_bytes_to_host = si.bytes_to_host_total;
     report->surface_host_seconds = si.host_seconds_total;
   }
+  if (writer && !writer->finish() && !rc) {
+    g_plugin_error = "writing surface.dat failed";
+    rc = GVH_ERR_INVALID;
+  }
+  writer.reset();
   gvh_surface_destroy(surf);
   if (surf_file) fclose(surf_file);
   if (rc) return pfail(rc, g_plugin_error.empty() ? gvh_last_error() : g_plugin_error);

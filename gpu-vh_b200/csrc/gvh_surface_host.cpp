@@ -12,6 +12,7 @@
 
 #include "../../include/gvh.h"
 #include "gvh_cornelius.hpp"
+#include "gvh_format.hpp"
 #include "gvh_surface_internal.h"
 
 namespace gvh {
@@ -80,13 +81,13 @@ double interp3(double x0, double x1, double x2, const double a[2][2][2][2]) {
 }
 
 // One row as the reference's ofstream writes it: default format (%g, 6 significant digits),
-// values separated by spaces, a newline after the last. std::to_chars with the general
-// format and precision 6 gives the same characters as printf's %g.
+// values separated by spaces, a newline after the last (gvh_format.hpp: the same characters
+// as printf's %g).
 void append_row_text(std::string &out, const double *row) {
   char buf[kColumns * 32];
   char *p = buf;
   for (int c = 0; c < kColumns; ++c) {
-    p = std::to_chars(p, buf + sizeof buf, row[c], std::chars_format::general, 6).ptr;
+    p = fmt::g6(p, buf + sizeof buf, row[c]);
     *p++ = c + 1 < kColumns ? ' ' : '\n';
   }
   out.append(buf, p - buf);
