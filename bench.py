@@ -583,15 +583,23 @@ def run_ours(args):
     b_cell = bytes_per_cell_update(L.nq)
     achieved = cells * b_cell / (ms / args.steps / 1e3) / 1e9
     traffic = None
+    fp64_pipe = None
     tp = os.path.join(ROOT, "profiles", "kt_stage_traffic.json")
     if os.path.exists(tp):
         try:
-            traffic = json.load(open(tp)).get("bytes_per_step")
+            prof = json.load(open(tp))
+            traffic = prof.get("bytes_per_step")
+            fp64_pipe = prof.get("fp64_pipe_active_pct")
         except Exception:
             traffic = None
+    # One step is the kernel's two launches (stage 1 + stage 2): achieved, traffic and the
+    # algorithmic bytes are all per step. The kernel's real limit is FP64 issue, so the FP64
+    # pipe's busy fraction from the same capture is given beside the HBM roofline.
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "peak_source": peak_kind,
                 "algorithmic_bytes_per_step": cells * b_cell,
+                "per": "step (2 launches of kt_stage_kernel)",
+                "fp64_pipe_active_pct": fp64_pipe,
                 "kernel": "kt_stage_kernel (stage 1 + stage 2 per step)"}
 
     extras = {}
