@@ -51,6 +51,37 @@ def test_cuda_matches_golden(case):
         assert err <= tol, f"{case} final {k}: rel err {err:.3e} > {tol:g}"
 
 
+# Physics variants the golden fixtures do not hold, against the oracle (pinned bit for bit to
+# the reference's CPU build, tests/test_oracle_pin.py): QCD ideal (no dissipative currents),
+# QCD shear without bulk, conformal shear + bulk.
+VARIANTS = {
+    "qcd_ideal": dict(conformal=False, shear=False, bulk=False, theta=2.0, etabar=0.16),
+    "qcd_shear": dict(conformal=False, shear=True, bulk=False, theta=2.0, etabar=0.16),
+    "conf_bulk": dict(conformal=True, shear=True, bulk=True, theta=1.8, etabar=0.2),
+}
+
+
+@pytest.mark.parametrize("case", sorted(VARIANTS))
+def test_physics_variants_match_oracle(case):
+    kw = dict(nx=9, ny=8, nz=7, dx=0.3, dy=0.3, dz=0.3, dt=0.01, **VARIANTS[case])
+    G = gvh.Lattice(**kw)
+    O = oracle.OracleLattice(**kw)
+    prim = rich_state(G, seed=21)
+    G.set_primitive(prim)
+    O.set_primitive(prim)
+    t = 0.5
+    for n in range(6):
+        G.step(t, kw["dt"])
+        O.step(t, kw["dt"])
+        t = 0.5 + (n + 1) * kw["dt"]
+    assert G.status() == 0
+    tol = tol_for(kw)
+    sg, so = G.get_state(), O.get_state()
+    for k in G.field_names:
+        err = rel_err(G.interior(sg[k]), O.interior(so[k]))
+        assert err <= tol, f"{case} {k}: {err:.3e}"
+
+
 def test_config1_100_steps_matches_oracle():
     """The benchmark's small event (33x33x17, conformal, shear, theta 1.8, 100 steps)."""
     w = workloads.CONFIG1
