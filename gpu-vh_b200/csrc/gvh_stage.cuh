@@ -100,7 +100,9 @@ __device__ __forceinline__ FaceSpeeds<double> face_speeds(const StageArgs &a, in
   // recoveries then read them back one at a time (runtime loops keep the code small:
   // instruction fetch, not arithmetic, is what the long straight-line variant waited on).
   constexpr int NR = 4 + (SHEAR ? 4 : 0) + (BULK ? 1 : 0);
-#pragma unroll 1
+  // three components per pass: their 15 stencil loads are in flight together (one at a time
+  // the loop waited on each component's loads; 3 measured 4% faster than 1, 2 and 9 slower)
+#pragma unroll 3
   for (int r = 0; r < NR; ++r) {
     const int c = (r < 8) ? r : 14;
     const double *q = a.qin + (size_t)c * a.cs + s;
@@ -225,20 +227,25 @@ __device__ __forceinline__ void axis_update(const StageArgs &a, int s, int axis,
   R Sa[4];
   axis_pi_sources<SHEAR, BULK, R>(a, s, axis, o, inv_d, uc, Sa);
   const R th = (R)a.theta;
+  // the root-find components from the cache
+  constexpr int NRC = 4 + (SHEAR ? 4 : 0) + (BULK ? 1 : 0);
 #pragma unroll 1
-  for (int n = 0; n < NQ; ++n) {
-    // T^{tau mu}, pi^{tau mu} and Pi: the states phase A cached; pi^{ij}: from the lattice
-    const int r_cached = n < 8 ? n : (BULK && n == NQ - 1) ? 8 : -1;
-    R r;
-    if (r_cached >= 0) {
-      const double *c = cache + 4 * r_cached * kBlock;
-      r = flux_from_states<R>((R)c[0], (R)c[kBlock], (R)c[2 * kBlock], (R)c[3 * kBlock], f);
-    } else {
-      r = flux_difference<R>(th, a.qin + (size_t)n * a.cs + s, o, f);
-    }
+  for (int rc = 0; rc < NRC; ++rc) {
+    const int n = rc < 8 ? rc : NQ - 1;
+    const double *c = cache + 4 * rc * kBlock;
+    R r = flux_from_states<R>((R)c[0], (R)c[kBlock], (R)c[2 * kBlock], (R)c[3 * kBlock], f);
     r = r * half_inv_d;
     if (SHEAR && n < 4) r += Sa[n];
     out[n * kBlock] += (double)r * a.dt;
+  }
+  // pi^{ij} from the lattice, two components' stencil loads in flight at once (2 measured
+  // faster than 1, 3 and 6)
+  if (SHEAR) {
+#pragma unroll 2
+    for (int n = 8; n < 14; ++n) {
+      R r = flux_difference<R>(th, a.qin + (size_t)n * a.cs + s, o, f);
+      out[n * kBlock] += (double)(r * half_inv_d) * a.dt;
+    }
   }
 }
 
