@@ -170,6 +170,19 @@ def test_pipelined_set_get_matches_blocking_calls():
         want = G.get_state()
         for f, k in enumerate(names):
             np.testing.assert_array_equal(t_out[f].numpy(), want[k], err_msg=k)
+    # fields in separate host allocations (one copy each instead of one per run of adjacent
+    # fields) give the same result
+    sep_in = [torch.empty(G.ng, dtype=torch.float64, pin_memory=True) for _ in names]
+    sep_out = [torch.full((G.ng,), np.nan, dtype=torch.float64, pin_memory=True) for _ in names]
+    for f, k in enumerate(names):
+        sep_in[f].copy_(torch.from_numpy(states[1][k]))
+    G.join_async()
+    G.set_state_async_ptrs([t.data_ptr() for t in sep_in])
+    G.step(t1, lat_kw["dt"])
+    G.get_state_async_ptrs([t.data_ptr() for t in sep_out])
+    G.synchronize()
+    for f in range(n):
+        np.testing.assert_array_equal(sep_out[f].numpy(), pin_out[1][f].numpy(), err_msg=names[f])
     # a null output field is skipped and its host array left alone
     t_out = pin_out[0]
     t_out.fill_(-7.0)
