@@ -443,11 +443,14 @@ __device__ __forceinline__ float with_sign_of(float m, float s) {
 // half-cell states q +- D/2 become q +- D2/4, a derivative D/dx becomes D2 (1/(2 dx))).
 // Power-of-two scalings commute with rounding, so every value is the same.
 template <class R>
-__device__ __forceinline__ R limited_slope2(R theta2, R x, R y, R z) {
-  const R dl = y - x, dc = z - x, dr = z - y;
+__device__ __forceinline__ R slope2_from_differences(R theta2, R dl, R dc, R dr) {
   const unsigned sl = sign_bit(dl);
   const R m = fmin(theta2 * fmin(fabs(dl), fabs(dr)), fabs(dc));
   return ((sl ^ sign_bit(dc)) | (sl ^ sign_bit(dr))) ? R(0) : with_sign_of(m, dl);
+}
+template <class R>
+__device__ __forceinline__ R limited_slope2(R theta2, R x, R y, R z) {
+  return slope2_from_differences(theta2, y - x, z - x, z - y);
 }
 
 }  // namespace gvh

@@ -93,7 +93,7 @@ struct FaceSpeeds {
 // :41-44) with the cell's own energy density as guess.
 // The half-cell states go to this thread's column of the shared-memory cache
 // (cache[(4 r + f) * kBlock]), from which phase B takes them instead of recomputing them.
-template <int EOS, bool SHEAR, bool BULK>
+template <int EOS, bool SHEAR, bool BULK, bool MIXED>
 __device__ __forceinline__ FaceSpeeds<double> face_speeds(const StageArgs &a, int s, int axis, const int (&o)[5],
                                                        const GuessEos &g0, double *cache, unsigned &status) {
   // index f: 0 fwd R, 1 fwd L, 2 bwd R, 3 bwd L. The states go to the cache first; the four
@@ -108,9 +108,19 @@ __device__ __forceinline__ FaceSpeeds<double> face_speeds(const StageArgs &a, in
     const double *q = a.qin + (size_t)c * a.cs + s;
     const double q0 = __ldg(q + o[0]), q1 = __ldg(q + o[1]), q2 = __ldg(q), q3 = __ldg(q + o[3]), q4 = __ldg(q + o[4]);
     const double theta2 = 2 * a.theta;  // the slopes come doubled: q -+ D/2 = q -+ D2/4
-    const double Dm = limited_slope2(theta2, q0, q1, q2);
-    const double D0 = limited_slope2(theta2, q1, q2, q3);
-    const double Dp = limited_slope2(theta2, q2, q3, q4);
+    double Dm, D0, Dp;
+    if (MIXED) {
+      // mixed: the limiter in FP32 on the FP64 differences (rounded), the states in FP64
+      const float t2f = (float)theta2;
+      const float d10 = (float)(q1 - q0), d21 = (float)(q2 - q1), d32 = (float)(q3 - q2), d43 = (float)(q4 - q3);
+      Dm = slope2_from_differences(t2f, d10, (float)(q2 - q0), d21);
+      D0 = slope2_from_differences(t2f, d21, (float)(q3 - q1), d32);
+      Dp = slope2_from_differences(t2f, d32, (float)(q4 - q2), d43);
+    } else {
+      Dm = limited_slope2(theta2, q0, q1, q2);
+      D0 = limited_slope2(theta2, q1, q2, q3);
+      Dp = limited_slope2(theta2, q2, q3, q4);
+    }
     double *cr = cache + 4 * r * kBlock;
     cr[0] = q3 - Dp * 0.25;           // fwd qR
     cr[kBlock] = q2 + D0 * 0.25;      // fwd qL
@@ -219,7 +229,7 @@ __device__ __forceinline__ void axis_update(const StageArgs &a, int s, int axis,
   // Face states are recovered in FP64 on both paths (the mixed path rounds only the
   // resulting speeds): an FP32 recovery was tried and let a 2+1D hotspot event run away
   // to NaN that the FP64 recovery keeps finite.
-  const FaceSpeeds<double> fd = face_speeds<EOS, SHEAR, BULK>(a, s, axis, o, g0, cache, status);
+  const FaceSpeeds<double> fd = face_speeds<EOS, SHEAR, BULK, MIXED>(a, s, axis, o, g0, cache, status);
   FaceSpeeds<R> f;
   f.wRf = (R)fd.wRf; f.wLf = (R)fd.wLf; f.wRb = (R)fd.wRb; f.wLb = (R)fd.wLb;
   f.af = (R)fd.af; f.ab = (R)fd.ab;
