@@ -64,6 +64,8 @@ def parse():
                     help="skip the mixed-precision, event-to-freeze-out and serving measurements")
     ap.add_argument("--serving-seconds", type=float, default=45.0)
     ap.add_argument("--serving-rate", type=float, default=4.0)
+    ap.add_argument("--batch64-seconds", type=float, default=120.0,
+                    help="time limit of the 64-event batched run (0 skips it)")
     return ap.parse_args()
 
 
@@ -470,6 +472,32 @@ def serving_run(args, device, rate=None, seconds=None):
     return out
 
 
+def batch64_run(args, device, per_grid):
+    """The batched configuration: 64 seeded events of the serving mix (grids
+    {61x61x1, 101x101x31, 131x131x61}, b ~ U(0, 12) fm, eta/s ~ U(0.08, 0.24), QCD, shear +
+    bulk, mixed precision) all offered at once to one batch (CUDA graph per step, tiles
+    autotuned), run until every event has frozen out. Beside it, the plain FP64 single-event
+    path's time for the same 64 events from the per-grid times measured alone (per_grid)."""
+    from gvh import serve
+
+    rng = np.random.default_rng(64)
+    reqs = [serve.make_request(i, 0.0, rng) for i in range(64)]
+    srv = serve.Server(int(60 * (1 << 30)), precision="mixed", steps_per_round=10, device=device, autotune=True)
+    out = srv.run(reqs, time_limit=args.batch64_seconds)
+    out.pop("steps", None)
+    secs = {tuple(r["grid"]): r["seconds"] for r in per_grid}
+    fp64_s = sum(secs[(r.lattice["nx"], r.lattice["ny"], r.lattice["nz"])] for r in reqs)
+    out["events"] = len(reqs)
+    out["grids"] = {f"{g[0]}x{g[1]}x{g[2]}": sum(1 for r in reqs if (r.lattice["nx"], r.lattice["ny"],
+                                                                     r.lattice["nz"]) == g)
+                    for g in secs}
+    out["fp64_single_path_seconds_same_events"] = fp64_s
+    out["fp64_single_path_events_per_hour"] = 3600.0 * len(reqs) / fp64_s
+    if out.get("events_per_hour"):
+        out["events_per_hour_vs_fp64_single_path"] = out["events_per_hour"] / out["fp64_single_path_events_per_hour"]
+    return out
+
+
 def run_ours(args):
     import torch
 
@@ -654,6 +682,8 @@ def run_ours(args):
             sv = serving_run(args, local)
             sv["events_per_hour_vs_fp64_single_path"] = sv["events_per_hour"] / fp64_mix["events_per_hour"]
             extras["batched_mixed_serving"] = sv
+            if args.batch64_seconds > 0:
+                extras["batched_64_events"] = batch64_run(args, local, per_grid)
             # the offered-rate sweep of the serving configuration (1-50 req/s), shorter windows
             sweep = []
             for rate in [float(r) for r in args.serving_sweep.split(",") if r.strip()]:
