@@ -15,10 +15,11 @@
 // face solution depends on that guess through the solver's stop test, so sharing a face
 // between two cells would change the answer.
 //
-// Per axis the flux is done in two phases to keep few values live: (A) the face states of
-// the components the root find needs (T^{tau mu}, pi^{tau mu}, Pi) give u^axis/u^tau on both
-// sides of both faces (4 Newton solves iterated together); (B) every component is then
-// streamed through: 5 loads, 3 limited slopes, two KT fluxes, accumulate.
+// Per axis the flux is done in two phases to keep few values live: (A) the half-cell states
+// of the components the root find needs (T^{tau mu}, pi^{tau mu}, Pi) go to a shared-memory
+// cache, and the four face recoveries (one Newton solve at a time) give u^axis/u^tau on both
+// sides of both faces; (B) the cached components, then pi^{ij} (5 loads, 3 limited slopes),
+// go through the two KT fluxes into the running update.
 //
 // Layout in HBM (interior only, no ghosts): component-major SoA, cell index
 // s = i + sy*j + sz*k, component c at c*cs + s.
