@@ -29,6 +29,14 @@
 
 #include <math.h>
 
+// Host and device: the same code runs in the host pool (gvh_surface_host.cpp) and in the
+// device row kernel (gvh_surface_rows.cu, compiled without FMA contraction).
+#ifdef __CUDACC__
+#define GVH_HD __host__ __device__
+#else
+#define GVH_HD
+#endif
+
 namespace gvh {
 namespace iso {
 
@@ -49,9 +57,9 @@ struct Segment {
   double p[2][kDim];
   double out[kDim];
   int s;  // which of p[] is the start; flipping the segment swaps start and end
-  const double *start() const { return p[s]; }
-  const double *end() const { return p[1 - s]; }
-  void flip() { s = 1 - s; }
+  GVH_HD const double *start() const { return p[s]; }
+  GVH_HD const double *end() const { return p[1 - s]; }
+  GVH_HD void flip() { s = 1 - s; }
 };
 
 struct Polygon {
@@ -75,7 +83,11 @@ struct Result {
   double normal[kMaxElements][kDim];
 };
 
-inline void orient(double *nrm, const double *outp, const double *c) {
+// The published code's pow(x, 2.0): the host compiler folds that call into this product
+// (the square is exact to rounding either way), which is what its builds compute.
+GVH_HD inline double sq(double x) { return x * x; }
+
+GVH_HD inline void orient(double *nrm, const double *outp, const double *c) {
   double dot = 0;
   for (int k = 0; k < kDim; ++k) dot += (outp[k] - c[k]) * nrm[k];
   if (dot < 0)
@@ -87,7 +99,7 @@ inline void orient(double *nrm, const double *outp, const double *c) {
 // Segments of the square whose corner values are v[i][j] (i along free axis a, j along free
 // axis b, a < b); the constant axes c0, c1 sit at values w0, w1. Returns the number of
 // segments (0..2) or an error; *amb is set when the square had four cuts.
-inline int square_segments(const double v[2][2], int c0, double w0, int c1, double w1, const double *dx,
+GVH_HD inline int square_segments(const double v[2][2], int c0, double w0, int c1, double w1, const double *dx,
                            double iso, Segment *seg, bool *amb) {
   *amb = false;
   const int high = (v[0][0] >= iso) + (v[0][1] >= iso) + (v[1][0] >= iso) + (v[1][1] >= iso);
@@ -172,7 +184,7 @@ inline int square_segments(const double v[2][2], int c0, double w0, int c1, doub
 }
 
 // Centroid and normal of a segment of a 2-cube (constant axes 0 and 1; free axes 2 and 3).
-inline void segment_element(const Segment &g, double *centroid, double *normal) {
+GVH_HD inline void segment_element(const Segment &g, double *centroid, double *normal) {
   const double *p0 = g.start(), *p1 = g.end();
   for (int k = 0; k < kDim; ++k) centroid[k] = (p0[k] + p1[k]) / 2.0;
   normal[2] = -(p1[3] - p0[3]);
@@ -184,7 +196,7 @@ inline void segment_element(const Segment &g, double *centroid, double *normal) 
 
 // ---- polygons ------------------------------------------------------------------------
 
-inline void polygon_init(Polygon &P, int cax) {
+GVH_HD inline void polygon_init(Polygon &P, int cax) {
   P.n = 0;
   P.cax = cax;
   P.has_centroid = false;
@@ -193,14 +205,14 @@ inline void polygon_init(Polygon &P, int cax) {
     if (k != cax) P.ax[m++] = k;
 }
 
-inline double l1_distance(const double *x, const double *y) {
+GVH_HD inline double l1_distance(const double *x, const double *y) {
   double d = 0;
   for (int k = 0; k < kDim; ++k) d += fabs(x[k] - y[k]);
   return d;
 }
 
 // Appends g when it continues the chain (its start or end is the last segment's end).
-inline bool polygon_extend(Polygon &P, Segment *g) {
+GVH_HD inline bool polygon_extend(Polygon &P, Segment *g) {
   if (P.n == 0) {
     P.seg[0] = g;
     P.n = 1;
@@ -218,9 +230,9 @@ inline bool polygon_extend(Polygon &P, Segment *g) {
   return false;
 }
 
-inline void polygon_add(Polygon &P, Segment *g) { P.seg[P.n++] = g; }
+GVH_HD inline void polygon_add(Polygon &P, Segment *g) { P.seg[P.n++] = g; }
 
-inline const double *polygon_centroid(Polygon &P) {
+GVH_HD inline const double *polygon_centroid(Polygon &P) {
   if (P.has_centroid) return P.centroid;
   double mean[kDim] = {0, 0, 0, 0};
   for (int i = 0; i < P.n; ++i) {
@@ -244,8 +256,8 @@ inline const double *polygon_centroid(Polygon &P) {
       u[k] = p0[k] - mean[k];
       w[k] = p1[k] - mean[k];
     }
-    const double A = 0.5 * sqrt(pow(u[y] * w[z] - u[z] * w[y], 2.0) + pow(u[x] * w[z] - u[z] * w[x], 2.0) +
-                                pow(u[y] * w[x] - u[x] * w[y], 2.0));
+    const double A = 0.5 * sqrt(sq(u[y] * w[z] - u[z] * w[y]) + sq(u[x] * w[z] - u[z] * w[x]) +
+                                sq(u[y] * w[x] - u[x] * w[y]));
     for (int k = 0; k < kDim; ++k) wsum[k] += cm[k] * A;
     area += A;
   }
@@ -254,7 +266,7 @@ inline const double *polygon_centroid(Polygon &P) {
   return P.centroid;
 }
 
-inline void polygon_normal(Polygon &P, double *normal) {
+GVH_HD inline void polygon_normal(Polygon &P, double *normal) {
   const double *c = polygon_centroid(P);
   const int x = P.ax[0], y = P.ax[1], z = P.ax[2];
   for (int k = 0; k < kDim; ++k) normal[k] = 0;
@@ -286,7 +298,7 @@ struct CubeWork {
 
 // Polygons of the cube with corner values v[i][j][k] over the free axes (ascending); its
 // constant axis cax sits at value w.
-inline int cube_polygons(const double v[2][2][2], int cax, double w, const double *dx, double iso, CubeWork &cw) {
+GVH_HD inline int cube_polygons(const double v[2][2][2], int cax, double w, const double *dx, double iso, CubeWork &cw) {
   int fa[3], m = 0;
   for (int k = 0; k < kDim; ++k)
     if (k != cax) fa[m++] = k;
@@ -342,7 +354,7 @@ inline int cube_polygons(const double v[2][2][2], int cax, double w, const doubl
 
 // Segments l (of the new polygon) and m (already in the polyhedron) share a point: m's start
 // is one of l's end points.
-inline bool segments_touch(const Segment *l, const Segment *m) {
+GVH_HD inline bool segments_touch(const Segment *l, const Segment *m) {
   const double *l0 = l->start(), *l1 = l->end(), *m0 = m->start();
   double d0 = 0, d1 = 0;
   for (int k = 0; k < kDim; ++k) {
@@ -353,7 +365,7 @@ inline bool segments_touch(const Segment *l, const Segment *m) {
   return true;
 }
 
-inline bool polyhedron_extend(Polyhedron &H, Polygon *P) {
+GVH_HD inline bool polyhedron_extend(Polyhedron &H, Polygon *P) {
   if (H.n == 0) {
     H.poly[0] = P;
     H.n = 1;
@@ -372,7 +384,7 @@ inline bool polyhedron_extend(Polyhedron &H, Polygon *P) {
 }
 
 // The 3-volume normal (a x b x c)/6 of the tetrahedron spanned by a, b, c.
-inline void tetra_normal(const double *a, const double *b, const double *c, double *n) {
+GVH_HD inline void tetra_normal(const double *a, const double *b, const double *c, double *n) {
   const double bc01 = b[0] * c[1] - b[1] * c[0];
   const double bc02 = b[0] * c[2] - b[2] * c[0];
   const double bc03 = b[0] * c[3] - b[3] * c[0];
@@ -385,7 +397,7 @@ inline void tetra_normal(const double *a, const double *b, const double *c, doub
   n[3] = -1.0 / 6.0 * (a[0] * bc12 - a[1] * bc02 + a[2] * bc01);
 }
 
-inline void polyhedron_element(Polyhedron &H, double *centroid, double *normal) {
+GVH_HD inline void polyhedron_element(Polyhedron &H, double *centroid, double *normal) {
   double mean[kDim] = {0, 0, 0, 0};
   for (int i = 0; i < H.n; ++i)
     for (int j = 0; j < H.poly[i]->n; ++j) {
@@ -436,7 +448,7 @@ inline void polyhedron_element(Polyhedron &H, double *centroid, double *normal) 
 // ---- the three entry points ------------------------------------------------------------
 
 // 2-cube: corner values v[i][j] over (axis 2, axis 3) with spacings dx[2], dx[3].
-inline int find_2d(const double v[2][2], const double *dx4, double iso, Result &r) {
+GVH_HD inline int find_2d(const double v[2][2], const double *dx4, double iso, Result &r) {
   r.n = 0;
   Segment seg[2];
   bool amb;
@@ -448,7 +460,7 @@ inline int find_2d(const double v[2][2], const double *dx4, double iso, Result &
 }
 
 // 3-cube: corner values v[i][j][k] over axes 1, 2, 3.
-inline int find_3d(const double v[2][2][2], const double *dx4, double iso, Result &r, CubeWork &cw) {
+GVH_HD inline int find_3d(const double v[2][2][2], const double *dx4, double iso, Result &r, CubeWork &cw) {
   r.n = 0;
   int high = 0;
   for (int i = 0; i < 2; ++i)
@@ -474,7 +486,7 @@ struct HypercubeWork {
 };
 
 // 4-cube: corner values v[i][j][k][l] over axes 0..3.
-inline int find_4d(const double v[2][2][2][2], const double *dx4, double iso, Result &r, HypercubeWork &hw) {
+GVH_HD inline int find_4d(const double v[2][2][2][2], const double *dx4, double iso, Result &r, HypercubeWork &hw) {
   r.n = 0;
   int high = 0;
   for (int i = 0; i < 16; ++i) high += (&v[0][0][0][0])[i] >= iso;

@@ -16,9 +16,12 @@
 //   fo_scan          block offsets (one block)
 //   fo_write         ordered hypercube keys; the points' 2 x 10 values
 //
-// and the host receives only those keys and points (about 170 bytes per crossed hypercube
-// instead of ~160 bytes per lattice cell per level), then runs the algorithm of
-// gvh_cornelius.hpp on them with a pool of host threads (gvh_surface_host.cpp).
+// and then, for the QCD EoS (the default), the rows themselves are made on the device
+// (gvh_surface_rows.cu: cornelius, interpolation and the row, one thread per crossed
+// hypercube, the host's code without FMA contraction) and only they are copied to the host,
+// which formats them; otherwise the host receives the keys and points (about 170 bytes per
+// crossed hypercube instead of ~160 bytes per lattice cell per level) and runs the same code
+// with a pool of host threads (gvh_surface_host.cpp).
 #include <cuda_runtime.h>
 #include <stdarg.h>
 #include <stdio.h>
@@ -33,6 +36,7 @@
 
 #include "../../include/gvh.h"
 #include "gvh_handle.h"
+#include "gvh_surface_device.h"
 #include "gvh_surface_internal.h"
 
 using gvh::surface::kVars;
@@ -257,6 +261,16 @@ struct gvh_surface {
   std::vector<int> c2p;
   std::unique_ptr<gvh::surface::Pool> pool;
   int outputs;       // gvh::surface::OUT_ROWS | OUT_TEXT
+  // rows made on the device (gvh_surface_rows.cu; the default for the QCD EoS): scratch and
+  // output grown to the largest slab, the rows' copy on the host
+  bool device_rows;
+  int *d_c2p;
+  char *rowdev;
+  long long rowdev_cap;
+  long long *h_rowtot;  // pinned: rows, errors
+  double *h_rows;       // pinned
+  long long cap_rows;
+  long long p_nrows, p_errors;
   gvh::surface::Result last;
   gvh_surface_info info;
   // a slab between gvh_surface_find_begin and _end: its copies to the pinned buffers are in
@@ -299,7 +313,7 @@ int gvh_surface_create(gvh_handle *h, double e_freezeout, gvh_surface **out) {
   const long long n = g.ncells;
   auto al = [](long long b) { return (b + 255) / 256 * 256; };
   const long long bytes = 2 * al(kVars * n * 8) + al(g.ncubes) + al(n) + al(4 * (s->nbc + s->nbp + 2)) +
-                          al(4 * g.ncubes) + al(4 * n) + al(2 * kVars * n * 8);
+                          al(4 * g.ncubes) + al(4 * n) + al(2 * kVars * n * 8) + al(4 * n);
   if (cudaMalloc(&s->dev, (size_t)bytes) != cudaSuccess) {
     delete s;
     return sfail(GVH_ERR_NOMEM, "gvh_surface_create: cannot allocate %lld bytes", bytes);
@@ -313,8 +327,15 @@ int gvh_surface_create(gvh_handle *h, double e_freezeout, gvh_surface **out) {
   s->totals = s->counts + s->nbc + s->nbp;
   s->cube_key = reinterpret_cast<int *>(p); p += al(4 * g.ncubes);
   s->point_cell = reinterpret_cast<int *>(p); p += al(4 * n);
-  s->point_vals = reinterpret_cast<double *>(p);
-  if (cudaHostAlloc(reinterpret_cast<void **>(&s->h_totals), 4 * sizeof(int), cudaHostAllocDefault) != cudaSuccess) {
+  s->point_vals = reinterpret_cast<double *>(p); p += al(2 * kVars * n * 8);
+  s->d_c2p = reinterpret_cast<int *>(p);
+  // the device rows repeat the host's arithmetic exactly for the QCD EoS; the conformal T(e)
+  // is a pow, which the device does not evaluate as the host's libm does
+  s->device_rows = h->eos == GVH_EOS_QCD;
+  if (cudaHostAlloc(reinterpret_cast<void **>(&s->h_totals), 4 * sizeof(int), cudaHostAllocDefault) != cudaSuccess ||
+      cudaHostAlloc(reinterpret_cast<void **>(&s->h_rowtot), 2 * sizeof(long long), cudaHostAllocDefault) !=
+          cudaSuccess) {
+    if (s->h_totals) cudaFreeHost(s->h_totals);
     cudaFree(s->dev);
     delete s;
     return sfail(GVH_ERR_NOMEM, "gvh_surface_create: cannot pin host memory");
@@ -322,6 +343,7 @@ int gvh_surface_create(gvh_handle *h, double e_freezeout, gvh_surface **out) {
   memset(&s->info, 0, sizeof s->info);
   if (cudaEventCreateWithFlags(&s->copied, cudaEventDisableTiming) != cudaSuccess) {
     cudaFreeHost(s->h_totals);
+    cudaFreeHost(s->h_rowtot);
     cudaFree(s->dev);
     delete s;
     return sfail(GVH_ERR_CUDA, "gvh_surface_create: event creation failed");
@@ -338,7 +360,10 @@ int gvh_surface_destroy(gvh_surface *s) {
   cudaEventSynchronize(s->copied);
   cudaEventDestroy(s->copied);
   cudaFree(s->dev);
+  if (s->rowdev) cudaFree(s->rowdev);
   cudaFreeHost(s->h_totals);
+  if (s->h_rowtot) cudaFreeHost(s->h_rowtot);
+  if (s->h_rows) cudaFreeHost(s->h_rows);
   if (s->h_cube_key) cudaFreeHost(s->h_cube_key);
   if (s->h_point_cell) cudaFreeHost(s->h_point_cell);
   if (s->h_point_vals) cudaFreeHost(s->h_point_vals);
@@ -350,6 +375,16 @@ int gvh_surface_set_threads(gvh_surface *s, int nthreads) {
   if (!s || nthreads < 1) return sfail(GVH_ERR_INVALID, "gvh_surface_set_threads: bad argument");
   s->nthreads = nthreads;
   s->pool.reset();
+  return GVH_OK;
+}
+
+int gvh_surface_set_device_rows(gvh_surface *s, int on) {
+  if (!s) return sfail(GVH_ERR_INVALID, "gvh_surface_set_device_rows: null argument");
+  if (s->pending) return sfail(GVH_ERR_INVALID, "gvh_surface_set_device_rows: a slab is in flight");
+  if (on && s->h->eos != GVH_EOS_QCD)
+    return sfail(GVH_ERR_INVALID, "gvh_surface_set_device_rows: the device rows are for the QCD EoS only "
+                                  "(the conformal T(e) is a pow, evaluated on the host)");
+  s->device_rows = on != 0;
   return GVH_OK;
 }
 
@@ -379,6 +414,62 @@ int gvh_surface_set_lower(gvh_surface *s) {
   return GVH_OK;
 }
 
+// The slab's rows on the device (gvh_surface_rows.cu), then their copy to pinned host memory,
+// queued on the handle's stream; the row count is read back first to size the copy.
+static int device_rows_begin(gvh_surface *s, long long ncubes, long long npoints, double tau_label,
+                             double tau_scale) {
+  gvh_handle *h = s->h;
+  cudaStream_t st = h->stream;
+  const size_t per_cube = gvh::surface::device_rows_slot_bytes(1);
+  const size_t rows_per_cube = (size_t)gvh::iso::kMaxElements * gvh::surface::kRowColumns * sizeof(double);
+  if (ncubes > s->rowdev_cap) {
+    const long long cap = std::max<long long>(ncubes, s->rowdev_cap * 3 / 2 + 1024);
+    if (s->rowdev) {
+      SF_CUDA(cudaStreamSynchronize(st));
+      cudaFree(s->rowdev);
+      s->rowdev = nullptr;
+      s->rowdev_cap = 0;
+    }
+    const size_t bytes = (size_t)cap * (per_cube + rows_per_cube) + 256;
+    if (cudaMalloc(&s->rowdev, bytes) != cudaSuccess)
+      return sfail(GVH_ERR_NOMEM, "gvh_surface: cannot allocate %zu bytes for the device rows", bytes);
+    s->rowdev_cap = cap;
+  }
+  const long long cap = s->rowdev_cap;
+  gvh::surface::DeviceRows d;
+  d.g.dim = s->dim;
+  d.g.nx = s->g.nx; d.g.ny = s->g.ny; d.g.nz = s->g.nz;
+  d.g.dt = h->dt_lattice; d.g.dx = h->dx; d.g.dy = h->dy; d.g.dz = h->dz;
+  d.g.iso = s->iso;
+  d.g.eos = h->eos;
+  d.g.tau_label = tau_label;
+  d.g.tau_scale = tau_scale;
+  d.ncubes = ncubes;
+  d.npoints = npoints;
+  d.cube_key = s->cube_key;
+  d.point_cell = s->point_cell;
+  d.point_vals = s->point_vals;
+  d.c2p = s->d_c2p;
+  char *p = s->rowdev;
+  d.totals = reinterpret_cast<long long *>(p); p += 256;
+  d.slot_rows = reinterpret_cast<double *>(p); p += (size_t)cap * rows_per_cube;
+  d.rows = reinterpret_cast<double *>(p); p += (size_t)cap * rows_per_cube;
+  d.slot_n = reinterpret_cast<int *>(p); p += (size_t)cap * sizeof(int);
+  d.offsets = reinterpret_cast<int *>(p);
+  SF_CUDA(gvh::surface::launch_device_rows(d, st));
+  SF_CUDA(cudaMemcpyAsync(s->h_rowtot, d.totals, 2 * sizeof(long long), cudaMemcpyDeviceToHost, st));
+  SF_CUDA(cudaStreamSynchronize(st));
+  const long long nrows = s->h_rowtot[0];
+  int rc = grow_pinned(&s->h_rows, &s->cap_rows, std::max(1ll, nrows * gvh::surface::kRowColumns));
+  if (rc) return rc;
+  if (nrows)
+    SF_CUDA(cudaMemcpyAsync(s->h_rows, d.rows, (size_t)nrows * gvh::surface::kRowColumns * sizeof(double),
+                            cudaMemcpyDeviceToHost, st));
+  s->p_nrows = nrows;
+  s->p_errors = s->h_rowtot[1];
+  return GVH_OK;
+}
+
 int gvh_surface_find_begin(gvh_surface *s, double tau_label, double tau_scale) {
   if (!s) return sfail(GVH_ERR_INVALID, "gvh_surface_find_begin: null argument");
   if (!s->have_lower) return sfail(GVH_ERR_INVALID, "gvh_surface_find_begin: no lower time level (gvh_surface_set_lower)");
@@ -403,6 +494,17 @@ int gvh_surface_find_begin(gvh_surface *s, double tau_label, double tau_scale) {
   SF_CUDA(cudaMemcpyAsync(s->h_totals, s->totals, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
   SF_CUDA(cudaStreamSynchronize(st));
   const long long ncubes = s->h_totals[0], npoints = s->h_totals[1];
+  if (s->device_rows) {
+    if ((rc = device_rows_begin(s, ncubes, npoints, tau_label, tau_scale))) return rc;
+    SF_CUDA(cudaEventRecord(s->copied, st));
+    s->lower = upper;
+    s->pending = true;
+    s->p_ncubes = ncubes;
+    s->p_npoints = npoints;
+    s->p_label = tau_label;
+    s->p_scale = tau_scale;
+    return GVH_OK;
+  }
   if ((rc = grow_pinned(&s->h_cube_key, &s->cap_cubes, std::max(1ll, ncubes))) ||
       (rc = grow_pinned(&s->h_point_cell, &s->cap_points, std::max(1ll, npoints))) ||
       (rc = grow_pinned(&s->h_point_vals, &s->cap_vals, std::max(1ll, npoints * 2 * kVars))))
@@ -445,8 +547,13 @@ int gvh_surface_find_end(gvh_surface *s, long long *n_elements) {
   slab.point_cell = s->h_point_cell;
   slab.point_vals = s->h_point_vals;
   if (!s->pool) s->pool.reset(new gvh::surface::Pool(s->nthreads));
-  gvh::surface::process_slab(slab, gvh::surface::Labels{s->p_label, s->p_scale}, *s->pool, s->outputs, s->c2p,
-                             s->last);
+  if (s->device_rows) {
+    gvh::surface::format_rows(s->h_rows, s->p_nrows, *s->pool, s->outputs, s->last);
+    s->last.errors = s->p_errors;
+  } else {
+    gvh::surface::process_slab(slab, gvh::surface::Labels{s->p_label, s->p_scale}, *s->pool, s->outputs, s->c2p,
+                               s->last);
+  }
   const auto t2 = std::chrono::steady_clock::now();
   gvh_surface_info &in = s->info;
   in.slabs += 1;
@@ -456,7 +563,8 @@ int gvh_surface_find_end(gvh_surface *s, long long *n_elements) {
   in.elements_last = s->last.elements;
   in.elements_total += s->last.elements;
   in.errors_total += s->last.errors;
-  in.bytes_to_host_total += (double)ncubes * 4 + (double)npoints * (4 + 2 * kVars * 8) + 8;
+  in.bytes_to_host_total += s->device_rows ? (double)s->p_nrows * gvh::surface::kRowColumns * 8 + 24
+                                           : (double)ncubes * 4 + (double)npoints * (4 + 2 * kVars * 8) + 8;
   in.device_seconds_total += std::chrono::duration<double>(t1 - s->p_t0).count();
   in.host_seconds_total += std::chrono::duration<double>(t2 - t1).count();
   if (n_elements) *n_elements = s->last.elements;

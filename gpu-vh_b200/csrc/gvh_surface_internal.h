@@ -83,6 +83,10 @@ class Pool {
   bool stop_ = false;
 };
 
+// Formats rows the device produced (n rows of kColumns) into out's parts on the pool, in
+// order; keeps the rows too when outputs has OUT_ROWS.
+void format_rows(const double *rows, long long n, Pool &pool, int outputs, Result &out);
+
 // Runs the surface finder on every crossed hypercube of the slab on the pool, in order.
 // outputs: OUT_ROWS and/or OUT_TEXT. cell_to_point is scratch of at least nx*ny*nz entries
 // kept by the caller.

@@ -505,6 +505,7 @@ def _bind_surface(L):
     L.gvh_surface_create.argtypes = [vp, dp, ctypes.POINTER(vp)]
     L.gvh_surface_destroy.argtypes = [vp]
     L.gvh_surface_set_threads.argtypes = [vp, ctypes.c_int]
+    L.gvh_surface_set_device_rows.argtypes = [vp, ctypes.c_int]
     L.gvh_surface_set_lower.argtypes = [vp]
     L.gvh_surface_find.argtypes = [vp, dp, dp, ctypes.POINTER(ll)]
     L.gvh_surface_get_rows.argtypes = [vp, ctypes.POINTER(dp), ll]
@@ -535,7 +536,8 @@ def slab_labels(k, tau0, dtau):
 
 class Surface:
     """Freeze-out hypersurface of a Lattice's evolution (gvh_surface_*): device marking of the
-    crossed hypercubes, host cornelius, rows in the reference's surface.dat layout."""
+    crossed hypercubes, cornelius and the rows on the device (QCD EoS) or the host pool, rows
+    in the reference's surface.dat layout."""
 
     def __init__(self, lattice, e_freezeout, threads=None):
         self._L = _bind_surface(load())
@@ -568,6 +570,10 @@ class Surface:
 
     def set_lower(self):
         self._check(self._L.gvh_surface_set_lower(self._h), "gvh_surface_set_lower")
+
+    def set_device_rows(self, on: bool):
+        """Make the rows on the device (default for the QCD EoS) or with the host pool."""
+        self._check(self._L.gvh_surface_set_device_rows(self._h, int(bool(on))), "gvh_surface_set_device_rows")
 
     def find(self, tau_label, tau_scale) -> int:
         n = ctypes.c_longlong()

@@ -20,7 +20,12 @@ NVCC_FLAGS = [
 def sources() -> list[str]:
     return [os.path.join(CSRC, "gvh_capi.cu"), os.path.join(CSRC, "gvh_batch.cu"), os.path.join(CSRC, "gvh_plugin.cpp"),
             os.path.join(CSRC, "gvh_noalloc.cu"), os.path.join(CSRC, "gvh_surface.cu"),
-            os.path.join(CSRC, "gvh_surface_host.cpp")]
+            os.path.join(CSRC, "gvh_surface_host.cpp"), os.path.join(CSRC, "gvh_surface_rows.cu")]
+
+
+# per-file flags: the device surface rows repeat the host's arithmetic operation for operation
+# (the host side is compiled with -ffp-contract=off), so no multiply-add contraction there
+FILE_FLAGS = {"gvh_surface_rows.cu": ["-fmad=false"]}
 
 
 def needs_rebuild() -> bool:
@@ -42,7 +47,8 @@ def build(verbose: bool = True, ptxas_info: bool = False) -> str:
 
     def compile_one(src):
         obj = os.path.join(obj_dir, os.path.basename(src) + ".o")
-        cmd = [nvcc] + compile_flags + (["-Xptxas", "-v"] if ptxas_info else []) + ["-c", src, "-o", obj]
+        cmd = [nvcc] + compile_flags + FILE_FLAGS.get(os.path.basename(src), []) + \
+              (["-Xptxas", "-v"] if ptxas_info else []) + ["-c", src, "-o", obj]
         r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
         if r.returncode != 0:
             raise RuntimeError("libgvh build failed:\n" + r.stdout)

@@ -385,6 +385,13 @@ int gvh_surface_set_threads(gvh_surface *s, int nthreads);
 #define GVH_SURFACE_ROWS 1
 #define GVH_SURFACE_TEXT 2
 int gvh_surface_set_outputs(gvh_surface *s, int outputs);
+/* Where a slab's elements and rows are made. 1 (the default for the QCD EoS): on the device,
+ * one thread per crossed hypercube running the same cornelius and row code as the host pool,
+ * without FMA contraction, so the rows are the same to the last bit; only the rows are
+ * copied to the host, which formats them. 0: the corner values go to the host and the host
+ * pool makes the rows (the only form for the conformal EoS, whose T(e) = (e/13.8997)^(1/4)
+ * is a pow the device does not evaluate as the host's libm does; 1 is refused there). */
+int gvh_surface_set_device_rows(gvh_surface *s, int on);
 /* Takes the handle's current state as the lower time level of the next slab. */
 int gvh_surface_set_lower(gvh_surface *s);
 /* Elements of the slab (lower level, handle's current level); then the current level becomes

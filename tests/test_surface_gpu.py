@@ -74,6 +74,40 @@ def test_same_states_same_surface_text(case, tmp_path):
     assert S.info()["errors_total"] == 0
 
 
+@pytest.mark.parametrize("case", ["qcd_bulk_3d", "qcd_bulk_2d"])
+def test_device_rows_equal_host_rows(case):
+    """The rows made on the device (the default for the QCD EoS) are the host pool's rows to
+    the last bit, slab by slab; the conformal EoS keeps the host form."""
+    lat = CASES[case]
+    t0, dt = 0.5, lat["dt"]
+    G = gvh.Lattice(**lat)
+    G.set_primitive(rich_state(G, seed=4, e0=25.0, emin=0.3, spacing=0.6))
+    efo = gvh.energy_density_of_temperature(0.150)
+    D = gvh.Surface(G, efo, threads=3)
+    H = gvh.Surface(G, efo, threads=3)
+    H.set_device_rows(False)
+    D.set_lower()
+    H.set_lower()
+    t, total = t0, 0
+    for n in range(1, 25):
+        G.step(t, dt)
+        t = t0 + n * dt
+        label, scale, _ = gvh.slab_labels(n - 1, t0, dt)
+        nd, nh = D.find(label, scale), H.find(label, scale)
+        assert nd == nh
+        rd, rh = D.rows(), H.rows()
+        assert np.array_equal(rd.view(np.uint64), rh.view(np.uint64)), n
+        assert D.text() == H.text()
+        total += nd
+    assert total > 50
+    assert D.info()["errors_total"] == H.info()["errors_total"] == 0
+    C = gvh.Lattice(**CASES["conformal_shear_3d"])
+    S = gvh.Surface(C, 1.0)
+    with pytest.raises(gvh.GvhError):
+        S.set_device_rows(True)
+    S.set_device_rows(False)
+
+
 def test_device_marking_counts():
     lat = CASES["qcd_bulk_3d"]
     R = oracle.RefLattice(**lat)
