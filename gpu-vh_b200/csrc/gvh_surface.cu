@@ -238,6 +238,22 @@ int grow_pinned(T **buf, long long *cap, long long need) {
   return GVH_OK;
 }
 
+// Mapped pinned host memory: the device writes into it directly.
+template <class T>
+int grow_mapped(T **buf, T **dev, long long *cap, long long need) {
+  if (need <= *cap) return GVH_OK;
+  long long n = std::max<long long>(need, *cap * 3 / 2 + 1024);
+  if (*buf) cudaFreeHost(*buf);
+  *buf = nullptr;
+  *dev = nullptr;
+  *cap = 0;
+  if (cudaHostAlloc(reinterpret_cast<void **>(buf), (size_t)n * sizeof(T), cudaHostAllocMapped) != cudaSuccess ||
+      cudaHostGetDevicePointer(reinterpret_cast<void **>(dev), *buf, 0) != cudaSuccess)
+    return sfail(GVH_ERR_NOMEM, "gvh_surface: cannot map %lld bytes of host memory", n * (long long)sizeof(T));
+  *cap = n;
+  return GVH_OK;
+}
+
 }  // namespace
 
 struct gvh_surface {
@@ -267,8 +283,8 @@ struct gvh_surface {
   int *d_c2p;
   char *rowdev;
   long long rowdev_cap;
-  long long *h_rowtot;  // pinned: rows, errors
-  double *h_rows;       // pinned
+  long long *h_rowtot, *d_rowtot_mapped;  // mapped pinned: rows, errors
+  double *h_rows, *d_rows_mapped;         // mapped pinned
   long long cap_rows;
   long long p_nrows, p_errors;
   gvh::surface::Result last;
@@ -333,8 +349,10 @@ int gvh_surface_create(gvh_handle *h, double e_freezeout, gvh_surface **out) {
   // is a pow, which the device does not evaluate as the host's libm does
   s->device_rows = h->eos == GVH_EOS_QCD;
   if (cudaHostAlloc(reinterpret_cast<void **>(&s->h_totals), 4 * sizeof(int), cudaHostAllocDefault) != cudaSuccess ||
-      cudaHostAlloc(reinterpret_cast<void **>(&s->h_rowtot), 2 * sizeof(long long), cudaHostAllocDefault) !=
-          cudaSuccess) {
+      cudaHostAlloc(reinterpret_cast<void **>(&s->h_rowtot), 2 * sizeof(long long), cudaHostAllocMapped) !=
+          cudaSuccess ||
+      cudaHostGetDevicePointer(reinterpret_cast<void **>(&s->d_rowtot_mapped), s->h_rowtot, 0) != cudaSuccess) {
+    if (s->h_rowtot) cudaFreeHost(s->h_rowtot);
     if (s->h_totals) cudaFreeHost(s->h_totals);
     cudaFree(s->dev);
     delete s;
@@ -414,14 +432,13 @@ int gvh_surface_set_lower(gvh_surface *s) {
   return GVH_OK;
 }
 
-// The slab's rows on the device (gvh_surface_rows.cu), then their copy to pinned host memory,
-// queued on the handle's stream; the row count is read back first to size the copy.
+// The slab's rows on the device (gvh_surface_rows.cu), queued on the handle's stream; they and
+// their count land in mapped pinned host memory, so nothing here waits for them.
 static int device_rows_begin(gvh_surface *s, long long ncubes, long long npoints, double tau_label,
                              double tau_scale) {
   gvh_handle *h = s->h;
   cudaStream_t st = h->stream;
   const size_t per_cube = gvh::surface::device_rows_slot_bytes(1);
-  const size_t rows_per_cube = (size_t)gvh::iso::kMaxElements * gvh::surface::kRowColumns * sizeof(double);
   if (ncubes > s->rowdev_cap) {
     const long long cap = std::max<long long>(ncubes, s->rowdev_cap * 3 / 2 + 1024);
     if (s->rowdev) {
@@ -430,11 +447,17 @@ static int device_rows_begin(gvh_surface *s, long long ncubes, long long npoints
       s->rowdev = nullptr;
       s->rowdev_cap = 0;
     }
-    const size_t bytes = (size_t)cap * (per_cube + rows_per_cube) + 256;
+    const size_t bytes = (size_t)cap * per_cube + 256;
     if (cudaMalloc(&s->rowdev, bytes) != cudaSuccess)
       return sfail(GVH_ERR_NOMEM, "gvh_surface: cannot allocate %zu bytes for the device rows", bytes);
     s->rowdev_cap = cap;
   }
+  // room for every crossed hypercube's largest number of rows (the previous slab's rows have
+  // been formatted by now: find_end waited for them)
+  const long long row_values = std::max(1ll, ncubes) * gvh::iso::kMaxElements * gvh::surface::kRowColumns;
+  int rc = grow_mapped(&s->h_rows, &s->d_rows_mapped, &s->cap_rows, row_values);
+  if (rc) return rc;
+  s->h_rowtot[0] = s->h_rowtot[1] = 0;
   const long long cap = s->rowdev_cap;
   gvh::surface::DeviceRows d;
   d.g.dim = s->dim;
@@ -452,21 +475,13 @@ static int device_rows_begin(gvh_surface *s, long long ncubes, long long npoints
   d.c2p = s->d_c2p;
   char *p = s->rowdev;
   d.totals = reinterpret_cast<long long *>(p); p += 256;
-  d.slot_rows = reinterpret_cast<double *>(p); p += (size_t)cap * rows_per_cube;
-  d.rows = reinterpret_cast<double *>(p); p += (size_t)cap * rows_per_cube;
+  d.slot_rows = reinterpret_cast<double *>(p);
+  p += (size_t)cap * gvh::iso::kMaxElements * gvh::surface::kRowColumns * sizeof(double);
   d.slot_n = reinterpret_cast<int *>(p); p += (size_t)cap * sizeof(int);
   d.offsets = reinterpret_cast<int *>(p);
+  d.rows = s->d_rows_mapped;
+  d.host_totals = s->d_rowtot_mapped;
   SF_CUDA(gvh::surface::launch_device_rows(d, st));
-  SF_CUDA(cudaMemcpyAsync(s->h_rowtot, d.totals, 2 * sizeof(long long), cudaMemcpyDeviceToHost, st));
-  SF_CUDA(cudaStreamSynchronize(st));
-  const long long nrows = s->h_rowtot[0];
-  int rc = grow_pinned(&s->h_rows, &s->cap_rows, std::max(1ll, nrows * gvh::surface::kRowColumns));
-  if (rc) return rc;
-  if (nrows)
-    SF_CUDA(cudaMemcpyAsync(s->h_rows, d.rows, (size_t)nrows * gvh::surface::kRowColumns * sizeof(double),
-                            cudaMemcpyDeviceToHost, st));
-  s->p_nrows = nrows;
-  s->p_errors = s->h_rowtot[1];
   return GVH_OK;
 }
 
@@ -548,6 +563,8 @@ int gvh_surface_find_end(gvh_surface *s, long long *n_elements) {
   slab.point_vals = s->h_point_vals;
   if (!s->pool) s->pool.reset(new gvh::surface::Pool(s->nthreads));
   if (s->device_rows) {
+    s->p_nrows = s->h_rowtot[0];
+    s->p_errors = s->h_rowtot[1];
     gvh::surface::format_rows(s->h_rows, s->p_nrows, *s->pool, s->outputs, s->last);
     s->last.errors = s->p_errors;
   } else {

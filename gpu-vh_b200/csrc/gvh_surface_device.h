@@ -19,12 +19,14 @@ struct DeviceRows {
   int *c2p;                 // lattice cell -> point (scratch, nx ny nz ints)
   double *slot_rows;        // scratch: iso::kMaxElements rows per hypercube
   int *slot_n, *offsets;    // scratch: rows per hypercube, and their exclusive offsets
-  double *rows;             // out: the slab's rows, in order (room for the slots' worth)
-  long long *totals;        // out: [0] rows, [1] hypercubes where cornelius stopped
+  long long *totals;        // scratch: [0] rows, [1] hypercubes where cornelius stopped
+  double *rows;             // out (mapped pinned host memory): the slab's rows, in order, room
+                            // for the slots' worth
+  long long *host_totals;   // out (mapped pinned host memory): totals, written last
 };
 
-// Bytes of scratch and output per batch of ncubes hypercubes: slot_rows + slot_n + offsets
-// (rows needs as much again as slot_rows).
+// Bytes of device scratch per batch of ncubes hypercubes: slot_rows + slot_n + offsets (the
+// host's mapped row buffer needs the slot rows' worth too).
 size_t device_rows_slot_bytes(long long ncubes);
 
 cudaError_t launch_device_rows(const DeviceRows &d, cudaStream_t st);

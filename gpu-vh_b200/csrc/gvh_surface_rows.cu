@@ -4,7 +4,8 @@
 // reference's interpolation to the element's centroid, the row) -- the code the host pool
 // runs -- and writes its rows to a fixed slot; a scan over the per-cube counts and a
 // compaction then give the rows in the reference's order (hypercubes in loop order, a
-// cube's elements in cornelius' order). This file is compiled without FMA contraction
+// cube's elements in cornelius' order), written straight into mapped pinned host memory, so
+// nothing waits between the kernels and the copy. This file is compiled without FMA contraction
 // (-fmad=false, like the host side's -ffp-contract=off), so device and host rows agree to
 // the last bit; the host then only formats them (gvh_surface.cu).
 #include <cuda_runtime.h>
@@ -47,7 +48,7 @@ __global__ void __launch_bounds__(kRowThreads) cube_rows_kernel(RowGeometry g, l
 
 // Exclusive offsets of slot_n (one block); totals[0] = the number of rows.
 __global__ void rows_scan_kernel(long long n, const int *__restrict__ slot_n, int *__restrict__ offsets,
-                                 long long *__restrict__ totals) {
+                                 long long *__restrict__ totals, long long *__restrict__ host_totals) {
   __shared__ long long part[1024];
   const long long per = (n + blockDim.x - 1) / blockDim.x;
   const long long lo = min(n, (long long)threadIdx.x * per), hi = min(n, lo + per);
@@ -66,18 +67,25 @@ __global__ void rows_scan_kernel(long long n, const int *__restrict__ slot_n, in
     offsets[i] = (int)run;
     run += slot_n[i];
   }
-  if (threadIdx.x == blockDim.x - 1) totals[0] = part[threadIdx.x];
+  if (threadIdx.x == blockDim.x - 1) {
+    totals[0] = part[threadIdx.x];
+    host_totals[0] = part[threadIdx.x];
+    host_totals[1] = totals[1];  // the row kernel's error count (it ran before this kernel)
+  }
 }
 
+// One thread per value of a slot (hypercube c, row i, column k): consecutive threads write
+// consecutive values of a row, so each row crosses the host link as one contiguous write.
 __global__ void rows_compact_kernel(long long ncubes, const double *__restrict__ slot_rows,
                                     const int *__restrict__ slot_n, const int *__restrict__ offsets,
                                     double *__restrict__ rows) {
-  const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long per_cube = (long long)kSlotRows * kRowColumns;
+  const long long c = t / per_cube;
   if (c >= ncubes) return;
-  const int n = slot_n[c];
-  const double *src = slot_rows + c * (long long)(kSlotRows * kRowColumns);
-  double *dst = rows + (long long)offsets[c] * kRowColumns;
-  for (int i = 0; i < n * kRowColumns; ++i) dst[i] = src[i];
+  const int v = (int)(t - c * per_cube);
+  if (v >= slot_n[c] * kRowColumns) return;
+  rows[(long long)offsets[c] * kRowColumns + v] = slot_rows[c * per_cube + v];
 }
 
 }  // namespace
@@ -87,15 +95,17 @@ size_t device_rows_slot_bytes(long long ncubes) {
 }
 
 cudaError_t launch_device_rows(const DeviceRows &d, cudaStream_t st) {
-  if (d.ncubes <= 0) return cudaMemsetAsync(d.totals, 0, 2 * sizeof(long long), st);
+  if (d.ncubes <= 0) return cudaSuccess;  // the caller sets the totals to zero
   cudaError_t e = cudaMemsetAsync(d.totals, 0, 2 * sizeof(long long), st);
   if (e != cudaSuccess) return e;
   point_index_kernel<<<(unsigned)((d.npoints + 255) / 256), 256, 0, st>>>(d.npoints, d.point_cell, d.c2p);
   const unsigned blocks = (unsigned)((d.ncubes + kRowThreads - 1) / kRowThreads);
   cube_rows_kernel<<<blocks, kRowThreads, 0, st>>>(d.g, d.ncubes, d.cube_key, d.c2p, d.point_vals, d.slot_rows,
                                                    d.slot_n, reinterpret_cast<unsigned long long *>(d.totals + 1));
-  rows_scan_kernel<<<1, 1024, 0, st>>>(d.ncubes, d.slot_n, d.offsets, d.totals);
-  rows_compact_kernel<<<blocks, kRowThreads, 0, st>>>(d.ncubes, d.slot_rows, d.slot_n, d.offsets, d.rows);
+  rows_scan_kernel<<<1, 1024, 0, st>>>(d.ncubes, d.slot_n, d.offsets, d.totals, d.host_totals);
+  const long long values = d.ncubes * (long long)(kSlotRows * kRowColumns);
+  rows_compact_kernel<<<(unsigned)((values + 255) / 256), 256, 0, st>>>(d.ncubes, d.slot_rows, d.slot_n, d.offsets,
+                                                                        d.rows);
   return cudaGetLastError();
 }
 
