@@ -389,6 +389,29 @@ int gvh_run_loop(gvh_handle *h, const gvh_lattice_params *L, const gvh_hydro_par
 
   std::unique_ptr<ChunkWriter> writer;
   if (surf_file) writer.reset(new ChunkWriter(surf_file));
+  // the slab found last, whose text is taken at the next slab (or at the end)
+  struct DeferredSlab {
+    bool active;
+    long long flush, n, elements;
+  } deferred{false, -1, -1, 0};
+  auto take_deferred = [&]() -> int {
+    if (!deferred.active) return GVH_OK;
+    deferred.active = false;
+    const auto s0 = std::chrono::steady_clock::now();
+    gvh::surface::take_text(surf, chunk_text);  // waits for its formatting
+    chunk_rows += deferred.elements;
+    if (deferred.flush == deferred.n) {
+      if (!writer->push(std::move(chunk_text))) {
+        g_plugin_error = "writing surface.dat failed";
+        return GVH_ERR_INVALID;
+      }
+      surf_rows += chunk_rows;
+      chunk_text.clear();
+      chunk_rows = 0;
+    }
+    surf_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - s0).count();
+    return GVH_OK;
+  };
 
   const int nf = gvh_num_fields(h), nq = gvh_num_conserved(h);
   std::vector<std::vector<double>> fields;
@@ -439,28 +462,22 @@ int gvh_run_loop(gvh_handle *h, const gvh_lattice_params *L, const gvh_hydro_par
       surf_pending = true;
       surf_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - s0).count();
     }
-    // the host half, and the chunk written at the reference's iteration (HydroPlugin.cpp:287)
+    // the host half: this slab's elements are counted now and its rows formatted on the
+    // surface's thread pool while the loop goes on; its text joins the chunk one iteration
+    // later, which is written at the reference's iteration (HydroPlugin.cpp:287)
     auto finish_surface = [&]() -> int {
       if (!surf_pending) return GVH_OK;
       surf_pending = false;
       const auto s0 = std::chrono::steady_clock::now();
+      int r = take_deferred();
+      if (r) return r;
       long long nel = 0;
-      int r = gvh_surface_find_end(surf, &nel);
+      r = gvh_surface_find_end(surf, &nel);
       if (r) {
         g_plugin_error = gvh_surface_last_error();
         return r;
       }
-      gvh::surface::take_text(surf, chunk_text);
-      chunk_rows += nel;
-      if (flush == n) {
-        if (!writer->push(std::move(chunk_text))) {
-          g_plugin_error = "writing surface.dat failed";
-          return GVH_ERR_INVALID;
-        }
-        surf_rows += chunk_rows;
-        chunk_text.clear();
-        chunk_rows = 0;
-      }
+      deferred = DeferredSlab{true, flush, n, nel};
       surf_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - s0).count();
       return GVH_OK;
     };
@@ -488,6 +505,7 @@ int gvh_run_loop(gvh_handle *h, const gvh_lattice_params *L, const gvh_hydro_par
     ++steps;
     t = t0 + n * dt;
   }
+  if (!rc) rc = take_deferred();
   cudaEventDestroy(ev_begin);
   cudaEventDestroy(ev_end);
   unsigned flags = 0;

@@ -284,8 +284,12 @@ struct gvh_surface {
   char *rowdev;
   long long rowdev_cap;
   long long *h_rowtot, *d_rowtot_mapped;  // mapped pinned: rows, errors
-  double *h_rows, *d_rows_mapped;         // mapped pinned
-  long long cap_rows;
+  // two mapped pinned row buffers, alternating by slab: the host formats one slab's rows on
+  // the pool's workers while the device writes the next slab's into the other
+  double *h_rows[2], *d_rows_mapped[2];
+  long long cap_rows[2];
+  int rbuf;             // buffer of the slab begun last
+  bool formatting;      // a slab's rows are being formatted on the pool (format_rows async)
   long long p_nrows, p_errors;
   gvh::surface::Result last;
   gvh_surface_info info;
@@ -370,8 +374,19 @@ int gvh_surface_create(gvh_handle *h, double e_freezeout, gvh_surface **out) {
   return GVH_OK;
 }
 
+// Waits for the pool's formatting of the last slab (format_rows async), if any.
+static void wait_format(gvh_surface *s) {
+  if (s->formatting) {
+    const auto t0 = std::chrono::steady_clock::now();
+    s->pool->wait();
+    s->info.host_seconds_total += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    s->formatting = false;
+  }
+}
+
 int gvh_surface_destroy(gvh_surface *s) {
   if (!s) return GVH_OK;
+  wait_format(s);
   // touches nothing of the handle, which may be gone already; cudaFree waits for the
   // device work that uses the buffers
   cudaSetDevice(s->device);
@@ -381,7 +396,8 @@ int gvh_surface_destroy(gvh_surface *s) {
   if (s->rowdev) cudaFree(s->rowdev);
   cudaFreeHost(s->h_totals);
   if (s->h_rowtot) cudaFreeHost(s->h_rowtot);
-  if (s->h_rows) cudaFreeHost(s->h_rows);
+  for (int b = 0; b < 2; ++b)
+    if (s->h_rows[b]) cudaFreeHost(s->h_rows[b]);
   if (s->h_cube_key) cudaFreeHost(s->h_cube_key);
   if (s->h_point_cell) cudaFreeHost(s->h_point_cell);
   if (s->h_point_vals) cudaFreeHost(s->h_point_vals);
@@ -391,6 +407,7 @@ int gvh_surface_destroy(gvh_surface *s) {
 
 int gvh_surface_set_threads(gvh_surface *s, int nthreads) {
   if (!s || nthreads < 1) return sfail(GVH_ERR_INVALID, "gvh_surface_set_threads: bad argument");
+  wait_format(s);
   s->nthreads = nthreads;
   s->pool.reset();
   return GVH_OK;
@@ -398,6 +415,7 @@ int gvh_surface_set_threads(gvh_surface *s, int nthreads) {
 
 int gvh_surface_set_device_rows(gvh_surface *s, int on) {
   if (!s) return sfail(GVH_ERR_INVALID, "gvh_surface_set_device_rows: null argument");
+  wait_format(s);
   if (s->pending) return sfail(GVH_ERR_INVALID, "gvh_surface_set_device_rows: a slab is in flight");
   if (on && s->h->eos != GVH_EOS_QCD)
     return sfail(GVH_ERR_INVALID, "gvh_surface_set_device_rows: the device rows are for the QCD EoS only "
@@ -409,6 +427,7 @@ int gvh_surface_set_device_rows(gvh_surface *s, int on) {
 int gvh_surface_set_outputs(gvh_surface *s, int outputs) {
   if (!s || (outputs & ~(GVH_SURFACE_ROWS | GVH_SURFACE_TEXT)))
     return sfail(GVH_ERR_INVALID, "gvh_surface_set_outputs: bad argument");
+  wait_format(s);
   s->outputs = (outputs & GVH_SURFACE_ROWS ? gvh::surface::OUT_ROWS : 0) |
                (outputs & GVH_SURFACE_TEXT ? gvh::surface::OUT_TEXT : 0);
   return GVH_OK;
@@ -455,7 +474,9 @@ static int device_rows_begin(gvh_surface *s, long long ncubes, long long npoints
   // room for every crossed hypercube's largest number of rows (the previous slab's rows have
   // been formatted by now: find_end waited for them)
   const long long row_values = std::max(1ll, ncubes) * gvh::iso::kMaxElements * gvh::surface::kRowColumns;
-  int rc = grow_mapped(&s->h_rows, &s->d_rows_mapped, &s->cap_rows, row_values);
+  s->rbuf = 1 - s->rbuf;  // the other buffer: the slab before the last one is formatted by now
+  const int b = s->rbuf;
+  int rc = grow_mapped(&s->h_rows[b], &s->d_rows_mapped[b], &s->cap_rows[b], row_values);
   if (rc) return rc;
   s->h_rowtot[0] = s->h_rowtot[1] = 0;
   const long long cap = s->rowdev_cap;
@@ -479,7 +500,7 @@ static int device_rows_begin(gvh_surface *s, long long ncubes, long long npoints
   p += (size_t)cap * gvh::iso::kMaxElements * gvh::surface::kRowColumns * sizeof(double);
   d.slot_n = reinterpret_cast<int *>(p); p += (size_t)cap * sizeof(int);
   d.offsets = reinterpret_cast<int *>(p);
-  d.rows = s->d_rows_mapped;
+  d.rows = s->d_rows_mapped[b];
   d.host_totals = s->d_rowtot_mapped;
   SF_CUDA(gvh::surface::launch_device_rows(d, st));
   return GVH_OK;
@@ -562,10 +583,14 @@ int gvh_surface_find_end(gvh_surface *s, long long *n_elements) {
   slab.point_cell = s->h_point_cell;
   slab.point_vals = s->h_point_vals;
   if (!s->pool) s->pool.reset(new gvh::surface::Pool(s->nthreads));
+  wait_format(s);
   if (s->device_rows) {
     s->p_nrows = s->h_rowtot[0];
     s->p_errors = s->h_rowtot[1];
-    gvh::surface::format_rows(s->h_rows, s->p_nrows, *s->pool, s->outputs, s->last);
+    // formatted on the pool's workers while the caller goes on (the next step, the next
+    // slab's device work); anything that reads the rows or text waits for it
+    gvh::surface::format_rows(s->h_rows[s->rbuf], s->p_nrows, *s->pool, s->outputs, s->last, true);
+    s->formatting = s->p_nrows > 0;
     s->last.errors = s->p_errors;
   } else {
     gvh::surface::process_slab(slab, gvh::surface::Labels{s->p_label, s->p_scale}, *s->pool, s->outputs, s->c2p,
@@ -596,6 +621,7 @@ int gvh_surface_find(gvh_surface *s, double tau_label, double tau_scale, long lo
 
 int gvh_surface_get_rows(gvh_surface *s, double *rows, long long max_rows) {
   if (!s || (!rows && max_rows > 0)) return sfail(GVH_ERR_INVALID, "gvh_surface_get_rows: bad argument");
+  wait_format(s);
   if (max_rows < s->last.elements)
     return sfail(GVH_ERR_INVALID, "gvh_surface_get_rows: %lld rows do not fit in %lld", s->last.elements, max_rows);
   if (s->last.elements && !(s->outputs & gvh::surface::OUT_ROWS))
@@ -609,6 +635,7 @@ int gvh_surface_get_rows(gvh_surface *s, double *rows, long long max_rows) {
 
 int gvh_surface_get_text(gvh_surface *s, const char **text, long long *length) {
   if (!s || !text || !length) return sfail(GVH_ERR_INVALID, "gvh_surface_get_text: null argument");
+  wait_format(s);
   const std::string &t = s->last.text();
   *text = t.c_str();
   *length = (long long)t.size();
@@ -626,6 +653,7 @@ int gvh_surface_get_info(const gvh_surface *s, gvh_surface_info *info) {
 namespace gvh {
 namespace surface {
 void take_text(gvh_surface *s, std::vector<std::string> &out) {
+  wait_format(s);
   for (auto &p : s->last.parts) {
     out.emplace_back(std::move(p.text));
     p.text.clear();

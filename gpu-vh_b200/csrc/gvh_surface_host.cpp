@@ -109,6 +109,28 @@ void Pool::loop() {
   }
 }
 
+void Pool::start(int n, std::function<void(int)> f) {
+  if (n <= 0) return;
+  if (workers_.empty()) {  // no workers: do it now
+    for (int i = 0; i < n; ++i) f(i);
+    return;
+  }
+  std::unique_lock<std::mutex> lock(mu_);
+  owned_ = std::move(f);
+  job_ = &owned_;
+  njobs_ = n;
+  next_ = 0;
+  pending_ = n;
+  ++generation_;
+  wake_.notify_all();
+}
+
+void Pool::wait() {
+  std::unique_lock<std::mutex> lock(mu_);
+  done_.wait(lock, [&] { return pending_ == 0; });
+  job_ = nullptr;
+}
+
 void Pool::run(int n, const std::function<void(int)> &f) {
   if (n <= 0) return;
   std::unique_lock<std::mutex> lock(mu_);
@@ -129,7 +151,7 @@ void Pool::run(int n, const std::function<void(int)> &f) {
   job_ = nullptr;
 }
 
-void format_rows(const double *rows, long long n, Pool &pool, int outputs, Result &out) {
+void format_rows(const double *rows, long long n, Pool &pool, int outputs, Result &out, bool async) {
   out.elements = n;
   out.errors = 0;
   out.joined_valid = false;
@@ -139,7 +161,9 @@ void format_rows(const double *rows, long long n, Pool &pool, int outputs, Resul
   }
   const int nparts = (int)std::max<long long>(1, std::min<long long>(4ll * pool.size(), n / 256));
   out.parts.resize(nparts);
-  pool.run(nparts, [&](int i) {
+  Result *res = &out;
+  auto job = [rows, n, nparts, outputs, res](int i) {
+    Result &out = *res;
     const long long r0 = n * i / nparts, r1 = n * (i + 1) / nparts;
     Part &part = out.parts[i];
     part.rows.clear();
@@ -151,7 +175,9 @@ void format_rows(const double *rows, long long n, Pool &pool, int outputs, Resul
       part.text.reserve((size_t)(r1 - r0) * 240);
       for (long long r = r0; r < r1; ++r) append_row_text(part.text, rows + r * kColumns);
     }
-  });
+  };
+  if (async) pool.start(nparts, job);
+  else pool.run(nparts, job);
 }
 
 void process_slab(const Slab &s, const Labels &lab, Pool &pool, int outputs, std::vector<int> &c2p, Result &out) {

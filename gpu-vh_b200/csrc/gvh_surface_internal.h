@@ -71,6 +71,10 @@ class Pool {
   ~Pool();
   int size() const { return (int)workers_.size() + 1; }
   void run(int n, const std::function<void(int)> &f);
+  // start(): f(0..n-1) on the workers only, returning at once (inline when there are no
+  // workers); wait(): until a started job is done. A pool runs one job at a time.
+  void start(int n, std::function<void(int)> f);
+  void wait();
 
  private:
   void loop();
@@ -78,14 +82,17 @@ class Pool {
   std::mutex mu_;
   std::condition_variable wake_, done_;
   const std::function<void(int)> *job_ = nullptr;
+  std::function<void(int)> owned_;  // the started job
   int njobs_ = 0, next_ = 0, pending_ = 0;
   long long generation_ = 0;
   bool stop_ = false;
 };
 
 // Formats rows the device produced (n rows of kColumns) into out's parts on the pool, in
-// order; keeps the rows too when outputs has OUT_ROWS.
-void format_rows(const double *rows, long long n, Pool &pool, int outputs, Result &out);
+// order; keeps the rows too when outputs has OUT_ROWS. With async the work is started on the
+// pool's workers and format_rows returns at once: pool.wait() before reading out or reusing
+// rows.
+void format_rows(const double *rows, long long n, Pool &pool, int outputs, Result &out, bool async = false);
 
 // Runs the surface finder on every crossed hypercube of the slab on the pool, in order.
 // outputs: OUT_ROWS and/or OUT_TEXT. cell_to_point is scratch of at least nx*ny*nz entries
