@@ -423,7 +423,10 @@ int gvh_run_loop(gvh_handle *h, const gvh_lattice_params *L, const gvh_hydro_par
   const int nt = L->numProperTimePoints;
   cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
   cudaSetDevice(h->device);
-  if (cudaEventCreate(&ev_begin) != cudaSuccess || cudaEventCreate(&ev_end) != cudaSuccess) {
+  // the wait for each step blocks the thread instead of spinning on a core: the surface's
+  // formatting threads and the file writer need the host cores meanwhile
+  if (cudaEventCreate(&ev_begin) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ev_end, surf ? cudaEventBlockingSync : cudaEventDefault) != cudaSuccess) {
     gvh_surface_destroy(surf);
     if (surf_file) fclose(surf_file);
     return pfail(GVH_ERR_CUDA, "gvh_run_loop: event creation failed");

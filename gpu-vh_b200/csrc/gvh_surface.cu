@@ -363,7 +363,8 @@ int gvh_surface_create(gvh_handle *h, double e_freezeout, gvh_surface **out) {
     return sfail(GVH_ERR_NOMEM, "gvh_surface_create: cannot pin host memory");
   }
   memset(&s->info, 0, sizeof s->info);
-  if (cudaEventCreateWithFlags(&s->copied, cudaEventDisableTiming) != cudaSuccess) {
+  // waited on by blocking, not spinning: the pool's formatting threads need the cores
+  if (cudaEventCreateWithFlags(&s->copied, cudaEventDisableTiming | cudaEventBlockingSync) != cudaSuccess) {
     cudaFreeHost(s->h_totals);
     cudaFreeHost(s->h_rowtot);
     cudaFree(s->dev);
