@@ -299,6 +299,7 @@ struct gvh_surface {
   long long p_ncubes, p_npoints;
   double p_label, p_scale;
   cudaEvent_t copied;
+  cudaStream_t rows_stream;  // the device rows run here, beside the handle's next step
   std::chrono::steady_clock::time_point p_t0;
 };
 
@@ -364,7 +365,8 @@ int gvh_surface_create(gvh_handle *h, double e_freezeout, gvh_surface **out) {
   }
   memset(&s->info, 0, sizeof s->info);
   // waited on by blocking, not spinning: the pool's formatting threads need the cores
-  if (cudaEventCreateWithFlags(&s->copied, cudaEventDisableTiming | cudaEventBlockingSync) != cudaSuccess) {
+  if (cudaEventCreateWithFlags(&s->copied, cudaEventDisableTiming | cudaEventBlockingSync) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&s->rows_stream, cudaStreamNonBlocking) != cudaSuccess) {
     cudaFreeHost(s->h_totals);
     cudaFreeHost(s->h_rowtot);
     cudaFree(s->dev);
@@ -392,7 +394,9 @@ int gvh_surface_destroy(gvh_surface *s) {
   // device work that uses the buffers
   cudaSetDevice(s->device);
   cudaEventSynchronize(s->copied);
+  cudaStreamSynchronize(s->rows_stream);
   cudaEventDestroy(s->copied);
+  cudaStreamDestroy(s->rows_stream);
   cudaFree(s->dev);
   if (s->rowdev) cudaFree(s->rowdev);
   cudaFreeHost(s->h_totals);
@@ -457,7 +461,10 @@ int gvh_surface_set_lower(gvh_surface *s) {
 static int device_rows_begin(gvh_surface *s, long long ncubes, long long npoints, double tau_label,
                              double tau_scale) {
   gvh_handle *h = s->h;
-  cudaStream_t st = h->stream;
+  // The marking kernels are complete (find_begin read their totals); the rows run on the
+  // surface's own stream, so the handle's next step does not wait for them. The previous
+  // slab's rows are complete too (find_end waited for them), so the buffers are free.
+  cudaStream_t st = s->rows_stream;
   const size_t per_cube = gvh::surface::device_rows_slot_bytes(1);
   if (ncubes > s->rowdev_cap) {
     const long long cap = std::max<long long>(ncubes, s->rowdev_cap * 3 / 2 + 1024);
@@ -533,7 +540,7 @@ int gvh_surface_find_begin(gvh_surface *s, double tau_label, double tau_scale) {
   const long long ncubes = s->h_totals[0], npoints = s->h_totals[1];
   if (s->device_rows) {
     if ((rc = device_rows_begin(s, ncubes, npoints, tau_label, tau_scale))) return rc;
-    SF_CUDA(cudaEventRecord(s->copied, st));
+    SF_CUDA(cudaEventRecord(s->copied, s->rows_stream));
     s->lower = upper;
     s->pending = true;
     s->p_ncubes = ncubes;
