@@ -283,14 +283,21 @@ struct gvh_surface {
   int *d_c2p;
   char *rowdev;
   long long rowdev_cap;
-  long long *h_rowtot, *d_rowtot_mapped;  // mapped pinned: rows, errors
-  // two mapped pinned row buffers, alternating by slab: the host formats one slab's rows on
-  // the pool's workers while the device writes the next slab's into the other
+  // mapped pinned: rows, errors, text bytes, text fits, rows without text
+  long long *h_rowtot, *d_rowtot_mapped;
+  // two sets of mapped pinned buffers, alternating by slab: the host assembles one slab's
+  // text on the pool's workers while the device writes the next slab's into the other. The
+  // device writes the text and the rows the host formats itself (all rows with OUT_ROWS).
   double *h_rows[2], *d_rows_mapped[2];
   long long cap_rows[2];
+  char *h_text[2], *d_text_mapped[2];
+  long long cap_text[2];
+  long long *h_toff[2], *d_toff_mapped[2];  // text offsets, rows + 1
+  long long cap_toff[2];
+  double text_per_cube;  // the most text bytes per crossed hypercube seen; sizes h_text
   int rbuf;             // buffer of the slab begun last
   bool formatting;      // a slab's rows are being formatted on the pool (format_rows async)
-  long long p_nrows, p_errors;
+  long long p_nrows, p_errors, p_text_bytes, p_rows_sent;
   gvh::surface::Result last;
   gvh_surface_info info;
   // a slab between gvh_surface_find_begin and _end: its copies to the pinned buffers are in
@@ -317,6 +324,7 @@ int gvh_surface_create(gvh_handle *h, double e_freezeout, gvh_surface **out) {
   if (h->ncells >= (1ll << 31)) return sfail(GVH_ERR_INVALID, "gvh_surface_create: lattice too large");
   SF_CUDA(cudaSetDevice(h->device));
   gvh_surface *s = new gvh_surface();
+  s->text_per_cube = 320;
   s->h = h;
   s->device = h->device;
   s->iso = e_freezeout;
@@ -354,7 +362,7 @@ int gvh_surface_create(gvh_handle *h, double e_freezeout, gvh_surface **out) {
   // is a pow, which the device does not evaluate as the host's libm does
   s->device_rows = h->eos == GVH_EOS_QCD;
   if (cudaHostAlloc(reinterpret_cast<void **>(&s->h_totals), 4 * sizeof(int), cudaHostAllocDefault) != cudaSuccess ||
-      cudaHostAlloc(reinterpret_cast<void **>(&s->h_rowtot), 2 * sizeof(long long), cudaHostAllocMapped) !=
+      cudaHostAlloc(reinterpret_cast<void **>(&s->h_rowtot), 8 * sizeof(long long), cudaHostAllocMapped) !=
           cudaSuccess ||
       cudaHostGetDevicePointer(reinterpret_cast<void **>(&s->d_rowtot_mapped), s->h_rowtot, 0) != cudaSuccess) {
     if (s->h_rowtot) cudaFreeHost(s->h_rowtot);
@@ -401,8 +409,11 @@ int gvh_surface_destroy(gvh_surface *s) {
   if (s->rowdev) cudaFree(s->rowdev);
   cudaFreeHost(s->h_totals);
   if (s->h_rowtot) cudaFreeHost(s->h_rowtot);
-  for (int b = 0; b < 2; ++b)
+  for (int b = 0; b < 2; ++b) {
     if (s->h_rows[b]) cudaFreeHost(s->h_rows[b]);
+    if (s->h_text[b]) cudaFreeHost(s->h_text[b]);
+    if (s->h_toff[b]) cudaFreeHost(s->h_toff[b]);
+  }
   if (s->h_cube_key) cudaFreeHost(s->h_cube_key);
   if (s->h_point_cell) cudaFreeHost(s->h_point_cell);
   if (s->h_point_vals) cudaFreeHost(s->h_point_vals);
@@ -465,7 +476,6 @@ static int device_rows_begin(gvh_surface *s, long long ncubes, long long npoints
   // surface's own stream, so the handle's next step does not wait for them. The previous
   // slab's rows are complete too (find_end waited for them), so the buffers are free.
   cudaStream_t st = s->rows_stream;
-  const size_t per_cube = gvh::surface::device_rows_slot_bytes(1);
   if (ncubes > s->rowdev_cap) {
     const long long cap = std::max<long long>(ncubes, s->rowdev_cap * 3 / 2 + 1024);
     if (s->rowdev) {
@@ -474,7 +484,7 @@ static int device_rows_begin(gvh_surface *s, long long ncubes, long long npoints
       s->rowdev = nullptr;
       s->rowdev_cap = 0;
     }
-    const size_t bytes = (size_t)cap * per_cube + 256;
+    const size_t bytes = gvh::surface::device_rows_slot_bytes(cap) + 1024;
     if (cudaMalloc(&s->rowdev, bytes) != cudaSuccess)
       return sfail(GVH_ERR_NOMEM, "gvh_surface: cannot allocate %zu bytes for the device rows", bytes);
     s->rowdev_cap = cap;
@@ -486,7 +496,17 @@ static int device_rows_begin(gvh_surface *s, long long ncubes, long long npoints
   const int b = s->rbuf;
   int rc = grow_mapped(&s->h_rows[b], &s->d_rows_mapped[b], &s->cap_rows[b], row_values);
   if (rc) return rc;
-  s->h_rowtot[0] = s->h_rowtot[1] = 0;
+  const bool text = s->outputs & gvh::surface::OUT_TEXT;
+  if (text) {
+    // text room for the most text per hypercube seen so far (a slab whose text does not fit
+    // sends all its rows instead, and the host formats them)
+    const long long slots = std::max(1ll, ncubes) * gvh::iso::kMaxElements;
+    if ((rc = grow_mapped(&s->h_toff[b], &s->d_toff_mapped[b], &s->cap_toff[b], slots + 1)) ||
+        (rc = grow_mapped(&s->h_text[b], &s->d_text_mapped[b], &s->cap_text[b],
+                          (long long)(std::max(1ll, ncubes) * s->text_per_cube * 1.25) + 4096)))
+      return rc;
+  }
+  for (int i = 0; i < 5; ++i) s->h_rowtot[i] = 0;
   const long long cap = s->rowdev_cap;
   gvh::surface::DeviceRows d;
   d.g.dim = s->dim;
@@ -502,14 +522,13 @@ static int device_rows_begin(gvh_surface *s, long long ncubes, long long npoints
   d.point_cell = s->point_cell;
   d.point_vals = s->point_vals;
   d.c2p = s->d_c2p;
-  char *p = s->rowdev;
-  d.totals = reinterpret_cast<long long *>(p); p += 256;
-  d.slot_rows = reinterpret_cast<double *>(p);
-  p += (size_t)cap * gvh::iso::kMaxElements * gvh::surface::kRowColumns * sizeof(double);
-  d.slot_n = reinterpret_cast<int *>(p); p += (size_t)cap * sizeof(int);
-  d.offsets = reinterpret_cast<int *>(p);
+  gvh::surface::device_rows_carve(d, s->rowdev, cap);
   d.rows = s->d_rows_mapped[b];
   d.host_totals = s->d_rowtot_mapped;
+  d.text = text ? s->d_text_mapped[b] : nullptr;
+  d.text_cap = text ? s->cap_text[b] : 0;
+  d.host_text_off = text ? s->d_toff_mapped[b] : nullptr;
+  d.keep_rows = s->outputs & gvh::surface::OUT_ROWS;
   SF_CUDA(gvh::surface::launch_device_rows(d, st));
   return GVH_OK;
 }
@@ -595,9 +614,18 @@ int gvh_surface_find_end(gvh_surface *s, long long *n_elements) {
   if (s->device_rows) {
     s->p_nrows = s->h_rowtot[0];
     s->p_errors = s->h_rowtot[1];
-    // formatted on the pool's workers while the caller goes on (the next step, the next
-    // slab's device work); anything that reads the rows or text waits for it
-    gvh::surface::format_rows(s->h_rows[s->rbuf], s->p_nrows, *s->pool, s->outputs, s->last, true);
+    const int b = s->rbuf;
+    const bool text = (s->outputs & gvh::surface::OUT_TEXT) && s->p_nrows > 0;
+    const bool text_fits = text && s->h_rowtot[3];
+    if (text && ncubes > 0)
+      s->text_per_cube = std::max(s->text_per_cube, (double)s->h_rowtot[2] / (double)ncubes);
+    // assembled (text) or formatted (rows the device left to the host) on the pool's workers
+    // while the caller goes on (the next step, the next slab's device work); anything that
+    // reads the rows or text waits for it
+    gvh::surface::format_rows(s->h_rows[b], s->p_nrows, *s->pool, s->outputs, s->last, true,
+                              text_fits ? s->h_text[b] : nullptr, text_fits ? s->h_toff[b] : nullptr);
+    s->p_text_bytes = text_fits ? s->h_rowtot[2] : 0;
+    s->p_rows_sent = text_fits && !(s->outputs & gvh::surface::OUT_ROWS) ? s->h_rowtot[4] : s->p_nrows;
     s->formatting = s->p_nrows > 0;
     s->last.errors = s->p_errors;
   } else {
@@ -613,7 +641,8 @@ int gvh_surface_find_end(gvh_surface *s, long long *n_elements) {
   in.elements_last = s->last.elements;
   in.elements_total += s->last.elements;
   in.errors_total += s->last.errors;
-  in.bytes_to_host_total += s->device_rows ? (double)s->p_nrows * gvh::surface::kRowColumns * 8 + 24
+  in.bytes_to_host_total += s->device_rows ? (double)s->p_text_bytes + (s->p_text_bytes ? 8.0 * (s->p_nrows + 1) : 0) +
+                                                 (double)s->p_rows_sent * gvh::surface::kRowColumns * 8 + 32
                                            : (double)ncubes * 4 + (double)npoints * (4 + 2 * kVars * 8) + 8;
   in.device_seconds_total += std::chrono::duration<double>(t1 - s->p_t0).count();
   in.host_seconds_total += std::chrono::duration<double>(t2 - t1).count();

@@ -151,7 +151,8 @@ void Pool::run(int n, const std::function<void(int)> &f) {
   job_ = nullptr;
 }
 
-void format_rows(const double *rows, long long n, Pool &pool, int outputs, Result &out, bool async) {
+void format_rows(const double *rows, long long n, Pool &pool, int outputs, Result &out, bool async, const char *text,
+                 const long long *text_off) {
   out.elements = n;
   out.errors = 0;
   out.joined_valid = false;
@@ -162,7 +163,7 @@ void format_rows(const double *rows, long long n, Pool &pool, int outputs, Resul
   const int nparts = (int)std::max<long long>(1, std::min<long long>(4ll * pool.size(), n / 256));
   out.parts.resize(nparts);
   Result *res = &out;
-  auto job = [rows, n, nparts, outputs, res](int i) {
+  auto job = [rows, n, nparts, outputs, res, text, text_off](int i) {
     Result &out = *res;
     const long long r0 = n * i / nparts, r1 = n * (i + 1) / nparts;
     Part &part = out.parts[i];
@@ -171,9 +172,21 @@ void format_rows(const double *rows, long long n, Pool &pool, int outputs, Resul
     part.elements = r1 - r0;
     part.errors = 0;
     if (outputs & OUT_ROWS) part.rows.assign(rows + r0 * kColumns, rows + r1 * kColumns);
-    if (outputs & OUT_TEXT) {
+    if (!(outputs & OUT_TEXT)) return;
+    if (!text) {
       part.text.reserve((size_t)(r1 - r0) * 240);
       for (long long r = r0; r < r1; ++r) append_row_text(part.text, rows + r * kColumns);
+      return;
+    }
+    // the device's text, in runs of rows it formatted; a row of no text is formatted here
+    part.text.reserve((size_t)(text_off[r1] - text_off[r0]) + 64);
+    long long r = r0;
+    while (r < r1) {
+      long long e = r;
+      while (e < r1 && text_off[e + 1] > text_off[e]) ++e;
+      if (e > r) part.text.append(text + text_off[r], (size_t)(text_off[e] - text_off[r]));
+      if (e < r1) append_row_text(part.text, rows + e * kColumns);
+      r = e + 1;
     }
   };
   if (async) pool.start(nparts, job);

@@ -89,10 +89,13 @@ class Pool {
 };
 
 // Formats rows the device produced (n rows of kColumns) into out's parts on the pool, in
-// order; keeps the rows too when outputs has OUT_ROWS. With async the work is started on the
-// pool's workers and format_rows returns at once: pool.wait() before reading out or reusing
-// rows.
-void format_rows(const double *rows, long long n, Pool &pool, int outputs, Result &out, bool async = false);
+// order; keeps the rows too when outputs has OUT_ROWS. With text (the device's text of the
+// rows, row r at text_off[r] .. text_off[r + 1]) the parts take their text from it, and only
+// rows of no text (text_off[r + 1] == text_off[r]) are formatted from rows. With async the
+// work is started on the pool's workers and format_rows returns at once: pool.wait() before
+// reading out or reusing rows or text.
+void format_rows(const double *rows, long long n, Pool &pool, int outputs, Result &out, bool async = false,
+                 const char *text = nullptr, const long long *text_off = nullptr);
 
 // Runs the surface finder on every crossed hypercube of the slab on the pool, in order.
 // outputs: OUT_ROWS and/or OUT_TEXT. cell_to_point is scratch of at least nx*ny*nz entries

@@ -486,6 +486,7 @@ class Batch:
 # ---- freeze-out hypersurface ------------------------------------------------------------
 
 SURFACE_COLUMNS = 20
+SURFACE_ROWS, SURFACE_TEXT = 1, 2  # gvh_surface_set_outputs
 SURFACE_COLUMN_NAMES = ["tau", "x", "y", "eta", "dsigma_tau", "dsigma_x", "dsigma_y", "dsigma_eta", "ux", "uy",
                         "un", "e", "T", "p", "pixx", "pixy", "pixn", "piyy", "piyn", "Pi"]
 
@@ -506,6 +507,7 @@ def _bind_surface(L):
     L.gvh_surface_destroy.argtypes = [vp]
     L.gvh_surface_set_threads.argtypes = [vp, ctypes.c_int]
     L.gvh_surface_set_device_rows.argtypes = [vp, ctypes.c_int]
+    L.gvh_surface_set_outputs.argtypes = [vp, ctypes.c_int]
     L.gvh_surface_set_lower.argtypes = [vp]
     L.gvh_surface_find.argtypes = [vp, dp, dp, ctypes.POINTER(ll)]
     L.gvh_surface_get_rows.argtypes = [vp, ctypes.POINTER(dp), ll]
@@ -574,6 +576,11 @@ class Surface:
     def set_device_rows(self, on: bool):
         """Make the rows on the device (default for the QCD EoS) or with the host pool."""
         self._check(self._L.gvh_surface_set_device_rows(self._h, int(bool(on))), "gvh_surface_set_device_rows")
+
+    def set_outputs(self, rows: bool = True, text: bool = True):
+        """Keep the slab's rows, its surface.dat text, or both (the default)."""
+        self._check(self._L.gvh_surface_set_outputs(self._h, (SURFACE_ROWS if rows else 0) |
+                                                    (SURFACE_TEXT if text else 0)), "gvh_surface_set_outputs")
 
     def find(self, tau_label, tau_scale) -> int:
         n = ctypes.c_longlong()

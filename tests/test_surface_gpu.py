@@ -85,19 +85,22 @@ def test_device_rows_equal_host_rows(case):
     efo = gvh.energy_density_of_temperature(0.150)
     D = gvh.Surface(G, efo, threads=3)
     H = gvh.Surface(G, efo, threads=3)
+    T = gvh.Surface(G, efo, threads=3)  # text only: the device sends text, rows only where needed
     H.set_device_rows(False)
+    T.set_outputs(rows=False, text=True)
     D.set_lower()
     H.set_lower()
+    T.set_lower()
     t, total = t0, 0
     for n in range(1, 25):
         G.step(t, dt)
         t = t0 + n * dt
         label, scale, _ = gvh.slab_labels(n - 1, t0, dt)
-        nd, nh = D.find(label, scale), H.find(label, scale)
-        assert nd == nh
+        nd, nh, nt = D.find(label, scale), H.find(label, scale), T.find(label, scale)
+        assert nd == nh == nt
         rd, rh = D.rows(), H.rows()
         assert np.array_equal(rd.view(np.uint64), rh.view(np.uint64)), n
-        assert D.text() == H.text()
+        assert D.text() == H.text() == T.text()
         total += nd
     assert total > 50
     assert D.info()["errors_total"] == H.info()["errors_total"] == 0
@@ -106,6 +109,41 @@ def test_device_rows_equal_host_rows(case):
     with pytest.raises(gvh.GvhError):
         S.set_device_rows(True)
     S.set_device_rows(False)
+
+
+def test_device_text_splices_host_formatted_rows():
+    """A row with a number the device's fast %g leaves to the exact path (here bulk pressures
+    of order 1e-28, outside its exponent range) is formatted on the host and spliced into the
+    device's text in order: text-only, rows + text and the host pool's text agree. The time
+    levels are set, not stepped (a step would relax the bulk pressure): the energy density
+    falls by a fifth from level to level, so the surface is a shell crossing both halves."""
+    lat = CASES["qcd_bulk_3d"]
+    G = gvh.Lattice(**lat)
+    prim = rich_state(G, seed=4, e0=25.0, emin=0.3, spacing=0.6)
+    Pi = prim["Pi"].reshape(G.ncz, G.ncy, G.ncx).copy()
+    Pi[:, :, : G.ncx // 2] *= 1e-27
+    prim["Pi"] = Pi.reshape(-1)
+    efo = gvh.energy_density_of_temperature(0.150)
+    D, H, T = (gvh.Surface(G, efo, threads=3) for _ in range(3))
+    H.set_device_rows(False)
+    T.set_outputs(rows=False, text=True)
+    G.set_primitive(prim)
+    for S in (D, H, T):
+        S.set_lower()
+    tiny = plain = 0
+    for n in range(1, 4):
+        G.set_primitive(dict(prim, e=prim["e"] * 0.8 ** n))
+        label, scale, _ = gvh.slab_labels(n - 1, 0.5, lat["dt"])
+        assert D.find(label, scale) == H.find(label, scale) == T.find(label, scale)
+        text = H.text()
+        assert D.text() == text and T.text() == text, n
+        for line in text.splitlines():
+            ex = line.split()[-1].partition("e-")[2]
+            if ex and int(ex) > 17:
+                tiny += 1
+            else:
+                plain += 1
+    assert tiny > 0 and plain > 0, (tiny, plain)
 
 
 def test_device_marking_counts():
