@@ -450,8 +450,12 @@ int gvh_run_loop(gvh_handle *h, const gvh_lattice_params *L, const gvh_hydro_par
       gvh_write_field(output_dir, "ut", t, L, fp[base + 2]);
       for (int c = 4; c < nq; ++c) gvh_write_field(output_dir, qn[c], t, L, fp[c]);
     }
-    // The slab (n-2, n-1) is marked and copied now; its host half runs while the GPU takes
-    // the next step (the copies are queued on the handle's stream before it).
+    // the stop test's reduction first: it waits for its result, which must not queue behind
+    // the surface's device work
+    double emax = 0.0;
+    if ((rc = gvh_max_energy_density(h, &emax))) break;
+    // The slab (n-2, n-1) is marked now and its rows made on the surface's stream beside the
+    // next step; its host half runs while the GPU takes that step.
     bool surf_pending = false;
     long long flush = -1;
     if (surf && n >= 2) {
@@ -484,8 +488,6 @@ int gvh_run_loop(gvh_handle *h, const gvh_lattice_params *L, const gvh_hydro_par
       surf_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - s0).count();
       return GVH_OK;
     };
-    double emax = 0.0;
-    if ((rc = gvh_max_energy_density(h, &emax))) break;
     if (emax <= e_fo) ++frozen;
     if (frozen >= kFreezeoutChecks) {
       rc = finish_surface();

@@ -18,8 +18,9 @@
 //
 // and then, for the QCD EoS (the default), the rows themselves are made on the device
 // (gvh_surface_rows.cu: cornelius, interpolation and the row, one thread per crossed
-// hypercube, the host's code without FMA contraction) and only they are copied to the host,
-// which formats them; otherwise the host receives the keys and points (about 170 bytes per
+// hypercube, the host's code without FMA contraction), and with them their surface.dat text,
+// which the copy engine brings to the host; the host formats only the few rows whose numbers
+// the device's fast %g leaves to the exact path. Otherwise the host receives the keys and points (about 170 bytes per
 // crossed hypercube instead of ~160 bytes per lattice cell per level) and runs the same code
 // with a pool of host threads (gvh_surface_host.cpp).
 #include <cuda_runtime.h>
@@ -283,21 +284,22 @@ struct gvh_surface {
   int *d_c2p;
   char *rowdev;
   long long rowdev_cap;
-  // mapped pinned: rows, errors, text bytes, text fits, rows without text
-  long long *h_rowtot, *d_rowtot_mapped;
-  // two sets of mapped pinned buffers, alternating by slab: the host assembles one slab's
-  // text on the pool's workers while the device writes the next slab's into the other. The
-  // device writes the text and the rows the host formats itself (all rows with OUT_ROWS).
+  long long *h_rowtot, *d_rowtot_mapped;  // mapped pinned: rows, errors, text bytes, host rows
+  // two sets of host buffers, alternating by slab: the host assembles one slab's text on the
+  // pool's workers while the device writes the next slab's into the other. The device's text
+  // comes by copy (pinned); the host rows, and all rows when they are kept (or the host rows
+  // overflow), are written by the device into mapped pinned memory.
   double *h_rows[2], *d_rows_mapped[2];
   long long cap_rows[2];
-  char *h_text[2], *d_text_mapped[2];
+  gvh::surface::HostRow *h_hrows[2], *d_hrows_mapped[2];
+  long long cap_hrows[2];
+  char *h_text[2];
   long long cap_text[2];
-  long long *h_toff[2], *d_toff_mapped[2];  // text offsets, rows + 1
-  long long cap_toff[2];
-  double text_per_cube;  // the most text bytes per crossed hypercube seen; sizes h_text
+  cudaEvent_t text_copied[2];
   int rbuf;             // buffer of the slab begun last
   bool formatting;      // a slab's rows are being formatted on the pool (format_rows async)
-  long long p_nrows, p_errors, p_text_bytes, p_rows_sent;
+  long long p_nrows, p_errors, p_text_bytes, p_host_rows;
+  bool p_all_rows;
   gvh::surface::Result last;
   gvh_surface_info info;
   // a slab between gvh_surface_find_begin and _end: its copies to the pinned buffers are in
@@ -324,7 +326,6 @@ int gvh_surface_create(gvh_handle *h, double e_freezeout, gvh_surface **out) {
   if (h->ncells >= (1ll << 31)) return sfail(GVH_ERR_INVALID, "gvh_surface_create: lattice too large");
   SF_CUDA(cudaSetDevice(h->device));
   gvh_surface *s = new gvh_surface();
-  s->text_per_cube = 320;
   s->h = h;
   s->device = h->device;
   s->iso = e_freezeout;
@@ -374,6 +375,8 @@ int gvh_surface_create(gvh_handle *h, double e_freezeout, gvh_surface **out) {
   memset(&s->info, 0, sizeof s->info);
   // waited on by blocking, not spinning: the pool's formatting threads need the cores
   if (cudaEventCreateWithFlags(&s->copied, cudaEventDisableTiming | cudaEventBlockingSync) != cudaSuccess ||
+      cudaEventCreateWithFlags(&s->text_copied[0], cudaEventDisableTiming | cudaEventBlockingSync) != cudaSuccess ||
+      cudaEventCreateWithFlags(&s->text_copied[1], cudaEventDisableTiming | cudaEventBlockingSync) != cudaSuccess ||
       cudaStreamCreateWithFlags(&s->rows_stream, cudaStreamNonBlocking) != cudaSuccess) {
     cudaFreeHost(s->h_totals);
     cudaFreeHost(s->h_rowtot);
@@ -404,6 +407,8 @@ int gvh_surface_destroy(gvh_surface *s) {
   cudaEventSynchronize(s->copied);
   cudaStreamSynchronize(s->rows_stream);
   cudaEventDestroy(s->copied);
+  for (int b = 0; b < 2; ++b)
+    if (s->text_copied[b]) cudaEventDestroy(s->text_copied[b]);
   cudaStreamDestroy(s->rows_stream);
   cudaFree(s->dev);
   if (s->rowdev) cudaFree(s->rowdev);
@@ -412,7 +417,7 @@ int gvh_surface_destroy(gvh_surface *s) {
   for (int b = 0; b < 2; ++b) {
     if (s->h_rows[b]) cudaFreeHost(s->h_rows[b]);
     if (s->h_text[b]) cudaFreeHost(s->h_text[b]);
-    if (s->h_toff[b]) cudaFreeHost(s->h_toff[b]);
+    if (s->h_hrows[b]) cudaFreeHost(s->h_hrows[b]);
   }
   if (s->h_cube_key) cudaFreeHost(s->h_cube_key);
   if (s->h_point_cell) cudaFreeHost(s->h_point_cell);
@@ -467,8 +472,9 @@ int gvh_surface_set_lower(gvh_surface *s) {
   return GVH_OK;
 }
 
-// The slab's rows on the device (gvh_surface_rows.cu), queued on the handle's stream; they and
-// their count land in mapped pinned host memory, so nothing here waits for them.
+// The slab's rows and text on the device (gvh_surface_rows.cu), queued on the surface's
+// stream; the counts, the host rows (and the rows, when kept) land in mapped pinned host
+// memory and the text stays on the device for find_end to copy, so nothing here waits.
 static int device_rows_begin(gvh_surface *s, long long ncubes, long long npoints, double tau_label,
                              double tau_scale) {
   gvh_handle *h = s->h;
@@ -484,29 +490,23 @@ static int device_rows_begin(gvh_surface *s, long long ncubes, long long npoints
       s->rowdev = nullptr;
       s->rowdev_cap = 0;
     }
-    const size_t bytes = gvh::surface::device_rows_slot_bytes(cap) + 1024;
+    const size_t bytes = gvh::surface::device_rows_scratch_bytes(cap);
     if (cudaMalloc(&s->rowdev, bytes) != cudaSuccess)
       return sfail(GVH_ERR_NOMEM, "gvh_surface: cannot allocate %zu bytes for the device rows", bytes);
     s->rowdev_cap = cap;
   }
-  // room for every crossed hypercube's largest number of rows (the previous slab's rows have
-  // been formatted by now: find_end waited for them)
-  const long long row_values = std::max(1ll, ncubes) * gvh::iso::kMaxElements * gvh::surface::kRowColumns;
-  s->rbuf = 1 - s->rbuf;  // the other buffer: the slab before the last one is formatted by now
+  // room for every crossed hypercube's largest number of rows, and for host rows up to a
+  // sixteenth of the slots (more send every row instead); the slab before the last one is
+  // formatted by now, so its buffers are free
+  const long long slots = std::max(1ll, ncubes) * gvh::iso::kMaxElements;
+  s->rbuf = 1 - s->rbuf;
   const int b = s->rbuf;
-  int rc = grow_mapped(&s->h_rows[b], &s->d_rows_mapped[b], &s->cap_rows[b], row_values);
+  int rc = grow_mapped(&s->h_rows[b], &s->d_rows_mapped[b], &s->cap_rows[b], slots * gvh::surface::kRowColumns);
   if (rc) return rc;
   const bool text = s->outputs & gvh::surface::OUT_TEXT;
-  if (text) {
-    // text room for the most text per hypercube seen so far (a slab whose text does not fit
-    // sends all its rows instead, and the host formats them)
-    const long long slots = std::max(1ll, ncubes) * gvh::iso::kMaxElements;
-    if ((rc = grow_mapped(&s->h_toff[b], &s->d_toff_mapped[b], &s->cap_toff[b], slots + 1)) ||
-        (rc = grow_mapped(&s->h_text[b], &s->d_text_mapped[b], &s->cap_text[b],
-                          (long long)(std::max(1ll, ncubes) * s->text_per_cube * 1.25) + 4096)))
-      return rc;
-  }
-  for (int i = 0; i < 5; ++i) s->h_rowtot[i] = 0;
+  if (text && (rc = grow_mapped(&s->h_hrows[b], &s->d_hrows_mapped[b], &s->cap_hrows[b], slots / 16 + 1024)))
+    return rc;
+  for (int i = 0; i < 4; ++i) s->h_rowtot[i] = 0;
   const long long cap = s->rowdev_cap;
   gvh::surface::DeviceRows d;
   d.g.dim = s->dim;
@@ -525,9 +525,9 @@ static int device_rows_begin(gvh_surface *s, long long ncubes, long long npoints
   gvh::surface::device_rows_carve(d, s->rowdev, cap);
   d.rows = s->d_rows_mapped[b];
   d.host_totals = s->d_rowtot_mapped;
-  d.text = text ? s->d_text_mapped[b] : nullptr;
-  d.text_cap = text ? s->cap_text[b] : 0;
-  d.host_text_off = text ? s->d_toff_mapped[b] : nullptr;
+  if (!text) d.text = nullptr;
+  d.host_rows = text ? s->d_hrows_mapped[b] : nullptr;
+  d.host_rows_cap = text ? s->cap_hrows[b] : 0;
   d.keep_rows = s->outputs & gvh::surface::OUT_ROWS;
   SF_CUDA(gvh::surface::launch_device_rows(d, st));
   return GVH_OK;
@@ -616,16 +616,44 @@ int gvh_surface_find_end(gvh_surface *s, long long *n_elements) {
     s->p_errors = s->h_rowtot[1];
     const int b = s->rbuf;
     const bool text = (s->outputs & gvh::surface::OUT_TEXT) && s->p_nrows > 0;
-    const bool text_fits = text && s->h_rowtot[3];
-    if (text && ncubes > 0)
-      s->text_per_cube = std::max(s->text_per_cube, (double)s->h_rowtot[2] / (double)ncubes);
-    // assembled (text) or formatted (rows the device left to the host) on the pool's workers
-    // while the caller goes on (the next step, the next slab's device work); anything that
-    // reads the rows or text waits for it
+    const long long bytes = s->h_rowtot[2], nhost = s->h_rowtot[3];
+    // the device's text, unless its host rows overflowed (then every row came as values)
+    const bool device_text = text && nhost <= s->cap_hrows[b];
+    gvh::surface::DeviceText dt;
+    int rc;
+    if (device_text) {
+      // the copy engine brings the text while the caller goes on; it is queued on the rows'
+      // stream before the next slab's kernels, which reuse the device buffer
+      if ((rc = grow_pinned(&s->h_text[b], &s->cap_text[b], std::max(1ll, bytes)))) return rc;
+      if (bytes) {
+        gvh::surface::DeviceRows d;
+        gvh::surface::device_rows_carve(d, s->rowdev, s->rowdev_cap);
+        SF_CUDA(cudaMemcpyAsync(s->h_text[b], d.text, (size_t)bytes, cudaMemcpyDeviceToHost, s->rows_stream));
+      }
+      SF_CUDA(cudaEventRecord(s->text_copied[b], s->rows_stream));
+      gvh::surface::HostRow *hr = s->h_hrows[b];
+      std::sort(hr, hr + nhost, [](const gvh::surface::HostRow &x, const gvh::surface::HostRow &y) {
+        return x.row < y.row;
+      });
+      dt.text = s->h_text[b];
+      dt.bytes = bytes;
+      dt.host_rows = hr;
+      dt.n_host = nhost;
+      cudaEvent_t ev = s->text_copied[b];
+      const int dev = s->device;
+      dt.ready = [ev, dev] {
+        cudaSetDevice(dev);
+        cudaEventSynchronize(ev);
+      };
+    }
+    // assembled (the device's text) or formatted (rows) on the pool's workers while the
+    // caller goes on (the next step, the next slab's device work); anything that reads the
+    // rows or text waits for it
     gvh::surface::format_rows(s->h_rows[b], s->p_nrows, *s->pool, s->outputs, s->last, true,
-                              text_fits ? s->h_text[b] : nullptr, text_fits ? s->h_toff[b] : nullptr);
-    s->p_text_bytes = text_fits ? s->h_rowtot[2] : 0;
-    s->p_rows_sent = text_fits && !(s->outputs & gvh::surface::OUT_ROWS) ? s->h_rowtot[4] : s->p_nrows;
+                              device_text ? &dt : nullptr);
+    s->p_text_bytes = device_text ? bytes : 0;
+    s->p_host_rows = device_text ? nhost : 0;
+    s->p_all_rows = !device_text || (s->outputs & gvh::surface::OUT_ROWS);
     s->formatting = s->p_nrows > 0;
     s->last.errors = s->p_errors;
   } else {
@@ -641,8 +669,10 @@ int gvh_surface_find_end(gvh_surface *s, long long *n_elements) {
   in.elements_last = s->last.elements;
   in.elements_total += s->last.elements;
   in.errors_total += s->last.errors;
-  in.bytes_to_host_total += s->device_rows ? (double)s->p_text_bytes + (s->p_text_bytes ? 8.0 * (s->p_nrows + 1) : 0) +
-                                                 (double)s->p_rows_sent * gvh::surface::kRowColumns * 8 + 32
+  in.bytes_to_host_total += s->device_rows ? (double)s->p_text_bytes +
+                                                 (double)s->p_host_rows * sizeof(gvh::surface::HostRow) +
+                                                 (s->p_all_rows ? (double)s->p_nrows * gvh::surface::kRowColumns * 8 : 0.0) +
+                                                 32
                                            : (double)ncubes * 4 + (double)npoints * (4 + 2 * kVars * 8) + 8;
   in.device_seconds_total += std::chrono::duration<double>(t1 - s->p_t0).count();
   in.host_seconds_total += std::chrono::duration<double>(t2 - t1).count();

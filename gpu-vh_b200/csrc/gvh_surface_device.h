@@ -21,36 +21,36 @@ struct DeviceRows {
   const int *point_cell;    // lattice cell of each point
   const double *point_vals; // per point: kRowVars values at the lower level, then the upper
   int *c2p;                 // lattice cell -> point (scratch, nx ny nz ints)
-  double *slot_rows;        // scratch: iso::kMaxElements rows per hypercube
-  int *slot_n, *offsets;    // scratch: rows per hypercube, and their exclusive offsets
-  long long *totals;        // scratch: [0] rows, [1] hypercubes where cornelius stopped, [2] text
-                            // bytes, [3] 1 when the text fits text_cap, [4] rows without text
-  double *rows;             // out (mapped pinned host memory): the slab's rows, in order, room
-                            // for the slots' worth. With text, only the rows the host formats
-                            // itself are written, unless keep_rows
-  long long *host_totals;   // out (mapped pinned host memory): totals, written last
-  // The rows' text as the reference's ofstream writes it (printf's %g), made with the fast
-  // path of gvh_format.hpp. A row with a number the fast path leaves to the exact one gets
-  // no text (length 0), and its values go to rows for the host to format. text == nullptr:
-  // no text, every row to rows.
-  char *text_slots;         // scratch: kTextSlot bytes per row slot
-  int *row_len;             // scratch: text bytes per row, -1 for a row the host formats
-  long long *text_off;      // scratch: exclusive offsets of the rows' text, rows + 1 entries
-  char *text;               // out (mapped): the rows' text, concatenated
-  long long text_cap;       // bytes text can hold; when the text is longer, every row goes to
-                            // rows and no text is written (totals[3] = 0)
-  long long *host_text_off; // out (mapped): text_off
-  bool keep_rows;           // every row to rows, text or not
+  // scratch, per slot (hypercube c, element i: slot c kMaxElements + i; the rows are the
+  // filled slots in slot order)
+  double *slot_rows;        // kRowColumns values per slot
+  int *slot_n, *offsets;    // rows per hypercube (+1 entry), and their exclusive offsets
+  long long *slot_len;      // text bytes per slot (+1 entry; 0 for an empty slot or a host row)
+  long long *text_off;      // their exclusive offsets
+  unsigned char *slot_host; // 1 for a host row
+  char *text_slots;         // kTextSlot bytes per slot
+  void *scan_temp;          // the scans' work space
+  size_t scan_temp_bytes;
+  long long *totals;        // [0] rows, [1] hypercubes where cornelius stopped, [2] text bytes,
+                            // [3] host rows
+  // out
+  long long *host_totals;   // mapped pinned host memory: totals, written last
+  char *text;               // device: the slab's text (rows in order, host rows left out), or
+                            // nullptr for no text
+  HostRow *host_rows;       // mapped: the host rows, in no particular order
+  long long host_rows_cap;
+  double *rows;             // mapped: every row, in order (slot_rows' worth of room), when
+                            // keep_rows, when there is no text, or when the host rows
+                            // overflow host_rows_cap
+  bool keep_rows;
 };
 
-// Bytes of device scratch per hypercube (the slots, their counts and offsets, the text
-// slots, lengths and offsets); the host's mapped row buffer needs the slot rows' worth.
-size_t device_rows_slot_bytes(long long ncubes);
-
-// Carves the scratch for cap hypercubes out of one allocation of device_rows_slot_bytes(cap)
-// + 1024 bytes at base (256-byte aligned) into d's scratch pointers.
+// Bytes of device scratch for cap hypercubes (slots, their text, scan space; 256-byte
+// aligned pieces), and the carving of one such allocation into d's scratch pointers.
+size_t device_rows_scratch_bytes(long long cap);
 void device_rows_carve(DeviceRows &d, char *base, long long cap);
 
+// The rows (and text) of d's slab, queued on st. d.totals must be the carve's.
 cudaError_t launch_device_rows(const DeviceRows &d, cudaStream_t st);
 
 }  // namespace surface

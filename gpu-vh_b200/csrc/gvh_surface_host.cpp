@@ -151,8 +151,8 @@ void Pool::run(int n, const std::function<void(int)> &f) {
   job_ = nullptr;
 }
 
-void format_rows(const double *rows, long long n, Pool &pool, int outputs, Result &out, bool async, const char *text,
-                 const long long *text_off) {
+void format_rows(const double *rows, long long n, Pool &pool, int outputs, Result &out, bool async,
+                 const DeviceText *dt) {
   out.elements = n;
   out.errors = 0;
   out.joined_valid = false;
@@ -160,34 +160,43 @@ void format_rows(const double *rows, long long n, Pool &pool, int outputs, Resul
     out.parts.clear();
     return;
   }
-  const int nparts = (int)std::max<long long>(1, std::min<long long>(4ll * pool.size(), n / 256));
+  const bool text = outputs & OUT_TEXT, device_text = text && dt;
+  const long long work = device_text ? (dt->bytes + dt->n_host * 240) / 65536 : n / 256;
+  const int nparts = (int)std::max<long long>(1, std::min<long long>(4ll * pool.size(), work));
   out.parts.resize(nparts);
   Result *res = &out;
-  auto job = [rows, n, nparts, outputs, res, text, text_off](int i) {
-    Result &out = *res;
-    const long long r0 = n * i / nparts, r1 = n * (i + 1) / nparts;
-    Part &part = out.parts[i];
+  DeviceText d = device_text ? *dt : DeviceText{};
+  auto job = [rows, n, nparts, outputs, res, text, device_text, d](int i) {
+    Part &part = res->parts[i];
     part.rows.clear();
     part.text.clear();
+    const long long r0 = n * i / nparts, r1 = n * (i + 1) / nparts;
     part.elements = r1 - r0;
     part.errors = 0;
     if (outputs & OUT_ROWS) part.rows.assign(rows + r0 * kColumns, rows + r1 * kColumns);
-    if (!(outputs & OUT_TEXT)) return;
-    if (!text) {
+    if (!text) return;
+    if (!device_text) {
       part.text.reserve((size_t)(r1 - r0) * 240);
       for (long long r = r0; r < r1; ++r) append_row_text(part.text, rows + r * kColumns);
       return;
     }
-    // the device's text, in runs of rows it formatted; a row of no text is formatted here
-    part.text.reserve((size_t)(text_off[r1] - text_off[r0]) + 64);
-    long long r = r0;
-    while (r < r1) {
-      long long e = r;
-      while (e < r1 && text_off[e + 1] > text_off[e]) ++e;
-      if (e > r) part.text.append(text + text_off[r], (size_t)(text_off[e] - text_off[r]));
-      if (e < r1) append_row_text(part.text, rows + e * kColumns);
-      r = e + 1;
+    // bytes [lo, hi) of the device's text, with the host rows that go before byte lo .. hi - 1
+    // (and, in the last part, those at the end)
+    if (d.ready) d.ready();
+    const long long lo = d.bytes * i / nparts, hi = d.bytes * (i + 1) / nparts;
+    const HostRow *hb = d.host_rows, *he = d.host_rows + d.n_host;
+    auto first_at = [](const HostRow *b, const HostRow *e, long long off) {
+      return std::lower_bound(b, e, off, [](const HostRow &h, long long o) { return h.text_off < o; });
+    };
+    const HostRow *h0 = first_at(hb, he, lo), *h1 = i + 1 == nparts ? he : first_at(hb, he, hi);
+    part.text.reserve((size_t)(hi - lo) + (size_t)(h1 - h0) * 240);
+    long long pos = lo;
+    for (const HostRow *h = h0; h < h1; ++h) {
+      part.text.append(d.text + pos, (size_t)(h->text_off - pos));
+      append_row_text(part.text, h->v);
+      pos = h->text_off;
     }
+    part.text.append(d.text + pos, (size_t)(hi - pos));
   };
   if (async) pool.start(nparts, job);
   else pool.run(nparts, job);

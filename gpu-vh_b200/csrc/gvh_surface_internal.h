@@ -8,6 +8,8 @@
 #include <thread>
 #include <vector>
 
+#include "gvh_surface_rows.hpp"
+
 namespace gvh {
 namespace surface {
 
@@ -88,14 +90,23 @@ class Pool {
   bool stop_ = false;
 };
 
+// The device's text of a slab (gvh_surface_rows.cu): its rows' text in order with the host
+// rows left out, and the host rows, sorted by row.
+struct DeviceText {
+  const char *text = nullptr;
+  long long bytes = 0;
+  const HostRow *host_rows = nullptr;
+  long long n_host = 0;
+  std::function<void()> ready;  // each job calls it before reading text (the copy's wait)
+};
+
 // Formats rows the device produced (n rows of kColumns) into out's parts on the pool, in
-// order; keeps the rows too when outputs has OUT_ROWS. With text (the device's text of the
-// rows, row r at text_off[r] .. text_off[r + 1]) the parts take their text from it, and only
-// rows of no text (text_off[r + 1] == text_off[r]) are formatted from rows. With async the
-// work is started on the pool's workers and format_rows returns at once: pool.wait() before
-// reading out or reusing rows or text.
+// order; keeps the rows too when outputs has OUT_ROWS. With dt the text is the device's, with
+// the host rows formatted here and spliced in. With async the work is started on the pool's
+// workers and format_rows returns at once: pool.wait() before reading out or reusing rows or
+// the device text.
 void format_rows(const double *rows, long long n, Pool &pool, int outputs, Result &out, bool async = false,
-                 const char *text = nullptr, const long long *text_off = nullptr);
+                 const DeviceText *dt = nullptr);
 
 // Runs the surface finder on every crossed hypercube of the slab on the pool, in order.
 // outputs: OUT_ROWS and/or OUT_TEXT. cell_to_point is scratch of at least nx*ny*nz entries

@@ -1,14 +1,20 @@
-// gvh_surface_rows.cu -- the surface.dat rows of a slab's crossed hypercubes on the device.
+// gvh_surface_rows.cu -- the surface.dat rows of a slab's crossed hypercubes on the device,
+// and their text.
 //
 // One thread per crossed hypercube runs the code of gvh_surface_rows.hpp (cornelius, the
 // reference's interpolation to the element's centroid, the row) -- the code the host pool
-// runs -- and writes its rows to a fixed slot; a scan over the per-cube counts and a
-// compaction then give the rows in the reference's order (hypercubes in loop order, a
-// cube's elements in cornelius' order), written straight into mapped pinned host memory, so
-// nothing waits between the kernels and the copy. This file is compiled without FMA contraction
-// (-fmad=false, like the host side's -ffp-contract=off), so device and host rows agree to
-// the last bit; the host then only formats them (gvh_surface.cu).
+// runs -- and writes its rows to fixed slots (kMaxElements per hypercube); the rows are the
+// filled slots in slot order, which is the reference's order (hypercubes in loop order, a
+// cube's elements in cornelius' order). One thread per slot then writes the row's text with
+// the fast path of %g (gvh_format.hpp); a scan over the slots' text lengths places each row's
+// text in the slab's text, compacted in device memory for one copy to the host by the copy
+// engine. Rows with a number the fast path leaves to the exact one go to the host as values
+// (HostRow), which formats them and splices them in. This file is compiled without FMA
+// contraction (-fmad=false, like the host side's -ffp-contract=off), so device and host rows
+// agree to the last bit.
 #include <cuda_runtime.h>
+
+#include <cub/device/device_scan.cuh>
 
 #include "gvh_format.hpp"
 #include "gvh_surface_device.h"
@@ -47,145 +53,113 @@ __global__ void __launch_bounds__(kRowThreads) cube_rows_kernel(RowGeometry g, l
   }
 }
 
-// Exclusive offsets of slot_n (one block); totals[0] = the number of rows.
-__global__ void rows_scan_kernel(long long n, const int *__restrict__ slot_n, int *__restrict__ offsets,
-                                 long long *__restrict__ totals) {
-  __shared__ long long part[1024];
-  const long long per = (n + blockDim.x - 1) / blockDim.x;
-  const long long lo = min(n, (long long)threadIdx.x * per), hi = min(n, lo + per);
-  long long sum = 0;
-  for (long long i = lo; i < hi; ++i) sum += slot_n[i];
-  part[threadIdx.x] = sum;
-  __syncthreads();
-  for (int off = 1; off < (int)blockDim.x; off <<= 1) {
-    const long long v = threadIdx.x >= (unsigned)off ? part[threadIdx.x - off] : 0;
-    __syncthreads();
-    part[threadIdx.x] += v;
-    __syncthreads();
-  }
-  long long run = part[threadIdx.x] - sum;
-  for (long long i = lo; i < hi; ++i) {
-    offsets[i] = (int)run;
-    run += slot_n[i];
-  }
-  if (threadIdx.x == blockDim.x - 1) totals[0] = part[threadIdx.x];
-}
-
-// The text of slot (c, i) (hypercube c, its i-th element), row offsets[c] + i: the fast path
-// of %g for each number, a space between them, a newline after the last; -1 as the length
-// when the fast path leaves a number to the exact one.
-__global__ void rows_text_kernel(long long ncubes, const double *__restrict__ slot_rows,
-                                 const int *__restrict__ slot_n, const int *__restrict__ offsets,
-                                 char *__restrict__ text_slots, int *__restrict__ row_len) {
+// The text of slot t (hypercube t / kSlotRows, its element t % kSlotRows): the fast path of
+// %g for each number, a space between them, a newline after the last. An empty slot, or a
+// row with a number the fast path leaves to the exact one (a host row), gets length 0.
+// Thread n_slots writes the scan's closing 0.
+__global__ void slot_text_kernel(long long n_slots, const double *__restrict__ slot_rows,
+                                 const int *__restrict__ slot_n, char *__restrict__ text_slots,
+                                 long long *__restrict__ slot_len, unsigned char *__restrict__ slot_host) {
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const long long c = t / kSlotRows;
-  if (c >= ncubes) return;
-  const int i = (int)(t - c * kSlotRows);
-  if (i >= slot_n[c]) return;
-  const long long r = (long long)offsets[c] + i;
+  if (t > n_slots) return;
+  slot_len[t] = 0;
+  if (t == n_slots) return;
+  slot_host[t] = 0;
+  if ((int)(t % kSlotRows) >= slot_n[t / kSlotRows]) return;
   const double *row = slot_rows + t * kRowColumns;
-  char *out = text_slots + r * kTextSlot;
+  char *out = text_slots + t * kTextSlot;
   char *p = out;
   for (int k = 0; k < kRowColumns; ++k) {
     char *q = fmt::g6_fast(p, row[k]);
     if (!q) {
-      row_len[r] = -1;
+      slot_host[t] = 1;
       return;
     }
     p = q;
     *p++ = k + 1 < kRowColumns ? ' ' : '\n';
   }
-  row_len[r] = (int)(p - out);
+  slot_len[t] = p - out;
 }
 
-// Exclusive offsets of the rows' text (one block; a row of length -1 counts 0), into
-// text_off and the host's copy; totals[2] = the text's bytes, totals[3] = whether they fit,
-// totals[4] = the rows the host formats.
-__global__ void text_scan_kernel(const int *__restrict__ row_len, long long text_cap,
-                                 long long *__restrict__ totals, long long *__restrict__ text_off,
-                                 long long *__restrict__ host_text_off) {
-  __shared__ long long part[1024];
-  const long long n = totals[0];
-  const long long per = (n + blockDim.x - 1) / blockDim.x;
-  const long long lo = min(n, (long long)threadIdx.x * per), hi = min(n, lo + per);
-  long long sum = 0;
-  unsigned long long host_rows = 0;
-  for (long long i = lo; i < hi; ++i) {
-    sum += max(row_len[i], 0);
-    host_rows += row_len[i] < 0;
-  }
-  if (host_rows) atomicAdd(reinterpret_cast<unsigned long long *>(totals + 4), host_rows);
-  part[threadIdx.x] = sum;
-  __syncthreads();
-  for (int off = 1; off < (int)blockDim.x; off <<= 1) {
-    const long long v = threadIdx.x >= (unsigned)off ? part[threadIdx.x - off] : 0;
-    __syncthreads();
-    part[threadIdx.x] += v;
-    __syncthreads();
-  }
-  long long run = part[threadIdx.x] - sum;
-  for (long long i = lo; i < hi; ++i) {
-    text_off[i] = run;
-    host_text_off[i] = run;
-    run += max(row_len[i], 0);
-  }
-  if (threadIdx.x == blockDim.x - 1) {
-    const long long bytes = part[threadIdx.x];
-    text_off[n] = bytes;
-    host_text_off[n] = bytes;
-    totals[2] = bytes;
-    totals[3] = bytes <= text_cap ? 1 : 0;
-  }
-}
-
-// One thread per value of a slot (hypercube c, row i, column k): consecutive threads write
-// consecutive values of a row, so each row crosses the host link as one contiguous write.
-// With row_len (text made) a row is written only when the host formats it, the text did not
-// fit, or copy_all.
-__global__ void rows_compact_kernel(long long ncubes, const double *__restrict__ slot_rows,
-                                    const int *__restrict__ slot_n, const int *__restrict__ offsets,
-                                    const int *__restrict__ row_len, const long long *__restrict__ totals,
-                                    bool copy_all, double *__restrict__ rows) {
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const long long per_cube = (long long)kSlotRows * kRowColumns;
-  const long long c = t / per_cube;
-  if (c >= ncubes) return;
-  const int v = (int)(t - c * per_cube);
-  if (v >= slot_n[c] * kRowColumns) return;
-  const long long at = (long long)offsets[c] * kRowColumns + v;
-  if (row_len && !copy_all && totals[3] && row_len[at / kRowColumns] >= 0) return;
-  rows[at] = slot_rows[c * per_cube + v];
-}
-
-// One warp per row (grid-stride): the row's text to its place in the concatenated text, in
-// mapped host memory, 32 consecutive bytes per warp store.
-__global__ void text_compact_kernel(const long long *__restrict__ totals, const int *__restrict__ row_len,
-                                    const long long *__restrict__ text_off, const char *__restrict__ text_slots,
-                                    char *__restrict__ text) {
-  if (!totals[3]) return;
-  const long long n = totals[0];
+// One warp per hypercube (grid-stride): each of its rows' text to its place in the slab's
+// text (32 consecutive bytes per warp store), a host row's values and places to host_rows.
+__global__ void text_compact_kernel(long long ncubes, const int *__restrict__ slot_n,
+                                    const int *__restrict__ offsets, const double *__restrict__ slot_rows,
+                                    const long long *__restrict__ slot_len, const long long *__restrict__ text_off,
+                                    const unsigned char *__restrict__ slot_host, const char *__restrict__ text_slots,
+                                    char *__restrict__ text, HostRow *__restrict__ host_rows, long long host_rows_cap,
+                                    long long *__restrict__ totals) {
   const int lane = threadIdx.x & 31;
   const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
-  for (long long r = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; r < n; r += warps) {
-    const int len = row_len[r];
-    const char *src = text_slots + r * kTextSlot;
-    char *dst = text + text_off[r];
-    for (int b = lane; b < len; b += 32) dst[b] = src[b];
+  for (long long c = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; c < ncubes; c += warps) {
+    const int n = slot_n[c];
+    for (int i = 0; i < n; ++i) {
+      const long long s = c * kSlotRows + i;
+      if (slot_host[s]) {
+        long long j = 0;
+        if (lane == 0) j = (long long)atomicAdd(reinterpret_cast<unsigned long long *>(totals + 3), 1ull);
+        j = __shfl_sync(0xffffffffu, j, 0);
+        if (j < host_rows_cap) {
+          HostRow &h = host_rows[j];
+          if (lane < kRowColumns) h.v[lane] = slot_rows[s * kRowColumns + lane];
+          if (lane == kRowColumns) h.text_off = text_off[s];
+          if (lane == kRowColumns + 1) h.row = (long long)offsets[c] + i;
+        }
+      } else {
+        const int len = (int)slot_len[s];
+        const char *src = text_slots + s * kTextSlot;
+        char *dst = text + text_off[s];
+        for (int b = lane; b < len; b += 32) dst[b] = src[b];
+      }
+    }
   }
 }
 
-__global__ void host_totals_kernel(const long long *__restrict__ totals, long long *__restrict__ host_totals) {
-  for (int i = 0; i < 5; ++i) host_totals[i] = totals[i];
+// Every row in order to rows (grid-stride over the slots' values, one thread per value, so
+// that a row crosses the host link as one contiguous write) when all rows are wanted: always
+// (copy_all), or when the host rows overflowed their buffer.
+__global__ void rows_compact_kernel(long long ncubes, const double *__restrict__ slot_rows,
+                                    const int *__restrict__ slot_n, const int *__restrict__ offsets,
+                                    const long long *__restrict__ totals, bool copy_all, long long host_rows_cap,
+                                    double *__restrict__ rows) {
+  if (!copy_all && totals[3] <= host_rows_cap) return;
+  const long long per_cube = (long long)kSlotRows * kRowColumns;
+  const long long values = ncubes * per_cube;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < values; t += stride) {
+    const long long c = t / per_cube;
+    const int v = (int)(t - c * per_cube);
+    if (v < slot_n[c] * kRowColumns) rows[(long long)offsets[c] * kRowColumns + v] = slot_rows[t];
+  }
+}
+
+// totals[0] (rows) and [2] (text bytes) from the scans' closing entries, then all of them to
+// the host.
+__global__ void totals_kernel(long long ncubes, const int *__restrict__ offsets, long long n_slots,
+                              const long long *__restrict__ text_off, bool text, long long *__restrict__ totals,
+                              long long *__restrict__ host_totals) {
+  totals[0] = offsets[ncubes];
+  totals[2] = text ? text_off[n_slots] : 0;
+  for (int i = 0; i < 4; ++i) host_totals[i] = totals[i];
 }
 
 size_t align256(size_t b) { return (b + 255) / 256 * 256; }
 
+size_t scan_temp_bytes(long long cap) {
+  size_t a = 0, b = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, a, (const int *)nullptr, (int *)nullptr, (int)(cap + 1));
+  cub::DeviceScan::ExclusiveSum(nullptr, b, (const long long *)nullptr, (long long *)nullptr,
+                                (int)(cap * kSlotRows + 1));
+  return align256(a > b ? a : b);
+}
+
 }  // namespace
 
-size_t device_rows_slot_bytes(long long ncubes) {
-  const size_t slots = (size_t)ncubes * kSlotRows;
-  return align256(slots * kRowColumns * sizeof(double)) + 2 * align256((size_t)ncubes * sizeof(int)) +
-         align256(slots * sizeof(int)) + align256((slots + 1) * sizeof(long long)) + align256(slots * kTextSlot);
+size_t device_rows_scratch_bytes(long long cap) {
+  const size_t slots = (size_t)cap * kSlotRows;
+  return 1024 + align256(slots * kRowColumns * sizeof(double)) + 2 * align256((size_t)(cap + 1) * sizeof(int)) +
+         2 * align256((slots + 1) * sizeof(long long)) + align256(slots) + 2 * align256(slots * kTextSlot) +
+         scan_temp_bytes(cap);
 }
 
 void device_rows_carve(DeviceRows &d, char *base, long long cap) {
@@ -193,33 +167,44 @@ void device_rows_carve(DeviceRows &d, char *base, long long cap) {
   char *p = base;
   d.totals = reinterpret_cast<long long *>(p); p += 1024;
   d.slot_rows = reinterpret_cast<double *>(p); p += align256(slots * kRowColumns * sizeof(double));
-  d.slot_n = reinterpret_cast<int *>(p); p += align256((size_t)cap * sizeof(int));
-  d.offsets = reinterpret_cast<int *>(p); p += align256((size_t)cap * sizeof(int));
-  d.row_len = reinterpret_cast<int *>(p); p += align256(slots * sizeof(int));
+  d.slot_n = reinterpret_cast<int *>(p); p += align256((size_t)(cap + 1) * sizeof(int));
+  d.offsets = reinterpret_cast<int *>(p); p += align256((size_t)(cap + 1) * sizeof(int));
+  d.slot_len = reinterpret_cast<long long *>(p); p += align256((slots + 1) * sizeof(long long));
   d.text_off = reinterpret_cast<long long *>(p); p += align256((slots + 1) * sizeof(long long));
-  d.text_slots = p;
+  d.slot_host = reinterpret_cast<unsigned char *>(p); p += align256(slots);
+  d.text_slots = p; p += align256(slots * kTextSlot);
+  d.text = p; p += align256(slots * kTextSlot);
+  d.scan_temp = p;
+  d.scan_temp_bytes = scan_temp_bytes(cap);
 }
 
 cudaError_t launch_device_rows(const DeviceRows &d, cudaStream_t st) {
   if (d.ncubes <= 0) return cudaSuccess;  // the caller sets the totals to zero
-  cudaError_t e = cudaMemsetAsync(d.totals, 0, 5 * sizeof(long long), st);
+  cudaError_t e = cudaMemsetAsync(d.totals, 0, 4 * sizeof(long long), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d.slot_n + d.ncubes, 0, sizeof(int), st);  // the scan's closing 0
   if (e != cudaSuccess) return e;
   point_index_kernel<<<(unsigned)((d.npoints + 255) / 256), 256, 0, st>>>(d.npoints, d.point_cell, d.c2p);
   const unsigned blocks = (unsigned)((d.ncubes + kRowThreads - 1) / kRowThreads);
   cube_rows_kernel<<<blocks, kRowThreads, 0, st>>>(d.g, d.ncubes, d.cube_key, d.c2p, d.point_vals, d.slot_rows,
                                                    d.slot_n, reinterpret_cast<unsigned long long *>(d.totals + 1));
-  rows_scan_kernel<<<1, 1024, 0, st>>>(d.ncubes, d.slot_n, d.offsets, d.totals);
-  const long long slots = d.ncubes * (long long)kSlotRows;
-  if (d.text) {
-    rows_text_kernel<<<(unsigned)((slots + 255) / 256), 256, 0, st>>>(d.ncubes, d.slot_rows, d.slot_n, d.offsets,
-                                                                     d.text_slots, d.row_len);
-    text_scan_kernel<<<1, 1024, 0, st>>>(d.row_len, d.text_cap, d.totals, d.text_off, d.host_text_off);
+  size_t temp = d.scan_temp_bytes;
+  if ((e = cub::DeviceScan::ExclusiveSum(d.scan_temp, temp, d.slot_n, d.offsets, (int)(d.ncubes + 1), st)))
+    return e;
+  const long long n_slots = d.ncubes * kSlotRows;
+  const bool text = d.text != nullptr;
+  if (text) {
+    slot_text_kernel<<<(unsigned)((n_slots + 256) / 256), 256, 0, st>>>(n_slots, d.slot_rows, d.slot_n,
+                                                                       d.text_slots, d.slot_len, d.slot_host);
+    temp = d.scan_temp_bytes;
+    if ((e = cub::DeviceScan::ExclusiveSum(d.scan_temp, temp, d.slot_len, d.text_off, (int)(n_slots + 1), st)))
+      return e;
+    text_compact_kernel<<<148 * 8, 256, 0, st>>>(d.ncubes, d.slot_n, d.offsets, d.slot_rows, d.slot_len, d.text_off,
+                                                 d.slot_host, d.text_slots, d.text, d.host_rows, d.host_rows_cap,
+                                                 d.totals);
   }
-  const long long values = slots * kRowColumns;
-  rows_compact_kernel<<<(unsigned)((values + 255) / 256), 256, 0, st>>>(
-      d.ncubes, d.slot_rows, d.slot_n, d.offsets, d.text ? d.row_len : nullptr, d.totals, d.keep_rows, d.rows);
-  if (d.text) text_compact_kernel<<<148 * 8, 256, 0, st>>>(d.totals, d.row_len, d.text_off, d.text_slots, d.text);
-  host_totals_kernel<<<1, 1, 0, st>>>(d.totals, d.host_totals);
+  rows_compact_kernel<<<148 * 8, 256, 0, st>>>(d.ncubes, d.slot_rows, d.slot_n, d.offsets, d.totals,
+                                               d.keep_rows || !text, d.host_rows_cap, d.rows);
+  totals_kernel<<<1, 1, 0, st>>>(d.ncubes, d.offsets, n_slots, d.text_off, text, d.totals, d.host_totals);
   return cudaGetLastError();
 }
 

@@ -17,6 +17,15 @@ constexpr int kRowVars = 10;     // u^x u^y u^eta e pi^xx pi^xy pi^x eta pi^yy p
 constexpr int kRowColumns = 20;  // one surface.dat row (HydroPlugin.cpp:315-372)
 constexpr int kEosConformal = 1; // GVH_EOS_CONFORMAL
 
+// A row whose text the host makes (a number the device's fast %g leaves to the exact path):
+// its values, its row index and where its text goes in the slab's text (before byte
+// text_off of the device's text).
+struct HostRow {
+  long long text_off;
+  long long row;
+  double v[kRowColumns];
+};
+
 // What a row needs to know about the slab.
 struct RowGeometry {
   int dim;                // 4 (3+1D) or 3 (2+1D)

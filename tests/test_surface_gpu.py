@@ -111,17 +111,23 @@ def test_device_rows_equal_host_rows(case):
     S.set_device_rows(False)
 
 
-def test_device_text_splices_host_formatted_rows():
+@pytest.mark.parametrize("tiny_part", ["half", "all"])
+def test_device_text_splices_host_formatted_rows(tiny_part):
     """A row with a number the device's fast %g leaves to the exact path (here bulk pressures
-    of order 1e-28, outside its exponent range) is formatted on the host and spliced into the
-    device's text in order: text-only, rows + text and the host pool's text agree. The time
-    levels are set, not stepped (a step would relax the bulk pressure): the energy density
-    falls by a fifth from level to level, so the surface is a shell crossing both halves."""
-    lat = CASES["qcd_bulk_3d"]
+    of order 1e-28, outside its exponent range) is sent as values, formatted on the host and
+    spliced into the device's text in order; with more such rows than their buffer holds
+    ("all": every row of a slab of ~3.8 k crossed hypercubes) every row is sent and formatted
+    on the host. Text-only, rows + text and the host pool's text agree. The time levels are
+    set, not stepped (a step would relax the bulk pressure): the energy density falls by a
+    fifth from level to level, so the surface is a shell crossing both halves."""
+    lat = dict(CASES["qcd_bulk_3d"], nx=40, ny=40, nz=16)
     G = gvh.Lattice(**lat)
-    prim = rich_state(G, seed=4, e0=25.0, emin=0.3, spacing=0.6)
+    prim = rich_state(G, seed=4, e0=25.0, emin=0.3, spacing=0.3)
     Pi = prim["Pi"].reshape(G.ncz, G.ncy, G.ncx).copy()
-    Pi[:, :, : G.ncx // 2] *= 1e-27
+    if tiny_part == "half":
+        Pi[:, :, : G.ncx // 2] *= 1e-27
+    else:
+        Pi *= 1e-27
     prim["Pi"] = Pi.reshape(-1)
     efo = gvh.energy_density_of_temperature(0.150)
     D, H, T = (gvh.Surface(G, efo, threads=3) for _ in range(3))
@@ -131,19 +137,24 @@ def test_device_text_splices_host_formatted_rows():
     for S in (D, H, T):
         S.set_lower()
     tiny = plain = 0
-    for n in range(1, 4):
+    for n in range(1, 3):
         G.set_primitive(dict(prim, e=prim["e"] * 0.8 ** n))
         label, scale, _ = gvh.slab_labels(n - 1, 0.5, lat["dt"])
         assert D.find(label, scale) == H.find(label, scale) == T.find(label, scale)
         text = H.text()
         assert D.text() == text and T.text() == text, n
+        rd, rh = D.rows(), H.rows()
+        assert np.array_equal(rd.view(np.uint64), rh.view(np.uint64)), n
         for line in text.splitlines():
             ex = line.split()[-1].partition("e-")[2]
             if ex and int(ex) > 17:
                 tiny += 1
             else:
                 plain += 1
-    assert tiny > 0 and plain > 0, (tiny, plain)
+    if tiny_part == "half":
+        assert tiny > 1000 and plain > 1000, (tiny, plain)
+    else:
+        assert tiny > 5000 and plain == 0, (tiny, plain)
 
 
 def test_device_marking_counts():
