@@ -66,6 +66,9 @@ def parse():
     ap.add_argument("--serving-rate", type=float, default=4.0)
     ap.add_argument("--batch64-seconds", type=float, default=120.0,
                     help="time limit of the 64-event batched run (0 skips it)")
+    ap.add_argument("--surface-slabs", type=int, default=0,
+                    help="only the freeze-out surface of N slabs of the 131x131x61 event after "
+                         "300 steps (text only, as the run loop keeps it); for profiling its kernels")
     return ap.parse_args()
 
 
@@ -724,10 +727,47 @@ def run_ours(args):
     return 0
 
 
+def surface_slabs(n_slabs, warm_steps=300):
+    """The surface of n_slabs consecutive slabs of the benchmark event, taken after
+    warm_steps steps (where the surface is about 47 k crossed hypercubes a slab): step, then
+    find the slab, as the run loop does; one JSON line with the slabs' wall time."""
+    import gvh
+
+    w, prim, _ = make_event(workloads.CONFIG2, 0)
+    L = gvh.Lattice(device=0, precision="fp64", tau0=w.tau0, T_fo_GeV=w.T_fo_GeV, **w.lattice_kwargs())
+    L.set_primitive(prim)
+    t = w.tau0
+    for _ in range(warm_steps):
+        L.step(t, w.dtau)
+        t += w.dtau
+    S = gvh.Surface(L, gvh.energy_density_of_temperature(w.T_fo_GeV))
+    S.set_outputs(rows=False, text=True)
+    S.set_lower()
+    L.synchronize()
+    t0 = time.perf_counter()
+    elements = 0
+    for k in range(n_slabs):
+        L.step(t, w.dtau)
+        t += w.dtau
+        label, scale, _ = gvh.slab_labels(warm_steps + k, w.tau0, w.dtau)
+        elements += S.find(label, scale)
+    S.text()
+    el = time.perf_counter() - t0
+    info = S.info()
+    print(json.dumps({"surface_slabs": n_slabs, "seconds": el, "elements": elements,
+                      "hypercubes_per_slab": info["hypercubes_total"] / max(1, n_slabs),
+                      "bytes_to_host_per_slab": info["bytes_to_host_total"] / max(1, n_slabs)}))
+    S.close()
+    L.close()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.surface_slabs > 0:
+        return surface_slabs(args.surface_slabs)
     return run_ours(args)
 
 

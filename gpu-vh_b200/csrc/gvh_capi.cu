@@ -252,6 +252,7 @@ int gvh_destroy(gvh_handle *h) {
   cudaFree(h->block);
   if (h->staging) cudaFree(h->staging);
   if (h->diag) cudaFree(h->diag);
+  if (h->host_word) cudaFreeHost(h->host_word);
   if (h->async_ready) {
     cudaStreamSynchronize(h->s_h2d);
     cudaStreamSynchronize(h->s_d2h);
@@ -433,9 +434,15 @@ int gvh_max_energy_density(gvh_handle *h, double *out) {
   const unsigned blocks = (unsigned)std::min<long long>(1024, (h->ncells + 255) / 256);
   max_e_kernel<<<blocks, 256, 0, h->stream>>>(h->e, h->ncells, scratch);
   GVH_CUDA(cudaGetLastError());
-  unsigned long long bits = 0;
-  GVH_CUDA(cudaMemcpyAsync(&bits, scratch, sizeof bits, cudaMemcpyDeviceToHost, h->stream));
+  if (!h->host_word) {
+    if (cudaHostAlloc(reinterpret_cast<void **>(&h->host_word), 64, cudaHostAllocMapped) != cudaSuccess)
+      return fail(GVH_ERR_NOMEM, "gvh_max_energy_density: cannot map host memory");
+    GVH_CUDA(cudaHostGetDevicePointer(reinterpret_cast<void **>(&h->host_word_dev), h->host_word, 0));
+  }
+  word_to_host_kernel<<<1, 1, 0, h->stream>>>(scratch, h->host_word_dev);
+  GVH_CUDA(cudaGetLastError());
   GVH_CUDA(cudaStreamSynchronize(h->stream));
+  const unsigned long long bits = *reinterpret_cast<volatile unsigned long long *>(h->host_word);
   memcpy(out, &bits, sizeof *out);
   return GVH_OK;
 }

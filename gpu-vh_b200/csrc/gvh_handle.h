@@ -25,6 +25,10 @@ struct gvh_handle {
   cudaStream_t s_h2d, s_d2h;
   cudaEvent_t ev_in_ready, ev_in_free, ev_out_ready, ev_out_free, ev_fence;
   int async_ready;
+  // mapped pinned word for small results read on the host (allocated on first use): a
+  // kernel writes it, so the read needs no copy that could queue behind another stream's
+  // large copy to the host
+  unsigned long long *host_word, *host_word_dev;
 };
 
 // The current time level's fields in the handle's interior-only layout (cell

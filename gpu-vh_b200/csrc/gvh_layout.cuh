@@ -87,4 +87,7 @@ __global__ void max_e_kernel(const double *e, long long n, unsigned long long *o
   if ((threadIdx.x & 31) == 0) atomicMax(out, b);
 }
 
+// One word to (mapped) host memory.
+__global__ void word_to_host_kernel(const unsigned long long *src, unsigned long long *dst) { *dst = *src; }
+
 }  // namespace

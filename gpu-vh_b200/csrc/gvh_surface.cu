@@ -149,8 +149,11 @@ __global__ void fo_count(Geometry g, int nbc, const unsigned char *__restrict__ 
   if (threadIdx.x == 0) counts[b] = total;
 }
 
-// Exclusive offsets of the two count segments, and the two totals at the end.
-__global__ void fo_scan(int nbc, int nbp, int *__restrict__ counts, int *__restrict__ totals) {
+// Exclusive offsets of the two count segments, and the two totals at the end (also written to
+// mapped host memory: the host reads them without a copy, which could queue behind another
+// stream's large copy to the host).
+__global__ void fo_scan(int nbc, int nbp, int *__restrict__ counts, int *__restrict__ totals,
+                        volatile int *__restrict__ host_totals) {
   __shared__ int part[1024];
   for (int seg = 0; seg < 2; ++seg) {
     int *c = counts + (seg ? nbc : 0);
@@ -173,7 +176,10 @@ __global__ void fo_scan(int nbc, int nbp, int *__restrict__ counts, int *__restr
       c[i] = run;
       run += v;
     }
-    if (threadIdx.x == blockDim.x - 1) totals[seg] = part[threadIdx.x];
+    if (threadIdx.x == blockDim.x - 1) {
+      totals[seg] = part[threadIdx.x];
+      host_totals[seg] = part[threadIdx.x];
+    }
     __syncthreads();
   }
 }
@@ -271,7 +277,7 @@ struct gvh_surface {
   unsigned char *flag, *pflag;
   int *counts, *totals, *cube_key, *point_cell;
   double *point_vals;
-  int *h_totals;     // pinned
+  int *h_totals, *d_totals_mapped;  // mapped pinned: crossed hypercubes, points
   int *h_cube_key, *h_point_cell;
   double *h_point_vals;
   long long cap_cubes, cap_points, cap_vals;
@@ -286,16 +292,16 @@ struct gvh_surface {
   long long rowdev_cap;
   long long *h_rowtot, *d_rowtot_mapped;  // mapped pinned: rows, errors, text bytes, host rows
   // two sets of host buffers, alternating by slab: the host assembles one slab's text on the
-  // pool's workers while the device writes the next slab's into the other. The device's text
-  // comes by copy (pinned); the host rows, and all rows when they are kept (or the host rows
-  // overflow), are written by the device into mapped pinned memory.
-  double *h_rows[2], *d_rows_mapped[2];
+  // pool's workers while the device makes the next slab's. The device's text, and all rows
+  // when they are kept (or the host rows overflow), come by copy into pinned memory; the host
+  // rows are written by the device into mapped pinned memory.
+  double *h_rows[2];
   long long cap_rows[2];
   gvh::surface::HostRow *h_hrows[2], *d_hrows_mapped[2];
   long long cap_hrows[2];
   char *h_text[2];
   long long cap_text[2];
-  cudaEvent_t text_copied[2];
+  cudaEvent_t copied_out[2];  // after a slab's copies of text and rows
   int rbuf;             // buffer of the slab begun last
   bool formatting;      // a slab's rows are being formatted on the pool (format_rows async)
   long long p_nrows, p_errors, p_text_bytes, p_host_rows;
@@ -362,7 +368,8 @@ int gvh_surface_create(gvh_handle *h, double e_freezeout, gvh_surface **out) {
   // the device rows repeat the host's arithmetic exactly for the QCD EoS; the conformal T(e)
   // is a pow, which the device does not evaluate as the host's libm does
   s->device_rows = h->eos == GVH_EOS_QCD;
-  if (cudaHostAlloc(reinterpret_cast<void **>(&s->h_totals), 4 * sizeof(int), cudaHostAllocDefault) != cudaSuccess ||
+  if (cudaHostAlloc(reinterpret_cast<void **>(&s->h_totals), 4 * sizeof(int), cudaHostAllocMapped) != cudaSuccess ||
+      cudaHostGetDevicePointer(reinterpret_cast<void **>(&s->d_totals_mapped), s->h_totals, 0) != cudaSuccess ||
       cudaHostAlloc(reinterpret_cast<void **>(&s->h_rowtot), 8 * sizeof(long long), cudaHostAllocMapped) !=
           cudaSuccess ||
       cudaHostGetDevicePointer(reinterpret_cast<void **>(&s->d_rowtot_mapped), s->h_rowtot, 0) != cudaSuccess) {
@@ -375,8 +382,8 @@ int gvh_surface_create(gvh_handle *h, double e_freezeout, gvh_surface **out) {
   memset(&s->info, 0, sizeof s->info);
   // waited on by blocking, not spinning: the pool's formatting threads need the cores
   if (cudaEventCreateWithFlags(&s->copied, cudaEventDisableTiming | cudaEventBlockingSync) != cudaSuccess ||
-      cudaEventCreateWithFlags(&s->text_copied[0], cudaEventDisableTiming | cudaEventBlockingSync) != cudaSuccess ||
-      cudaEventCreateWithFlags(&s->text_copied[1], cudaEventDisableTiming | cudaEventBlockingSync) != cudaSuccess ||
+      cudaEventCreateWithFlags(&s->copied_out[0], cudaEventDisableTiming | cudaEventBlockingSync) != cudaSuccess ||
+      cudaEventCreateWithFlags(&s->copied_out[1], cudaEventDisableTiming | cudaEventBlockingSync) != cudaSuccess ||
       cudaStreamCreateWithFlags(&s->rows_stream, cudaStreamNonBlocking) != cudaSuccess) {
     cudaFreeHost(s->h_totals);
     cudaFreeHost(s->h_rowtot);
@@ -408,7 +415,7 @@ int gvh_surface_destroy(gvh_surface *s) {
   cudaStreamSynchronize(s->rows_stream);
   cudaEventDestroy(s->copied);
   for (int b = 0; b < 2; ++b)
-    if (s->text_copied[b]) cudaEventDestroy(s->text_copied[b]);
+    if (s->copied_out[b]) cudaEventDestroy(s->copied_out[b]);
   cudaStreamDestroy(s->rows_stream);
   cudaFree(s->dev);
   if (s->rowdev) cudaFree(s->rowdev);
@@ -501,8 +508,7 @@ static int device_rows_begin(gvh_surface *s, long long ncubes, long long npoints
   const long long slots = std::max(1ll, ncubes) * gvh::iso::kMaxElements;
   s->rbuf = 1 - s->rbuf;
   const int b = s->rbuf;
-  int rc = grow_mapped(&s->h_rows[b], &s->d_rows_mapped[b], &s->cap_rows[b], slots * gvh::surface::kRowColumns);
-  if (rc) return rc;
+  int rc;
   const bool text = s->outputs & gvh::surface::OUT_TEXT;
   if (text && (rc = grow_mapped(&s->h_hrows[b], &s->d_hrows_mapped[b], &s->cap_hrows[b], slots / 16 + 1024)))
     return rc;
@@ -523,7 +529,6 @@ static int device_rows_begin(gvh_surface *s, long long ncubes, long long npoints
   d.point_vals = s->point_vals;
   d.c2p = s->d_c2p;
   gvh::surface::device_rows_carve(d, s->rowdev, cap);
-  d.rows = s->d_rows_mapped[b];
   d.host_totals = s->d_rowtot_mapped;
   if (!text) d.text = nullptr;
   d.host_rows = text ? s->d_hrows_mapped[b] : nullptr;
@@ -550,13 +555,13 @@ int gvh_surface_find_begin(gvh_surface *s, double tau_label, double tau_scale) {
                                                                                        hi + 3 * g.ncells, s->iso,
                                                                                        s->flag);
   fo_count<<<s->nbc + s->nbp, kFoThreads, 0, st>>>(g, s->nbc, s->flag, s->pflag, s->counts);
-  fo_scan<<<1, 1024, 0, st>>>(s->nbc, s->nbp, s->counts, s->totals);
+  fo_scan<<<1, 1024, 0, st>>>(s->nbc, s->nbp, s->counts, s->totals, s->d_totals_mapped);
   fo_write<<<s->nbc + s->nbp, kFoThreads, 0, st>>>(g, s->nbc, s->flag, s->pflag, s->counts, lo, hi, s->cube_key,
                                                    s->point_cell, s->point_vals);
   SF_CUDA(cudaGetLastError());
-  SF_CUDA(cudaMemcpyAsync(s->h_totals, s->totals, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
   SF_CUDA(cudaStreamSynchronize(st));
-  const long long ncubes = s->h_totals[0], npoints = s->h_totals[1];
+  const long long ncubes = reinterpret_cast<volatile int *>(s->h_totals)[0];
+  const long long npoints = reinterpret_cast<volatile int *>(s->h_totals)[1];
   if (s->device_rows) {
     if ((rc = device_rows_begin(s, ncubes, npoints, tau_label, tau_scale))) return rc;
     SF_CUDA(cudaEventRecord(s->copied, s->rows_stream));
@@ -619,18 +624,25 @@ int gvh_surface_find_end(gvh_surface *s, long long *n_elements) {
     const long long bytes = s->h_rowtot[2], nhost = s->h_rowtot[3];
     // the device's text, unless its host rows overflowed (then every row came as values)
     const bool device_text = text && nhost <= s->cap_hrows[b];
-    gvh::surface::DeviceText dt;
+    // every row comes as values when they are kept, when there is no text or when the host
+    // rows overflowed
+    const bool all_rows = s->p_nrows > 0 && (!device_text || (s->outputs & gvh::surface::OUT_ROWS));
+    // the copy engine brings the text and rows while the caller goes on; the copies are
+    // queued on the rows' stream before the next slab's kernels, which reuse the device buffers
+    gvh::surface::DeviceRows d;
+    gvh::surface::device_rows_carve(d, s->rowdev, s->rowdev_cap);
     int rc;
+    if (all_rows) {
+      const long long values = s->p_nrows * gvh::surface::kRowColumns;
+      if ((rc = grow_pinned(&s->h_rows[b], &s->cap_rows[b], values))) return rc;
+      SF_CUDA(cudaMemcpyAsync(s->h_rows[b], d.rows, (size_t)values * sizeof(double), cudaMemcpyDeviceToHost,
+                              s->rows_stream));
+    }
+    gvh::surface::DeviceText dt;
     if (device_text) {
-      // the copy engine brings the text while the caller goes on; it is queued on the rows'
-      // stream before the next slab's kernels, which reuse the device buffer
       if ((rc = grow_pinned(&s->h_text[b], &s->cap_text[b], std::max(1ll, bytes)))) return rc;
-      if (bytes) {
-        gvh::surface::DeviceRows d;
-        gvh::surface::device_rows_carve(d, s->rowdev, s->rowdev_cap);
+      if (bytes)
         SF_CUDA(cudaMemcpyAsync(s->h_text[b], d.text, (size_t)bytes, cudaMemcpyDeviceToHost, s->rows_stream));
-      }
-      SF_CUDA(cudaEventRecord(s->text_copied[b], s->rows_stream));
       gvh::surface::HostRow *hr = s->h_hrows[b];
       std::sort(hr, hr + nhost, [](const gvh::surface::HostRow &x, const gvh::surface::HostRow &y) {
         return x.row < y.row;
@@ -639,21 +651,22 @@ int gvh_surface_find_end(gvh_surface *s, long long *n_elements) {
       dt.bytes = bytes;
       dt.host_rows = hr;
       dt.n_host = nhost;
-      cudaEvent_t ev = s->text_copied[b];
-      const int dev = s->device;
-      dt.ready = [ev, dev] {
-        cudaSetDevice(dev);
-        cudaEventSynchronize(ev);
-      };
     }
+    SF_CUDA(cudaEventRecord(s->copied_out[b], s->rows_stream));
+    cudaEvent_t ev = s->copied_out[b];
+    const int dev = s->device;
+    dt.ready = [ev, dev] {
+      cudaSetDevice(dev);
+      cudaEventSynchronize(ev);
+    };
     // assembled (the device's text) or formatted (rows) on the pool's workers while the
     // caller goes on (the next step, the next slab's device work); anything that reads the
     // rows or text waits for it
-    gvh::surface::format_rows(s->h_rows[b], s->p_nrows, *s->pool, s->outputs, s->last, true,
-                              device_text ? &dt : nullptr);
+    gvh::surface::format_rows(all_rows ? s->h_rows[b] : nullptr, s->p_nrows, *s->pool, s->outputs, s->last, true,
+                              dt);
     s->p_text_bytes = device_text ? bytes : 0;
     s->p_host_rows = device_text ? nhost : 0;
-    s->p_all_rows = !device_text || (s->outputs & gvh::surface::OUT_ROWS);
+    s->p_all_rows = all_rows;
     s->formatting = s->p_nrows > 0;
     s->last.errors = s->p_errors;
   } else {

@@ -39,9 +39,9 @@ struct DeviceRows {
                             // nullptr for no text
   HostRow *host_rows;       // mapped: the host rows, in no particular order
   long long host_rows_cap;
-  double *rows;             // mapped: every row, in order (slot_rows' worth of room), when
+  double *rows;             // device: every row, in order (slot_rows' worth of room), when
                             // keep_rows, when there is no text, or when the host rows
-                            // overflow host_rows_cap
+                            // overflow host_rows_cap (then the host copies them)
   bool keep_rows;
 };
 

@@ -152,7 +152,7 @@ void Pool::run(int n, const std::function<void(int)> &f) {
 }
 
 void format_rows(const double *rows, long long n, Pool &pool, int outputs, Result &out, bool async,
-                 const DeviceText *dt) {
+                 const DeviceText &dt) {
   out.elements = n;
   out.errors = 0;
   out.joined_valid = false;
@@ -160,13 +160,14 @@ void format_rows(const double *rows, long long n, Pool &pool, int outputs, Resul
     out.parts.clear();
     return;
   }
-  const bool text = outputs & OUT_TEXT, device_text = text && dt;
-  const long long work = device_text ? (dt->bytes + dt->n_host * 240) / 65536 : n / 256;
+  const bool text = outputs & OUT_TEXT, device_text = text && dt.text;
+  const long long work = device_text ? (dt.bytes + dt.n_host * 240) / 65536 : n / 256;
   const int nparts = (int)std::max<long long>(1, std::min<long long>(4ll * pool.size(), work));
   out.parts.resize(nparts);
   Result *res = &out;
-  DeviceText d = device_text ? *dt : DeviceText{};
+  DeviceText d = dt;
   auto job = [rows, n, nparts, outputs, res, text, device_text, d](int i) {
+    if (d.ready) d.ready();
     Part &part = res->parts[i];
     part.rows.clear();
     part.text.clear();
@@ -182,7 +183,6 @@ void format_rows(const double *rows, long long n, Pool &pool, int outputs, Resul
     }
     // bytes [lo, hi) of the device's text, with the host rows that go before byte lo .. hi - 1
     // (and, in the last part, those at the end)
-    if (d.ready) d.ready();
     const long long lo = d.bytes * i / nparts, hi = d.bytes * (i + 1) / nparts;
     const HostRow *hb = d.host_rows, *he = d.host_rows + d.n_host;
     auto first_at = [](const HostRow *b, const HostRow *e, long long off) {

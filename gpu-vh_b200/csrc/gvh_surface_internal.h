@@ -101,12 +101,13 @@ struct DeviceText {
 };
 
 // Formats rows the device produced (n rows of kColumns) into out's parts on the pool, in
-// order; keeps the rows too when outputs has OUT_ROWS. With dt the text is the device's, with
-// the host rows formatted here and spliced in. With async the work is started on the pool's
+// order; keeps the rows too when outputs has OUT_ROWS. With dt.text the text is the device's,
+// with the host rows formatted here and spliced in (rows may then be null unless OUT_ROWS).
+// Each job calls dt.ready first, when set. With async the work is started on the pool's
 // workers and format_rows returns at once: pool.wait() before reading out or reusing rows or
 // the device text.
-void format_rows(const double *rows, long long n, Pool &pool, int outputs, Result &out, bool async = false,
-                 const DeviceText *dt = nullptr);
+void format_rows(const double *rows, long long n, Pool &pool, int outputs, Result &out, bool async,
+                 const DeviceText &dt);
 
 // Runs the surface finder on every crossed hypercube of the slab on the pool, in order.
 // outputs: OUT_ROWS and/or OUT_TEXT. cell_to_point is scratch of at least nx*ny*nz entries

@@ -5,7 +5,7 @@
 // reference's interpolation to the element's centroid, the row) -- the code the host pool
 // runs -- and writes its rows to fixed slots (kMaxElements per hypercube); the rows are the
 // filled slots in slot order, which is the reference's order (hypercubes in loop order, a
-// cube's elements in cornelius' order). One thread per slot then writes the row's text with
+// cube's elements in cornelius' order). One thread per hypercube then writes its rows' text with
 // the fast path of %g (gvh_format.hpp); a scan over the slots' text lengths places each row's
 // text in the slab's text, compacted in device memory for one copy to the host by the copy
 // engine. Rows with a number the fast path leaves to the exact one go to the host as values
@@ -53,32 +53,39 @@ __global__ void __launch_bounds__(kRowThreads) cube_rows_kernel(RowGeometry g, l
   }
 }
 
-// The text of slot t (hypercube t / kSlotRows, its element t % kSlotRows): the fast path of
-// %g for each number, a space between them, a newline after the last. An empty slot, or a
-// row with a number the fast path leaves to the exact one (a host row), gets length 0.
-// Thread n_slots writes the scan's closing 0.
-__global__ void slot_text_kernel(long long n_slots, const double *__restrict__ slot_rows,
+// The text of hypercube c's rows, one thread per hypercube: for each of its filled slots the
+// fast path of %g for each number, a space between them, a newline after the last. An empty
+// slot, or a row with a number the fast path leaves to the exact one (a host row), gets
+// length 0; thread 0 also writes the scan's closing 0 (slot_len[ncubes kSlotRows]).
+__global__ void slot_text_kernel(long long ncubes, const double *__restrict__ slot_rows,
                                  const int *__restrict__ slot_n, char *__restrict__ text_slots,
                                  long long *__restrict__ slot_len, unsigned char *__restrict__ slot_host) {
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (t > n_slots) return;
-  slot_len[t] = 0;
-  if (t == n_slots) return;
-  slot_host[t] = 0;
-  if ((int)(t % kSlotRows) >= slot_n[t / kSlotRows]) return;
-  const double *row = slot_rows + t * kRowColumns;
-  char *out = text_slots + t * kTextSlot;
-  char *p = out;
-  for (int k = 0; k < kRowColumns; ++k) {
-    char *q = fmt::g6_fast(p, row[k]);
-    if (!q) {
-      slot_host[t] = 1;
-      return;
+  const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (c == 0) slot_len[ncubes * kSlotRows] = 0;
+  if (c >= ncubes) return;
+  const int n = slot_n[c];
+  for (int i = 0; i < kSlotRows; ++i) {
+    const long long t = c * kSlotRows + i;
+    long long len = 0;
+    if (i < n) {
+      const double *row = slot_rows + t * kRowColumns;
+      char *out = text_slots + t * kTextSlot;
+      char *p = out;
+      unsigned char host = 0;
+      for (int k = 0; k < kRowColumns; ++k) {
+        char *q = fmt::g6_fast(p, row[k]);
+        if (!q) {
+          host = 1;
+          break;
+        }
+        p = q;
+        *p++ = k + 1 < kRowColumns ? ' ' : '\n';
+      }
+      slot_host[t] = host;
+      len = host ? 0 : p - out;
     }
-    p = q;
-    *p++ = k + 1 < kRowColumns ? ' ' : '\n';
+    slot_len[t] = len;
   }
-  slot_len[t] = p - out;
 }
 
 // One warp per hypercube (grid-stride): each of its rows' text to its place in the slab's
@@ -115,9 +122,8 @@ __global__ void text_compact_kernel(long long ncubes, const int *__restrict__ sl
   }
 }
 
-// Every row in order to rows (grid-stride over the slots' values, one thread per value, so
-// that a row crosses the host link as one contiguous write) when all rows are wanted: always
-// (copy_all), or when the host rows overflowed their buffer.
+// Every row in order to rows (grid-stride over the slots' values, one thread per value) when
+// all rows are wanted: always (copy_all), or when the host rows overflowed their buffer.
 __global__ void rows_compact_kernel(long long ncubes, const double *__restrict__ slot_rows,
                                     const int *__restrict__ slot_n, const int *__restrict__ offsets,
                                     const long long *__restrict__ totals, bool copy_all, long long host_rows_cap,
@@ -157,7 +163,7 @@ size_t scan_temp_bytes(long long cap) {
 
 size_t device_rows_scratch_bytes(long long cap) {
   const size_t slots = (size_t)cap * kSlotRows;
-  return 1024 + align256(slots * kRowColumns * sizeof(double)) + 2 * align256((size_t)(cap + 1) * sizeof(int)) +
+  return 1024 + 2 * align256(slots * kRowColumns * sizeof(double)) + 2 * align256((size_t)(cap + 1) * sizeof(int)) +
          2 * align256((slots + 1) * sizeof(long long)) + align256(slots) + 2 * align256(slots * kTextSlot) +
          scan_temp_bytes(cap);
 }
@@ -167,6 +173,7 @@ void device_rows_carve(DeviceRows &d, char *base, long long cap) {
   char *p = base;
   d.totals = reinterpret_cast<long long *>(p); p += 1024;
   d.slot_rows = reinterpret_cast<double *>(p); p += align256(slots * kRowColumns * sizeof(double));
+  d.rows = reinterpret_cast<double *>(p); p += align256(slots * kRowColumns * sizeof(double));
   d.slot_n = reinterpret_cast<int *>(p); p += align256((size_t)(cap + 1) * sizeof(int));
   d.offsets = reinterpret_cast<int *>(p); p += align256((size_t)(cap + 1) * sizeof(int));
   d.slot_len = reinterpret_cast<long long *>(p); p += align256((slots + 1) * sizeof(long long));
@@ -193,8 +200,8 @@ cudaError_t launch_device_rows(const DeviceRows &d, cudaStream_t st) {
   const long long n_slots = d.ncubes * kSlotRows;
   const bool text = d.text != nullptr;
   if (text) {
-    slot_text_kernel<<<(unsigned)((n_slots + 256) / 256), 256, 0, st>>>(n_slots, d.slot_rows, d.slot_n,
-                                                                       d.text_slots, d.slot_len, d.slot_host);
+    slot_text_kernel<<<(unsigned)((d.ncubes + 127) / 128), 128, 0, st>>>(d.ncubes, d.slot_rows, d.slot_n,
+                                                                        d.text_slots, d.slot_len, d.slot_host);
     temp = d.scan_temp_bytes;
     if ((e = cub::DeviceScan::ExclusiveSum(d.scan_temp, temp, d.slot_len, d.text_off, (int)(n_slots + 1), st)))
       return e;
