@@ -647,6 +647,11 @@ int gvh_surface_find_end(gvh_surface *s, long long *n_elements) {
       std::sort(hr, hr + nhost, [](const gvh::surface::HostRow &x, const gvh::surface::HostRow &y) {
         return x.row < y.row;
       });
+      // the splice needs the places in row order, within the text
+      for (long long i = 0; i < nhost; ++i)
+        if (hr[i].row < 0 || hr[i].row >= s->p_nrows || hr[i].text_off < (i ? hr[i - 1].text_off : 0) ||
+            hr[i].text_off > bytes)
+          return sfail(GVH_ERR_CUDA, "gvh_surface_find_end: the device's host rows are inconsistent");
       dt.text = s->h_text[b];
       dt.bytes = bytes;
       dt.host_rows = hr;
