@@ -480,8 +480,8 @@ int gvh_surface_set_lower(gvh_surface *s) {
 }
 
 // The slab's rows and text on the device (gvh_surface_rows.cu), queued on the surface's
-// stream; the counts, the host rows (and the rows, when kept) land in mapped pinned host
-// memory and the text stays on the device for find_end to copy, so nothing here waits.
+// stream; the counts and the host rows land in mapped pinned host memory, the text (and the
+// rows, when needed) stay on the device for find_end to copy, so nothing here waits.
 static int device_rows_begin(gvh_surface *s, long long ncubes, long long npoints, double tau_label,
                              double tau_scale) {
   gvh_handle *h = s->h;
