@@ -24,6 +24,7 @@
 // crossed hypercube instead of ~160 bytes per lattice cell per level) and runs the same code
 // with a pool of host threads (gvh_surface_host.cpp).
 #include <cuda_runtime.h>
+#include <limits.h>
 #include <stdarg.h>
 #include <stdio.h>
 #include <string.h>
@@ -489,6 +490,10 @@ static int device_rows_begin(gvh_surface *s, long long ncubes, long long npoints
   // surface's own stream, so the handle's next step does not wait for them. The previous
   // slab's rows are complete too (find_end waited for them), so the buffers are free.
   cudaStream_t st = s->rows_stream;
+  // the scans count slots in int
+  if (ncubes >= (long long)(INT_MAX / gvh::iso::kMaxElements) - 1)
+    return sfail(GVH_ERR_INVALID, "gvh_surface: %lld crossed hypercubes in one slab are more than the device rows "
+                                  "handle", ncubes);
   if (ncubes > s->rowdev_cap) {
     const long long cap = std::max<long long>(ncubes, s->rowdev_cap * 3 / 2 + 1024);
     if (s->rowdev) {
