@@ -17,6 +17,8 @@
 //  * the first call on a device looks up the array's device address and raises the stage
 //    kernels' shared-memory limit (once per device, with that device current); make that
 //    first call before any stream capture;
+//  * with opts->device >= 0 the call runs on that device and makes the caller's current
+//    device current again before it returns (on every path, errors included);
 //  * every call shares the one array and it keeps the last call's contents: the status word
 //    is cleared at the start of each call, and two calls whose work overlaps on the GPU
 //    (different streams, or host threads without ordering) race on it -- order them.
@@ -80,6 +82,15 @@ int scratch_address(int dev, unsigned char **out) {
   return GVH_OK;
 }
 
+// Puts the caller's current device back when the call returns (the entry point makes
+// opts->device current for its work and must not leave the calling thread switched).
+struct DeviceRestore {
+  int saved = -1;
+  ~DeviceRestore() {
+    if (saved >= 0) cudaSetDevice(saved);
+  }
+};
+
 template <int EOS, bool SHEAR, bool BULK, bool MIXED>
 void launch_pair(const StageArgs &a1, const StageArgs &a2, long long n, cudaStream_t st) {
   const unsigned blocks = (unsigned)((n + kBlock - 1) / kBlock);
@@ -131,13 +142,18 @@ int gvh_rk2_step_noalloc(const gvh_lattice_params *L, const gvh_hydro_params *H,
                  "gvh_rk2_step_noalloc: a %dx%dx%d lattice needs %llu bytes of intermediate storage, more than the "
                  "%zu-byte static scratch; use gvh_create/gvh_rk2_step for lattices this large",
                  nx, ny, nz, need, kNoallocScratchBytes);
-  int dev = o.device;
-  if (dev < 0) {
-    cudaError_t err = cudaGetDevice(&dev);
+  int dev = o.device, caller_dev = -1;
+  {
+    cudaError_t err = cudaGetDevice(&caller_dev);
     if (err != cudaSuccess) return nfail(GVH_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(err));
-  } else {
+  }
+  DeviceRestore restore;
+  if (dev < 0) {
+    dev = caller_dev;
+  } else if (dev != caller_dev) {
     cudaError_t err = cudaSetDevice(dev);
     if (err != cudaSuccess) return nfail(GVH_ERR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(err));
+    restore.saved = caller_dev;  // every return from here on switches back
   }
   unsigned char *scratch = nullptr;
   int rc = scratch_address(dev, &scratch);

@@ -312,6 +312,9 @@ struct gvh_surface {
   // a slab between gvh_surface_find_begin and _end: its copies to the pinned buffers are in
   // flight on the handle's stream, ordered before whatever the caller queues next
   bool pending;
+  // an internal consistency check failed in gvh_surface_find_end: the last slab's rows are
+  // dropped and every later call on this surface is refused
+  bool failed;
   long long p_ncubes, p_npoints;
   double p_label, p_scale;
   cudaEvent_t copied;
@@ -547,6 +550,7 @@ int gvh_surface_find_begin(gvh_surface *s, double tau_label, double tau_scale) {
   if (!s) return sfail(GVH_ERR_INVALID, "gvh_surface_find_begin: null argument");
   if (!s->have_lower) return sfail(GVH_ERR_INVALID, "gvh_surface_find_begin: no lower time level (gvh_surface_set_lower)");
   if (s->pending) return sfail(GVH_ERR_INVALID, "gvh_surface_find_begin: the previous slab has not been ended");
+  if (s->failed) return sfail(GVH_ERR_INTERNAL, "gvh_surface_find_begin: an earlier slab failed");
   gvh_handle *h = s->h;
   SF_CUDA(cudaSetDevice(h->device));
   s->p_t0 = std::chrono::steady_clock::now();
@@ -655,8 +659,15 @@ int gvh_surface_find_end(gvh_surface *s, long long *n_elements) {
       // the splice needs the places in row order, within the text
       for (long long i = 0; i < nhost; ++i)
         if (hr[i].row < 0 || hr[i].row >= s->p_nrows || hr[i].text_off < (i ? hr[i - 1].text_off : 0) ||
-            hr[i].text_off > bytes)
-          return sfail(GVH_ERR_CUDA, "gvh_surface_find_end: the device's host rows are inconsistent");
+            hr[i].text_off > bytes) {
+          // the copies just queued still land in h_text[b] / h_rows[b]: mark them, so that
+          // nothing reuses those buffers before they finish, and drop the previous slab's
+          // rows so that no later call hands them out as this slab's
+          cudaEventRecord(s->copied_out[b], s->rows_stream);
+          s->last = gvh::surface::Result();
+          s->failed = true;
+          return sfail(GVH_ERR_INTERNAL, "gvh_surface_find_end: the device's host rows are inconsistent");
+        }
       dt.text = s->h_text[b];
       dt.bytes = bytes;
       dt.host_rows = hr;
@@ -711,6 +722,7 @@ int gvh_surface_find(gvh_surface *s, double tau_label, double tau_scale, long lo
 
 int gvh_surface_get_rows(gvh_surface *s, double *rows, long long max_rows) {
   if (!s || (!rows && max_rows > 0)) return sfail(GVH_ERR_INVALID, "gvh_surface_get_rows: bad argument");
+  if (s->failed) return sfail(GVH_ERR_INTERNAL, "gvh_surface_get_rows: the last slab failed");
   wait_format(s);
   if (max_rows < s->last.elements)
     return sfail(GVH_ERR_INVALID, "gvh_surface_get_rows: %lld rows do not fit in %lld", s->last.elements, max_rows);
@@ -725,6 +737,7 @@ int gvh_surface_get_rows(gvh_surface *s, double *rows, long long max_rows) {
 
 int gvh_surface_get_text(gvh_surface *s, const char **text, long long *length) {
   if (!s || !text || !length) return sfail(GVH_ERR_INVALID, "gvh_surface_get_text: null argument");
+  if (s->failed) return sfail(GVH_ERR_INTERNAL, "gvh_surface_get_text: the last slab failed");
   wait_format(s);
   const std::string &t = s->last.text();
   *text = t.c_str();
@@ -744,6 +757,7 @@ namespace gvh {
 namespace surface {
 void take_text(gvh_surface *s, std::vector<std::string> &out) {
   wait_format(s);
+  if (s->failed) return;  // nothing of a failed slab is handed out
   for (auto &p : s->last.parts) {
     out.emplace_back(std::move(p.text));
     p.text.clear();

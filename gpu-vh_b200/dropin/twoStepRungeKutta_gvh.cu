@@ -1,7 +1,7 @@
 // twoStepRungeKutta_gvh.cu -- drop-in for gpu-vh's FullyDiscreteKurganovTadmorScheme.cu.
 //
 // Build it inside the gpu-vh tree in place of rhic/src/FullyDiscreteKurganovTadmorScheme.cu
-// and link libgvh.so. It defines twoStepRungeKutta with the reference's
+// and link libgvh.so (gpu-vh_b200/libgvh.so; include/gvh.h). It defines twoStepRungeKutta with the reference's
 // signature (FullyDiscreteKurganovTadmorScheme.cuh:18) and leaves the reference's device
 // globals exactly as the reference's own step would (FullyDiscreteKurganovTadmorScheme.cu
 // :109-139): d_Q holds the new conserved variables, d_e/d_p the new e and p, d_u the new

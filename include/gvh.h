@@ -43,6 +43,8 @@ extern "C" {
 #define GVH_ERR_CUDA -2      /* a CUDA call failed (message in gvh_last_error) */
 #define GVH_ERR_NUMERIC -3   /* the step raised a status bit (see gvh_status) */
 #define GVH_ERR_NOMEM -4     /* device allocation failed */
+#define GVH_ERR_INTERNAL -5  /* an internal consistency check failed; the object that
+                                reported it refuses further work */
 
 /* status bits (gvh_status) */
 #define GVH_STATUS_NAN 1u          /* an energy density came out NaN */
@@ -164,9 +166,11 @@ int gvh_synchronize(gvh_handle *h);
  * step earlier) and u (current u^mu, 4 components each; read only), u_next (out u^{n+1};
  * must not alias u or u_prev). The step is queued on `stream` (a cudaStream_t, NULL = the
  * legacy default stream); if status_out is not null the call waits and stores the
- * GVH_STATUS_* bits. The first call on a device looks up the scratch address (do it before
- * any stream capture). All calls share the scratch and its status word, which each call
- * clears: calls whose work overlaps on the GPU race, so order them. */
+ * GVH_STATUS_* bits. With opts->device >= 0 the work runs on that device and the caller's
+ * current device is current again when the call returns. The first call on a device looks
+ * up the scratch address (do it before any stream capture). All calls share the scratch and
+ * its status word, which each call clears: calls whose work overlaps on the GPU race, so
+ * order them. */
 int gvh_rk2_step_noalloc(const gvh_lattice_params *lattice, const gvh_hydro_params *hydro, const gvh_options *opts,
                          double t, double dt, double T_reg, double *q, double *e, double *p, const double *u_prev,
                          const double *u, double *u_next, unsigned *status_out, void *stream);

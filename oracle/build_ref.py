@@ -29,7 +29,11 @@ import sys
 from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_ROOT = os.environ.get("GVH_REFERENCE_ROOT", "/root/reference")
+# Where this recipe reads the reference tree: $GVH_REFERENCE_ROOT, else the location the
+# build container mounts it at. This is the only place the location is written down; the
+# fixture scripts and the compile test take it from here. Hosts without the tree (the GPU
+# hosts) skip every step that needs it and use the libraries built before.
+REF_ROOT = os.environ.get("GVH_REFERENCE_ROOT") or "/root/reference"
 OUT = os.path.join(HERE, "_ref")
 
 SOURCES = [

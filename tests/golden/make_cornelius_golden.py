@@ -19,7 +19,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = os.environ.get("GVH_REFERENCE_ROOT", "/root/reference")
+sys.path.insert(0, ROOT)
+from oracle.build_ref import REF_ROOT as REF  # noqa: E402
+
 CUBES = 2500
 RAND_MAX = 2147483647
 

@@ -6,7 +6,9 @@ import subprocess
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF_SRC = os.path.join(os.environ.get("GVH_REFERENCE_ROOT", "/root/reference"), "rhic", "src")
+from oracle.build_ref import REF_ROOT  # noqa: E402
+
+REF_SRC = os.path.join(REF_ROOT, "rhic", "src")
 
 
 @pytest.mark.skipif(not os.path.isdir(REF_SRC), reason="reference tree not present")

@@ -46,15 +46,31 @@ def rel(a, b):
     return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
 
 
+HBARC = 0.197326938
+
+# (eos, shear, bulk, T_reg [fm^-1], state kwargs): the scratch holds nq + 5 values per cell,
+# so each component count (4, 14, 15) lays it out differently; T_reg > 0 on a state with
+# large pi regulates cells (the regulation branch of the stage kernel).
+CASES = {
+    "qcd_shear_bulk": (False, True, True, 0.0, dict(seed=31)),
+    "qcd_shear": (False, True, False, 0.0, dict(seed=32)),
+    "conformal_ideal": (True, False, False, 0.0, dict(seed=33)),
+    "conformal_shear": (True, True, False, 0.0, dict(seed=34)),
+    "qcd_shear_regulated": (False, True, False, 0.5 / HBARC, dict(seed=35, pi=0.3)),
+}
+
+
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_noalloc_step_matches_handle_on_two_calls(precision):
+@pytest.mark.parametrize("case", list(CASES))
+def test_noalloc_step_matches_handle_on_two_calls(case, precision):
     import torch
 
+    conformal, shear, bulk, T_reg, st_kw = CASES[case]
     L = bound()
-    kw = dict(nx=12, ny=10, nz=7, dx=0.3, dy=0.3, dz=0.3, dt=0.01, etabar=0.16, theta=2.0, conformal=False,
-              shear=True, bulk=True)
+    kw = dict(nx=12, ny=10, nz=7, dx=0.3, dy=0.3, dz=0.3, dt=0.01, etabar=0.16, theta=2.0, conformal=conformal,
+              shear=shear, bulk=bulk)
     G = gvh.Lattice(precision=precision, **kw)
-    G.set_primitive(rich_state(G, seed=31))
+    G.set_primitive(rich_state(G, **st_kw))
     s = G.get_state()
     dev = torch.device("cuda", torch.cuda.current_device())
     q = torch.tensor(stack(G, s, G.qnames), device=dev).contiguous()
@@ -64,15 +80,21 @@ def test_noalloc_step_matches_handle_on_two_calls(precision):
     u = torch.tensor(stack(G, s, ["ut", "ux", "uy", "un"]), device=dev).contiguous()
     u_next = torch.empty_like(u)
     stream = torch.cuda.current_stream(dev).cuda_stream
+    opts = gvh.Options()
+    ctypes.memmove(ctypes.byref(opts), ctypes.byref(G.options), ctypes.sizeof(opts))
+    opts.device = dev.index  # an explicit device: the call must leave the caller's current
     t = 0.5
     for call in range(2):
         status = ctypes.c_uint(123)
-        rc = L.gvh_rk2_step_noalloc(ctypes.byref(G.lattice), ctypes.byref(G.hydro), ctypes.byref(G.options), t,
-                                    kw["dt"], 0.0, q.data_ptr(), e.data_ptr(), p.data_ptr(), u_prev.data_ptr(),
+        before = torch.cuda.current_device()
+        rc = L.gvh_rk2_step_noalloc(ctypes.byref(G.lattice), ctypes.byref(G.hydro), ctypes.byref(opts), t,
+                                    kw["dt"], T_reg, q.data_ptr(), e.data_ptr(), p.data_ptr(), u_prev.data_ptr(),
                                     u.data_ptr(), u_next.data_ptr(), ctypes.byref(status), stream)
         assert rc == 0, L.gvh_noalloc_last_error()
-        assert status.value == 0
-        G.step(t, kw["dt"])
+        assert torch.cuda.current_device() == before
+        G.clear_status()
+        G.step(t, kw["dt"], T_reg)
+        assert status.value == G.status(), (call, status.value, G.status())
         ref = G.get_state()
         torch.cuda.synchronize()
         for n, name in enumerate(G.qnames):
@@ -84,6 +106,14 @@ def test_noalloc_step_matches_handle_on_two_calls(precision):
         # next step: u^n becomes the previous level, u^{n+1} the current one
         u_prev, u, u_next = u, u_next, u_prev
         t = 0.5 + (call + 1) * kw["dt"]
+    if T_reg > 0 and shear:
+        # the case is meant to regulate: the regulated run differs from an unregulated one
+        H = gvh.Lattice(precision=precision, **kw)
+        H.set_primitive(rich_state(H, **st_kw))
+        H.step(0.5, kw["dt"])
+        H.step(0.5 + kw["dt"], kw["dt"])
+        free = H.get_state()
+        assert rel(q[8].cpu().numpy(), H.interior(free["pixx"]).reshape(-1)) > 1e-6
 
 
 def test_noalloc_rejects_lattices_beyond_its_scratch():
