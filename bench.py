@@ -310,6 +310,34 @@ def reference_gpu_timings(args, w, prim):
     return out
 
 
+def dropin_seam_timings(args, w, prim):
+    """The drop-in twoStepRungeKutta (gpu-vh_b200/dropin/twoStepRungeKutta_gvh.cu) built into
+    the reference's own program in place of FullyDiscreteKurganovTadmorScheme.cu and driven
+    by the reference's own loop (oracle/ref_gpu_driver.cu): per step one gather of its device
+    arrays into libgvh, the two stage launches, one scatter back and the reference's closing
+    cudaDeviceSynchronize. W warm-up steps, then K steps timed with CUDA events on the legacy
+    stream; both the FP64 build and the as-shipped FP32 build. {} without the builds."""
+    import oracle
+
+    out = {}
+    kw = w.lattice_kwargs()
+    cells = w.nx * w.ny * w.nz
+    for prec in ("fp64", "fp32"):
+        variant = oracle.ref_gpu_variant(prec, w.conformal, w.shear, w.bulk, w.theta)
+        if not oracle.ref_gpu_available(variant, dropin=True):
+            continue
+        D = oracle.RefGpuLattice(precision=prec, dropin=True, **kw)
+        D.set_primitive(prim)
+        if args.warmup:
+            D.time_steps(args.warmup, w.tau0, w.dtau)
+        ms = D.time_steps(args.steps, w.tau0 + args.warmup * w.dtau, w.dtau)
+        out[prec] = {"ms_per_step": ms / args.steps, "cell_updates_per_s": cells * args.steps / (ms / 1e3),
+                     "build": f"reference rhic/src with the drop-in twoStepRungeKutta, PRECISION "
+                              f"{'double' if prec == 'fp64' else 'float'}",
+                     "timing": "CUDA events around the reference's own step loop (legacy stream)"}
+    return out
+
+
 def time_steps(L, w, steps, warmup, stream):
     """ms per RK2 step of lattice L (CUDA events on its stream)."""
     import torch
@@ -458,6 +486,64 @@ def precision_report(device):
     return report
 
 
+def serving_mix_requests(n, seed=64):
+    """n seeded requests of the serving mix, all offered at time 0, initial states not yet
+    generated (the path that runs them generates each inside its own timing)."""
+    from gvh import serve
+
+    rng = np.random.default_rng(seed)
+    return [serve.make_request(i, 0.0, rng, materialize=False) for i in range(n)]
+
+
+def fp64_single_path_requests(reqs, device, max_steps=6000):
+    """The plain FP64 single-event path on the given requests, one after another: generate
+    the initial state, run the event alone on a gvh.Lattice the way the reference's loop runs
+    it (max e against e(T_fo) before every step, stop after 11 all-frozen checks,
+    HydroPlugin.cpp:396-413), or until a NaN status bit retires it. events_per_hour counts
+    the events that reached freeze-out over the total time."""
+    import gvh
+
+    runs = []
+    total = 0.0
+    for r in reqs:
+        t0 = time.perf_counter()
+        prim = r.initial_state()
+        lat = r.lattice
+        L = gvh.Lattice(device=device, precision="fp64", nx=lat["nx"], ny=lat["ny"], nz=lat["nz"], dx=lat["dx"],
+                        dy=lat["dy"], dz=lat["dz"], dt=lat["dt"], etabar=lat["etabar"], theta=2.0, conformal=False,
+                        shear=True, bulk=True, tau0=r.tau0, T_fo_GeV=r.T_fo_GeV)
+        L.set_primitive(prim)
+        e_fo = gvh.energy_density_of_temperature(r.T_fo_GeV, conformal=False)
+        frozen, n, t, st = 0, 0, r.tau0, 0
+        while n < max_steps:
+            if L.max_energy_density() <= e_fo:
+                frozen += 1
+            if frozen >= 11:
+                break
+            if n % 10 == 0:
+                st = L.status()
+                if st & gvh.GVH_STATUS_ERRORS:
+                    break
+            L.step(t, lat["dt"])
+            n += 1
+            t = r.tau0 + n * lat["dt"]
+        st = L.status()
+        L.close()
+        el = time.perf_counter() - t0
+        total += el
+        runs.append({"grid": [lat["nx"], lat["ny"], lat["nz"]], "steps": n, "seconds": el, "frozen_out": frozen >= 11,
+                     "status": st})
+    frozen_n = sum(x["frozen_out"] for x in runs)
+    return {"events": len(runs), "frozen_out": frozen_n, "seconds": total,
+            "events_per_hour": 3600.0 * frozen_n / total if total > 0 else None,
+            "completed_per_hour": 3600.0 * len(runs) / total if total > 0 else None,
+            "statuses": sorted(set(x["status"] for x in runs)),
+            "per_grid_mean_seconds": {f"{g[0]}x{g[1]}x{g[2]}": float(np.mean([x["seconds"] for x in runs
+                                                                              if tuple(x["grid"]) == g]))
+                                      for g in sorted(set(tuple(x["grid"]) for x in runs))},
+            "path": "gvh.Lattice, plain FP64, one event at a time, initial state generated inside the timing"}
+
+
 def serving_run(args, device, rate=None, seconds=None):
     from gvh import serve
 
@@ -466,7 +552,7 @@ def serving_run(args, device, rate=None, seconds=None):
     rng = np.random.default_rng(2024)
     n_req = max(8, int(rate * seconds))
     arrivals = serve.poisson_arrivals(rate, n_req, rng)
-    reqs = [serve.make_request(i, a, rng) for i, a in enumerate(arrivals)]
+    reqs = [serve.make_request(i, a, rng, materialize=False) for i, a in enumerate(arrivals)]
     srv = serve.Server(int(60 * (1 << 30)), precision="mixed", steps_per_round=10, device=device)
     out = srv.run(reqs, time_limit=seconds)
     out.pop("steps", None)
@@ -475,29 +561,28 @@ def serving_run(args, device, rate=None, seconds=None):
     return out
 
 
-def batch64_run(args, device, per_grid):
+def batch64_run(args, device, fp64_same):
     """The batched configuration: 64 seeded events of the serving mix (grids
     {61x61x1, 101x101x31, 131x131x61}, b ~ U(0, 12) fm, eta/s ~ U(0.08, 0.24), QCD, shear +
     bulk, mixed precision) all offered at once to one batch (CUDA graph per step, tiles
-    autotuned), run until every event has frozen out. Beside it, the plain FP64 single-event
-    path's time for the same 64 events from the per-grid times measured alone (per_grid)."""
+    autotuned), run until every event has frozen out, initial states generated at admission.
+    Beside it, the plain FP64 single-event path run on the same 64 events (fp64_same, from
+    fp64_single_path_requests)."""
     from gvh import serve
 
-    rng = np.random.default_rng(64)
-    reqs = [serve.make_request(i, 0.0, rng) for i in range(64)]
+    reqs = serving_mix_requests(64)
     srv = serve.Server(int(60 * (1 << 30)), precision="mixed", steps_per_round=10, device=device, autotune=True)
     out = srv.run(reqs, time_limit=args.batch64_seconds)
     out.pop("steps", None)
-    secs = {tuple(r["grid"]): r["seconds"] for r in per_grid}
-    fp64_s = sum(secs[(r.lattice["nx"], r.lattice["ny"], r.lattice["nz"])] for r in reqs)
     out["events"] = len(reqs)
+    grids = sorted(set((r.lattice["nx"], r.lattice["ny"], r.lattice["nz"]) for r in reqs))
     out["grids"] = {f"{g[0]}x{g[1]}x{g[2]}": sum(1 for r in reqs if (r.lattice["nx"], r.lattice["ny"],
-                                                                     r.lattice["nz"]) == g)
-                    for g in secs}
-    out["fp64_single_path_seconds_same_events"] = fp64_s
-    out["fp64_single_path_events_per_hour"] = 3600.0 * len(reqs) / fp64_s
-    if out.get("events_per_hour"):
-        out["events_per_hour_vs_fp64_single_path"] = out["events_per_hour"] / out["fp64_single_path_events_per_hour"]
+                                                                     r.lattice["nz"]) == g) for g in grids}
+    if fp64_same and fp64_same.get("events") == len(reqs):
+        out["fp64_single_path_seconds_same_events"] = fp64_same["seconds"]
+        out["fp64_single_path_events_per_hour"] = fp64_same["events_per_hour"]
+        if out.get("events_per_hour") and fp64_same.get("events_per_hour"):
+            out["events_per_hour_vs_fp64_single_path"] = out["events_per_hour"] / fp64_same["events_per_hour"]
     return out
 
 
@@ -653,6 +738,11 @@ def run_ours(args):
         L1.close()
         extras["config1_fp64"] = {"workload": w1.name, "ms_per_step": ms1,
                                   "cell_updates_per_s": w1.nx * w1.ny * w1.nz / (ms1 / 1e3), "steps": w1.steps}
+        if rank == 0 and world == 1:
+            try:
+                extras["dropin_seam"] = dropin_seam_timings(args, w, prim)
+            except Exception as ex:  # reported beside the arm, never required
+                extras["dropin_seam"] = {"error": str(ex)}
         ev = event_to_freezeout(w, prim, "fp64", local)
         ev["events_per_hour"] = 3600.0 / ev["seconds"] if ev["seconds"] > 0 else None
         extras["fp64_single_event_to_freezeout"] = ev
@@ -665,28 +755,16 @@ def run_ours(args):
             extras["fp64_single_event_to_freezeout_with_surface"] = evs
             extras["mixed_vs_fp64_config1"] = precision_report(local)
         if args.serving_seconds > 0:
-            # the plain FP64 single-event path on the serving mix: one event of each grid of
-            # the mix run alone to freeze-out; the mix draws the grids uniformly
-            import dataclasses
-
-            from gvh import serve
-
-            per_grid = []
-            for (nx, ny, nz, dx) in serve.GRIDS:
-                wg = dataclasses.replace(w, nx=nx, ny=ny, nz=nz, dx=dx, dy=dx, dz=0.1, dtau=dx / 10)
-                pg = workloads.glauber_hotspots(wg)
-                pg.pop("_meta")
-                rg = event_to_freezeout(wg, pg, "fp64", local)
-                rg["grid"] = [nx, ny, nz]
-                per_grid.append(rg)
-            mean_s = float(np.mean([r["seconds"] for r in per_grid]))
-            fp64_mix = {"events_per_hour": 3600.0 / mean_s, "per_grid": per_grid}
+            # the plain FP64 single-event path on the serving mix: the 64 seeded events of the
+            # batched configuration (16 when that run is skipped), each run alone to freeze-out
+            fp64_mix = fp64_single_path_requests(serving_mix_requests(64 if args.batch64_seconds > 0 else 16), local)
             extras["fp64_single_event_path_on_serving_mix"] = fp64_mix
             sv = serving_run(args, local)
-            sv["events_per_hour_vs_fp64_single_path"] = sv["events_per_hour"] / fp64_mix["events_per_hour"]
+            if fp64_mix.get("events_per_hour"):
+                sv["events_per_hour_vs_fp64_single_path"] = sv["events_per_hour"] / fp64_mix["events_per_hour"]
             extras["batched_mixed_serving"] = sv
             if args.batch64_seconds > 0:
-                extras["batched_64_events"] = batch64_run(args, local, per_grid)
+                extras["batched_64_events"] = batch64_run(args, local, fp64_mix)
             # the offered-rate sweep of the serving configuration (1-50 req/s), shorter windows
             sweep = []
             for rate in [float(r) for r in args.serving_sweep.split(",") if r.strip()]:

@@ -313,6 +313,49 @@ int gvh_get_state(gvh_handle *h, double *const *fields, int n_fields) {
   return GVH_OK;
 }
 
+int gvh_gather_state_device(gvh_handle *h, const void *const *fields, int n_fields, int elem_bytes) {
+  if (!h || !fields) return fail(GVH_ERR_INVALID, "gvh_gather_state_device: null argument");
+  if (n_fields != h->nq + 10)
+    return fail(GVH_ERR_INVALID, "gvh_gather_state_device: expected %d fields", h->nq + 10);
+  if (elem_bytes != 4 && elem_bytes != 8)
+    return fail(GVH_ERR_INVALID, "gvh_gather_state_device: elem_bytes must be 4 or 8");
+  RefTable src = {};
+  for (int f = 0; f < n_fields; ++f) {
+    const void *a = fields[f];
+    if (!a && f >= h->nq + 6) a = fields[f - 4];  // up defaults to u
+    if (!a) return fail(GVH_ERR_INVALID, "gvh_gather_state_device: field %d is null", f);
+    src.p[f] = const_cast<void *>(a);
+  }
+  int rc;
+  if ((rc = set_device(h))) return rc;
+  FieldTable dst = {};
+  internal_fields(h, dst.p);
+  const unsigned blocks = (unsigned)((h->ncells + 255) / 256);
+  if (elem_bytes == 4) gather_ref_kernel<float><<<blocks, 256, 0, h->stream>>>(make_pack(h), n_fields, src, dst);
+  else gather_ref_kernel<double><<<blocks, 256, 0, h->stream>>>(make_pack(h), n_fields, src, dst);
+  GVH_CUDA(cudaGetLastError());
+  return GVH_OK;
+}
+
+int gvh_scatter_state_device(gvh_handle *h, void *const *fields, int n_fields, int elem_bytes) {
+  if (!h || !fields) return fail(GVH_ERR_INVALID, "gvh_scatter_state_device: null argument");
+  if (n_fields != h->nq + 10)
+    return fail(GVH_ERR_INVALID, "gvh_scatter_state_device: expected %d fields", h->nq + 10);
+  if (elem_bytes != 4 && elem_bytes != 8)
+    return fail(GVH_ERR_INVALID, "gvh_scatter_state_device: elem_bytes must be 4 or 8");
+  int rc;
+  if ((rc = set_device(h))) return rc;
+  RefTable dst = {};
+  for (int f = 0; f < n_fields; ++f) dst.p[f] = fields[f];
+  FieldTable src = {};
+  internal_fields(h, src.p);
+  const unsigned blocks = (unsigned)((h->ng + 255) / 256);
+  if (elem_bytes == 4) scatter_ref_kernel<float><<<blocks, 256, 0, h->stream>>>(make_pack(h), n_fields, src, dst);
+  else scatter_ref_kernel<double><<<blocks, 256, 0, h->stream>>>(make_pack(h), n_fields, src, dst);
+  GVH_CUDA(cudaGetLastError());
+  return GVH_OK;
+}
+
 int gvh_set_primitive_state_p(gvh_handle *h, const double *const *prim, int n_prim, const double *p_ghosted) {
   if (!h || !prim) return fail(GVH_ERR_INVALID, "gvh_set_primitive_state: null argument");
   const int want = 5 + (h->nq - 4);

@@ -52,6 +52,40 @@ __global__ void unpack_kernel(Pack p, int nf, FieldTable src, double *__restrict
     if (src.p[f]) staging[f * p.ng + id] = src.p[f][s];
 }
 
+// Arrays in the element type of the caller (the reference's PRECISION: float as shipped,
+// double in its FP64 build), passed by value like FieldTable.
+struct RefTable {
+  void *p[32];
+};
+
+// The reference's ghosted device arrays (type T) -> internal fields dst.p[f] (interior),
+// converted to double; one launch for every field. Null entries on either side are skipped.
+template <class T>
+__global__ void gather_ref_kernel(Pack p, int nf, RefTable src, FieldTable dst) {
+  const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long n = (long long)p.nx * p.ny * p.nz;
+  if (id >= n) return;
+  const int i = id % p.nx, j = (id / p.nx) % p.ny, k = id / ((long long)p.nx * p.ny);
+  const long long r = ref_index(p, i, j, k), s = i + p.sy * j + p.sz * k;
+  for (int f = 0; f < nf; ++f)
+    if (dst.p[f] && src.p[f]) dst.p[f][s] = (double)static_cast<const T *>(src.p[f])[r];
+}
+
+// Internal fields src.p[f] -> the reference's ghosted device arrays (type T), every ghost
+// cell filled from the nearest interior cell (GhostCells.cu:15-144 fills the faces; edges and
+// corners get the same clamped value); null entries are skipped.
+template <class T>
+__global__ void scatter_ref_kernel(Pack p, int nf, FieldTable src, RefTable dst) {
+  const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= p.ng) return;
+  const int gi = id % (p.nx + 4), gj = (id / (p.nx + 4)) % (p.ny + 4);
+  const int gk = id / ((long long)(p.nx + 4) * (p.ny + 4));
+  const int i = min(max(gi - 2, 0), p.nx - 1), j = min(max(gj - 2, 0), p.ny - 1), k = min(max(gk - 2, 0), p.nz - 1);
+  const long long s = i + p.sy * j + p.sz * k;
+  for (int f = 0; f < nf; ++f)
+    if (dst.p[f] && src.p[f]) static_cast<T *>(dst.p[f])[id] = (T)src.p[f][s];
+}
+
 // T^{tau mu} from primitives (DynamicalVariables.cu:349-392 with EnergyMomentumTensor.cu
 // :159-177) and p = p(e) (InitialConditions.cpp:124-127), in the internal layout.
 template <int EOS>

@@ -13,10 +13,12 @@ Requests arrive over time (a Poisson stream in the benchmark). The server keeps 
      frozen out by the reference's stop rule (or hit the request's step cap), freeing
      their memory for the next admissions.
 
-Latency of a request = completion time - arrival time. The report gives events/hour,
-p50/p99 latency and cell-updates/s. Initial conditions are produced by the client before
-the request arrives (their generation is not the server's work); the server copies them
-to the device at admission.
+Latency of a request = completion time - arrival time. A request carries the recipe of
+its initial condition (grid, impact parameter, eta/s, seed); the server generates the
+initial state when it admits the request, so that generation is part of the server's time
+and of the request's latency, then copies it to the device. The report gives events/hour
+(events that reached freeze-out; events retired by a status bit or a step cap are
+reported beside it as `completed`), p50/p99 latency and cell-updates/s.
 """
 from __future__ import annotations
 
@@ -42,11 +44,22 @@ class Request:
     rid: int
     arrival: float                     # seconds after the start of the run
     lattice: dict                      # nx ny nz dx dy dz dt etabar
-    prim: dict
+    prim: dict | None                  # the initial state, or None: generated from `ic`
     tau0: float = 0.6
     T_fo_GeV: float = 0.150
     max_steps: int = 100000
     meta: dict = field(default_factory=dict)
+    ic: tuple | None = None            # (workload, impact parameter): the generator's inputs
+
+    def initial_state(self) -> dict:
+        """The primitive initial state, generated on first use (seeded, so the same request
+        always gives the same state)."""
+        if self.prim is None:
+            w, b = self.ic
+            prim = workloads.glauber_hotspots(w, b=b)
+            self.meta = prim.pop("_meta")
+            self.prim = prim
+        return self.prim
 
 
 @dataclass
@@ -66,17 +79,20 @@ class Completed:
 
 
 def make_request(rid: int, arrival: float, rng: np.random.Generator, max_steps: int = 100000,
-                 grids=GRIDS, eta_over_s=(0.08, 0.24), b_max=12.0) -> Request:
+                 grids=GRIDS, eta_over_s=(0.08, 0.24), b_max=12.0, materialize: bool = True) -> Request:
     """One event of the serving mix: grid drawn from `grids`, b ~ U(0, b_max),
-    eta/s ~ U(eta_over_s), Glauber-hotspot initial state, dtau = dx/10."""
+    eta/s ~ U(eta_over_s), Glauber-hotspot initial state, dtau = dx/10. materialize=False
+    leaves the initial state to be generated at admission (Request.initial_state)."""
     nx, ny, nz, dx = grids[int(rng.integers(len(grids)))]
     etabar = float(rng.uniform(*eta_over_s))
     w = replace(workloads.CONFIG2, name=f"serve_{nx}x{ny}x{nz}", nx=nx, ny=ny, nz=nz, dx=dx, dy=dx, dz=0.1,
                 dtau=dx / 10, etabar=etabar, seed=int(rng.integers(1 << 30)))
-    prim = workloads.glauber_hotspots(w, b=float(rng.uniform(0, b_max)))
-    meta = prim.pop("_meta")
+    b = float(rng.uniform(0, b_max))
     lat = dict(nx=nx, ny=ny, nz=nz, dx=dx, dy=dx, dz=0.1, dt=dx / 10, etabar=etabar)
-    return Request(rid, arrival, lat, prim, tau0=w.tau0, max_steps=max_steps, meta=meta)
+    r = Request(rid, arrival, lat, None, tau0=w.tau0, max_steps=max_steps, ic=(w, b))
+    if materialize:
+        r.initial_state()
+    return r
 
 
 def poisson_arrivals(rate: float, n: int, rng: np.random.Generator) -> list[float]:
@@ -104,6 +120,7 @@ class Server:
         cell_updates = 0
         t0 = time.perf_counter()
         busy = 0.0
+        ic_seconds = 0.0
         while pending or waiting or resident:
             now = time.perf_counter() - t0
             if time_limit is not None and now > time_limit:
@@ -118,7 +135,10 @@ class Server:
                     break
                 if resident and B.active_cells + cells > self.max_resident_cells:
                     break
-                eid = B.add_event(**r.lattice, prim=r.prim, tau0=r.tau0, T_fo_GeV=r.T_fo_GeV)
+                tg = time.perf_counter()
+                prim = r.initial_state()  # generated here: part of the request's latency
+                ic_seconds += time.perf_counter() - tg
+                eid = B.add_event(**r.lattice, prim=prim, tau0=r.tau0, T_fo_GeV=r.T_fo_GeV)
                 if eid is None:
                     break
                 waiting.popleft()
@@ -146,16 +166,22 @@ class Server:
                     B.remove_event(eid)
                     del resident[eid]
         elapsed = time.perf_counter() - t0
-        return summarize(done, elapsed, cell_updates, busy)
+        out = summarize(done, elapsed, cell_updates, busy)
+        out["initial_state_seconds"] = ic_seconds
+        return out
 
 
 def summarize(done: list[Completed], elapsed: float, cell_updates: int, busy: float) -> dict:
+    """events_per_hour counts the events that reached freeze-out; `completed` also counts
+    those retired by a status bit (NaN) or by the request's step cap."""
     lat = np.array([c.latency for c in done]) if done else np.array([float("nan")])
+    frozen = sum(c.frozen_out for c in done)
     return {
         "completed": len(done),
-        "frozen_out": sum(c.frozen_out for c in done),
+        "frozen_out": frozen,
         "elapsed_s": elapsed,
-        "events_per_hour": len(done) / elapsed * 3600.0 if elapsed > 0 else 0.0,
+        "events_per_hour": frozen / elapsed * 3600.0 if elapsed > 0 else 0.0,
+        "completed_per_hour": len(done) / elapsed * 3600.0 if elapsed > 0 else 0.0,
         "p50_latency_s": float(np.percentile(lat, 50)),
         "p99_latency_s": float(np.percentile(lat, 99)),
         "cell_updates_per_s": cell_updates / elapsed if elapsed > 0 else 0.0,

@@ -125,6 +125,19 @@ int gvh_set_state(gvh_handle *h, const double *const *fields, int n_fields);
 /* Null entries are skipped. Ghost layers come back zero-gradient filled, edges and
  * corners included. Synchronises the handle's stream. */
 int gvh_get_state(gvh_handle *h, double *const *fields, int n_fields);
+/* The seam of the drop-in twoStepRungeKutta (gpu-vh_b200/dropin/twoStepRungeKutta_gvh.cu),
+ * which replaces FullyDiscreteKurganovTadmorScheme.cu:109-139 inside the reference's own
+ * program: the reference's device state arrays -- the components behind d_q / d_Q, d_e, d_p,
+ * and the components behind d_u, d_up (DynamicalVariables.cuh:101-117) -- go into and out of
+ * the handle with one gather launch and one scatter launch for all fields, converted from and
+ * to the reference's PRECISION (elem_bytes 4: float, as shipped; 8: its double build). Device
+ * pointers only, in gvh_set_state's field order, ghosted layout. Both calls are queued on the
+ * handle's stream and return without waiting. gather: a null up entry takes u.
+ * scatter: null entries are skipped; every ghost cell of a written field is filled with its
+ * nearest interior cell (the reference's zero-gradient faces, setGhostCells, GhostCells.cu
+ * :15-144; edges and corners alike). */
+int gvh_gather_state_device(gvh_handle *h, const void *const *fields, int n_fields, int elem_bytes);
+int gvh_scatter_state_device(gvh_handle *h, void *const *fields, int n_fields, int elem_bytes);
 /* Pipelined set/get for a caller that streams states through the handle (a new state in,
  * one or more steps, the result out, again and again): the copies go on the handle's own
  * copy streams, one each way, with separate device staging for inputs and outputs, and are

@@ -302,8 +302,8 @@ def ref_gpu_variant(precision: str, conformal: bool, shear: bool, bulk: bool, th
     return f"{precision}_{'conf' if conformal else 'qcd'}_{phys}_th{theta:.1f}"
 
 
-def ref_gpu_available(variant: str) -> bool:
-    return os.path.exists(os.path.join(REF_DIR, f"libref_gpu_{variant}.so"))
+def ref_gpu_available(variant: str, dropin: bool = False) -> bool:
+    return os.path.exists(os.path.join(REF_DIR, f"libref_gpu_{'dropin_' if dropin else ''}{variant}.so"))
 
 
 class RefGpuLattice(_Base):
@@ -312,10 +312,12 @@ class RefGpuLattice(_Base):
     one lattice in globals, so a process holds at most one lattice per variant library (a
     second instance must have the same sizes and reuses the buffers)."""
 
-    def __init__(self, precision="fp64", **kw):
+    def __init__(self, precision="fp64", dropin=False, **kw):
         super().__init__(**kw)
         self.variant = ref_gpu_variant(precision, self.conformal, self.shear, self.bulk, kw["theta"])
-        path = os.path.join(REF_DIR, f"libref_gpu_{self.variant}.so")
+        # dropin: the same program with gpu-vh_b200/dropin/twoStepRungeKutta_gvh.cu in place of
+        # FullyDiscreteKurganovTadmorScheme.cu (libgvh's step behind the reference's loop)
+        path = os.path.join(REF_DIR, f"libref_gpu_{'dropin_' if dropin else ''}{self.variant}.so")
         if not os.path.exists(path):
             raise FileNotFoundError(path)
         L = ctypes.CDLL(path)

@@ -218,6 +218,47 @@ def build_gpu_variant(prec: str, eos: str, phys: str, theta: str) -> str:
     return lib
 
 
+# The drop-in (gpu-vh_b200/dropin/twoStepRungeKutta_gvh.cu) built into the reference's own
+# program in place of FullyDiscreteKurganovTadmorScheme.cu, as a maintainer would build it,
+# and linked against libgvh.so: the same driver then runs the reference's allocation, set-up
+# and step loop with libgvh's step behind twoStepRungeKutta.
+DROPIN_VARIANTS = [
+    ("fp64", "conf", "shear", "1.8"),
+    ("fp64", "qcd", "bulk", "2.0"),
+    ("fp32", "qcd", "bulk", "2.0"),
+]
+REPO = os.path.dirname(HERE)
+PKG = os.path.join(REPO, "gpu-vh_b200")
+
+
+def gpu_dropin_lib_path(name: str) -> str:
+    return os.path.join(OUT, f"libref_gpu_dropin_{name}.so")
+
+
+def build_gpu_dropin_variant(prec: str, eos: str, phys: str, theta: str) -> str:
+    name = gpu_variant_name(prec, eos, phys, theta)
+    flags = PRECISIONS[prec] + EOS[eos] + PHYSICS[phys] + [f"-DGVH_REF_THETA={theta}", f"-DGVH_THETA={theta}"]
+    obj_dir = os.path.join(OUT, "obj", "gpu_dropin_" + name)
+    os.makedirs(obj_dir, exist_ok=True)
+    src_dir = os.path.join(REF_ROOT, "rhic", "src")
+    inc = ["-I", os.path.join(HERE, "ref_gpu_shim"), "-I", os.path.join(REF_ROOT, "rhic", "include"), "-I", src_dir,
+           "-I", os.path.join(REPO, "include")]
+    common = ["nvcc"] + NVCC_ARCH + ["-O3", "-rdc=true", "-Xcompiler", "-fPIC", "-w", "-std=c++14"] + inc + flags
+    flux = os.path.join(src_dir, "FluxLimiter.cu") if theta == "2.0" else _overlay_flux_limiter_theta(theta)
+    sources = [os.path.join(src_dir, x) for x in GPU_SOURCES if x != "FullyDiscreteKurganovTadmorScheme.cu"]
+    sources += [flux, os.path.join(PKG, "dropin", "twoStepRungeKutta_gvh.cu"), os.path.join(HERE, "ref_gpu_driver.cu")]
+    objs = []
+    for s in sources:
+        o = os.path.join(obj_dir, os.path.basename(s) + ".o")
+        extra = ["-maxrregcount=128"] if prec == "fp64" and os.path.basename(s) == "HydrodynamicValidity.cu" else []
+        _run(common + extra + ["-x", "cu", "-c", s, "-o", o])
+        objs.append(o)
+    lib = gpu_dropin_lib_path(name)
+    _run(["nvcc"] + NVCC_ARCH + ["-shared", "-rdc=true", "-Xcompiler", "-fPIC", "-o", lib] + objs +
+         ["-L" + PKG, "-lgvh", "-Xlinker", "-rpath=$ORIGIN/../../gpu-vh_b200"])
+    return lib
+
+
 def build_gpu(jobs: int | None = None, verbose: bool = True) -> list[str]:
     """Build the reference's CUDA variants (nvcc cross-compiles without a GPU). Skips
     (returns []) when the reference tree is not present."""
@@ -226,6 +267,8 @@ def build_gpu(jobs: int | None = None, verbose: bool = True) -> list[str]:
     os.makedirs(OUT, exist_ok=True)
     with ThreadPoolExecutor(max_workers=jobs or min(4, os.cpu_count() or 4)) as ex:
         libs = list(ex.map(lambda v: build_gpu_variant(*v), GPU_VARIANTS))
+        if os.path.exists(os.path.join(PKG, "libgvh.so")):
+            libs += list(ex.map(lambda v: build_gpu_dropin_variant(*v), DROPIN_VARIANTS))
     if verbose:
         print(f"[oracle/_ref] built {len(libs)} CUDA variants of the reference into {OUT}")
     return libs

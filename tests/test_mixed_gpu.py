@@ -61,6 +61,69 @@ def test_mixed_config2_lattice_10_steps():
     assert err["e"] <= E_TOL and err["u"] <= U_TOL and err["pi"] <= PI_TOL, err
 
 
+def test_mixed_config1_event_at_100_freezeout_and_500_steps():
+    """Configuration 3 (the config-1 event in mixed precision) against the FP64 oracle at
+    step 100, at freeze-out (the step after which the oracle's maximum e has been at or below
+    e(T_fo = 150 MeV) for 11 checks, the reference's stop rule, HydroPlugin.cpp:396-413:
+    step 297) and at step 500, within the stated tolerances. Measured on a B200: e 9.7e-8,
+    6.5e-7, 7.7e-6; u 2.4e-8, 7.1e-8, 1.7e-6; pi/(e+p) 1.2e-8, 2.9e-8, 1.1e-6."""
+    w = workloads.CONFIG1
+    kw = w.lattice_kwargs()
+    G = gvh.Lattice(precision="mixed", **kw)
+    O = oracle.OracleLattice(**kw)
+    prim = workloads.gaussian_profile(w)
+    G.set_primitive(prim)
+    O.set_primitive(prim)
+    e_fo = O.energy_density(w.T_fo_GeV / 0.197326938)
+    t, n, frozen, checked = w.tau0, 0, 0, []
+    while True:
+        so = O.get_state()
+        if frozen < 11 and float(np.max(O.interior(so["e"]))) <= e_fo:
+            frozen += 1
+            if frozen == 11:
+                checked.append(("freezeout", n))
+        if n in (100, 500):
+            checked.append((n, n))
+        if checked and checked[-1][1] == n:
+            err = mixed_errors(G, G.get_state(), so)
+            assert err["e"] <= E_TOL and err["u"] <= U_TOL and err["pi"] <= PI_TOL, (checked[-1], err)
+        if n == 500:
+            break
+        G.step(t, w.dtau)
+        O.step(t, w.dtau)
+        n += 1
+        t = w.tau0 + n * w.dtau
+    assert [c[0] for c in checked] == [100, "freezeout", 500], checked
+
+
+def test_mixed_benchmark_event_at_100_and_500_steps():
+    """The 131x131x61 QCD + bulk event in mixed precision against the plain FP64 path (which
+    the reference's FP64 CUDA build pins to 1e-10 over these steps, test_ref_gpu.py) after
+    100 and 500 steps, within the stated tolerances. Measured on a B200: e 2.5e-6 and 7.1e-5,
+    u 1.0e-6 and 5.0e-5, pi/(e+p) 5.2e-7 and 2.2e-5. At this event's freeze-out (1160 steps)
+    the mixed path is further off than the stated tolerance in e and u (e 1.7e-3, u 5.0e-4,
+    pi/(e+p) 3.4e-4); the last check bounds that drift so that a change that makes it worse
+    is noticed."""
+    w = workloads.CONFIG2
+    prim = workloads.glauber_hotspots(w)
+    prim.pop("_meta")
+    kw = w.lattice_kwargs()
+    M = gvh.Lattice(precision="mixed", **kw)
+    D = gvh.Lattice(precision="fp64", **kw)
+    M.set_primitive(prim)
+    D.set_primitive(prim)
+    t, n = w.tau0, 0
+    for check, (et, ut, pt) in [(100, (E_TOL, U_TOL, PI_TOL)), (500, (E_TOL, U_TOL, PI_TOL)), (1160, (1e-2, 2e-3, 2e-3))]:
+        while n < check:
+            n += 1
+            M.step(t, w.dtau)
+            D.step(t, w.dtau)
+            t = w.tau0 + n * w.dtau
+        assert M.status() == 0
+        err = mixed_errors(M, M.get_state(), D.get_state())
+        assert err["e"] <= et and err["u"] <= ut and err["pi"] <= pt, (n, err)
+
+
 def test_mixed_hotspot_event_stays_finite():
     """A 2+1D hotspot event of the serving mix (61x61, 0.2 fm) that ran away to NaN when the
     mixed path recovered face states in FP32; with FP64 recovery it stays finite and close

@@ -73,6 +73,58 @@ def test_benchmark_event_matches_reference_cuda_fp64():
         assert err <= QCD_TOL, f"{k}: {err:.3e}"
 
 
+# The benchmark event to freeze-out against the reference's FP64 CUDA build, measured on a
+# B200 (max over interior cells, per field, |cuda - ref| / max |ref|):
+#   step 100:  every field <= 1.6e-10 (pi^{x eta}); e 2.4e-12, u^mu <= 3.1e-12, T^{tau mu}
+#              <= 1.2e-11; per-cell relative e <= 2.4e-12
+#   step 1160 (the event's freeze-out): every field <= 8.6e-7 (pi^{x eta}); e 1.2e-8, u^mu
+#              <= 5.8e-9; per-cell relative e <= 1.3e-8
+# The difference starts at rounding (the Newton update's arithmetic is reordered: Horner
+# polynomials, two divisions instead of six) and grows smoothly with the flow's own
+# amplification of perturbations; no cell flips across the Newton stop test
+# (EnergyMomentumTensor.cu:39), which would change its e by ~1e-7..1e-6 at once. The bounds
+# below keep ~10x headroom over the measurement.
+HORIZON = {
+    100: dict(field=1e-9, flow=1e-10, cell_e=1e-10),
+    1160: dict(field=1e-5, flow=1e-7, cell_e=1e-7),
+}
+FLOW_FIELDS = ["e", "p", "ut", "ux", "uy", "un", "ttt", "ttx", "tty", "ttn"]
+
+
+def test_benchmark_event_to_freezeout_matches_reference_cuda_fp64():
+    """The 131x131x61 QCD + bulk hotspot event of the benchmark against the reference's own
+    FP64 CUDA build, checked after 100 steps and at freeze-out (1160 steps): per-field
+    errors, and the cells whose energy density differs by more than the bound (a Newton
+    stop-test flip)."""
+    w = workloads.CONFIG2
+    _need(oracle.ref_gpu_variant("fp64", w.conformal, w.shear, w.bulk, w.theta))
+    prim = workloads.glauber_hotspots(w)
+    prim.pop("_meta")
+    kw = w.lattice_kwargs()
+    G = gvh.Lattice(**kw)
+    R = oracle.RefGpuLattice(precision="fp64", **kw)
+    G.set_primitive(prim)
+    R.set_primitive(prim)
+    t, n = w.tau0, 0
+    for check in sorted(HORIZON):
+        while n < check:
+            n += 1
+            G.step(t, w.dtau)
+            R.step(t, w.dtau)
+            t = w.tau0 + n * w.dtau
+        assert G.status() == 0
+        sg, sr = G.get_state(), R.get_state()
+        tol = HORIZON[check]
+        errs = {k: rel_err(G.interior(sg[k]), G.interior(sr[k])) for k in G.field_names}
+        report = ", ".join(f"{k} {v:.1e}" for k, v in errs.items())
+        for k, v in errs.items():
+            assert v <= (tol["flow"] if k in FLOW_FIELDS else tol["field"]), f"step {n}: {k}; {report}"
+        ea, eb = G.interior(sg["e"]), G.interior(sr["e"])
+        cell = np.abs(ea - eb) / np.abs(eb)
+        flipped = int(np.count_nonzero(cell > tol["cell_e"]))
+        assert flipped == 0, f"step {n}: {flipped} cells with relative e error > {tol['cell_e']:g} (max {cell.max():.2e})"
+
+
 @pytest.mark.parametrize("which", ["config1", "config2"])
 def test_reference_cuda_fp32_build_tracks_the_event(which):
     """The as-shipped FP32 build computes the same event to single precision (e and u after
