@@ -80,7 +80,8 @@ __device__ __forceinline__ StageArgs make_args(EventDev &E, bool stage2) {
   a.inv_dx = E.inv_dx; a.inv_dy = E.inv_dy; a.inv_dz = E.inv_dz; a.inv_dt = E.inv_dt;
   a.etabar = E.etabar; a.theta = E.theta; a.e_reg = E.e_reg;
   a.status = &E.status;
-  a.diag = nullptr;  // validity diagnostics are a single-lattice option
+  a.diag = nullptr;       // validity diagnostics are a single-lattice option
+  a.speed_max = nullptr;  // so is the propagation-speed maximum
   a.e = E.e;
   // twoStepRungeKutta receives t = t0 + n dt (HydroPlugin.cpp:424) and advances it by dt
   const double t = E.t0 + (double)E.step * E.dt;
@@ -109,8 +110,8 @@ __global__ void __launch_bounds__(kBlock, GVH_MIN_BLOCKS)
     if (!E.active) continue;
     const StageArgs a = make_args(E, STAGE2);
     const long long id = (long long)(tile - E.first_tile) * kBlock + threadIdx.x;
-    double en = 0.0;
-    if (id < a.ncells) en = stage_cell<EOS, SHEAR, BULK, STAGE2, MIXED>(a, id);
+    double en = 0.0, speed;
+    if (id < a.ncells) en = stage_cell<EOS, SHEAR, BULK, STAGE2, MIXED>(a, id, speed);
     if (STAGE2) {
       unsigned long long b = __double_as_longlong(fmax(en, 0.0));
 #pragma unroll

@@ -58,10 +58,10 @@ namespace {
 
 template <int EOS, bool SHEAR, bool BULK, bool MIXED>
 int launch_stage_p(const gvh_handle *h, const StageArgs &a, bool stage2) {
-  const long long blocks = (h->ncells + kThreads - 1) / kThreads;
+  const dim3 grid = stage_grid(h->ncells);
   const size_t smem = stage_smem_bytes<SHEAR, BULK>();
-  if (stage2) kt_stage_kernel<EOS, SHEAR, BULK, true, MIXED><<<(unsigned)blocks, kThreads, smem, h->stream>>>(a);
-  else kt_stage_kernel<EOS, SHEAR, BULK, false, MIXED><<<(unsigned)blocks, kThreads, smem, h->stream>>>(a);
+  if (stage2) kt_stage_kernel<EOS, SHEAR, BULK, true, MIXED><<<grid, kThreads, smem, h->stream>>>(a);
+  else kt_stage_kernel<EOS, SHEAR, BULK, false, MIXED><<<grid, kThreads, smem, h->stream>>>(a);
   GVH_CUDA(cudaGetLastError());
   return GVH_OK;
 }
@@ -409,13 +409,16 @@ int gvh_rk2_step(gvh_handle *h, double t, double dt, double T_reg) {
   a.status = h->status;
   a.e = h->e;
   const double t1 = t + dt;
-  // stage 1 (predictor)
+  // stage 1 (predictor); it also keeps the running maximum of the propagation speed
+  // (gvh_max_propagation_speed) in the third 8-byte word after the status word
+  a.speed_max = reinterpret_cast<unsigned long long *>(h->status) + 2;
   a.t_euler = t; a.t_after = t1;
   a.qin = h->qA; a.qn = nullptr; a.qout = h->qB;
   a.pin = h->pA; a.pout = h->pB;
   a.uin = h->u[h->ucur]; a.uprev = h->u[h->uprev]; a.uout = h->u[h->uprev];
   if ((rc = dispatch(h, a, false))) return rc;
   // stage 2 (corrector + Heun combination)
+  a.speed_max = nullptr;
   a.t_euler = t1; a.t_after = t1;
   a.qin = h->qB; a.qn = h->qA; a.qout = h->qA;
   a.pin = h->pB; a.pout = h->pA;
@@ -466,6 +469,18 @@ int gvh_set_stream(gvh_handle *h, void *stream) {
   GVH_CUDA(cudaSetDevice(h->device));
   GVH_CUDA(cudaStreamSynchronize(h->stream));
   h->stream = stream ? reinterpret_cast<cudaStream_t>(stream) : h->own_stream;
+  return GVH_OK;
+}
+
+int gvh_max_propagation_speed(gvh_handle *h, double *out) {
+  if (!h || !out) return fail(GVH_ERR_INVALID, "null argument");
+  GVH_CUDA(cudaSetDevice(h->device));
+  unsigned long long *word = reinterpret_cast<unsigned long long *>(h->status) + 2;
+  unsigned long long bits = 0;
+  GVH_CUDA(cudaMemcpyAsync(&bits, word, sizeof bits, cudaMemcpyDeviceToHost, h->stream));
+  GVH_CUDA(cudaMemsetAsync(word, 0, sizeof bits, h->stream));
+  GVH_CUDA(cudaStreamSynchronize(h->stream));
+  memcpy(out, &bits, sizeof bits);
   return GVH_OK;
 }
 

@@ -92,11 +92,11 @@ struct DeviceRestore {
 };
 
 template <int EOS, bool SHEAR, bool BULK, bool MIXED>
-void launch_pair(const StageArgs &a1, const StageArgs &a2, long long n, cudaStream_t st) {
-  const unsigned blocks = (unsigned)((n + kBlock - 1) / kBlock);
+void launch_pair(const StageArgs &a1, const StageArgs &a2, long long, cudaStream_t st) {
+  const dim3 grid = stage_grid(a1.ncells);
   const size_t smem = stage_smem_bytes<SHEAR, BULK>();
-  kt_stage_kernel<EOS, SHEAR, BULK, false, MIXED><<<blocks, kBlock, smem, st>>>(a1);
-  kt_stage_kernel<EOS, SHEAR, BULK, true, MIXED><<<blocks, kBlock, smem, st>>>(a2);
+  kt_stage_kernel<EOS, SHEAR, BULK, false, MIXED><<<grid, kBlock, smem, st>>>(a1);
+  kt_stage_kernel<EOS, SHEAR, BULK, true, MIXED><<<grid, kBlock, smem, st>>>(a2);
 }
 
 template <int EOS, bool MIXED>

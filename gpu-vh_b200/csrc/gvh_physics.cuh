@@ -34,21 +34,57 @@ constexpr double kF16 = (double)1.6f;      // SourceTerms.cu:57
 // in Horner form (the reference builds explicit powers e^2..e^13 first). The two agree to
 // rounding.
 
+// The QCD fit's coefficients in Horner order (highest power first), one table per
+// polynomial; every evaluation below runs the same multiply-adds in the same order.
+__constant__ double kQcdPa[13] = {
+    1.9531729608963267e-11, 3.1188455176941583e-7, 0.0009417586777847889,
+    0.7158279081255019, 141.5073484468774, 6340.448389300905,
+    41913.439282708554, 334334.4309240126, 1.6357487344679043e6,
+    3.1729694865420084e6, 1.077580993288114e6, 9737.845799644809,
+    -0.25181736420168666};
+__constant__ double kQcdPb[13] = {
+    3.2581066229887368e-18, 5.928138360995685e-11, 9.601103399348206e-7,
+    0.002962497695527404, 2.3405487982094204, 499.04919730607065,
+    26452.34905933697, 278581.2989342773, 1.7851642641834426e6,
+    1.3512402226067686e7, 2.0931169138134286e7, 4.0574329080826794e6,
+    45829.44617893836};
+__constant__ double kQcdCa[14] = {
+    8.189430244031285e-6, 0.03009027913262399, 6.504847576502024,
+    58.60283714484669, 275.0492627924299, 1612.4245252438795,
+    460.6487249985994, 15.382615282179595, 0.02969737949090831,
+    6.087136671592452e-6, 1.4170364808063119e-10, 3.1955868410879504e-16,
+    4.123605749683891e-23, 5.191934309650155e-32};
+__constant__ double kQcdCb[14] = {
+    0.000024810902623582917, 0.09301685073435291, 21.461303090563028,
+    293.99144775704605, 590.2572000057821, 15190.225535036281,
+    1800.5461219450308, 60.85769171450653, 0.13653226327408863,
+    0.00003551782901018317, 1.1225580509306008e-9, 3.5477700458515908e-15,
+    6.716598285341542e-22, 1.4637868900982493e-30};
+__constant__ double kQcdTa[12] = {
+    1.5780479034557783e-6, 0.015421252394182246, 14.055788949565482,
+    1471.6180520527757, 14109.766109389702, 6686.07424325115,
+    207.48582344326206, 0.4873490574161924, 0.000063810382643387,
+    2.4954778310451065e-10, 8.014062800678687e-18, 1.510073201405604e-29};
+__constant__ double kQcdTb[12] = {
+    1.8472801679382593e-7, 0.003778342768228011, 5.916312075925817,
+    1051.0730543534657, 17965.67607192861, 11179.193315394154,
+    578.0778724946719, 2.316902328874072, 0.0005036835870305458,
+    2.998130743142826e-9, 1.3686372302041508e-16, 7.558667139355393e-28};
+
+// Horner evaluation of a constant-bank polynomial (coefficients highest power first).
+template <int N>
+__device__ __forceinline__ double horner(const double (&c)[N], double e) {
+  double a = c[0];
+#pragma unroll
+  for (int k = 1; k < N; ++k) a = fma(a, e, c[k]);
+  return a;
+}
+
 // p(e): EquationOfState.cu:30-80; conformal p = e/3.
 template <int EOS>
 __device__ __forceinline__ double eq_pressure(double e) {
   if (EOS == EOS_CONFORMAL) return e / 3;
-  double a = 1.9531729608963267e-11;
-  a = fma(a, e, 3.1188455176941583e-7); a = fma(a, e, 0.0009417586777847889); a = fma(a, e, 0.7158279081255019);
-  a = fma(a, e, 141.5073484468774); a = fma(a, e, 6340.448389300905); a = fma(a, e, 41913.439282708554);
-  a = fma(a, e, 334334.4309240126); a = fma(a, e, 1.6357487344679043e6); a = fma(a, e, 3.1729694865420084e6);
-  a = fma(a, e, 1.077580993288114e6); a = fma(a, e, 9737.845799644809); a = fma(a, e, -0.25181736420168666);
-  double b = 3.2581066229887368e-18;
-  b = fma(b, e, 5.928138360995685e-11); b = fma(b, e, 9.601103399348206e-7); b = fma(b, e, 0.002962497695527404);
-  b = fma(b, e, 2.3405487982094204); b = fma(b, e, 499.04919730607065); b = fma(b, e, 26452.34905933697);
-  b = fma(b, e, 278581.2989342773); b = fma(b, e, 1.7851642641834426e6); b = fma(b, e, 1.3512402226067686e7);
-  b = fma(b, e, 2.0931169138134286e7); b = fma(b, e, 4.0574329080826794e6); b = fma(b, e, 45829.44617893836);
-  return a / b;
+  return horner(kQcdPa, e) / horner(kQcdPb, e);
 }
 
 // c_s^2(e): EquationOfState.cu:82-116. The conformal branch of the reference returns the
@@ -56,36 +92,14 @@ __device__ __forceinline__ double eq_pressure(double e) {
 template <int EOS>
 __device__ __forceinline__ double sound_speed2(double e) {
   if (EOS == EOS_CONFORMAL) return 0.0;
-  double c = 8.189430244031285e-6;
-  c = fma(c, e, 0.03009027913262399); c = fma(c, e, 6.504847576502024); c = fma(c, e, 58.60283714484669);
-  c = fma(c, e, 275.0492627924299); c = fma(c, e, 1612.4245252438795); c = fma(c, e, 460.6487249985994);
-  c = fma(c, e, 15.382615282179595); c = fma(c, e, 0.02969737949090831); c = fma(c, e, 6.087136671592452e-6);
-  c = fma(c, e, 1.4170364808063119e-10); c = fma(c, e, 3.1955868410879504e-16);
-  c = fma(c, e, 4.123605749683891e-23); c = fma(c, e, 5.191934309650155e-32);
-  double d = 0.000024810902623582917;
-  d = fma(d, e, 0.09301685073435291); d = fma(d, e, 21.461303090563028); d = fma(d, e, 293.99144775704605);
-  d = fma(d, e, 590.2572000057821); d = fma(d, e, 15190.225535036281); d = fma(d, e, 1800.5461219450308);
-  d = fma(d, e, 60.85769171450653); d = fma(d, e, 0.13653226327408863); d = fma(d, e, 0.00003551782901018317);
-  d = fma(d, e, 1.1225580509306008e-9); d = fma(d, e, 3.5477700458515908e-15);
-  d = fma(d, e, 6.716598285341542e-22); d = fma(d, e, 1.4637868900982493e-30);
-  return c / d;
+  return horner(kQcdCa, e) / horner(kQcdCb, e);
 }
 
 // T(e): EquationOfState.cu:118-148; conformal T = (e/13.8997)^(1/4).
 template <int EOS>
 __device__ __forceinline__ double temperature(double e) {
   if (EOS == EOS_CONFORMAL) return pow(e / kEosFactor, 0.25);
-  double a = 1.5780479034557783e-6;
-  a = fma(a, e, 0.015421252394182246); a = fma(a, e, 14.055788949565482); a = fma(a, e, 1471.6180520527757);
-  a = fma(a, e, 14109.766109389702); a = fma(a, e, 6686.07424325115); a = fma(a, e, 207.48582344326206);
-  a = fma(a, e, 0.4873490574161924); a = fma(a, e, 0.000063810382643387); a = fma(a, e, 2.4954778310451065e-10);
-  a = fma(a, e, 8.014062800678687e-18); a = fma(a, e, 1.510073201405604e-29);
-  double b = 1.8472801679382593e-7;
-  b = fma(b, e, 0.003778342768228011); b = fma(b, e, 5.916312075925817); b = fma(b, e, 1051.0730543534657);
-  b = fma(b, e, 17965.67607192861); b = fma(b, e, 11179.193315394154); b = fma(b, e, 578.0778724946719);
-  b = fma(b, e, 2.316902328874072); b = fma(b, e, 0.0005036835870305458); b = fma(b, e, 2.998130743142826e-9);
-  b = fma(b, e, 1.3686372302041508e-16); b = fma(b, e, 7.558667139355393e-28);
-  return a / b;
+  return horner(kQcdTa, e) / horner(kQcdTb, e);
 }
 
 // e(T): EquationOfState.cu:150-204; conformal e = 13.8997 T^4. Host-callable: the host
@@ -149,28 +163,7 @@ constexpr int kNewtonMaxIters = 2000;
 // form (the reference evaluates the same polynomials from explicit powers,
 // EquationOfState.cu:30-116; the two agree to rounding).
 __device__ __forceinline__ void qcd_p_cs2(double e, double &p, double &cs2) {
-  double a = 1.9531729608963267e-11;
-  a = fma(a, e, 3.1188455176941583e-7); a = fma(a, e, 0.0009417586777847889); a = fma(a, e, 0.7158279081255019);
-  a = fma(a, e, 141.5073484468774); a = fma(a, e, 6340.448389300905); a = fma(a, e, 41913.439282708554);
-  a = fma(a, e, 334334.4309240126); a = fma(a, e, 1.6357487344679043e6); a = fma(a, e, 3.1729694865420084e6);
-  a = fma(a, e, 1.077580993288114e6); a = fma(a, e, 9737.845799644809); a = fma(a, e, -0.25181736420168666);
-  double b = 3.2581066229887368e-18;
-  b = fma(b, e, 5.928138360995685e-11); b = fma(b, e, 9.601103399348206e-7); b = fma(b, e, 0.002962497695527404);
-  b = fma(b, e, 2.3405487982094204); b = fma(b, e, 499.04919730607065); b = fma(b, e, 26452.34905933697);
-  b = fma(b, e, 278581.2989342773); b = fma(b, e, 1.7851642641834426e6); b = fma(b, e, 1.3512402226067686e7);
-  b = fma(b, e, 2.0931169138134286e7); b = fma(b, e, 4.0574329080826794e6); b = fma(b, e, 45829.44617893836);
-  double c = 8.189430244031285e-6;
-  c = fma(c, e, 0.03009027913262399); c = fma(c, e, 6.504847576502024); c = fma(c, e, 58.60283714484669);
-  c = fma(c, e, 275.0492627924299); c = fma(c, e, 1612.4245252438795); c = fma(c, e, 460.6487249985994);
-  c = fma(c, e, 15.382615282179595); c = fma(c, e, 0.02969737949090831); c = fma(c, e, 6.087136671592452e-6);
-  c = fma(c, e, 1.4170364808063119e-10); c = fma(c, e, 3.1955868410879504e-16);
-  c = fma(c, e, 4.123605749683891e-23); c = fma(c, e, 5.191934309650155e-32);
-  double d = 0.000024810902623582917;
-  d = fma(d, e, 0.09301685073435291); d = fma(d, e, 21.461303090563028); d = fma(d, e, 293.99144775704605);
-  d = fma(d, e, 590.2572000057821); d = fma(d, e, 15190.225535036281); d = fma(d, e, 1800.5461219450308);
-  d = fma(d, e, 60.85769171450653); d = fma(d, e, 0.13653226327408863); d = fma(d, e, 0.00003551782901018317);
-  d = fma(d, e, 1.1225580509306008e-9); d = fma(d, e, 3.5477700458515908e-15);
-  d = fma(d, e, 6.716598285341542e-22); d = fma(d, e, 1.4637868900982493e-30);
+  const double a = horner(kQcdPa, e), b = horner(kQcdPb, e), c = horner(kQcdCa, e), d = horner(kQcdCb, e);
   p = a / b;
   cs2 = c / d;
 }
@@ -178,45 +171,16 @@ __device__ __forceinline__ void qcd_p_cs2(double e, double &p, double &cs2) {
 // The four polynomials of the QCD fit, p = pa/pb and c_s^2 = ca/cb, without the divisions (the
 // Newton update below shares one reciprocal between them).
 __device__ __forceinline__ void qcd_poly(double e, double &pa, double &pb, double &ca, double &cb) {
-  double a = 1.9531729608963267e-11;
-  a = fma(a, e, 3.1188455176941583e-7); a = fma(a, e, 0.0009417586777847889); a = fma(a, e, 0.7158279081255019);
-  a = fma(a, e, 141.5073484468774); a = fma(a, e, 6340.448389300905); a = fma(a, e, 41913.439282708554);
-  a = fma(a, e, 334334.4309240126); a = fma(a, e, 1.6357487344679043e6); a = fma(a, e, 3.1729694865420084e6);
-  a = fma(a, e, 1.077580993288114e6); a = fma(a, e, 9737.845799644809); a = fma(a, e, -0.25181736420168666);
-  double b = 3.2581066229887368e-18;
-  b = fma(b, e, 5.928138360995685e-11); b = fma(b, e, 9.601103399348206e-7); b = fma(b, e, 0.002962497695527404);
-  b = fma(b, e, 2.3405487982094204); b = fma(b, e, 499.04919730607065); b = fma(b, e, 26452.34905933697);
-  b = fma(b, e, 278581.2989342773); b = fma(b, e, 1.7851642641834426e6); b = fma(b, e, 1.3512402226067686e7);
-  b = fma(b, e, 2.0931169138134286e7); b = fma(b, e, 4.0574329080826794e6); b = fma(b, e, 45829.44617893836);
-  double c = 8.189430244031285e-6;
-  c = fma(c, e, 0.03009027913262399); c = fma(c, e, 6.504847576502024); c = fma(c, e, 58.60283714484669);
-  c = fma(c, e, 275.0492627924299); c = fma(c, e, 1612.4245252438795); c = fma(c, e, 460.6487249985994);
-  c = fma(c, e, 15.382615282179595); c = fma(c, e, 0.02969737949090831); c = fma(c, e, 6.087136671592452e-6);
-  c = fma(c, e, 1.4170364808063119e-10); c = fma(c, e, 3.1955868410879504e-16);
-  c = fma(c, e, 4.123605749683891e-23); c = fma(c, e, 5.191934309650155e-32);
-  double d = 0.000024810902623582917;
-  d = fma(d, e, 0.09301685073435291); d = fma(d, e, 21.461303090563028); d = fma(d, e, 293.99144775704605);
-  d = fma(d, e, 590.2572000057821); d = fma(d, e, 15190.225535036281); d = fma(d, e, 1800.5461219450308);
-  d = fma(d, e, 60.85769171450653); d = fma(d, e, 0.13653226327408863); d = fma(d, e, 0.00003551782901018317);
-  d = fma(d, e, 1.1225580509306008e-9); d = fma(d, e, 3.5477700458515908e-15);
-  d = fma(d, e, 6.716598285341542e-22); d = fma(d, e, 1.4637868900982493e-30);
-  pa = a; pb = b; ca = c; cb = d;
+  pa = horner(kQcdPa, e);
+  pb = horner(kQcdPb, e);
+  ca = horner(kQcdCa, e);
+  cb = horner(kQcdCb, e);
 }
 
 // The two polynomials of p = pa/pb alone.
 __device__ __forceinline__ void qcd_poly_p(double e, double &pa, double &pb) {
-  double a = 1.9531729608963267e-11;
-  a = fma(a, e, 3.1188455176941583e-7); a = fma(a, e, 0.0009417586777847889); a = fma(a, e, 0.7158279081255019);
-  a = fma(a, e, 141.5073484468774); a = fma(a, e, 6340.448389300905); a = fma(a, e, 41913.439282708554);
-  a = fma(a, e, 334334.4309240126); a = fma(a, e, 1.6357487344679043e6); a = fma(a, e, 3.1729694865420084e6);
-  a = fma(a, e, 1.077580993288114e6); a = fma(a, e, 9737.845799644809); a = fma(a, e, -0.25181736420168666);
-  double b = 3.2581066229887368e-18;
-  b = fma(b, e, 5.928138360995685e-11); b = fma(b, e, 9.601103399348206e-7); b = fma(b, e, 0.002962497695527404);
-  b = fma(b, e, 2.3405487982094204); b = fma(b, e, 499.04919730607065); b = fma(b, e, 26452.34905933697);
-  b = fma(b, e, 278581.2989342773); b = fma(b, e, 1.7851642641834426e6); b = fma(b, e, 1.3512402226067686e7);
-  b = fma(b, e, 2.0931169138134286e7); b = fma(b, e, 4.0574329080826794e6); b = fma(b, e, 45829.44617893836);
-  pa = a;
-  pb = b;
+  pa = horner(kQcdPa, e);
+  pb = horner(kQcdPb, e);
 }
 
 // The Newton update of EnergyMomentumTensor.cu:22-40 at an iterate e0 where the fit's

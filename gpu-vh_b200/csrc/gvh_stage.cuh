@@ -57,6 +57,8 @@ struct StageArgs {
   unsigned *status;       // or-ed STATUS_* bits
   double *diag;           // stage 2, optional: regulation factor (component 0) and the centre's
                           // q^n pi^{mu nu}, Pi (components 13..23) for the validity diagnostics
+  unsigned long long *speed_max;  // stage 1, optional: running max of a / dx_axis over cells, as
+                                  // the bit pattern of a non-negative double (see kt_stage_kernel)
 };
 
 // Components of the validity block (VALIDITY_DOMAIN, DynamicalVariables.cuh:82-98, in that
@@ -217,10 +219,11 @@ __device__ __forceinline__ void axis_pi_sources(const StageArgs &a, int s, int a
   }
 }
 
+// Returns the axis's local propagation speed, max(a(i+1/2), a(i-1/2)) (SpectralRadius.cu:17-30).
 template <int EOS, bool SHEAR, bool BULK, bool MIXED>
-__device__ __forceinline__ void axis_update(const StageArgs &a, int s, int axis, int idx, int n_axis, int stride,
-                                            double inv_spacing, const GuessEos &g0, const double *uc, double *out,
-                                            double *cache, unsigned &status) {
+__device__ __forceinline__ double axis_update(const StageArgs &a, int s, int axis, int idx, int n_axis, int stride,
+                                              double inv_spacing, const GuessEos &g0, const double *uc, double *out,
+                                              double *cache, unsigned &status) {
   using R = typename std::conditional<MIXED, float, double>::type;
   constexpr int NQ = NComp<SHEAR, BULK>::value;
   const int o[5] = {(max(idx - 2, 0) - idx) * stride, (max(idx - 1, 0) - idx) * stride, 0,
@@ -258,6 +261,7 @@ __device__ __forceinline__ void axis_update(const StageArgs &a, int s, int axis,
       out[n * kBlock] += (double)(r * half_inv_d) * a.dt;
     }
   }
+  return fmax(fd.af, fd.ab);
 }
 
 // Shared memory of one stage block: the running update (NQ per thread) and the half-cell
@@ -437,13 +441,12 @@ __device__ __forceinline__ double stage_finish(const StageArgs &a, long long s, 
   return pr.e;
 }
 
+// speed: max over the three axes of the local propagation speed over the lattice spacing,
+// a / dx_axis (the CFL bound of the step is dt times its maximum over cells).
 template <int EOS, bool SHEAR, bool BULK, bool STAGE2, bool MIXED>
-__device__ __forceinline__ double stage_cell(const StageArgs &a, long long id) {
+__device__ __forceinline__ double stage_cell_ijk(const StageArgs &a, int i, int j, int k, double &speed) {
   using R = typename std::conditional<MIXED, float, double>::type;
   constexpr int NQ = NComp<SHEAR, BULK>::value;
-  const int i = (int)(id % a.nx);
-  const int j = (int)((id / a.nx) % a.ny);
-  const int k = (int)(id / ((long long)a.nx * a.ny));
   const long long s = i + a.sy * j + a.sz * k;
   unsigned status = 0;
 
@@ -463,26 +466,55 @@ __device__ __forceinline__ double stage_cell(const StageArgs &a, long long id) {
 
   // ---- flux divergence along x, y, eta (EulerStep.cu:1011-1277) -------------------------
   const GuessEos g0 = guess_eos<EOS>(ePrev);
+  speed = 0.0;
 #pragma unroll 1
   for (int axis = 0; axis < 3; ++axis) {
     const int idx = axis == 0 ? i : axis == 1 ? j : k;
     const int n_axis = axis == 0 ? a.nx : axis == 1 ? a.ny : a.nz;
     const int stride = axis == 0 ? 1 : axis == 1 ? (int)a.sy : (int)a.sz;
     const double inv_spacing = axis == 0 ? a.inv_dx : axis == 1 ? a.inv_dy : a.inv_dz;
-    axis_update<EOS, SHEAR, BULK, MIXED>(a, (int)s, axis, idx, n_axis, stride, inv_spacing, g0, uc, out, cache,
-                                         status);
+    const double as = axis_update<EOS, SHEAR, BULK, MIXED>(a, (int)s, axis, idx, n_axis, stride, inv_spacing, g0,
+                                                           uc, out, cache, status);
+    speed = fmax(speed, as * inv_spacing);
   }
 
   return stage_finish<EOS, SHEAR, BULK, STAGE2, kBlock>(a, s, out, g0, status);
 }
 
+// The cell with interior index id (i fastest).
+template <int EOS, bool SHEAR, bool BULK, bool STAGE2, bool MIXED>
+__device__ __forceinline__ double stage_cell(const StageArgs &a, long long id, double &speed) {
+  const int i = (int)(id % a.nx);
+  const int j = (int)((id / a.nx) % a.ny);
+  const int k = (int)(id / ((long long)a.nx * a.ny));
+  return stage_cell_ijk<EOS, SHEAR, BULK, STAGE2, MIXED>(a, i, j, k, speed);
+}
+
+// The grid of a stage launch: one block per kBlock consecutive cells (interior index order).
+// (Blocks of 16x8 and 32x4 cells of one eta plane were measured too: the same time per step
+// on the 131x131x61 event, so the stencil's y and eta neighbours do not limit the kernel.)
+inline dim3 stage_grid(long long ncells) { return dim3((unsigned)((ncells + kBlock - 1) / kBlock)); }
+
 // One RK substep over one lattice: one thread per interior cell. Launch with
 // stage_smem_bytes<SHEAR, BULK>() of dynamic shared memory (above the 48 KB default: the
 // launcher raises the kernel's cudaFuncAttributeMaxDynamicSharedMemorySize first).
+//
+// Stage 1 with a.speed_max set also reduces the cells' speed (a / dx_axis, stage_cell) to one
+// maximum: a warp-shuffle max over the warp's cells, then one atomic max per warp on the
+// value's bit pattern (for non-negative doubles the integer order of the bits is the numeric
+// order). It is a by-product of the face recoveries the step does anyway: the step keeps the
+// caller's dt.
 template <int EOS, bool SHEAR, bool BULK, bool STAGE2, bool MIXED>
 __global__ void __launch_bounds__(kBlock, GVH_MIN_BLOCKS) kt_stage_kernel(const StageArgs a) {
   const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (id < a.ncells) stage_cell<EOS, SHEAR, BULK, STAGE2, MIXED>(a, id);
+  double speed = 0.0;
+  if (id < a.ncells) stage_cell<EOS, SHEAR, BULK, STAGE2, MIXED>(a, id, speed);
+  if (!STAGE2 && a.speed_max) {
+    unsigned long long b = (unsigned long long)__double_as_longlong(fmax(speed, 0.0));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) b = max(b, __shfl_xor_sync(0xffffffffu, b, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(a.speed_max, b);
+  }
 }
 
 // Raises a stage kernel's dynamic shared-memory limit to what it is launched with. A kernel

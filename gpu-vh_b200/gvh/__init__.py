@@ -81,7 +81,7 @@ EXPORTS = [
     "gvh_default_options", "gvh_create", "gvh_destroy", "gvh_num_conserved", "gvh_num_fields",
     "gvh_num_lattice_cells", "gvh_set_primitive_state", "gvh_set_state", "gvh_get_state", "gvh_rk2_step",
     "gvh_status", "gvh_clear_status", "gvh_synchronize", "gvh_launches_per_step", "gvh_last_error",
-    "gvh_set_stream", "gvh_max_energy_density", "gvh_set_state_async", "gvh_get_state_async", "gvh_join_async",
+    "gvh_set_stream", "gvh_max_energy_density", "gvh_max_propagation_speed", "gvh_set_state_async", "gvh_get_state_async", "gvh_join_async",
 ]
 
 
@@ -117,6 +117,7 @@ def load(path: str | None = None):
     L.gvh_launches_per_step.argtypes = [vp]
     L.gvh_set_stream.argtypes = [vp, vp]
     L.gvh_max_energy_density.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
+    L.gvh_max_propagation_speed.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
     L.gvh_last_error.restype = ctypes.c_char_p
     if path is None:
         _lib = L
@@ -295,6 +296,12 @@ class Lattice:
     def max_energy_density(self) -> float:
         v = ctypes.c_double()
         _check(self._L.gvh_max_energy_density(self._h, ctypes.byref(v)), "gvh_max_energy_density")
+        return v.value
+
+    def max_propagation_speed(self) -> float:
+        """Max of a / dx_axis (fm^-1) over the steps since the last call (the CFL bound)."""
+        v = ctypes.c_double()
+        _check(self._L.gvh_max_propagation_speed(self._h, ctypes.byref(v)), "gvh_max_propagation_speed")
         return v.value
 
     def set_stream(self, stream_ptr: int | None):

@@ -195,6 +195,18 @@ const char *gvh_noalloc_last_error(void);
  * the lattice to the host. Synchronises the handle's stream. */
 int gvh_max_energy_density(gvh_handle *h, double *out);
 
+/* The CFL bound of the step: the largest local propagation speed over the lattice spacing,
+ * max over interior cells, both faces and the three axes of a / dx_axis, where a is the KT
+ * spectral radius max(|u^i/u^tau| left, |u^i/u^tau| right) of the face
+ * (SpectralRadius.cu:17-30, LocalPropagationSpeed.cu:15-24), in fm^-1 (dtau times it is the
+ * CFL number). The first stage of every gvh_rk2_step keeps a running maximum of it, reduced on
+ * the device by warp shuffles from the face recoveries the step does anyway; the step itself
+ * keeps the caller's dt, as the reference does. Returns the maximum over the steps since the
+ * previous call (or since gvh_create) and starts a new one; 0 before any step. Synchronises
+ * the handle's stream. (The reference computes these speeds inside its flux and keeps no
+ * maximum.) */
+int gvh_max_propagation_speed(gvh_handle *h, double *out);
+
 /* Validity diagnostics of the fluid-dynamic description (checkValidityKernel,
  * HydrodynamicValidity.cu:18-226, and the regulation factor of RegulateDissipativeCurrents.cu:132):
  * when enabled, every gvh_rk2_step also computes them for the new level, one extra kernel

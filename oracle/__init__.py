@@ -81,6 +81,8 @@ def _load_oracle():
             getattr(L, fn).argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         L.kt_rk2_step.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_double]
         L.kt_rk2_step.restype = None
+        L.kt_max_propagation_speed.argtypes = [ctypes.c_void_p]
+        L.kt_max_propagation_speed.restype = ctypes.c_double
         for fn in ("kt_equilibrium_pressure", "kt_speed_of_sound_squared", "kt_effective_temperature",
                    "kt_equilibrium_energy_density"):
             getattr(L, fn).argtypes = [ctypes.POINTER(KtParams), ctypes.c_double]
@@ -164,6 +166,10 @@ class OracleLattice(_Base):
         self._L.kt_rk2_step(self._h, t, dt, T_reg)
 
     # scalar physics, for unit tests
+    def max_propagation_speed(self) -> float:
+        """Max of a / dx_axis over the predictor stages since the last call."""
+        return self._L.kt_max_propagation_speed(self._h)
+
     def pressure(self, e):
         return self._L.kt_equilibrium_pressure(ctypes.byref(self._p), e)
 

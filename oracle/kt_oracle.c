@@ -208,7 +208,7 @@ static double approximate_derivative(double theta, double x, double y, double z)
  * `stencil` holds the 5 points (i-2..i+2) of each component; `forward` selects the face
  * i+1/2 (else i-1/2); `axis` 1,2,3 = x,y,eta. */
 static void kt_flux(const kt_params *P, int nq, const double *stencil, double *H, int forward, int axis, double t,
-                    double ePrev) {
+                    double ePrev, double *a_out) {
 	double qR[KT_MAX_NQ], qL[KT_MAX_NQ];
 	const double th = P->theta;
 	for (int n = 0; n < nq; ++n) {
@@ -227,6 +227,7 @@ static void kt_flux(const kt_params *P, int nq, const double *stencil, double *H
 	kt_get_inferred_variables(P, t, qL, ePrev, &eL, &pL, &utL, &uL[0], &uL[1], &uL[2]);
 	double vR = uR[axis - 1], vL = uL[axis - 1];
 	double a = fmax(fabs(vL / utL), fabs(vR / utR));
+	*a_out = a;
 	for (int n = 0; n < nq; ++n) {
 		double FqR = vR * qR[n] / utR;
 		double FqL = vL * qL[n] / utL;
@@ -400,6 +401,10 @@ struct kt_lattice {
 	double *q[KT_MAX_NQ], *Q[KT_MAX_NQ], *qS[KT_MAX_NQ];
 	double *e, *p, *u[4], *up[4], *uS[4];
 	double *block;
+	/* max over the axes of a / dx_axis per cell in the predictor stage (the CFL bound,
+	 * SpectralRadius.cu:17-30), and its running maximum over cells and steps */
+	double *speed;
+	double speed_max;
 };
 
 static int idx(const kt_lattice *L, int i, int j, int k) { return i + L->ncx * (j + L->ncy * k); }
@@ -425,12 +430,14 @@ kt_lattice *kt_create(const kt_params *P) {
 	for (int m = 0; m < 4; ++m) { L->u[m] = b; b += L->ng; }
 	for (int m = 0; m < 4; ++m) { L->up[m] = b; b += L->ng; }
 	for (int m = 0; m < 4; ++m) { L->uS[m] = b; b += L->ng; }
+	L->speed = (double *)calloc(L->ng, sizeof(double));
 	return L;
 }
 
 void kt_destroy(kt_lattice *L) {
 	if (!L) return;
 	free(L->block);
+	free(L->speed);
 	free(L);
 }
 
@@ -528,9 +535,11 @@ static void euler_axis_cell(kt_lattice *L, int s, int axis, double t, double **c
 	double I[5 * KT_MAX_NQ], H[KT_MAX_NQ], result[KT_MAX_NQ];
 	for (int n = 0; n < nq; ++n)
 		for (int o = 0; o < 5; ++o) I[5 * n + o] = cur[n][s + (o - 2) * stride];
-	kt_flux(P, nq, I, H, 1, axis, t, e[s]);
+	double af, ab;
+	kt_flux(P, nq, I, H, 1, axis, t, e[s], &af);
 	for (int n = 0; n < nq; ++n) result[n] = -H[n];
-	kt_flux(P, nq, I, H, 0, axis, t, e[s]);
+	kt_flux(P, nq, I, H, 0, axis, t, e[s], &ab);
+	L->speed[s] = fmax(L->speed[s], fmax(af, ab) * (1.0 / d));
 	for (int n = 0; n < nq; ++n) {
 		result[n] += H[n];
 		result[n] /= d;
@@ -673,7 +682,9 @@ static void convex_combination(kt_lattice *L, double **q, double **Q) {
  * (line 137) writes diagnostics only. */
 void kt_rk2_step(kt_lattice *L, double t, double dt, double T_reg) {
 	double *tmp[KT_MAX_NQ];
+	memset(L->speed, 0, L->ng * sizeof(double));
 	euler_step(L, t, L->q, L->qS, L->e, L->p, L->u, L->up);
+	for (size_t s = 0; s < L->ng; ++s) L->speed_max = fmax(L->speed_max, L->speed[s]);
 	t += dt;
 	set_inferred(L, L->qS, L->e, L->p, L->uS, t);
 	regulate(L, t, L->qS, L->e, L->p, L->uS, T_reg);
@@ -689,6 +700,14 @@ void kt_rk2_step(kt_lattice *L, double t, double dt, double T_reg) {
 	memcpy(tmp, L->q, sizeof(tmp));
 	memcpy(L->q, L->Q, sizeof(tmp));
 	memcpy(L->Q, tmp, sizeof(tmp));
+}
+
+/* The running maximum of a / dx_axis over cells, faces, axes and the predictor stages of the
+ * steps since the last call; it starts again at 0. */
+double kt_max_propagation_speed(kt_lattice *L) {
+	double v = L->speed_max;
+	L->speed_max = 0;
+	return v;
 }
 
 /* Full state: nq conserved components, e, p, u(4), up(4); a null up pointer means up = u. */

@@ -32,6 +32,7 @@ int kt_set_state(kt_lattice *L, const double *const *fields);
 int kt_get_state(const kt_lattice *L, double *const *fields);
 int kt_set_primitive_state(kt_lattice *L, const double *const *prim);
 void kt_rk2_step(kt_lattice *L, double t, double dt, double T_reg);
+double kt_max_propagation_speed(kt_lattice *L);
 
 double kt_equilibrium_pressure(const kt_params *P, double e);
 double kt_speed_of_sound_squared(const kt_params *P, double e);

@@ -294,3 +294,27 @@ def test_non_converging_newton_takes_the_damped_phase():
         assert np.isfinite(sg[k]).all()
         err = rel_err(G.interior(sg[k]), O.interior(so[k]))
         assert err <= DAMPED_TOL, f"{k}: {err:.3e}"
+
+
+@pytest.mark.parametrize("case", ["conf_shear", "qcd_bulk", "qcd_bulk_dilute_2d"])
+def test_cfl_speed_maximum_matches_oracle(case):
+    """The stage kernel's warp-shuffle maximum of the local propagation speed over the
+    lattice spacing (max over cells, faces and axes of a / dx_axis, SpectralRadius.cu:17-30)
+    against the oracle's maximum over the same predictor stages: after the first step, then
+    over the next three steps together (the running maximum restarts at each read)."""
+    lat_kw, steps, T_reg, st_kw = make_golden.CASES[case]
+    G = gvh.Lattice(**lat_kw)
+    O = oracle.OracleLattice(**lat_kw)
+    prim = rich_state(G, **st_kw)
+    G.set_primitive(prim)
+    O.set_primitive(prim)
+    assert G.max_propagation_speed() == 0.0
+    t = make_golden.TAU0
+    for block in ([1], [2, 3, 4]):
+        for n in block:
+            G.step(t, lat_kw["dt"], T_reg)
+            O.step(t, lat_kw["dt"], T_reg)
+            t = make_golden.TAU0 + n * lat_kw["dt"]
+        a, b = G.max_propagation_speed(), O.max_propagation_speed()
+        assert b > 0
+        assert abs(a - b) <= tol_for(lat_kw) * b, (case, block, a, b)
