@@ -6,16 +6,22 @@
 //    e, pA, pB, u[3] in the interior-only layout of gvh_stage.cuh). No cudaMalloc happens
 //    while the batch runs; admission fails cleanly (GVH_ERR_NOMEM) when the arena is full.
 //  * Every event's scalars, buffer pointers, time, step count, status word and freeze-out
-//    bookkeeping live in a device array of EventDev. A persistent stage kernel walks a packed
-//    queue of 128-cell tiles (tile -> event table, also on the device) with a grid sized to
-//    the GPU, so one launch covers every event whatever its lattice.
+//    bookkeeping live in a device array of EventDev. The stage kernel walks a packed queue
+//    of 128-cell tiles (tile -> event table, also on the device), so one launch covers every
+//    event whatever its lattice. A tile is 128 consecutive cells of its event, or a block of
+//    TX x (128 / TX) cells of one eta plane (the tile shape, chosen by the autotuner).
 //  * One RK2 step is three launches -- stage 1 over all tiles, stage 2 over all tiles, a
 //    per-event finish kernel (advance time, rotate the u buffers, freeze-out count) --
 //    captured once into a CUDA graph and replayed every step. Pointers in the graph never
 //    change: admissions and retirements only rewrite the device tables between replays.
 //  * Freeze-out follows the reference's stop rule (HydroPlugin.cpp:396-413): after every
 //    step the maximum interior e is compared with e(T_fo); an event is finished once that
-//    has held FOFREQ+1 = 11 times (the reference's counter is cumulative, never reset).
+//    has held FOFREQ+1 = 11 times (the reference's counter is cumulative, never reset), and
+//    from then on it is not advanced (the reference's loop ends there).
+//  * Nothing in admission, retirement or a serving round waits for the device: the initial
+//    state goes through a pinned staging ring, table updates through pinned buffers or
+//    kernel parameters, and a round ends with a kernel that copies every event's bookkeeping
+//    into mapped host memory, so the host reads round k while round k+1 runs.
 #include <cuda_runtime.h>
 #include <stdarg.h>
 #include <stdio.h>
@@ -70,6 +76,7 @@ struct EventDev {
   int frozen_checks;
   unsigned long long emax_bits;  // running max of e during stage 2 (bit pattern of e >= 0)
   double emax_last;              // max e after the last completed step
+  int done;                      // frozen out: no further steps
 };
 
 __device__ __forceinline__ StageArgs make_args(EventDev &E, bool stage2) {
@@ -100,18 +107,39 @@ __device__ __forceinline__ StageArgs make_args(EventDev &E, bool stage2) {
   return a;
 }
 
-// Persistent stage kernel over the packed tile queue of every active event.
+// The cell of thread t in local tile lt of an event: tile_x == 0, 128 consecutive cells
+// (interior index order); tile_x > 0, a tile_x x (kBlock / tile_x) block of one eta plane.
+__device__ __forceinline__ bool tile_cell(const EventDev &E, int tile_x, int lt, int t, int &i, int &j, int &k) {
+  if (tile_x == 0) {
+    const long long id = (long long)lt * kBlock + t;
+    i = (int)(id % E.nx);
+    j = (int)((id / E.nx) % E.ny);
+    k = (int)(id / ((long long)E.nx * E.ny));
+    return id < E.ncells;
+  }
+  const int tile_y = kBlock / tile_x;
+  const int tx = (E.nx + tile_x - 1) / tile_x, ty = (E.ny + tile_y - 1) / tile_y;
+  i = (lt % tx) * tile_x + t % tile_x;
+  j = ((lt / tx) % ty) * tile_y + t / tile_x;
+  k = lt / (tx * ty);
+  return i < E.nx && j < E.ny;
+}
+
+// Stage kernel over the packed tile queue of every active event (one block per tile, or a
+// persistent grid walking the queue).
 template <int EOS, bool SHEAR, bool BULK, bool STAGE2, bool MIXED>
 __global__ void __launch_bounds__(kBlock, GVH_MIN_BLOCKS)
-    batch_stage_kernel(EventDev *ev, const int *__restrict__ tile_event, const int *__restrict__ ntiles_p) {
+    batch_stage_kernel(EventDev *ev, const int *__restrict__ tile_event, const int *__restrict__ ntiles_p,
+                       int tile_x) {
   const int ntiles = *ntiles_p;
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     EventDev &E = ev[tile_event[tile]];
-    if (!E.active) continue;
+    if (!E.active || E.done) continue;
     const StageArgs a = make_args(E, STAGE2);
-    const long long id = (long long)(tile - E.first_tile) * kBlock + threadIdx.x;
+    int i, j, k;
     double en = 0.0, speed;
-    if (id < a.ncells) en = stage_cell<EOS, SHEAR, BULK, STAGE2, MIXED>(a, id, speed);
+    if (tile_cell(E, tile_x, tile - E.first_tile, threadIdx.x, i, j, k))
+      en = stage_cell_ijk<EOS, SHEAR, BULK, STAGE2, MIXED>(a, i, j, k, speed);
     if (STAGE2) {
       unsigned long long b = __double_as_longlong(fmax(en, 0.0));
 #pragma unroll
@@ -127,13 +155,59 @@ __global__ void batch_finish_kernel(EventDev *ev, int nslots) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nslots) return;
   EventDev &E = ev[i];
-  if (!E.active) return;
+  if (!E.active || E.done) return;
   E.step += 1;
   const int nc = E.ufree, np = E.ucur, nf = E.uprev;
   E.ucur = nc; E.uprev = np; E.ufree = nf;
   E.emax_last = __longlong_as_double(E.emax_bits);
   E.emax_bits = 0ull;
   if (E.emax_last <= E.e_fo) E.frozen_checks += 1;
+  if (E.frozen_checks >= kFreezeoutChecks) E.done = 1;
+}
+
+// Table updates as kernels (their arguments travel with the launch, so nothing on the host
+// has to outlive the call and nothing waits for the device).
+__global__ void event_write_kernel(EventDev *ev, int slot, EventDev E) { ev[slot] = E; }
+
+// The initial freeze-out check (the reference tests the state before every step, the first
+// one included: HydroPlugin.cpp:396-408), from the max-e reduction of the initial state.
+__global__ void event_first_check_kernel(EventDev *ev, int slot, const unsigned long long *emax_bits) {
+  EventDev &E = ev[slot];
+  E.emax_last = __longlong_as_double(*emax_bits);
+  E.frozen_checks = E.emax_last <= E.e_fo ? 1 : 0;
+}
+
+__global__ void event_deactivate_kernel(EventDev *ev, int slot) { ev[slot].active = 0; }
+
+// first_tile of every event from the tile -> event table (events' tiles are contiguous).
+__global__ void first_tiles_kernel(EventDev *ev, const int *__restrict__ tile_event, const int *__restrict__ ntiles_p) {
+  const int n = *ntiles_p;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+    if (t == 0 || tile_event[t] != tile_event[t - 1]) ev[tile_event[t]].first_tile = t;
+}
+
+// The end of a serving round: every slot's bookkeeping into mapped host memory, then the
+// round's ticket (after a system-scope fence, so a host that sees the ticket sees the rows).
+__global__ void publish_kernel(const EventDev *ev, int nslots, gvh_event_info *out, volatile long long *ticket_out,
+                               long long ticket) {
+  for (int i = threadIdx.x; i < nslots; i += blockDim.x) {
+    const EventDev &E = ev[i];
+    gvh_event_info r;
+    r.step = E.step;
+    r.tau = E.t0 + (double)E.step * E.dt;
+    r.max_energy_density = E.emax_last;
+    r.freezeout_energy_density = E.e_fo;
+    r.frozen_checks = E.frozen_checks;
+    r.frozen_out = E.frozen_checks >= kFreezeoutChecks;
+    r.status = E.status;
+    r.cells = E.ncells;
+    out[i] = r;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence_system();
+    *ticket_out = ticket;
+  }
 }
 
 struct HostEvent {
@@ -141,7 +215,23 @@ struct HostEvent {
   size_t off = 0, bytes = 0;
   int nx = 0, ny = 0, nz = 0;
   long long ncells = 0, ng = 0, cs = 0;
-  int ntiles = 0;
+  long long serial = 0;  // admission number: tells a re-used slot's events apart
+};
+
+// Tiles of an nx x ny x nz lattice for tile shape tile_x (see tile_cell).
+int tiles_of(int nx, int ny, int nz, int tile_x) {
+  if (tile_x == 0) return (int)(((long long)nx * ny * nz + kBlock - 1) / kBlock);
+  const int tile_y = kBlock / tile_x;
+  return ((nx + tile_x - 1) / tile_x) * ((ny + tile_y - 1) / tile_y) * nz;
+}
+
+// A pinned host buffer that the device copies from asynchronously, with the event that
+// marks the end of the last copy (the buffer is reused only after it).
+struct PinnedBuf {
+  void *h = nullptr;
+  size_t cap = 0;
+  cudaEvent_t done = nullptr;
+  bool pending = false;
 };
 
 }  // namespace
@@ -162,8 +252,20 @@ struct gvh_batch {
   unsigned long long *d_scratch = nullptr;
   cudaGraphExec_t graph = nullptr;
   int grid = 0;                          // persistent grid (blocks); 0 = one block per tile
+  int tile_x = 0;                        // tile shape (tile_cell): 0 = 128 consecutive cells
   int ntiles = 0;                        // tiles of the admitted events
   int active_slots = 0;                  // slots the finish kernel scans
+  long long next_serial = 1;
+  PinnedBuf prim_stage[2];               // initial states on their way to the device
+  int prim_next = 0;
+  PinnedBuf tile_stage[2];               // tile tables on their way to the device
+  int tile_next = 0;
+  // serving rounds: two snapshots in mapped host memory, alternating by ticket
+  gvh_event_info *snap_h[2] = {nullptr, nullptr}, *snap_d[2] = {nullptr, nullptr};
+  long long *ticket_h = nullptr, *ticket_d = nullptr;  // [2]: last ticket written per snapshot
+  cudaEvent_t round_start[2] = {nullptr, nullptr}, round_end[2] = {nullptr, nullptr};
+  long long next_ticket = 0;
+  std::vector<std::pair<int, long long>> round_events[2];  // (slot, serial) when queued
 };
 
 namespace {
@@ -208,22 +310,61 @@ void arena_free(gvh_batch *b, size_t off, size_t bytes) {
 
 int rebuild_graph(gvh_batch *b);
 
+// Makes a pinned buffer at least `bytes` long and free for reuse (its last copy finished).
+int pinned_reserve(PinnedBuf &p, size_t bytes) {
+  if (p.pending) {
+    BCUDA(cudaEventSynchronize(p.done));
+    p.pending = false;
+  }
+  if (p.cap >= bytes) return GVH_OK;
+  if (p.h) cudaFreeHost(p.h);
+  p.h = nullptr;
+  p.cap = 0;
+  if (cudaHostAlloc(&p.h, bytes, cudaHostAllocDefault) != cudaSuccess)
+    return bfail(GVH_ERR_NOMEM, "cannot allocate %zu bytes of pinned host memory", bytes);
+  p.cap = bytes;
+  if (!p.done) BCUDA(cudaEventCreateWithFlags(&p.done, cudaEventDisableTiming));
+  return GVH_OK;
+}
+
+int pinned_mark(gvh_batch *b, PinnedBuf &p) {
+  BCUDA(cudaEventRecord(p.done, b->stream));
+  p.pending = true;
+  return GVH_OK;
+}
+
+// The tile -> event table of the admitted events (each event's tiles contiguous, events in
+// slot order) and its count go to the device through a pinned buffer; first_tile of every
+// event is derived on the device. Nothing waits for the device unless the tile count changes
+// under a one-block-per-tile grid, which re-captures the step's graph.
 int rebuild_tiles(gvh_batch *b) {
-  std::vector<int> table;
-  int slots = 0;
+  int slots = 0, n = 0;
+  for (size_t i = 0; i < b->ev.size(); ++i)
+    if (b->ev[i].used) {
+      slots = (int)i + 1;
+      n += tiles_of(b->ev[i].nx, b->ev[i].ny, b->ev[i].nz, b->tile_x);
+    }
+  if (n > b->tile_capacity) return bfail(GVH_ERR_NOMEM, "tile table full");
+  PinnedBuf &pb = b->tile_stage[b->tile_next];
+  b->tile_next ^= 1;
+  int rc = pinned_reserve(pb, (size_t)(n + 1) * sizeof(int));
+  if (rc) return rc;
+  int *table = static_cast<int *>(pb.h);
+  int t = 0;
   for (size_t i = 0; i < b->ev.size(); ++i) {
     if (!b->ev[i].used) continue;
-    slots = (int)i + 1;
-    const int first = (int)table.size();
-    for (int t = 0; t < b->ev[i].ntiles; ++t) table.push_back((int)i);
-    BCUDA(cudaMemcpyAsync(&b->d_ev[i].first_tile, &first, sizeof(int), cudaMemcpyHostToDevice, b->stream));
+    const int m = tiles_of(b->ev[i].nx, b->ev[i].ny, b->ev[i].nz, b->tile_x);
+    for (int k = 0; k < m; ++k) table[t++] = (int)i;
   }
-  if ((int)table.size() > b->tile_capacity) return bfail(GVH_ERR_NOMEM, "tile table full");
-  const int n = (int)table.size();
-  if (n) BCUDA(cudaMemcpyAsync(b->d_tile_event, table.data(), n * sizeof(int), cudaMemcpyHostToDevice, b->stream));
-  BCUDA(cudaMemcpyAsync(b->d_ntiles, &n, sizeof(int), cudaMemcpyHostToDevice, b->stream));
-  // pageable sources: wait so the host vectors may go out of scope
-  BCUDA(cudaStreamSynchronize(b->stream));
+  table[n] = n;
+  if (n) BCUDA(cudaMemcpyAsync(b->d_tile_event, table, n * sizeof(int), cudaMemcpyHostToDevice, b->stream));
+  BCUDA(cudaMemcpyAsync(b->d_ntiles, table + n, sizeof(int), cudaMemcpyHostToDevice, b->stream));
+  if (n) {
+    first_tiles_kernel<<<(unsigned)std::min(1024, (n + 255) / 256), 256, 0, b->stream>>>(b->d_ev, b->d_tile_event,
+                                                                                         b->d_ntiles);
+    BCUDA(cudaGetLastError());
+  }
+  if ((rc = pinned_mark(b, pb))) return rc;
   b->active_slots = slots;
   const bool regrid = b->grid == 0 && n != b->ntiles;
   b->ntiles = n;
@@ -239,9 +380,9 @@ int launch_step_t(gvh_batch *b) {
   const int g = b->grid > 0 ? b->grid : (b->ntiles > 0 ? b->ntiles : 1);
   const size_t smem = stage_smem_bytes<SHEAR, BULK>();
   batch_stage_kernel<EOS, SHEAR, BULK, false, MIXED><<<g, kBlock, smem, b->stream>>>(b->d_ev, b->d_tile_event,
-                                                                                     b->d_ntiles);
+                                                                                     b->d_ntiles, b->tile_x);
   batch_stage_kernel<EOS, SHEAR, BULK, true, MIXED><<<g, kBlock, smem, b->stream>>>(b->d_ev, b->d_tile_event,
-                                                                                    b->d_ntiles);
+                                                                                    b->d_ntiles, b->tile_x);
   batch_finish_kernel<<<(kMaxEvents + 127) / 128, 128, 0, b->stream>>>(b->d_ev, kMaxEvents);
   BCUDA(cudaGetLastError());
   return GVH_OK;
@@ -363,6 +504,15 @@ int gvh_batch_create(const gvh_options *opts, long long arena_bytes, gvh_batch *
   ok = ok && cudaMalloc(&b->d_ntiles, sizeof(int)) == cudaSuccess;
   ok = ok && cudaMalloc(&b->d_scratch, sizeof(unsigned long long)) == cudaSuccess;
   ok = ok && cudaStreamCreateWithFlags(&b->own_stream, cudaStreamNonBlocking) == cudaSuccess;
+  for (int r = 0; r < 2 && ok; ++r) {
+    ok = cudaHostAlloc(&b->snap_h[r], kMaxEvents * sizeof(gvh_event_info), cudaHostAllocMapped) == cudaSuccess;
+    ok = ok && cudaHostGetDevicePointer(&b->snap_d[r], b->snap_h[r], 0) == cudaSuccess;
+    ok = ok && cudaEventCreate(&b->round_start[r]) == cudaSuccess;
+    ok = ok && cudaEventCreate(&b->round_end[r]) == cudaSuccess;
+  }
+  ok = ok && cudaHostAlloc(&b->ticket_h, 2 * sizeof(long long), cudaHostAllocMapped) == cudaSuccess;
+  ok = ok && cudaHostGetDevicePointer(&b->ticket_d, b->ticket_h, 0) == cudaSuccess;
+  if (ok) b->ticket_h[0] = b->ticket_h[1] = -1;
   if (!ok) {
     gvh_batch_destroy(b);
     return bfail(GVH_ERR_NOMEM, "gvh_batch_create: cannot allocate %lld bytes", arena_bytes);
@@ -392,6 +542,16 @@ int gvh_batch_destroy(gvh_batch *b) {
   cudaFree(b->d_ntiles);
   cudaFree(b->d_scratch);
   if (b->staging) cudaFree(b->staging);
+  for (PinnedBuf *pb : {&b->prim_stage[0], &b->prim_stage[1], &b->tile_stage[0], &b->tile_stage[1]}) {
+    if (pb->h) cudaFreeHost(pb->h);
+    if (pb->done) cudaEventDestroy(pb->done);
+  }
+  for (int r = 0; r < 2; ++r) {
+    if (b->snap_h[r]) cudaFreeHost(b->snap_h[r]);
+    if (b->round_start[r]) cudaEventDestroy(b->round_start[r]);
+    if (b->round_end[r]) cudaEventDestroy(b->round_end[r]);
+  }
+  if (b->ticket_h) cudaFreeHost(b->ticket_h);
   if (b->own_stream) cudaStreamDestroy(b->own_stream);
   delete b;
   return GVH_OK;
@@ -433,18 +593,34 @@ int gvh_batch_add_event(gvh_batch *b, const gvh_lattice_params *L, const gvh_hyd
   h.ncells = (long long)h.nx * h.ny * h.nz;
   h.ng = (long long)(h.nx + 4) * (h.ny + 4) * (h.nz + 4);
   h.bytes = event_bytes(b, h.ncells, &h.cs);
-  h.ntiles = (int)((h.ncells + kBlock - 1) / kBlock);
   if (!arena_alloc(b, h.bytes, &h.off)) return bfail(GVH_ERR_NOMEM, "arena full (%zu bytes needed)", h.bytes);
   h.used = true;
+  h.serial = b->next_serial++;
   int rc = ensure_staging(b, n_prim, h.ng);
   if (rc) { arena_free(b, h.off, h.bytes); return rc; }
-
+  // the initial state goes to the device through a pinned buffer: the host copy happens here,
+  // the transfer is queued behind the work in flight and nothing waits for it
+  PinnedBuf &pb = b->prim_stage[b->prim_next];
+  b->prim_next ^= 1;
+  const size_t fb = h.ng * sizeof(double);
+  if ((rc = pinned_reserve(pb, n_prim * fb))) { arena_free(b, h.off, h.bytes); return rc; }
   double *qA, *qB, *e, *pA, *pB, *u[3];
   event_pointers(b, h, &qA, &qB, &e, &pA, &pB, u);
   BCUDA(cudaMemsetAsync(b->arena + h.off, 0, h.bytes, b->stream));
-  const size_t fb = h.ng * sizeof(double);
-  for (int f = 0; f < n_prim; ++f)
-    BCUDA(cudaMemcpyAsync(b->staging + f * h.ng, prim[f], fb, cudaMemcpyDefault, b->stream));
+  for (int f = 0; f < n_prim; ++f) {
+    cudaPointerAttributes at;
+    const bool on_device = cudaPointerGetAttributes(&at, prim[f]) == cudaSuccess &&
+                           (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged);
+    cudaGetLastError();  // a plain host pointer is not an error
+    if (on_device) {
+      BCUDA(cudaMemcpyAsync(b->staging + f * h.ng, prim[f], fb, cudaMemcpyDeviceToDevice, b->stream));
+    } else {
+      memcpy(static_cast<char *>(pb.h) + f * fb, prim[f], fb);
+      BCUDA(cudaMemcpyAsync(b->staging + f * h.ng, static_cast<char *>(pb.h) + f * fb, fb, cudaMemcpyHostToDevice,
+                            b->stream));
+    }
+  }
+  if ((rc = pinned_mark(b, pb))) return rc;
   FieldTable dst = {};
   dst.p[0] = e;
   for (int m = 0; m < 4; ++m) dst.p[1 + m] = u[0] + m * h.cs;
@@ -457,15 +633,6 @@ int gvh_batch_add_event(gvh_batch *b, const gvh_lattice_params *L, const gvh_hyd
   else
     init_conserved_kernel<EOS_QCD><<<blocks, 256, 0, b->stream>>>(h.ncells, b->nq, h.cs, qA, e, pA, u[0], u[1], 0);
   BCUDA(cudaGetLastError());
-  // initial freeze-out check (the reference tests the state before every step, the first
-  // one included: HydroPlugin.cpp:396-408)
-  BCUDA(cudaMemsetAsync(b->d_scratch, 0, sizeof(unsigned long long), b->stream));
-  max_e_kernel<<<min(1024u, blocks), 256, 0, b->stream>>>(e, h.ncells, b->d_scratch);
-  unsigned long long emax_bits = 0;
-  BCUDA(cudaMemcpyAsync(&emax_bits, b->d_scratch, sizeof emax_bits, cudaMemcpyDeviceToHost, b->stream));
-  BCUDA(cudaStreamSynchronize(b->stream));
-  double emax0;
-  memcpy(&emax0, &emax_bits, sizeof emax0);
 
   EventDev E;
   memset(&E, 0, sizeof E);
@@ -490,9 +657,12 @@ int gvh_batch_add_event(gvh_batch *b, const gvh_lattice_params *L, const gvh_hyd
   E.qA = qA; E.qB = qB; E.e = e; E.pA = pA; E.pB = pB;
   for (int m = 0; m < 3; ++m) E.u[m] = u[m];
   E.ucur = 0; E.uprev = 1; E.ufree = 2;
-  E.emax_last = emax0;
-  E.frozen_checks = emax0 <= E.e_fo ? 1 : 0;
-  BCUDA(cudaMemcpyAsync(b->d_ev + slot, &E, sizeof E, cudaMemcpyHostToDevice, b->stream));
+  event_write_kernel<<<1, 1, 0, b->stream>>>(b->d_ev, slot, E);
+  // initial freeze-out check, on the device
+  BCUDA(cudaMemsetAsync(b->d_scratch, 0, sizeof(unsigned long long), b->stream));
+  max_e_kernel<<<min(1024u, blocks), 256, 0, b->stream>>>(e, h.ncells, b->d_scratch);
+  event_first_check_kernel<<<1, 1, 0, b->stream>>>(b->d_ev, slot, b->d_scratch);
+  BCUDA(cudaGetLastError());
   b->ev[slot] = h;
   rc = rebuild_tiles(b);
   if (rc) return rc;
@@ -503,8 +673,10 @@ int gvh_batch_add_event(gvh_batch *b, const gvh_lattice_params *L, const gvh_hyd
 int gvh_batch_remove_event(gvh_batch *b, int id) {
   if (!b || id < 0 || id >= (int)b->ev.size() || !b->ev[id].used) return bfail(GVH_ERR_INVALID, "bad event id");
   BCUDA(cudaSetDevice(b->device));
-  const int zero = 0;
-  BCUDA(cudaMemcpyAsync(&b->d_ev[id].active, &zero, sizeof zero, cudaMemcpyHostToDevice, b->stream));
+  // queued behind the work in flight, which may still read or write the event's memory; the
+  // memory's next user is queued after this, so reusing it at once is safe
+  event_deactivate_kernel<<<1, 1, 0, b->stream>>>(b->d_ev, id);
+  BCUDA(cudaGetLastError());
   arena_free(b, b->ev[id].off, b->ev[id].bytes);
   b->ev[id] = HostEvent();
   return rebuild_tiles(b);
@@ -605,41 +777,118 @@ int gvh_batch_set_grid(gvh_batch *b, int grid_blocks) {
   return rebuild_graph(b);
 }
 
-// Times `steps` real RK2 steps (the events do advance) with each candidate grid -- one
-// block per tile (0) and persistent grids of 1..GVH_MIN_BLOCKS blocks per SM -- and keeps
-// the fastest. Every candidate computes the same values; only the schedule differs.
+int gvh_batch_set_tile_shape(gvh_batch *b, int tile_x) {
+  if (!b || tile_x < 0 || tile_x > kBlock || (tile_x && kBlock % tile_x))
+    return bfail(GVH_ERR_INVALID, "tile_x must be 0 or a divisor of %d", kBlock);
+  BCUDA(cudaSetDevice(b->device));
+  b->tile_x = tile_x;
+  int rc = rebuild_tiles(b);
+  if (rc) return rc;
+  return rebuild_graph(b);  // the shape is a kernel argument of the captured step
+}
+
+int gvh_batch_tile_shape(const gvh_batch *b, int *tile_x, int *tile_y) {
+  if (!b) return GVH_ERR_INVALID;
+  if (tile_x) *tile_x = b->tile_x;
+  if (tile_y) *tile_y = b->tile_x ? kBlock / b->tile_x : 1;
+  return GVH_OK;
+}
+
+// Times `steps` real RK2 steps (the events do advance) with each candidate schedule -- tile
+// shapes 128 consecutive cells, 32 x 4 and 16 x 8 cells of an eta plane, each with one block
+// per tile (grid 0) and persistent grids of 1..GVH_MIN_BLOCKS blocks per SM -- and keeps the
+// fastest. Every candidate computes the same values; only the schedule differs.
 int gvh_batch_autotune(gvh_batch *b, int steps, int *chosen_grid) {
   if (!b || steps < 1) return bfail(GVH_ERR_INVALID, "bad arguments");
   BCUDA(cudaSetDevice(b->device));
-  int ntiles = 0;
-  for (const auto &h : b->ev) ntiles += h.used ? h.ntiles : 0;
-  std::vector<int> cands{0};
-  for (int k = 1; k <= GVH_MIN_BLOCKS; ++k) cands.push_back(b->num_sms * k);
+  std::vector<int> grids{0};
+  for (int k = 1; k <= GVH_MIN_BLOCKS; ++k) grids.push_back(b->num_sms * k);
+  const int shapes[] = {0, 32, 16};
   cudaEvent_t e0, e1;
   BCUDA(cudaEventCreate(&e0));
   BCUDA(cudaEventCreate(&e1));
   float best = 1e30f;
-  int best_grid = b->grid;
-  for (int g : cands) {
-    int rc = gvh_batch_set_grid(b, g);
+  int best_grid = b->grid, best_shape = b->tile_x;
+  for (int shape : shapes) {
+    b->tile_x = shape;
+    int rc = rebuild_tiles(b);
     if (rc) return rc;
-    BCUDA(cudaGraphLaunch(b->graph, b->stream));  // warm
-    BCUDA(cudaEventRecord(e0, b->stream));
-    for (int n = 0; n < steps; ++n) BCUDA(cudaGraphLaunch(b->graph, b->stream));
-    BCUDA(cudaEventRecord(e1, b->stream));
-    BCUDA(cudaEventSynchronize(e1));
-    float ms = 0;
-    BCUDA(cudaEventElapsedTime(&ms, e0, e1));
-    if (ms < best) {
-      best = ms;
-      best_grid = g;
+    for (int g : grids) {
+      if ((rc = gvh_batch_set_grid(b, g))) return rc;
+      BCUDA(cudaGraphLaunch(b->graph, b->stream));  // warm
+      BCUDA(cudaEventRecord(e0, b->stream));
+      for (int n = 0; n < steps; ++n) BCUDA(cudaGraphLaunch(b->graph, b->stream));
+      BCUDA(cudaEventRecord(e1, b->stream));
+      BCUDA(cudaEventSynchronize(e1));
+      float ms = 0;
+      BCUDA(cudaEventElapsedTime(&ms, e0, e1));
+      if (ms < best) {
+        best = ms;
+        best_grid = g;
+        best_shape = shape;
+      }
     }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  int rc = gvh_batch_set_grid(b, best_grid);
+  b->tile_x = best_shape;
+  int rc = rebuild_tiles(b);
+  if (rc) return rc;
+  rc = gvh_batch_set_grid(b, best_grid);
   if (chosen_grid) *chosen_grid = best_grid;
   return rc;
+}
+
+int gvh_batch_round(gvh_batch *b, int nsteps, long long *ticket) {
+  if (!b || nsteps < 0 || !ticket) return bfail(GVH_ERR_INVALID, "bad arguments");
+  BCUDA(cudaSetDevice(b->device));
+  const long long t = b->next_ticket++;
+  const int r = (int)(t & 1);
+  // the snapshot this round writes belongs to round t - 2: that round has finished (its copy
+  // to the host is in the stream before this one) once its end event has
+  if (t >= 2) BCUDA(cudaEventSynchronize(b->round_end[r]));
+  b->round_events[r].clear();
+  for (size_t i = 0; i < b->ev.size(); ++i)
+    if (b->ev[i].used) b->round_events[r].emplace_back((int)i, b->ev[i].serial);
+  BCUDA(cudaEventRecord(b->round_start[r], b->stream));
+  for (int n = 0; n < nsteps; ++n) BCUDA(cudaGraphLaunch(b->graph, b->stream));
+  publish_kernel<<<1, 256, 0, b->stream>>>(b->d_ev, std::max(1, b->active_slots), b->snap_d[r], b->ticket_d + r, t);
+  BCUDA(cudaGetLastError());
+  BCUDA(cudaEventRecord(b->round_end[r], b->stream));
+  *ticket = t;
+  return GVH_OK;
+}
+
+int gvh_batch_poll(gvh_batch *b, long long ticket, int max_events, int *event_ids, gvh_event_info *infos,
+                   int *n_events, double *round_ms) {
+  if (!b || !n_events || ticket < 0 || ticket >= b->next_ticket || max_events < 0 ||
+      (max_events > 0 && (!event_ids || !infos)))
+    return bfail(GVH_ERR_INVALID, "bad arguments");
+  if (ticket + 2 < b->next_ticket) return bfail(GVH_ERR_INVALID, "round %lld: its snapshot was overwritten", ticket);
+  BCUDA(cudaSetDevice(b->device));
+  const int r = (int)(ticket & 1);
+  BCUDA(cudaEventSynchronize(b->round_end[r]));
+  if (b->ticket_h[r] != ticket) return bfail(GVH_ERR_INTERNAL, "round %lld: snapshot not written", ticket);
+  if (round_ms) {
+    float ms = 0;
+    BCUDA(cudaEventElapsedTime(&ms, b->round_start[r], b->round_end[r]));
+    *round_ms = ms;
+  }
+  // the events of the round that are still admitted (a slot emptied or refilled since the
+  // round was queued reports nothing: its snapshot row belongs to the old event)
+  int n = 0;
+  for (const auto &se : b->round_events[r]) {
+    const int slot = se.first;
+    if (slot >= (int)b->ev.size() || !b->ev[slot].used || b->ev[slot].serial != se.second) continue;
+    if (n < max_events) {
+      event_ids[n] = slot;
+      infos[n] = b->snap_h[r][slot];
+    }
+    ++n;
+  }
+  *n_events = n;
+  if (n > max_events) return bfail(GVH_ERR_INVALID, "%d events do not fit in %d", n, max_events);
+  return GVH_OK;
 }
 
 }  // extern "C"

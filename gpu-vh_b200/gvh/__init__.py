@@ -340,7 +340,8 @@ BATCH_EXPORTS = [
     "gvh_batch_add_event", "gvh_batch_remove_event", "gvh_batch_num_events", "gvh_batch_free_bytes",
     "gvh_batch_active_cells", "gvh_batch_step", "gvh_batch_synchronize", "gvh_batch_event_info",
     "gvh_batch_get_state", "gvh_batch_launch_config", "gvh_batch_set_grid", "gvh_batch_autotune",
-    "gvh_batch_last_error",
+    "gvh_batch_last_error", "gvh_batch_set_tile_shape", "gvh_batch_tile_shape", "gvh_batch_round",
+    "gvh_batch_poll",
 ]
 EXPORTS += BATCH_EXPORTS
 
@@ -369,6 +370,11 @@ def _bind_batch(L):
     L.gvh_batch_launch_config.argtypes = [vp, ctypes.POINTER(ip), ctypes.POINTER(ip)]
     L.gvh_batch_set_grid.argtypes = [vp, ip]
     L.gvh_batch_autotune.argtypes = [vp, ip, ctypes.POINTER(ip)]
+    L.gvh_batch_set_tile_shape.argtypes = [vp, ip]
+    L.gvh_batch_tile_shape.argtypes = [vp, ctypes.POINTER(ip), ctypes.POINTER(ip)]
+    L.gvh_batch_round.argtypes = [vp, ip, ctypes.POINTER(ll)]
+    L.gvh_batch_poll.argtypes = [vp, ll, ip, ctypes.POINTER(ip), ctypes.POINTER(EventInfo), ctypes.POINTER(ip),
+                                 ctypes.POINTER(ctypes.c_double)]
     L.gvh_batch_last_error.restype = ctypes.c_char_p
     L._batch_bound = True
     return L
@@ -488,6 +494,34 @@ class Batch:
         g = ctypes.c_int()
         _bcheck(self._L.gvh_batch_autotune(self._h, int(steps), ctypes.byref(g)), "gvh_batch_autotune")
         return g.value
+
+    def set_tile_shape(self, tile_x):
+        _bcheck(self._L.gvh_batch_set_tile_shape(self._h, int(tile_x)), "gvh_batch_set_tile_shape")
+
+    @property
+    def tile_shape(self) -> tuple:
+        x, y = ctypes.c_int(), ctypes.c_int()
+        self._L.gvh_batch_tile_shape(self._h, ctypes.byref(x), ctypes.byref(y))
+        return x.value, y.value
+
+    def round(self, nsteps) -> int:
+        """Queue nsteps steps of every event and a snapshot of their bookkeeping; returns a
+        ticket for poll() (does not wait)."""
+        t = ctypes.c_longlong()
+        _bcheck(self._L.gvh_batch_round(self._h, int(nsteps), ctypes.byref(t)), "gvh_batch_round")
+        return t.value
+
+    def poll(self, ticket):
+        """Wait for round `ticket`; returns ({event id: EventInfo at the round's end} for the
+        events still admitted, the round's device time in ms)."""
+        n = max(1, len(self.events))
+        ids = (ctypes.c_int * n)()
+        infos = (EventInfo * n)()
+        cnt = ctypes.c_int()
+        ms = ctypes.c_double()
+        _bcheck(self._L.gvh_batch_poll(self._h, int(ticket), n, ids, infos, ctypes.byref(cnt), ctypes.byref(ms)),
+                "gvh_batch_poll")
+        return {ids[i]: infos[i] for i in range(cnt.value)}, ms.value
 
 
 # ---- freeze-out hypersurface ------------------------------------------------------------

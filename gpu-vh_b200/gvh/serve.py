@@ -100,8 +100,15 @@ def poisson_arrivals(rate: float, n: int, rng: np.random.Generator) -> list[floa
 
 
 class Server:
+    """The serving loop. Rounds of `steps_per_round` steps are queued `depth` ahead
+    (gvh_batch_round): while the device runs round k+1 the host reads round k's bookkeeping
+    from mapped memory (gvh_batch_poll), retires frozen-out events and admits new ones, whose
+    set-up is queued behind the rounds in flight. Nothing on the host waits for more than the
+    round it reads."""
+
     def __init__(self, arena_bytes: int, precision: str = "mixed", steps_per_round: int = 10, theta: float = 2.0,
-                 device: int = -1, autotune: bool = False, batch=None, max_resident_cells: int = 8_000_000):
+                 device: int = -1, autotune: bool = False, batch=None, max_resident_cells: int = 8_000_000,
+                 depth: int = 2):
         self.batch = batch if batch is not None else Batch(arena_bytes, conformal=False, shear=True, bulk=True,
                                                            precision=precision, theta=theta, device=device)
         self.steps_per_round = steps_per_round
@@ -110,18 +117,20 @@ class Server:
         self.max_resident_cells = max_resident_cells
         self.autotune = autotune
         self.tuned = False
+        self.depth = max(1, min(2, depth))  # a round's snapshot lives until two rounds later
 
     def run(self, requests: list[Request], time_limit: float | None = None) -> dict:
         B = self.batch
         pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
         waiting: collections.deque[Request] = collections.deque()
-        resident: dict[int, tuple[Request, float]] = {}
+        resident: dict[int, tuple[Request, float, int]] = {}  # id -> (request, admitted at, last step seen)
+        in_flight: collections.deque[int] = collections.deque()
         done: list[Completed] = []
         cell_updates = 0
         t0 = time.perf_counter()
         busy = 0.0
         ic_seconds = 0.0
-        while pending or waiting or resident:
+        while pending or waiting or resident or in_flight:
             now = time.perf_counter() - t0
             if time_limit is not None and now > time_limit:
                 break
@@ -142,32 +151,37 @@ class Server:
                 if eid is None:
                     break
                 waiting.popleft()
-                resident[eid] = (r, time.perf_counter() - t0)
-            if not resident:
+                resident[eid] = (r, time.perf_counter() - t0, 0)
+            if self.autotune and not self.tuned and len(resident) > 1 and not in_flight:
+                B.autotune(steps=1)
+                self.tuned = True
+                for eid, (r, t_adm, _) in list(resident.items()):
+                    resident[eid] = (r, t_adm, int(B.info(eid).step))
+            while resident and len(in_flight) < self.depth:
+                in_flight.append(B.round(self.steps_per_round))
+            if not in_flight:
                 if pending:
                     time.sleep(max(0.0, min(pending[0].arrival - now, 0.05)))
                 continue
-            if self.autotune and not self.tuned and len(resident) > 1:
-                B.autotune(steps=1)
-                self.tuned = True
-            active_cells = B.active_cells
-            tb = time.perf_counter()
-            B.step(self.steps_per_round)
-            B.synchronize()
-            busy += time.perf_counter() - tb
-            cell_updates += active_cells * self.steps_per_round
+            infos, ms = B.poll(in_flight.popleft())
+            busy += ms / 1e3
             now = time.perf_counter() - t0
-            for eid in list(resident):
-                r, t_adm = resident[eid]
-                inf = B.info(eid)
+            for eid, inf in infos.items():
+                if eid not in resident:
+                    continue
+                r, t_adm, last = resident[eid]
+                cell_updates += (int(inf.step) - last) * int(inf.cells)
+                resident[eid] = (r, t_adm, int(inf.step))
                 if inf.frozen_out or inf.step >= r.max_steps or (inf.status & GVH_STATUS_ERRORS):
                     done.append(Completed(r.rid, r.arrival, t_adm, now, int(inf.step), int(inf.cells),
                                           bool(inf.frozen_out), int(inf.status)))
                     B.remove_event(eid)
                     del resident[eid]
+        B.synchronize()
         elapsed = time.perf_counter() - t0
         out = summarize(done, elapsed, cell_updates, busy)
         out["initial_state_seconds"] = ic_seconds
+        out["rounds_in_flight"] = self.depth
         return out
 
 
@@ -206,7 +220,7 @@ def main(argv=None):
     args = ap.parse_args(argv)
     rng = np.random.default_rng(args.seed)
     arrivals = poisson_arrivals(args.rate, args.requests, rng)
-    reqs = [make_request(i, a, rng, args.max_steps) for i, a in enumerate(arrivals)]
+    reqs = [make_request(i, a, rng, args.max_steps, materialize=False) for i, a in enumerate(arrivals)]
     srv = Server(int(args.arena_gb * (1 << 30)), precision=args.precision, steps_per_round=args.steps_per_round,
                  autotune=args.autotune, max_resident_cells=args.max_resident_cells)
     out = srv.run(reqs, time_limit=args.time_limit)

@@ -237,11 +237,14 @@ const char *gvh_last_error(void);
 /* ------------------------------------------------------------------------------------
  * Batched events (no counterpart in the reference, which runs one event per process:
  * HydroPlugin.cpp:107-434). A batch owns one HBM arena and advances every admitted event
- * together: a persistent stage kernel walks a packed queue of 128-cell tiles of all events,
- * and one RK2 step (stage 1, stage 2, per-event bookkeeping) is a CUDA graph replayed per
- * step. All events of a batch share the options (EoS, shear/bulk, precision, theta); each
- * has its own lattice, spacings, dtau, tau0, eta/s, T_fo and T_reg (from its parameters).
- * Each event advances exactly as a gvh_handle with the same inputs would.
+ * together: the stage kernel walks a packed queue of 128-cell tiles of all events, and one
+ * RK2 step (stage 1, stage 2, per-event bookkeeping) is a CUDA graph replayed per step. All
+ * events of a batch share the options (EoS, shear/bulk, precision, theta); each has its own
+ * lattice, spacings, dtau, tau0, eta/s, T_fo and T_reg (from its parameters). Each event
+ * advances exactly as a gvh_handle with the same inputs would, until it has frozen out by
+ * the reference's stop rule; from then on it stays at that state (the reference's loop ends
+ * there). Admission, removal and serving rounds are queued on the batch's stream without
+ * waiting for the device.
  * ---------------------------------------------------------------------------------- */
 typedef struct gvh_batch gvh_batch;
 
@@ -262,8 +265,10 @@ long long gvh_batch_event_bytes(const gvh_lattice_params *lattice, const gvh_opt
 int gvh_batch_create(const gvh_options *opts, long long arena_bytes, gvh_batch **out);
 int gvh_batch_destroy(gvh_batch *b);
 int gvh_batch_set_stream(gvh_batch *b, void *stream);
-/* Admits an event from primitive fields (same arrays as gvh_set_primitive_state). Returns
- * GVH_ERR_NOMEM without side effects when the arena cannot hold it. */
+/* Admits an event from primitive fields (same arrays as gvh_set_primitive_state; host or
+ * device pointers). Returns GVH_ERR_NOMEM without side effects when the arena cannot hold it.
+ * The arrays are copied before the call returns (host arrays into pinned staging); the
+ * event's set-up is queued behind the work in flight. */
 int gvh_batch_add_event(gvh_batch *b, const gvh_lattice_params *lattice, const gvh_hydro_params *hydro,
                         const double *const *prim, int n_prim, int *event_id);
 int gvh_batch_remove_event(gvh_batch *b, int event_id);
@@ -279,9 +284,26 @@ int gvh_batch_get_state(gvh_batch *b, int event_id, double *const *fields, int n
  * persistent grid of n blocks walking the tile queue. */
 int gvh_batch_launch_config(const gvh_batch *b, int *grid_blocks, int *block_threads);
 int gvh_batch_set_grid(gvh_batch *b, int grid_blocks);
-/* Chooses the grid by timing `steps` real steps per candidate (the events advance; every
- * candidate computes the same values). */
+/* Tile shape: tile_x = 0 (the default), 128 consecutive cells of an event; tile_x > 0 (a
+ * divisor of 128), blocks of tile_x x (128 / tile_x) cells of one eta plane. */
+int gvh_batch_set_tile_shape(gvh_batch *b, int tile_x);
+int gvh_batch_tile_shape(const gvh_batch *b, int *tile_x, int *tile_y);
+/* Chooses the schedule by timing `steps` real steps per candidate -- tile shapes 128
+ * consecutive cells, 32 x 4 and 16 x 8, each with one block per tile and persistent grids of
+ * 1..4 blocks per SM (the events advance; every candidate computes the same values). The
+ * chosen grid is returned, the chosen shape is read with gvh_batch_tile_shape. */
 int gvh_batch_autotune(gvh_batch *b, int steps, int *chosen_grid);
+/* Serving rounds. gvh_batch_round queues nsteps RK2 steps of every admitted event and then a
+ * copy of every event's bookkeeping into mapped host memory, and returns the round's ticket
+ * without waiting. gvh_batch_poll waits for that round only (not for work queued after it)
+ * and gives, for each event admitted when the round was queued and still admitted now, its
+ * id and its gvh_event_info at the end of the round (up to max_events; *n_events is the
+ * count), and the round's device time in ms (round_ms may be null). Two rounds can be in
+ * flight: a round's snapshot is overwritten two rounds later, so poll ticket k before
+ * queueing round k + 2 (gvh_batch_round waits for round k - 2 to finish). */
+int gvh_batch_round(gvh_batch *b, int nsteps, long long *ticket);
+int gvh_batch_poll(gvh_batch *b, long long ticket, int max_events, int *event_ids, gvh_event_info *infos,
+                   int *n_events, double *round_ms);
 const char *gvh_batch_last_error(void);
 
 /* ------------------------------------------------------------------------------------

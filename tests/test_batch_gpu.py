@@ -78,6 +78,13 @@ def test_freezeout_stop_rule():
     assert B.info(eid).frozen_checks == 10 and not B.info(eid).frozen_out
     B.step(1)
     assert B.info(eid).frozen_out
+    # a frozen-out event is not advanced further (the reference's loop ends there)
+    frozen = B.get_state(eid)
+    B.step(4)
+    assert B.info(eid).step == 10
+    after = B.get_state(eid)
+    for k in frozen:
+        np.testing.assert_array_equal(frozen[k], after[k])
 
 
 def test_hot_event_is_not_frozen():
@@ -119,6 +126,96 @@ def test_autotune_does_not_change_results():
     assert g >= 0  # 0 = one block per tile
     nb = B.info(idb[0]).step
     A.step(nb)
+    for ea, eb in zip(ida, idb):
+        sa, sb = A.get_state(ea), B.get_state(eb)
+        for k in sa:
+            np.testing.assert_array_equal(sa[k], sb[k])
+
+
+def _alone(kw, prim, t0, steps, precision, conformal=False, shear=True, bulk=True):
+    L = gvh.Lattice(conformal=conformal, shear=shear, bulk=bulk, precision=precision, **kw)
+    L.set_primitive(prim)
+    t = t0
+    for n in range(1, steps + 1):
+        L.step(t, kw["dt"])
+        t = t0 + n * kw["dt"]
+    return L.get_state()
+
+
+def _close(shape, alone, inb, names, tol):
+    for k in names:
+        a, b = interior(shape, alone[k]), interior(shape, inb[k])
+        scale = max(np.abs(a).max(), 1e-300)
+        assert np.abs(a - b).max() / scale <= tol, (k, np.abs(a - b).max() / scale)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_event_admitted_mid_flight_is_the_same_as_alone(precision):
+    """Serving: event 0 runs for a while; event 1 is admitted while rounds are in flight (its
+    set-up queued behind them), event 2 after event 0 has been retired and its memory reused.
+    Each event's result equals the same event run alone on a gvh.Lattice for the same number
+    of steps (1e-12 FP64, 1e-6 mixed: the same per-cell code in two kernels)."""
+    evs = make_events(False, True, True)
+    B = gvh.Batch(1 << 26, precision=precision)
+    tol = 1e-12 if precision == "fp64" else 1e-6
+    e0 = B.add_event(**evs[0][0], prim=evs[0][1], tau0=evs[0][2])
+    t_a = B.round(3)
+    t_b = B.round(3)
+    e1 = B.add_event(**evs[1][0], prim=evs[1][1], tau0=evs[1][2])  # while two rounds are in flight
+    infos, ms = B.poll(t_a)
+    assert set(infos) == {e0} and infos[e0].step == 3 and ms > 0
+    t_c = B.round(4)
+    infos, _ = B.poll(t_b)
+    assert set(infos) == {e0} and infos[e0].step == 6
+    infos, _ = B.poll(t_c)
+    assert infos[e0].step == 10 and infos[e1].step == 4
+    st0 = B.get_state(e0)
+    B.remove_event(e0)
+    e2 = B.add_event(**evs[2][0], prim=evs[2][1], tau0=evs[2][2])
+    t_d = B.round(5)
+    infos, _ = B.poll(t_d)
+    assert infos[e1].step == 9 and infos[e2].step == 5
+    for eid, (kw, prim, t0), steps, state in [(e0, evs[0], 10, st0), (e1, evs[1], 9, None),
+                                              (e2, evs[2], 5, None)]:
+        alone = _alone(kw, prim, t0, steps, precision)
+        _close((kw["nx"], kw["ny"], kw["nz"]), alone, state if state is not None else B.get_state(eid),
+               B.field_names, tol)
+
+
+def test_poll_does_not_report_a_slot_refilled_after_its_round():
+    evs = make_events(False, True, True)
+    B = gvh.Batch(1 << 26, precision="fp64")
+    x = B.add_event(**evs[0][0], prim=evs[0][1], tau0=evs[0][2])
+    t = B.round(2)
+    B.remove_event(x)
+    y = B.add_event(**evs[2][0], prim=evs[2][1], tau0=evs[2][2])
+    assert y == x  # the slot is reused at once (the round in flight runs before the new set-up)
+    infos, _ = B.poll(t)
+    assert infos == {}
+    t2 = B.round(3)
+    infos, _ = B.poll(t2)
+    assert list(infos) == [y] and infos[y].step == 3
+    kw, prim, t0 = evs[2]
+    _close((kw["nx"], kw["ny"], kw["nz"]), _alone(kw, prim, t0, 3, "fp64"), B.get_state(y), B.field_names, 1e-12)
+    # a snapshot two rounds old is gone
+    t3, t4 = B.round(1), B.round(1)
+    with pytest.raises(gvh.GvhError):
+        B.poll(t2)
+    B.poll(t3)
+    B.poll(t4)
+
+
+@pytest.mark.parametrize("tile_x", [32, 16, 8])
+def test_tile_shapes_compute_the_same_values(tile_x):
+    evs = make_events(False, True, True)
+    A = gvh.Batch(1 << 26, precision="fp64")
+    B = gvh.Batch(1 << 26, precision="fp64")
+    B.set_tile_shape(tile_x)
+    assert B.tile_shape == (tile_x, 128 // tile_x)
+    ida = [A.add_event(**kw, prim=prim, tau0=t0) for kw, prim, t0 in evs]
+    idb = [B.add_event(**kw, prim=prim, tau0=t0) for kw, prim, t0 in evs]
+    A.step(4)
+    B.step(4)
     for ea, eb in zip(ida, idb):
         sa, sb = A.get_state(ea), B.get_state(eb)
         for k in sa:

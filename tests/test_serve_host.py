@@ -15,14 +15,19 @@ class FakeInfo:
 
 class FakeBatch:
     """Stands in for gvh.Batch: an arena of `capacity` bytes; an event needs
-    cells * 100 bytes and freezes out after `life` steps."""
+    cells * 100 bytes and freezes out after `life` steps (then stops advancing, as the
+    batch's events do). Rounds run in queue order when a poll needs them, each over the
+    events admitted when it was queued, as the device runs them in stream order."""
 
     def __init__(self, capacity, step_seconds=0.0):
         self.capacity = capacity
         self.step_seconds = step_seconds
-        self.events = {}
+        self.events = {}      # admitted now
+        self.state = {}       # every event ever admitted (rounds in flight may still step it)
         self.next_id = 0
         self.log = []
+        self.rounds = []      # [ticket, nsteps, members, snapshot or None]
+        self.max_in_flight = 0
 
     def event_bytes(self, nx, ny, nz):
         return nx * ny * nz * 100
@@ -41,7 +46,9 @@ class FakeBatch:
             return None
         eid = self.next_id
         self.next_id += 1
-        self.events[eid] = dict(bytes=need, cells=nx * ny * nz, step=0, life=int(prim["life"]))
+        st = dict(bytes=need, cells=nx * ny * nz, step=0, life=int(prim["life"]))
+        self.events[eid] = st
+        self.state[eid] = st
         self.log.append(("add", eid))
         return eid
 
@@ -49,13 +56,31 @@ class FakeBatch:
         self.log.append(("remove", eid))
         del self.events[eid]
 
-    def step(self, n):
+    def _run(self, rnd):
         time.sleep(self.step_seconds)
-        for e in self.events.values():
-            e["step"] += n
+        for eid in rnd[2]:
+            e = self.state[eid]
+            e["step"] = min(e["step"] + rnd[1], max(e["step"], e["life"]))  # frozen events stop
+        rnd[3] = {eid: FakeInfo(self.state[eid]["step"], self.state[eid]["step"] >= self.state[eid]["life"],
+                                self.state[eid]["cells"]) for eid in rnd[2]}
+
+    def round(self, n):
+        t = len(self.rounds)
+        self.rounds.append([t, n, list(self.events), None])
+        self.max_in_flight = max(self.max_in_flight, sum(1 for r in self.rounds if r[3] is None))
+        return t
+
+    def poll(self, ticket):
+        for rnd in self.rounds[:ticket + 1]:
+            if rnd[3] is None:
+                self._run(rnd)
+        snap = self.rounds[ticket][3]
+        return {eid: inf for eid, inf in snap.items() if eid in self.events}, 1.0
 
     def synchronize(self):
-        pass
+        for rnd in self.rounds:
+            if rnd[3] is None:
+                self._run(rnd)
 
     def info(self, eid):
         e = self.events[eid]
@@ -76,6 +101,7 @@ def test_admission_fifo_by_footprint_and_retirement():
     srv = serve.Server(0, steps_per_round=10, batch=fb)
     out = srv.run(reqs)
     assert out["completed"] == 4 and out["frozen_out"] == 4
+    assert fb.max_in_flight == 2  # the next round is queued before the host reads the last
     adds = [e for op, e in fb.log if op == "add"]
     # FIFO: request 2 waits for memory although the small request 3 would fit -- no overtaking
     first_remove = fb.log.index(("remove", 0))
@@ -100,6 +126,16 @@ def test_events_join_a_running_batch():
     # event 1 arrived while event 0 was resident and finished first
     removes = [e for op, e in fb.log if op == "remove"]
     assert removes == [1, 0]
+
+
+def test_a_retired_slot_reused_by_a_new_event_is_not_misread():
+    """A round queued before a retirement still reports the old event; the new event that
+    takes its place joins later rounds and is retired by its own bookkeeping only."""
+    fb = FakeBatch(capacity=100 * 10 * 10)  # room for one 10x10 event at a time
+    srv = serve.Server(0, steps_per_round=10, batch=fb)
+    out = srv.run([req(0, 0.0, 10, life=20), req(1, 0.0, 10, life=50)])
+    assert out["completed"] == 2 and out["frozen_out"] == 2
+    assert sorted(out["steps"]) == [20, 50]
 
 
 def test_poisson_arrivals_rate():
