@@ -101,34 +101,41 @@ GVH_HD inline double row_interp3(double x0, double x1, double x2, const double a
 // Work space of one hypercube (fixed size; on the device it lives in the thread's local
 // memory).
 struct RowWork {
+  iso::Result res;
+  // the corner (a, b, k)'s kRowVars values at the lower then the upper time level, read in
+  // place from the slab's point table; null for the absent eta layer of a 3-cube
+  const double *corner[2][2][2];
   iso::HypercubeWork hw;
   iso::CubeWork cw;
-  iso::Result res;
-  double f[kRowVars][2][2][2][2];
 };
 
-// The rows of hypercube `key` ((ix (ny-1) + iy) nzc + iz) whose corner fields the caller has
-// put in w.f[q][t][a][b][k] (k = 0 only in 3D). Writes up to kMaxElements rows of
-// kRowColumns values to rows and returns how many, or a negative cornelius error.
+// Field q at the corners, as f[t][a][b][k] (0 for an absent corner).
+GVH_HD inline void corner_field(const RowWork &w, int q, double f[2][2][2][2]) {
+  for (int t = 0; t < 2; ++t)
+    for (int a = 0; a < 2; ++a)
+      for (int b = 0; b < 2; ++b)
+        for (int k = 0; k < 2; ++k) f[t][a][b][k] = w.corner[a][b][k] ? w.corner[a][b][k][t * kRowVars + q] : 0.0;
+}
+
+// The rows of hypercube `key` ((ix (ny-1) + iy) nzc + iz) whose corners the caller has set
+// (gather_corners). Writes up to kMaxElements rows of kRowColumns values to rows and returns
+// how many, or a negative cornelius error.
 GVH_HD inline int cube_rows(const RowGeometry &g, int key, RowWork &w, double *rows) {
   const int nzc = g.dim == 4 ? g.nz - 1 : 1;
   const int iz = key % nzc;
   const int iy = (key / nzc) % (g.ny - 1);
   const int ix = key / nzc / (g.ny - 1);
   int rc;
+  double e4[2][2][2][2];
+  corner_field(w, 3, e4);
   if (g.dim == 4) {
-    double v4[2][2][2][2];
-    for (int t = 0; t < 2; ++t)
-      for (int a = 0; a < 2; ++a)
-        for (int b = 0; b < 2; ++b)
-          for (int k = 0; k < 2; ++k) v4[t][a][b][k] = w.f[3][t][a][b][k];
     const double dx4[4] = {g.dt, g.dx, g.dy, g.dz};
-    rc = iso::find_4d(v4, dx4, g.iso, w.res, w.hw);
+    rc = iso::find_4d(e4, dx4, g.iso, w.res, w.hw);
   } else {
     double v3[2][2][2];
     for (int t = 0; t < 2; ++t)
       for (int a = 0; a < 2; ++a)
-        for (int b = 0; b < 2; ++b) v3[t][a][b] = w.f[3][t][a][b][0];
+        for (int b = 0; b < 2; ++b) v3[t][a][b] = e4[t][a][b][0];
     // cornelius is set up with the spacings of the dimensions in use (HydroPlugin.cpp
     // :155-182); in 3D its first axis has unit length and is not used
     const double dx3[4] = {1.0, g.dt, g.dx, g.dy};
@@ -159,8 +166,11 @@ GVH_HD inline int cube_rows(const RowGeometry &g, int key, RowWork &w, double *r
     for (int k = 0; k < 3; ++k) row[4 + k] = g.tau_scale * nrm[k];
     row[7] = g.dim == 4 ? g.tau_scale * nrm[3] : 0.0;
     double val[kRowVars];
-    for (int q = 0; q < kRowVars; ++q)
-      val[q] = g.dim == 4 ? row_interp4(tf, xf, yf, zf, w.f[q]) : row_interp3(tf, xf, yf, w.f[q]);
+    for (int q = 0; q < kRowVars; ++q) {
+      double f[2][2][2][2];
+      corner_field(w, q, f);
+      val[q] = g.dim == 4 ? row_interp4(tf, xf, yf, zf, f) : row_interp3(tf, xf, yf, f);
+    }
     row[8] = val[0];
     row[9] = val[1];
     row[10] = val[2];
@@ -172,9 +182,8 @@ GVH_HD inline int cube_rows(const RowGeometry &g, int key, RowWork &w, double *r
   return res.n;
 }
 
-// Gathers the corner fields of hypercube `key` from the slab's point table into w.f:
-// c2p maps a lattice cell to its point, point_vals holds kRowVars values at the lower then
-// the upper level per point.
+// Points w's corners of hypercube `key` at the slab's point table: c2p maps a lattice cell
+// to its point, point_vals holds kRowVars values at the lower then the upper level per point.
 GVH_HD inline void gather_corners(const RowGeometry &g, int key, const int *c2p, const double *point_vals,
                                   RowWork &w) {
   const int nzc = g.dim == 4 ? g.nz - 1 : 1;
@@ -186,14 +195,11 @@ GVH_HD inline void gather_corners(const RowGeometry &g, int key, const int *c2p,
     for (int b = 0; b < 2; ++b)
       for (int k = 0; k < 2; ++k) {
         if (k >= nzk) {
-          for (int t = 0; t < 2; ++t)
-            for (int q = 0; q < kRowVars; ++q) w.f[q][t][a][b][k] = 0.0;
+          w.corner[a][b][k] = nullptr;
           continue;
         }
         const int cell = (ix + a) + g.nx * ((iy + b) + g.ny * (iz + k));
-        const double *pv = point_vals + (size_t)c2p[cell] * (2 * kRowVars);
-        for (int t = 0; t < 2; ++t)
-          for (int q = 0; q < kRowVars; ++q) w.f[q][t][a][b][k] = pv[t * kRowVars + q];
+        w.corner[a][b][k] = point_vals + (size_t)c2p[cell] * (2 * kRowVars);
       }
 }
 
