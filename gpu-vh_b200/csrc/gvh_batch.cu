@@ -34,6 +34,7 @@
 
 #include "../../include/gvh.h"
 #include "gvh_layout.cuh"
+#include "gvh_nvtx.h"
 #include "gvh_stage.cuh"
 
 using namespace gvh;
@@ -565,14 +566,25 @@ int gvh_batch_set_stream(gvh_batch *b, void *stream) {
   return GVH_OK;
 }
 
-int gvh_batch_add_event(gvh_batch *b, const gvh_lattice_params *L, const gvh_hydro_params *H,
-                        const double *const *prim, int n_prim, int *event_id) {
-  if (!b || !L || !H || !prim || !event_id) return bfail(GVH_ERR_INVALID, "null argument");
+}  // extern "C"
+
+namespace {
+
+// Admission of an event whose initial state is given either as primitive arrays (prim) or as
+// hotspot sources (hs) filled in on the device.
+int admit_event(gvh_batch *b, const gvh_lattice_params *L, const gvh_hydro_params *H, const double *const *prim,
+                int n_prim, const gvh_hotspots *hs, int *event_id) {
+  NvtxRange range("gvh batch admission");
+  if (!b || !L || !H || (!prim && !hs) || !event_id) return bfail(GVH_ERR_INVALID, "null argument");
   *event_id = -1;
-  const int want = 5 + (b->nq - 4);
-  if (n_prim != want) return bfail(GVH_ERR_INVALID, "expected %d primitive arrays", want);
-  for (int f = 0; f < n_prim; ++f)
-    if (!prim[f]) return bfail(GVH_ERR_INVALID, "primitive array %d is null", f);
+  if (prim) {
+    const int want = 5 + (b->nq - 4);
+    if (n_prim != want) return bfail(GVH_ERR_INVALID, "expected %d primitive arrays", want);
+    for (int f = 0; f < n_prim; ++f)
+      if (!prim[f]) return bfail(GVH_ERR_INVALID, "primitive array %d is null", f);
+  } else if (hs->n < 1 || !hs->x || !hs->y || !hs->w || !(hs->sigma > 0) || !(hs->sigma_eta > 0)) {
+    return bfail(GVH_ERR_INVALID, "hotspots: n >= 1 sources with positions and weights, sigma > 0, sigma_eta > 0");
+  }
   if (L->numLatticePointsX < 1 || L->numLatticePointsY < 1 || L->numLatticePointsRapidity < 1)
     return bfail(GVH_ERR_INVALID, "lattice sizes must be >= 1");
   if (!(L->latticeSpacingX > 0 && L->latticeSpacingY > 0 && L->latticeSpacingRapidity > 0 &&
@@ -596,18 +608,35 @@ int gvh_batch_add_event(gvh_batch *b, const gvh_lattice_params *L, const gvh_hyd
   if (!arena_alloc(b, h.bytes, &h.off)) return bfail(GVH_ERR_NOMEM, "arena full (%zu bytes needed)", h.bytes);
   h.used = true;
   h.serial = b->next_serial++;
-  int rc = ensure_staging(b, n_prim, h.ng);
+  const long long hs_doubles = hs ? 3ll * hs->n + (long long)h.nx * h.ny : 0;
+  int rc = prim ? ensure_staging(b, n_prim, h.ng) : ensure_staging(b, 1, hs_doubles);
   if (rc) { arena_free(b, h.off, h.bytes); return rc; }
-  // the initial state goes to the device through a pinned buffer: the host copy happens here,
-  // the transfer is queued behind the work in flight and nothing waits for it
+  // the initial state (or its sources) goes to the device through a pinned buffer: the host
+  // copy happens here, the transfer is queued behind the work in flight and nothing waits
   PinnedBuf &pb = b->prim_stage[b->prim_next];
   b->prim_next ^= 1;
   const size_t fb = h.ng * sizeof(double);
-  if ((rc = pinned_reserve(pb, n_prim * fb))) { arena_free(b, h.off, h.bytes); return rc; }
+  if ((rc = pinned_reserve(pb, prim ? n_prim * fb : 3 * hs->n * sizeof(double)))) {
+    arena_free(b, h.off, h.bytes);
+    return rc;
+  }
   double *qA, *qB, *e, *pA, *pB, *u[3];
   event_pointers(b, h, &qA, &qB, &e, &pA, &pB, u);
   BCUDA(cudaMemsetAsync(b->arena + h.off, 0, h.bytes, b->stream));
-  for (int f = 0; f < n_prim; ++f) {
+  const unsigned blocks = (unsigned)((h.ncells + 255) / 256);
+  if (hs) {
+    double *src = static_cast<double *>(pb.h);
+    memcpy(src, hs->x, hs->n * sizeof(double));
+    memcpy(src + hs->n, hs->y, hs->n * sizeof(double));
+    memcpy(src + 2 * hs->n, hs->w, hs->n * sizeof(double));
+    BCUDA(cudaMemcpyAsync(b->staging, src, 3 * hs->n * sizeof(double), cudaMemcpyHostToDevice, b->stream));
+    if ((rc = pinned_mark(b, pb))) return rc;
+    const HotspotArgs ha = hotspot_args(h.nx, h.ny, h.nz, h.nx, (long long)h.nx * h.ny, L, hs, b->staging);
+    double *plane = b->staging + 3 * hs->n;
+    hotspot_plane_kernel<<<(unsigned)((h.nx * h.ny + 255) / 256), 256, 0, b->stream>>>(ha, plane);
+    hotspot_fill_kernel<<<blocks, 256, 0, b->stream>>>(ha, plane, e, u[0], h.cs, qA, b->nq);
+  }
+  for (int f = 0; prim && f < n_prim; ++f) {
     cudaPointerAttributes at;
     const bool on_device = cudaPointerGetAttributes(&at, prim[f]) == cudaSuccess &&
                            (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged);
@@ -620,14 +649,15 @@ int gvh_batch_add_event(gvh_batch *b, const gvh_lattice_params *L, const gvh_hyd
                             b->stream));
     }
   }
-  if ((rc = pinned_mark(b, pb))) return rc;
-  FieldTable dst = {};
-  dst.p[0] = e;
-  for (int m = 0; m < 4; ++m) dst.p[1 + m] = u[0] + m * h.cs;
-  for (int n = 4; n < b->nq; ++n) dst.p[5 + n - 4] = qA + n * h.cs;
-  Pack pk{h.nx, h.ny, h.nz, (long long)h.nx, (long long)h.nx * h.ny, h.ng};
-  const unsigned blocks = (unsigned)((h.ncells + 255) / 256);
-  pack_kernel<<<blocks, 256, 0, b->stream>>>(pk, n_prim, b->staging, dst);
+  if (prim) {
+    if ((rc = pinned_mark(b, pb))) return rc;
+    FieldTable dst = {};
+    dst.p[0] = e;
+    for (int m = 0; m < 4; ++m) dst.p[1 + m] = u[0] + m * h.cs;
+    for (int n = 4; n < b->nq; ++n) dst.p[5 + n - 4] = qA + n * h.cs;
+    Pack pk{h.nx, h.ny, h.nz, (long long)h.nx, (long long)h.nx * h.ny, h.ng};
+    pack_kernel<<<blocks, 256, 0, b->stream>>>(pk, n_prim, b->staging, dst);
+  }
   if (b->opts.eos == GVH_EOS_CONFORMAL)
     init_conserved_kernel<EOS_CONFORMAL><<<blocks, 256, 0, b->stream>>>(h.ncells, b->nq, h.cs, qA, e, pA, u[0], u[1], 0);
   else
@@ -670,6 +700,22 @@ int gvh_batch_add_event(gvh_batch *b, const gvh_lattice_params *L, const gvh_hyd
   return GVH_OK;
 }
 
+}  // namespace
+
+extern "C" {
+
+int gvh_batch_add_event(gvh_batch *b, const gvh_lattice_params *L, const gvh_hydro_params *H,
+                        const double *const *prim, int n_prim, int *event_id) {
+  if (!prim) return bfail(GVH_ERR_INVALID, "null argument");
+  return admit_event(b, L, H, prim, n_prim, nullptr, event_id);
+}
+
+int gvh_batch_add_event_hotspots(gvh_batch *b, const gvh_lattice_params *L, const gvh_hydro_params *H,
+                                 const gvh_hotspots *hs, int *event_id) {
+  if (!hs) return bfail(GVH_ERR_INVALID, "null argument");
+  return admit_event(b, L, H, nullptr, 0, hs, event_id);
+}
+
 int gvh_batch_remove_event(gvh_batch *b, int id) {
   if (!b || id < 0 || id >= (int)b->ev.size() || !b->ev[id].used) return bfail(GVH_ERR_INVALID, "bad event id");
   BCUDA(cudaSetDevice(b->device));
@@ -705,6 +751,7 @@ long long gvh_batch_active_cells(const gvh_batch *b) {
 
 int gvh_batch_step(gvh_batch *b, int nsteps) {
   if (!b || nsteps < 0) return bfail(GVH_ERR_INVALID, "bad arguments");
+  NvtxRange r("gvh batch steps");
   BCUDA(cudaSetDevice(b->device));
   for (int n = 0; n < nsteps; ++n) BCUDA(cudaGraphLaunch(b->graph, b->stream));
   return GVH_OK;
@@ -841,6 +888,7 @@ int gvh_batch_autotune(gvh_batch *b, int steps, int *chosen_grid) {
 
 int gvh_batch_round(gvh_batch *b, int nsteps, long long *ticket) {
   if (!b || nsteps < 0 || !ticket) return bfail(GVH_ERR_INVALID, "bad arguments");
+  NvtxRange range("gvh batch round");
   BCUDA(cudaSetDevice(b->device));
   const long long t = b->next_ticket++;
   const int r = (int)(t & 1);

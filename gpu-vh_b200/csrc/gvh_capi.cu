@@ -24,6 +24,7 @@
 #include "../../include/gvh.h"
 #include "gvh_handle.h"
 #include "gvh_layout.cuh"
+#include "gvh_nvtx.h"
 #include "gvh_stage.cuh"
 #include "gvh_validity.cuh"
 
@@ -389,6 +390,38 @@ int gvh_set_primitive_state_p(gvh_handle *h, const double *const *prim, int n_pr
   return GVH_OK;
 }
 
+int gvh_set_hotspot_state(gvh_handle *h, const gvh_hotspots *hs) {
+  if (!h || !hs) return fail(GVH_ERR_INVALID, "gvh_set_hotspot_state: null argument");
+  if (hs->n < 1 || !hs->x || !hs->y || !hs->w || !(hs->sigma > 0) || !(hs->sigma_eta > 0))
+    return fail(GVH_ERR_INVALID, "gvh_set_hotspot_state: n >= 1 sources with positions and weights, sigma > 0 and "
+                                 "sigma_eta > 0");
+  int rc;
+  if ((rc = set_device(h)) || (rc = ensure_staging(h))) return rc;
+  // sources and the transverse plane in the staging area
+  if (3ll * hs->n + (long long)h->nx * h->ny > (long long)(h->nq + 10) * h->ng)
+    return fail(GVH_ERR_INVALID, "gvh_set_hotspot_state: too many sources for this lattice (%d)", hs->n);
+  const size_t nb = hs->n * sizeof(double);
+  GVH_CUDA(cudaMemcpyAsync(h->staging, hs->x, nb, cudaMemcpyHostToDevice, h->stream));
+  GVH_CUDA(cudaMemcpyAsync(h->staging + hs->n, hs->y, nb, cudaMemcpyHostToDevice, h->stream));
+  GVH_CUDA(cudaMemcpyAsync(h->staging + 2 * hs->n, hs->w, nb, cudaMemcpyHostToDevice, h->stream));
+  gvh_lattice_params L = {h->nx, h->ny, h->nz, h->nx + 4, h->ny + 4, h->nz + 4, 0, h->dx, h->dy, h->dz,
+                          h->dt_lattice};
+  const HotspotArgs ha = hotspot_args(h->nx, h->ny, h->nz, h->sy, h->sz, &L, hs, h->staging);
+  double *plane = h->staging + 3 * hs->n;
+  hotspot_plane_kernel<<<(unsigned)((h->nx * h->ny + 255) / 256), 256, 0, h->stream>>>(ha, plane);
+  const unsigned blocks = (unsigned)((h->ncells + 255) / 256);
+  hotspot_fill_kernel<<<blocks, 256, 0, h->stream>>>(ha, plane, h->e, h->u[h->ucur], h->cs, h->qA, h->nq);
+  if (h->eos == GVH_EOS_CONFORMAL)
+    init_conserved_kernel<EOS_CONFORMAL><<<blocks, 256, 0, h->stream>>>(h->ncells, h->nq, h->cs, h->qA, h->e, h->pA,
+                                                                        h->u[h->ucur], h->u[h->uprev], 0);
+  else
+    init_conserved_kernel<EOS_QCD><<<blocks, 256, 0, h->stream>>>(h->ncells, h->nq, h->cs, h->qA, h->e, h->pA,
+                                                                  h->u[h->ucur], h->u[h->uprev], 0);
+  GVH_CUDA(cudaGetLastError());
+  GVH_CUDA(cudaStreamSynchronize(h->stream));
+  return GVH_OK;
+}
+
 int gvh_set_primitive_state(gvh_handle *h, const double *const *prim, int n_prim) {
   return gvh_set_primitive_state_p(h, prim, n_prim, nullptr);
 }
@@ -416,7 +449,10 @@ int gvh_rk2_step(gvh_handle *h, double t, double dt, double T_reg) {
   a.qin = h->qA; a.qn = nullptr; a.qout = h->qB;
   a.pin = h->pA; a.pout = h->pB;
   a.uin = h->u[h->ucur]; a.uprev = h->u[h->uprev]; a.uout = h->u[h->uprev];
-  if ((rc = dispatch(h, a, false))) return rc;
+  {
+    NvtxRange r("gvh stage 1 (predictor)");
+    if ((rc = dispatch(h, a, false))) return rc;
+  }
   // stage 2 (corrector + Heun combination)
   a.speed_max = nullptr;
   a.t_euler = t1; a.t_after = t1;
@@ -424,7 +460,10 @@ int gvh_rk2_step(gvh_handle *h, double t, double dt, double T_reg) {
   a.pin = h->pB; a.pout = h->pA;
   a.uin = h->u[h->uprev]; a.uprev = h->u[h->ucur]; a.uout = h->u[h->ufree];
   a.diag = h->validity_on ? h->diag : nullptr;
-  if ((rc = dispatch(h, a, true))) return rc;
+  {
+    NvtxRange r("gvh stage 2 (corrector)");
+    if ((rc = dispatch(h, a, true))) return rc;
+  }
   if (h->validity_on && (rc = launch_validity(h, t1, h->u[h->ufree], h->u[h->ucur]))) return rc;
   const int nc = h->ufree, np = h->ucur, nf = h->uprev;
   h->ucur = nc; h->uprev = np; h->ufree = nf;

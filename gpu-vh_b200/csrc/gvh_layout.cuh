@@ -5,6 +5,7 @@
 
 #include <cuda_runtime.h>
 
+#include "../../include/gvh.h"
 #include "gvh_physics.cuh"
 
 namespace {
@@ -108,6 +109,80 @@ __global__ void init_conserved_kernel(long long n, int nq, long long cs, double 
   q[2 * cs + s] = (es + pp) * ut * uy + pity;
   q[3 * cs + s] = (es + pp) * ut * un + pitn;
   for (int m = 0; m < 4; ++m) up[m * cs + s] = u[m * cs + s];
+}
+
+// ---- Glauber-hotspot initial state on the device ----------------------------------------
+// e(x, y, eta) = fz(eta) * scale * sum_p w_p gy_p gx_p + background, gx_p = exp(-(x - x_p)^2 / s2),
+// fz = exp(-max(|eta| - eta_flat, 0)^2 / s2_eta), rounded to float and + 1e-3 as the type-10
+// reader stores a value written to its files (InitialConditions.cpp:106, 122-124). Every
+// operation is rounded on its own (no multiply-add contraction), in the order of the host
+// generator (gvh/workloads.py hotspot_field), so the two agree wherever the device's exp
+// agrees with the host's. Cell centres x_i = (i - (nx - 1)/2) dx (the centred grid).
+struct HotspotArgs {
+  int nx, ny, nz;
+  long long sy, sz;    // internal strides
+  double dx, dy, dz;
+  int n;               // sources: x[n], y[n], w[n] back to back in src
+  const double *src;
+  double s2, scale, eta_flat, s2_eta, background;
+};
+
+// The kernels' arguments for a lattice (internal strides sy, sz) and a gvh_hotspots whose
+// sources have been copied to src (x, y, w back to back). s2 = 2 sigma^2 as the host generator
+// forms it.
+inline HotspotArgs hotspot_args(int nx, int ny, int nz, long long sy, long long sz, const gvh_lattice_params *L,
+                                const gvh_hotspots *hs, const double *src) {
+  HotspotArgs a;
+  a.nx = nx; a.ny = ny; a.nz = nz; a.sy = sy; a.sz = sz;
+  a.dx = L->latticeSpacingX; a.dy = L->latticeSpacingY; a.dz = L->latticeSpacingRapidity;
+  a.n = hs->n;
+  a.src = src;
+  a.s2 = 2.0 * (hs->sigma * hs->sigma);
+  a.scale = hs->scale;
+  a.eta_flat = hs->eta_flat;
+  a.s2_eta = 2.0 * (hs->sigma_eta * hs->sigma_eta);
+  a.background = hs->background;
+  return a;
+}
+
+// The transverse profile scale * sum_p (w_p gy_p) gx_p, one thread per (i, j), into plane.
+__global__ void hotspot_plane_kernel(HotspotArgs h, double *__restrict__ plane) {
+  const int id = blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= h.nx * h.ny) return;
+  const int i = id % h.nx, j = id / h.nx;
+  const double x = __dmul_rn((double)i - (h.nx - 1) / 2.0, h.dx);
+  const double y = __dmul_rn((double)j - (h.ny - 1) / 2.0, h.dy);
+  const double *xs = h.src, *ys = h.src + h.n, *ws = h.src + 2 * h.n;
+  double T = 0.0;
+  for (int p = 0; p < h.n; ++p) {
+    const double ddx = __dsub_rn(x, xs[p]), ddy = __dsub_rn(y, ys[p]);
+    const double gx = exp(-__dmul_rn(ddx, ddx) / h.s2);
+    const double gy = exp(-__dmul_rn(ddy, ddy) / h.s2);
+    T = __dadd_rn(T, __dmul_rn(__dmul_rn(ws[p], gy), gx));
+  }
+  plane[id] = __dmul_rn(T, h.scale);
+}
+
+// Every interior cell: e from the plane and the eta profile, u = (1, 0, 0, 0) and the
+// dissipative components (q[4..nq)) zero, in the internal layout; init_conserved_kernel then
+// builds p and T^{tau mu} as for any primitive initial state.
+__global__ void hotspot_fill_kernel(HotspotArgs h, const double *__restrict__ plane, double *e, double *u, long long cs,
+                                    double *q, int nq) {
+  const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long n = (long long)h.nx * h.ny * h.nz;
+  if (id >= n) return;
+  const int i = id % h.nx, j = (id / h.nx) % h.ny, k = id / ((long long)h.nx * h.ny);
+  const long long s = i + h.sy * j + h.sz * k;
+  const double z = __dmul_rn((double)k - (h.nz - 1) / 2.0, h.dz);
+  const double m = fmax(__dsub_rn(fabs(z), h.eta_flat), 0.0);
+  const double fz = exp(-__dmul_rn(m, m) / h.s2_eta);
+  const double v = __dadd_rn(__dmul_rn(fz, plane[i + h.nx * j]), h.background);
+  e[s] = __dadd_rn((double)__double2float_rn(v), 1.0e-3);
+  u[s] = 1.0;
+  u[cs + s] = 0.0;
+  u[2 * cs + s] = 0.0;
+  u[3 * cs + s] = 0.0;
+  for (int c = 4; c < nq; ++c) q[c * cs + s] = 0.0;
 }
 
 // Max of a non-negative double array (interior energy densities), as the bit pattern of a

@@ -145,7 +145,9 @@ __device__ __forceinline__ double bulk_zeta_over_s(double T) {
 //   STATUS_NAN     an energy density came out NaN
 //   STATUS_NEWTON  a Newton solve failed to converge even with damping
 //   STATUS_DAMPED  informational: a Newton solve needed the damped phase (see below)
-enum : unsigned { STATUS_NAN = 1u, STATUS_NEWTON = 2u, STATUS_DAMPED = 4u };
+//   STATUS_BOUNDS  the bounds-checked build (GVH_BOUNDS_CHECK) found a stencil index outside
+//                  the arrays; the cell was skipped
+enum : unsigned { STATUS_NAN = 1u, STATUS_NEWTON = 2u, STATUS_DAMPED = 4u, STATUS_BOUNDS = 8u };
 
 // Newton iteration budget. The reference iterates e <- e - f/f' up to 5x10^5 times and
 // then switches to the damped update e <- e - 0.9 f/f' for up to another 5x10^5

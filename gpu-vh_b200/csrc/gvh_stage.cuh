@@ -441,6 +441,28 @@ __device__ __forceinline__ double stage_finish(const StageArgs &a, long long s, 
   return pr.e;
 }
 
+// Whether every index a stage uses for cell (i, j, k) lies inside a component array
+// [0, cs): the cell itself, its clamped stencil along each axis (axis_update's o[]) and its
+// clamped neighbours (stage_source). The bounds-checked build (GVH_BOUNDS_CHECK) runs it before
+// any load of the cell and skips a cell that fails, raising STATUS_BOUNDS; host-callable, so the
+// same function is tested on the CPU.
+__host__ __device__ inline bool cell_stencil_ok(const StageArgs &a, int i, int j, int k) {
+  if (i < 0 || j < 0 || k < 0 || i >= a.nx || j >= a.ny || k >= a.nz) return false;
+  const long long s = i + a.sy * j + a.sz * k;
+  if (s < 0 || s >= a.cs) return false;
+  for (int axis = 0; axis < 3; ++axis) {
+    const int idx = axis == 0 ? i : axis == 1 ? j : k;
+    const int n = axis == 0 ? a.nx : axis == 1 ? a.ny : a.nz;
+    const long long stride = axis == 0 ? 1 : axis == 1 ? a.sy : a.sz;
+    for (int d = -2; d <= 2; ++d) {
+      const int c = d < 0 ? (idx + d > 0 ? idx + d : 0) : (idx + d < n - 1 ? idx + d : n - 1);
+      const long long t = s + (long long)(c - idx) * stride;
+      if (t < 0 || t >= a.cs) return false;
+    }
+  }
+  return true;
+}
+
 // speed: max over the three axes of the local propagation speed over the lattice spacing,
 // a / dx_axis (the CFL bound of the step is dt times its maximum over cells).
 template <int EOS, bool SHEAR, bool BULK, bool STAGE2, bool MIXED>
@@ -449,6 +471,13 @@ __device__ __forceinline__ double stage_cell_ijk(const StageArgs &a, int i, int 
   constexpr int NQ = NComp<SHEAR, BULK>::value;
   const long long s = i + a.sy * j + a.sz * k;
   unsigned status = 0;
+#ifdef GVH_BOUNDS_CHECK
+  if (!cell_stencil_ok(a, i, j, k)) {
+    atomicOr(a.status, STATUS_BOUNDS);
+    speed = 0.0;
+    return 0.0;
+  }
+#endif
 
   const double ePrev = a.e[s];
   double uc[4];

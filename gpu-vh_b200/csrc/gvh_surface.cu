@@ -39,6 +39,7 @@
 #include "../../include/gvh.h"
 #include "gvh_handle.h"
 #include "gvh_surface_device.h"
+#include "gvh_nvtx.h"
 #include "gvh_surface_internal.h"
 
 using gvh::surface::kVars;
@@ -547,6 +548,7 @@ static int device_rows_begin(gvh_surface *s, long long ncubes, long long npoints
 }
 
 int gvh_surface_find_begin(gvh_surface *s, double tau_label, double tau_scale) {
+  gvh::NvtxRange range("gvh surface slab (device)");
   if (!s) return sfail(GVH_ERR_INVALID, "gvh_surface_find_begin: null argument");
   if (!s->have_lower) return sfail(GVH_ERR_INVALID, "gvh_surface_find_begin: no lower time level (gvh_surface_set_lower)");
   if (s->pending) return sfail(GVH_ERR_INVALID, "gvh_surface_find_begin: the previous slab has not been ended");
@@ -603,6 +605,7 @@ int gvh_surface_find_begin(gvh_surface *s, double tau_label, double tau_scale) {
 }
 
 int gvh_surface_find_end(gvh_surface *s, long long *n_elements) {
+  gvh::NvtxRange range("gvh surface slab (host)");
   if (!s) return sfail(GVH_ERR_INVALID, "gvh_surface_find_end: null argument");
   if (!s->pending) return sfail(GVH_ERR_INVALID, "gvh_surface_find_end: no slab begun");
   gvh_handle *h = s->h;

@@ -29,7 +29,9 @@ GVH_ERR_NUMERIC = -3
 GVH_STATUS_NAN = 1
 GVH_STATUS_NEWTON = 2
 GVH_STATUS_DAMPED = 4       # informational (see include/gvh.h)
-GVH_STATUS_ERRORS = 1       # NaN; a non-converged Newton solve is a warning, as in the reference
+GVH_STATUS_BOUNDS = 8       # the bounds-checked build skipped a cell (see include/gvh.h)
+GVH_STATUS_ERRORS = 9       # NaN or a bounds failure; a non-converged Newton solve is a
+                            # warning, as in the reference
 
 Q_NAMES = ["ttt", "ttx", "tty", "ttn", "pitt", "pitx", "pity", "pitn",
            "pixx", "pixy", "pixn", "piyy", "piyn", "pinn", "Pi"]
@@ -81,7 +83,7 @@ EXPORTS = [
     "gvh_default_options", "gvh_create", "gvh_destroy", "gvh_num_conserved", "gvh_num_fields",
     "gvh_num_lattice_cells", "gvh_set_primitive_state", "gvh_set_state", "gvh_get_state", "gvh_rk2_step",
     "gvh_status", "gvh_clear_status", "gvh_synchronize", "gvh_launches_per_step", "gvh_last_error",
-    "gvh_set_stream", "gvh_max_energy_density", "gvh_max_propagation_speed", "gvh_set_state_async", "gvh_get_state_async", "gvh_join_async",
+    "gvh_set_stream", "gvh_max_energy_density", "gvh_max_propagation_speed", "gvh_set_hotspot_state", "gvh_set_state_async", "gvh_get_state_async", "gvh_join_async",
 ]
 
 
@@ -90,7 +92,8 @@ def load(path: str | None = None):
     global _lib
     if _lib is not None and path is None:
         return _lib
-    p = path or LIB_PATH
+    # GVH_LIBRARY selects another build of the same library (the bounds-checked one)
+    p = path or os.environ.get("GVH_LIBRARY") or LIB_PATH
     if not os.path.exists(p):
         raise GvhError(f"libgvh.so not found at {p}: build it with __graft_entry__.build()")
     L = ctypes.CDLL(p)
@@ -118,6 +121,7 @@ def load(path: str | None = None):
     L.gvh_set_stream.argtypes = [vp, vp]
     L.gvh_max_energy_density.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
     L.gvh_max_propagation_speed.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
+    L.gvh_set_hotspot_state.argtypes = [vp, vp]
     L.gvh_last_error.restype = ctypes.c_char_p
     if path is None:
         _lib = L
@@ -211,6 +215,11 @@ class Lattice:
                                                           ctypes.c_void_p]
             _check(self._L.gvh_set_primitive_state_p(self._h, ptrs, len(arrs), pa.ctypes.data),
                    "gvh_set_primitive_state_p")
+
+    def set_hotspots(self, hs):
+        """Initial state from hotspot sources (a workloads.Hotspots), filled on the device."""
+        c, keep = _hotspots_c(hs)
+        _check(self._L.gvh_set_hotspot_state(self._h, ctypes.byref(c)), "gvh_set_hotspot_state")
 
     def set_state(self, state: dict):
         arrs = [None if state.get(k) is None else self._as_ghosted(state[k]) for k in self.field_names]
@@ -329,6 +338,20 @@ class Lattice:
 # ---------------------------------------------------------------------------------------
 # Batched events
 # ---------------------------------------------------------------------------------------
+class HotspotsC(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int), ("x", ctypes.c_void_p), ("y", ctypes.c_void_p), ("w", ctypes.c_void_p),
+                ("sigma", ctypes.c_double), ("scale", ctypes.c_double), ("eta_flat", ctypes.c_double),
+                ("sigma_eta", ctypes.c_double), ("background", ctypes.c_double)]
+
+
+def _hotspots_c(hs):
+    """A gvh_hotspots over the arrays of a workloads.Hotspots (kept alive by the caller)."""
+    x, y, w = (np.ascontiguousarray(a, dtype=np.float64) for a in (hs.x, hs.y, hs.w))
+    c = HotspotsC(len(w), x.ctypes.data, y.ctypes.data, w.ctypes.data, float(hs.sigma), float(hs.scale),
+                  float(hs.eta_flat), float(hs.sigma_eta), float(hs.background))
+    return c, (x, y, w)
+
+
 class EventInfo(ctypes.Structure):
     _fields_ = [("step", ctypes.c_longlong), ("tau", ctypes.c_double), ("max_energy_density", ctypes.c_double),
                 ("freezeout_energy_density", ctypes.c_double), ("frozen_checks", ctypes.c_int),
@@ -341,7 +364,7 @@ BATCH_EXPORTS = [
     "gvh_batch_active_cells", "gvh_batch_step", "gvh_batch_synchronize", "gvh_batch_event_info",
     "gvh_batch_get_state", "gvh_batch_launch_config", "gvh_batch_set_grid", "gvh_batch_autotune",
     "gvh_batch_last_error", "gvh_batch_set_tile_shape", "gvh_batch_tile_shape", "gvh_batch_round",
-    "gvh_batch_poll",
+    "gvh_batch_poll", "gvh_batch_add_event_hotspots",
 ]
 EXPORTS += BATCH_EXPORTS
 
@@ -358,6 +381,8 @@ def _bind_batch(L):
     L.gvh_batch_add_event.argtypes = [vp, ctypes.POINTER(LatticeParams), ctypes.POINTER(HydroParams), vp, ip,
                                       ctypes.POINTER(ip)]
     L.gvh_batch_remove_event.argtypes = [vp, ip]
+    L.gvh_batch_add_event_hotspots.argtypes = [vp, ctypes.POINTER(LatticeParams), ctypes.POINTER(HydroParams), vp,
+                                               ctypes.POINTER(ip)]
     L.gvh_batch_num_events.argtypes = [vp]
     L.gvh_batch_free_bytes.argtypes = [vp]
     L.gvh_batch_free_bytes.restype = ll
@@ -442,6 +467,21 @@ class Batch:
         if rc == GVH_ERR_NOMEM:
             return None
         _bcheck(rc, "gvh_batch_add_event")
+        self.events[eid.value] = (nx, ny, nz)
+        return eid.value
+
+    def add_event_hotspots(self, nx, ny, nz, dx, dy, dz, dt, etabar, hs, tau0=0.5, T_fo_GeV=0.15, T_reg_GeV=0.0):
+        """Admit an event whose initial state the device generates from hotspot sources (a
+        workloads.Hotspots); returns its id, or None when the arena cannot hold it."""
+        lat = LatticeParams(nx, ny, nz, nx + 4, ny + 4, nz + 4, 0, dx, dy, dz, dt)
+        hyd = HydroParams(tau0, etabar, T_fo_GeV, 0, T_reg_GeV)
+        c, keep = _hotspots_c(hs)
+        eid = ctypes.c_int(-1)
+        rc = self._L.gvh_batch_add_event_hotspots(self._h, ctypes.byref(lat), ctypes.byref(hyd), ctypes.byref(c),
+                                                  ctypes.byref(eid))
+        if rc == GVH_ERR_NOMEM:
+            return None
+        _bcheck(rc, "gvh_batch_add_event_hotspots")
         self.events[eid.value] = (nx, ny, nz)
         return eid.value
 

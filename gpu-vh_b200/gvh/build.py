@@ -8,6 +8,9 @@ PKG_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))  # gpu-vh
 REPO_ROOT = os.path.dirname(PKG_ROOT)
 CSRC = os.path.join(PKG_ROOT, "csrc")
 LIB = os.path.join(PKG_ROOT, "libgvh.so")
+# the same sources with every stage cell's stencil indices checked (GVH_BOUNDS_CHECK): a cell
+# whose indices leave the arrays is skipped and raises GVH_STATUS_BOUNDS; for debugging
+BOUNDS_LIB = os.path.join(PKG_ROOT, "libgvh_bounds.so")
 EXE = os.path.join(PKG_ROOT, "gvh-run")
 
 NVCC_FLAGS = [
@@ -36,14 +39,16 @@ def needs_rebuild() -> bool:
     return any(os.path.getmtime(d) > t for d in deps if os.path.isfile(d))
 
 
-def build(verbose: bool = True, ptxas_info: bool = False) -> str:
-    """Compiles every source to an object in parallel (gpu-vh_b200/_build/), then links."""
+def build(verbose: bool = True, ptxas_info: bool = False, bounds_check: bool = False) -> str:
+    """Compiles every source to an object in parallel (gpu-vh_b200/_build/), then links.
+    bounds_check builds BOUNDS_LIB instead of LIB (and no executable)."""
     from concurrent.futures import ThreadPoolExecutor
 
     nvcc = os.environ.get("NVCC", "nvcc")
-    obj_dir = os.path.join(PKG_ROOT, "_build")
+    obj_dir = os.path.join(PKG_ROOT, "_build", "bounds" if bounds_check else "")
     os.makedirs(obj_dir, exist_ok=True)
-    compile_flags = [f for f in NVCC_FLAGS if f != "-shared"]
+    compile_flags = [f for f in NVCC_FLAGS if f != "-shared"] + (["-DGVH_BOUNDS_CHECK"] if bounds_check else [])
+    lib = BOUNDS_LIB if bounds_check else LIB
 
     def compile_one(src):
         obj = os.path.join(obj_dir, os.path.basename(src) + ".o")
@@ -58,10 +63,14 @@ def build(verbose: bool = True, ptxas_info: bool = False) -> str:
         results = list(ex.map(compile_one, sources()))
     objs = [o for o, _ in results]
     log = "".join(out for _, out in results)
-    r = subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB] + objs,
+    r = subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", lib] + objs,
                        stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
     if r.returncode != 0:
         raise RuntimeError("libgvh link failed:\n" + r.stdout)
+    if bounds_check:
+        if verbose:
+            print(f"[gvh] built {lib}")
+        return log
     exe = [nvcc, "-O2", "-std=c++17", "-o", EXE, os.path.join(CSRC, "gvh_run_main.cpp"), "-L" + PKG_ROOT, "-lgvh",
            "-Xlinker", "-rpath=$ORIGIN"]
     r2 = subprocess.run(exe, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)

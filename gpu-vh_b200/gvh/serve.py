@@ -16,7 +16,8 @@ Requests arrive over time (a Poisson stream in the benchmark). The server keeps 
 Latency of a request = completion time - arrival time. A request carries the recipe of
 its initial condition (grid, impact parameter, eta/s, seed); the server generates the
 initial state when it admits the request, so that generation is part of the server's time
-and of the request's latency, then copies it to the device. The report gives events/hour
+and of the request's latency: the sources (nucleon participants) on the host, the lattice
+fill on the device (gvh_batch_add_event_hotspots). The report gives events/hour
 (events that reached freeze-out; events retired by a status bit or a step cap are
 reported beside it as `completed`), p50/p99 latency and cell-updates/s.
 """
@@ -50,6 +51,13 @@ class Request:
     max_steps: int = 100000
     meta: dict = field(default_factory=dict)
     ic: tuple | None = None            # (workload, impact parameter): the generator's inputs
+
+    def hotspots(self):
+        """The request's hotspot sources (host Monte Carlo; the device fills the lattice)."""
+        w, b = self.ic
+        hs = workloads.hotspot_sources(w, b=b)
+        self.meta = hs.meta
+        return hs
 
     def initial_state(self) -> dict:
         """The primitive initial state, generated on first use (seeded, so the same request
@@ -144,10 +152,14 @@ class Server:
                     break
                 if resident and B.active_cells + cells > self.max_resident_cells:
                     break
+                # the initial state is generated here, inside the request's latency: its
+                # sources on the host, the lattice fill on the device where the batch can
                 tg = time.perf_counter()
-                prim = r.initial_state()  # generated here: part of the request's latency
+                if r.prim is None and r.ic is not None and hasattr(B, "add_event_hotspots"):
+                    eid = B.add_event_hotspots(**r.lattice, hs=r.hotspots(), tau0=r.tau0, T_fo_GeV=r.T_fo_GeV)
+                else:
+                    eid = B.add_event(**r.lattice, prim=r.initial_state(), tau0=r.tau0, T_fo_GeV=r.T_fo_GeV)
                 ic_seconds += time.perf_counter() - tg
-                eid = B.add_event(**r.lattice, prim=prim, tau0=r.tau0, T_fo_GeV=r.T_fo_GeV)
                 if eid is None:
                     break
                 waiting.popleft()

@@ -99,19 +99,29 @@ def _sample_woods_saxon(rng, A, R, a):
     return np.array(out[:A])
 
 
-def glauber_hotspots(w: Workload, b=None, e0_GeV=40.0, A=197, R=6.4, a=0.54, sigma_nn=4.2, sigma_hot=0.4,
-                     eta_flat=1.0, sigma_eta=0.6, b_max=10.0, background_GeV=0.05) -> dict:
-    """Fluctuating event: Gaussian hotspots (width sigma_hot) at the participants of two
-    Woods-Saxon nuclei at impact parameter b ~ U(0, b_max), each with a Gamma(k=1) weight.
-    A nucleon participates when it passes within sqrt(sigma_nn/pi) of a nucleon of the
-    other nucleus. The transverse profile is scaled so that its mean over the participant
-    positions is e0; the rapidity profile is flat for |eta| < eta_flat with Gaussian tails.
+@dataclass
+class Hotspots:
+    """The sources of a Glauber-hotspot event: e(x, y, eta) = fz(eta) * scale *
+    sum_p w_p exp(-((x - x_p)^2 + (y - y_p)^2) / s2) + background with
+    fz = exp(-max(|eta| - eta_flat, 0)^2 / s2_eta), s2 = 2 sigma^2, s2_eta = 2 sigma_eta^2
+    (energy densities in fm^-4)."""
+    x: np.ndarray
+    y: np.ndarray
+    w: np.ndarray
+    sigma: float
+    scale: float
+    eta_flat: float
+    sigma_eta: float
+    background: float
+    meta: dict
 
-    background_GeV is a uniform energy density under the event (below e(T_fo) = 0.28
-    GeV/fm^3, so it never delays freeze-out). The reference scheme, with its 1e-3 fm^-4 floor
-    alone, runs away in the near-vacuum around steep hotspots: on a 61x61 lattice at 0.2 fm the
-    oracle (bit-identical to the reference's CPU build) reaches NaN after ~44 steps; with
-    0.05 GeV/fm^3 underneath it stays finite."""
+
+def hotspot_sources(w: Workload, b=None, e0_GeV=40.0, A=197, R=6.4, a=0.54, sigma_nn=4.2, sigma_hot=0.4,
+                    eta_flat=1.0, sigma_eta=0.6, b_max=10.0, background_GeV=0.05) -> Hotspots:
+    """The Monte-Carlo part of glauber_hotspots (seeded): two Woods-Saxon nuclei at impact
+    parameter b ~ U(0, b_max), their participants (a nucleon participates when it passes
+    within sqrt(sigma_nn/pi) of a nucleon of the other nucleus), Gamma(k=1) weights, and the
+    scale that makes the transverse profile's mean over the participant positions e0."""
     rng = np.random.default_rng(w.seed)
     if b is None:
         b = rng.uniform(0, b_max)
@@ -125,18 +135,47 @@ def glauber_hotspots(w: Workload, b=None, e0_GeV=40.0, A=197, R=6.4, a=0.54, sig
     if len(parts) == 0:
         parts = np.zeros((1, 2))
     weights = rng.gamma(1.0, 1.0, len(parts))
+    at_parts = (weights[:, None] * np.exp(-((parts[None, :, :] - parts[:, None, :]) ** 2).sum(-1)
+                                          / (2 * sigma_hot ** 2))).sum(0)
+    scale = (e0_GeV / HBARC) / max(at_parts.mean(), 1e-30)
+    return Hotspots(np.ascontiguousarray(parts[:, 0]), np.ascontiguousarray(parts[:, 1]), weights, sigma_hot, scale,
+                    eta_flat, sigma_eta, background_GeV / HBARC,
+                    dict(b=float(b), n_part=int(len(parts)), seed=w.seed))
+
+
+def hotspot_field(w: Workload, hs: Hotspots) -> np.ndarray:
+    """The ghosted energy density of the sources as the type-10 reader stores it (float,
+    + 1e-3). The device fill (gvh_set_hotspot_state) follows the same operations."""
     Z, Y, X = coords(w)
     x = X[0, 0, :]
     y = Y[0, :, 0]
-    gx = np.exp(-(x[None, :] - parts[:, 0:1]) ** 2 / (2 * sigma_hot ** 2))  # (P, ncx)
-    gy = np.exp(-(y[None, :] - parts[:, 1:2]) ** 2 / (2 * sigma_hot ** 2))  # (P, ncy)
-    T = np.einsum("p,py,px->yx", weights, gy, gx)
-    at_parts = (weights[:, None] * np.exp(-((parts[None, :, :] - parts[:, None, :]) ** 2).sum(-1)
-                                          / (2 * sigma_hot ** 2))).sum(0)
-    T *= (e0_GeV / HBARC) / max(at_parts.mean(), 1e-30)
+    s2 = 2 * hs.sigma ** 2
+    T = np.zeros((len(y), len(x)))
+    for p in range(len(hs.w)):  # sources in order: sum_p (w_p gy_p) gx_p
+        gx = np.exp(-(x - hs.x[p]) ** 2 / s2)
+        gy = np.exp(-(y - hs.y[p]) ** 2 / s2)
+        T += (hs.w[p] * gy)[:, None] * gx[None, :]
+    T = T * hs.scale
     z = Z[:, 0, 0]
-    fz = np.exp(-np.maximum(np.abs(z) - eta_flat, 0) ** 2 / (2 * sigma_eta ** 2))
-    e = fz[:, None, None] * T[None, :, :] + background_GeV / HBARC
-    prim = _primitive(w, _as_file_values(e))
-    prim["_meta"] = dict(b=float(b), n_part=int(len(parts)), seed=w.seed)
+    fz = np.exp(-np.maximum(np.abs(z) - hs.eta_flat, 0) ** 2 / (2 * hs.sigma_eta ** 2))
+    e = fz[:, None, None] * T[None, :, :] + hs.background
+    return _as_file_values(e)
+
+
+def glauber_hotspots(w: Workload, b=None, e0_GeV=40.0, A=197, R=6.4, a=0.54, sigma_nn=4.2, sigma_hot=0.4,
+                     eta_flat=1.0, sigma_eta=0.6, b_max=10.0, background_GeV=0.05) -> dict:
+    """Fluctuating event: Gaussian hotspots (width sigma_hot) at the participants of two
+    Woods-Saxon nuclei at impact parameter b ~ U(0, b_max), each with a Gamma(k=1) weight
+    (hotspot_sources), filled into the lattice (hotspot_field). The transverse profile is
+    scaled so that its mean over the participant positions is e0; the rapidity profile is
+    flat for |eta| < eta_flat with Gaussian tails.
+
+    background_GeV is a uniform energy density under the event (below e(T_fo) = 0.28
+    GeV/fm^3, so it never delays freeze-out). The reference scheme, with its 1e-3 fm^-4 floor
+    alone, runs away in the near-vacuum around steep hotspots: on a 61x61 lattice at 0.2 fm the
+    oracle (bit-identical to the reference's CPU build) reaches NaN after ~44 steps; with
+    0.05 GeV/fm^3 underneath it stays finite."""
+    hs = hotspot_sources(w, b, e0_GeV, A, R, a, sigma_nn, sigma_hot, eta_flat, sigma_eta, b_max, background_GeV)
+    prim = _primitive(w, hotspot_field(w, hs))
+    prim["_meta"] = hs.meta
     return prim

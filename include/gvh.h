@@ -54,7 +54,10 @@ extern "C" {
 #define GVH_STATUS_DAMPED 4u       /* informational: a Newton solve needed the damped update
                                       (the reference switches to it after 5e5 undamped
                                       iterations, EnergyMomentumTensor.cu:37-38; here after 200) */
-#define GVH_STATUS_ERRORS 1u       /* the bits that mean the state is not trustworthy */
+#define GVH_STATUS_BOUNDS 8u       /* the bounds-checked build (libgvh_bounds.so, compiled with
+                                      GVH_BOUNDS_CHECK) found a stencil index outside the
+                                      lattice's arrays and skipped that cell */
+#define GVH_STATUS_ERRORS 9u       /* the bits that mean the state is not trustworthy */
 
 #define GVH_EOS_QCD 0              /* Wuppertal-Budapest fit (the reference default) */
 #define GVH_EOS_CONFORMAL 1        /* p = e/3 (CONFORMAL_EOS, EquationOfState.cuh:16) */
@@ -122,6 +125,31 @@ int gvh_set_primitive_state(gvh_handle *h, const double *const *prim, int n_prim
  * (setConservedVariables, DynamicalVariables.cu:349-392). */
 int gvh_set_primitive_state_p(gvh_handle *h, const double *const *prim, int n_prim, const double *p_ghosted);
 int gvh_set_state(gvh_handle *h, const double *const *fields, int n_fields);
+
+/* A Glauber-hotspot initial state, generated on the device (the seeded event generator of
+ * the benchmark's events; the reference builds its initial states on the host, e.g. its
+ * Monte-Carlo Glauber model, MonteCarloGlauberModel.cpp:19-110 with InitialConditions.cpp
+ * :1168-1245). The caller draws the sources (nucleon participants and weights); the lattice
+ * fill runs on the device:
+ *   e(x, y, eta) = fz(eta) * scale * sum_p w_p exp(-((x - x_p)^2 + (y - y_p)^2) / (2 sigma^2))
+ *                  + background,   fz = exp(-max(|eta| - eta_flat, 0)^2 / (2 sigma_eta^2)),
+ * on the cell centres x_i = (i - (nx - 1)/2) dx (likewise y, eta), each value rounded to float
+ * and + 1e-3 as the type-10 reader stores a value written to its files
+ * (InitialConditions.cpp:106, 122-124); u = (1, 0, 0, 0), pi^{mu nu} = Pi = 0, p = p(e). Only
+ * the 3n source values cross to the device. */
+typedef struct gvh_hotspots {
+	int n;               /* sources */
+	const double *x;     /* source positions (fm) and weights: host arrays of n values */
+	const double *y;
+	const double *w;
+	double sigma;        /* Gaussian width of a source (fm) */
+	double scale;        /* multiplies the weighted sum (fm^-4) */
+	double eta_flat;     /* |eta| up to which the longitudinal profile is flat */
+	double sigma_eta;    /* width of its Gaussian tails */
+	double background;   /* added everywhere (fm^-4) */
+} gvh_hotspots;
+int gvh_set_hotspot_state(gvh_handle *h, const gvh_hotspots *hs);
+
 /* Null entries are skipped. Ghost layers come back zero-gradient filled, edges and
  * corners included. Synchronises the handle's stream. */
 int gvh_get_state(gvh_handle *h, double *const *fields, int n_fields);
@@ -271,6 +299,10 @@ int gvh_batch_set_stream(gvh_batch *b, void *stream);
  * event's set-up is queued behind the work in flight. */
 int gvh_batch_add_event(gvh_batch *b, const gvh_lattice_params *lattice, const gvh_hydro_params *hydro,
                         const double *const *prim, int n_prim, int *event_id);
+/* The same with the initial state generated on the device from hotspot sources (as
+ * gvh_set_hotspot_state): only the sources cross to the device. */
+int gvh_batch_add_event_hotspots(gvh_batch *b, const gvh_lattice_params *lattice, const gvh_hydro_params *hydro,
+                                 const gvh_hotspots *hotspots, int *event_id);
 int gvh_batch_remove_event(gvh_batch *b, int event_id);
 int gvh_batch_num_events(const gvh_batch *b);
 long long gvh_batch_free_bytes(const gvh_batch *b);
