@@ -66,6 +66,9 @@ def parse():
     ap.add_argument("--serving-rate", type=float, default=4.0)
     ap.add_argument("--batch64-seconds", type=float, default=120.0,
                     help="time limit of the 64-event batched run (0 skips it)")
+    ap.add_argument("--stage-case", default="", choices=["", "fp64", "mixed"],
+                    help="only --warmup + --steps RK2 steps of the 131x131x61 event in this precision "
+                         "(a small case for profiling the stage kernel); prints one JSON line")
     ap.add_argument("--surface-slabs", type=int, default=0,
                     help="only the freeze-out surface of N slabs of the 131x131x61 event after "
                          "300 steps (text only, as the run loop keeps it); for profiling its kernels")
@@ -805,6 +808,25 @@ def run_ours(args):
     return 0
 
 
+def stage_case(precision, steps, warmup):
+    """W + K steps of the benchmark event on one lattice in the given precision, timed with
+    CUDA events over the K steps (the profiling case of the stage kernel)."""
+    import torch
+
+    import gvh
+
+    w, prim, _ = make_event(workloads.CONFIG2, 0)
+    L = gvh.Lattice(device=0, precision=precision, **w.lattice_kwargs())
+    L.set_primitive(prim)
+    stream = torch.cuda.Stream()
+    L.set_stream(stream.cuda_stream)
+    ms = time_steps(L, w, steps, warmup, stream)
+    print(json.dumps({"stage_case": precision, "steps": steps, "warmup": warmup, "ms_per_step": ms,
+                      "status": L.status()}))
+    L.close()
+    return 0
+
+
 def surface_slabs(n_slabs, warm_steps=300):
     """The surface of n_slabs consecutive slabs of the benchmark event, taken after
     warm_steps steps (where the surface is about 47 k crossed hypercubes a slab): step, then
@@ -846,6 +868,8 @@ def main():
         return run_reference(args)
     if args.surface_slabs > 0:
         return surface_slabs(args.surface_slabs)
+    if args.stage_case:
+        return stage_case(args.stage_case, args.steps, args.warmup)
     return run_ours(args)
 
 
