@@ -257,9 +257,13 @@ struct gvh_batch {
   int ntiles = 0;                        // tiles of the admitted events
   int active_slots = 0;                  // slots the finish kernel scans
   long long next_serial = 1;
-  PinnedBuf prim_stage[2];               // initial states on their way to the device
+  // initial states and tile tables on their way to the device: rings deep enough that the
+  // admissions and retirements of one serving iteration do not wait for a copy that is queued
+  // behind the rounds in flight
+  static constexpr int kPrimRing = 4, kTileRing = 8;
+  PinnedBuf prim_stage[kPrimRing];
   int prim_next = 0;
-  PinnedBuf tile_stage[2];               // tile tables on their way to the device
+  PinnedBuf tile_stage[kTileRing];
   int tile_next = 0;
   // serving rounds: two snapshots in mapped host memory, alternating by ticket
   gvh_event_info *snap_h[2] = {nullptr, nullptr}, *snap_d[2] = {nullptr, nullptr};
@@ -347,7 +351,7 @@ int rebuild_tiles(gvh_batch *b) {
     }
   if (n > b->tile_capacity) return bfail(GVH_ERR_NOMEM, "tile table full");
   PinnedBuf &pb = b->tile_stage[b->tile_next];
-  b->tile_next ^= 1;
+  b->tile_next = (b->tile_next + 1) % gvh_batch::kTileRing;
   int rc = pinned_reserve(pb, (size_t)(n + 1) * sizeof(int));
   if (rc) return rc;
   int *table = static_cast<int *>(pb.h);
@@ -543,9 +547,13 @@ int gvh_batch_destroy(gvh_batch *b) {
   cudaFree(b->d_ntiles);
   cudaFree(b->d_scratch);
   if (b->staging) cudaFree(b->staging);
-  for (PinnedBuf *pb : {&b->prim_stage[0], &b->prim_stage[1], &b->tile_stage[0], &b->tile_stage[1]}) {
-    if (pb->h) cudaFreeHost(pb->h);
-    if (pb->done) cudaEventDestroy(pb->done);
+  for (PinnedBuf &pb : b->prim_stage) {
+    if (pb.h) cudaFreeHost(pb.h);
+    if (pb.done) cudaEventDestroy(pb.done);
+  }
+  for (PinnedBuf &pb : b->tile_stage) {
+    if (pb.h) cudaFreeHost(pb.h);
+    if (pb.done) cudaEventDestroy(pb.done);
   }
   for (int r = 0; r < 2; ++r) {
     if (b->snap_h[r]) cudaFreeHost(b->snap_h[r]);
@@ -614,7 +622,7 @@ int admit_event(gvh_batch *b, const gvh_lattice_params *L, const gvh_hydro_param
   // the initial state (or its sources) goes to the device through a pinned buffer: the host
   // copy happens here, the transfer is queued behind the work in flight and nothing waits
   PinnedBuf &pb = b->prim_stage[b->prim_next];
-  b->prim_next ^= 1;
+  b->prim_next = (b->prim_next + 1) % gvh_batch::kPrimRing;
   const size_t fb = h.ng * sizeof(double);
   if ((rc = pinned_reserve(pb, prim ? n_prim * fb : 3 * hs->n * sizeof(double)))) {
     arena_free(b, h.off, h.bytes);
