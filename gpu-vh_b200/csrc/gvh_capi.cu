@@ -503,6 +503,102 @@ int gvh_get_validity(gvh_handle *h, double *const *fields, int n_fields) {
   return GVH_OK;
 }
 
+// ---- checkpoint / resume ----------------------------------------------------------------
+// File: a fixed header (magic, version, lattice sizes, options, spacings, the caller's time
+// and step), then the nq + 10 fields of the interior lattice (field order of gvh_set_state,
+// cell s = i + nx (j + ny k)) as native doubles, then an FNV-1a 64 checksum of those bytes.
+namespace {
+
+struct SnapshotHeader {
+  char magic[8];          // "GVHSTATE"
+  unsigned version;       // 1
+  int nx, ny, nz, nq;
+  int eos, shear, bulk, precision;
+  double theta, dx, dy, dz, dt, etabar;
+  double tau;
+  long long step;
+};
+
+unsigned long long fnv1a(const void *data, size_t n, unsigned long long h) {
+  const unsigned char *p = static_cast<const unsigned char *>(data);
+  for (size_t i = 0; i < n; ++i) h = (h ^ p[i]) * 0x100000001b3ull;
+  return h;
+}
+
+}  // namespace
+
+int gvh_save_state(gvh_handle *h, const char *path, double tau, long long step) {
+  if (!h || !path) return fail(GVH_ERR_INVALID, "gvh_save_state: null argument");
+  int rc;
+  if ((rc = set_device(h))) return rc;
+  GVH_CUDA(cudaStreamSynchronize(h->stream));
+  SnapshotHeader hd;
+  memset(&hd, 0, sizeof hd);
+  memcpy(hd.magic, "GVHSTATE", 8);
+  hd.version = 1;
+  hd.nx = h->nx; hd.ny = h->ny; hd.nz = h->nz; hd.nq = h->nq;
+  hd.eos = h->eos; hd.shear = h->shear; hd.bulk = h->bulk; hd.precision = h->precision;
+  hd.theta = h->theta; hd.dx = h->dx; hd.dy = h->dy; hd.dz = h->dz; hd.dt = h->dt_lattice; hd.etabar = h->etabar;
+  hd.tau = tau;
+  hd.step = step;
+  FILE *f = fopen(path, "wb");
+  if (!f) return fail(GVH_ERR_INVALID, "gvh_save_state: cannot open %s", path);
+  double *fields[32];
+  internal_fields(h, fields);
+  std::string buf((size_t)h->ncells * sizeof(double), '\0');
+  unsigned long long sum = 0xcbf29ce484222325ull;
+  bool ok = fwrite(&hd, sizeof hd, 1, f) == 1;
+  for (int k = 0; ok && k < h->nq + 10; ++k) {
+    cudaError_t e = cudaMemcpy(&buf[0], fields[k], buf.size(), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) {
+      fclose(f);
+      return fail(GVH_ERR_CUDA, "gvh_save_state: %s", cudaGetErrorString(e));
+    }
+    sum = fnv1a(buf.data(), buf.size(), sum);
+    ok = fwrite(buf.data(), 1, buf.size(), f) == buf.size();
+  }
+  ok = ok && fwrite(&sum, sizeof sum, 1, f) == 1;
+  ok = (fclose(f) == 0) && ok;
+  if (!ok) return fail(GVH_ERR_INVALID, "gvh_save_state: writing %s failed", path);
+  return GVH_OK;
+}
+
+int gvh_load_state(gvh_handle *h, const char *path, double *tau, long long *step) {
+  if (!h || !path) return fail(GVH_ERR_INVALID, "gvh_load_state: null argument");
+  int rc;
+  if ((rc = set_device(h))) return rc;
+  FILE *f = fopen(path, "rb");
+  if (!f) return fail(GVH_ERR_INVALID, "gvh_load_state: cannot open %s", path);
+  SnapshotHeader hd;
+  if (fread(&hd, sizeof hd, 1, f) != 1 || memcmp(hd.magic, "GVHSTATE", 8) != 0 || hd.version != 1) {
+    fclose(f);
+    return fail(GVH_ERR_INVALID, "gvh_load_state: %s is not a state snapshot", path);
+  }
+  if (hd.nx != h->nx || hd.ny != h->ny || hd.nz != h->nz || hd.nq != h->nq || hd.eos != h->eos ||
+      hd.shear != h->shear || hd.bulk != h->bulk) {
+    fclose(f);
+    return fail(GVH_ERR_INVALID, "gvh_load_state: %s holds a %dx%dx%d lattice with %d components, eos %d; the handle "
+                                 "has %dx%dx%d, %d, eos %d", path, hd.nx, hd.ny, hd.nz, hd.nq, hd.eos, h->nx, h->ny,
+                h->nz, h->nq, h->eos);
+  }
+  // read and check everything before the device state changes
+  const size_t fb = (size_t)h->ncells * sizeof(double);
+  std::string data((size_t)(h->nq + 10) * fb, '\0');
+  unsigned long long sum_file = 0;
+  const bool got = fread(&data[0], 1, data.size(), f) == data.size() && fread(&sum_file, sizeof sum_file, 1, f) == 1;
+  fclose(f);
+  if (!got) return fail(GVH_ERR_INVALID, "gvh_load_state: %s is truncated", path);
+  if (fnv1a(data.data(), data.size(), 0xcbf29ce484222325ull) != sum_file)
+    return fail(GVH_ERR_INVALID, "gvh_load_state: %s fails its checksum", path);
+  GVH_CUDA(cudaStreamSynchronize(h->stream));
+  double *fields[32];
+  internal_fields(h, fields);
+  for (int k = 0; k < h->nq + 10; ++k) GVH_CUDA(cudaMemcpy(fields[k], data.data() + k * fb, fb, cudaMemcpyHostToDevice));
+  if (tau) *tau = hd.tau;
+  if (step) *step = hd.step;
+  return GVH_OK;
+}
+
 int gvh_set_stream(gvh_handle *h, void *stream) {
   if (!h) return fail(GVH_ERR_INVALID, "null handle");
   GVH_CUDA(cudaSetDevice(h->device));

@@ -83,7 +83,7 @@ EXPORTS = [
     "gvh_default_options", "gvh_create", "gvh_destroy", "gvh_num_conserved", "gvh_num_fields",
     "gvh_num_lattice_cells", "gvh_set_primitive_state", "gvh_set_state", "gvh_get_state", "gvh_rk2_step",
     "gvh_status", "gvh_clear_status", "gvh_synchronize", "gvh_launches_per_step", "gvh_last_error",
-    "gvh_set_stream", "gvh_max_energy_density", "gvh_max_propagation_speed", "gvh_set_hotspot_state", "gvh_set_state_async", "gvh_get_state_async", "gvh_join_async",
+    "gvh_set_stream", "gvh_max_energy_density", "gvh_max_propagation_speed", "gvh_set_hotspot_state", "gvh_save_state", "gvh_load_state", "gvh_set_state_async", "gvh_get_state_async", "gvh_join_async",
 ]
 
 
@@ -122,6 +122,8 @@ def load(path: str | None = None):
     L.gvh_max_energy_density.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
     L.gvh_max_propagation_speed.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
     L.gvh_set_hotspot_state.argtypes = [vp, vp]
+    L.gvh_save_state.argtypes = [vp, ctypes.c_char_p, dp, ctypes.c_longlong]
+    L.gvh_load_state.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(dp), ctypes.POINTER(ctypes.c_longlong)]
     L.gvh_last_error.restype = ctypes.c_char_p
     if path is None:
         _lib = L
@@ -215,6 +217,17 @@ class Lattice:
                                                           ctypes.c_void_p]
             _check(self._L.gvh_set_primitive_state_p(self._h, ptrs, len(arrs), pa.ctypes.data),
                    "gvh_set_primitive_state_p")
+
+    def save(self, path, tau=0.0, step=0):
+        """Binary snapshot of the state (with the caller's tau and step) to path."""
+        _check(self._L.gvh_save_state(self._h, os.fsencode(path), float(tau), int(step)), "gvh_save_state")
+
+    def load(self, path):
+        """Restore a snapshot written by save(); returns (tau, step)."""
+        t, n = ctypes.c_double(), ctypes.c_longlong()
+        _check(self._L.gvh_load_state(self._h, os.fsencode(path), ctypes.byref(t), ctypes.byref(n)),
+               "gvh_load_state")
+        return t.value, n.value
 
     def set_hotspots(self, hs):
         """Initial state from hotspot sources (a workloads.Hotspots), filled on the device."""

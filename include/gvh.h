@@ -253,6 +253,17 @@ int gvh_get_validity(gvh_handle *h, double *const *fields, int n_fields);
  * T = T_GeV / hbarc, in fm^-4: the freeze-out threshold of HydroPlugin.cpp:131-135. */
 double gvh_energy_density_of_temperature(int eos, double T_GeV);
 
+/* Checkpoint and resume (the reference has none: its field dumps are text in another order
+ * than its readers expect, FileIO.cpp:47-56 against InitialConditions.cpp:119-121). A binary
+ * snapshot of the handle's state -- the interior lattice's nq + 10 fields, with the lattice
+ * sizes, options, spacings, the caller's time tau and step count, and a checksum -- is written
+ * after the work queued so far; gvh_load_state restores it into a handle of the same lattice
+ * and physics (else GVH_ERR_INVALID), checking the file before changing anything, and returns
+ * tau and step (may be null). Steps from a restored state give the values the original run
+ * gives. */
+int gvh_save_state(gvh_handle *h, const char *path, double tau, long long step);
+int gvh_load_state(gvh_handle *h, const char *path, double *tau, long long *step);
+
 /* Runs the handle's work on a caller-owned stream (a cudaStream_t passed as void*); NULL
  * returns to the handle's own stream. Waits for work already queued on the old stream. */
 int gvh_set_stream(gvh_handle *h, void *stream);

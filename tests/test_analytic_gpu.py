@@ -1,0 +1,45 @@
+"""The known-answer physics tests of tests/test_analytic_host.py on the CUDA path, plus what
+only a fast path makes cheap: a uniform 3-D lattice stays uniform under Bjorken flow, and the
+Gubser-flow error shrinks with resolution (L1 error of e 1.03e-2 -> 3.9e-3 and of u^x
+6.0e-3 -> 1.9e-3 from 0.1 to 0.05 fm on the oracle, the same scheme)."""
+import numpy as np
+import pytest
+
+import analytic
+import gvh
+import oracle
+from test_analytic_host import E0, bjorken_run, gubser_run
+
+pytestmark = pytest.mark.gpu
+
+
+def test_bjorken_conformal_on_cuda():
+    _, e = bjorken_run(gvh.Lattice, True)
+    heun = analytic.heun_bjorken(E0, 1.0, 0.01, 4000, lambda x: x / 3)
+    assert abs(e[0] - heun) <= 1e-12 * heun
+    assert abs(e[0] - analytic.bjorken_conformal(E0, 1.0, 41.0)) <= 2e-5 * heun
+
+
+def test_bjorken_qcd_on_cuda_uniform_lattice_stays_uniform():
+    L, e = bjorken_run(gvh.Lattice, False, steps=1000, shape=(6, 5, 4))
+    assert np.all(e == e[0])
+    O = oracle.OracleLattice(nx=1, ny=1, nz=1, dx=0.1, dy=0.1, dz=0.1, dt=0.01, etabar=0.2, theta=1.8,
+                             conformal=False, shear=False, bulk=False)
+    ref = analytic.rk4_bjorken(E0, 1.0, 11.0, O.pressure, n=20000)
+    assert abs(e[0] - ref) <= 1e-5 * ref
+
+
+def test_gubser_flow_on_cuda_converges():
+    coarse = gubser_run(gvh.Lattice, 81, 0.1, 0.01)
+    fine = gubser_run(gvh.Lattice, 161, 0.05, 0.005)
+    assert coarse["l1_e"] <= 1.5e-2 and coarse["l1_ux"] <= 1e-2, coarse
+    assert fine["l1_e"] <= 0.5 * coarse["l1_e"] and fine["l1_ux"] <= 0.5 * coarse["l1_ux"], (coarse, fine)
+    assert fine["centre_e"] <= 5e-4, fine
+    # the CUDA path is the oracle's scheme: the coarse run agrees with it to rounding
+    ref = gubser_run(oracle.OracleLattice, 81, 0.1, 0.01)
+    L = oracle.OracleLattice(nx=81, ny=81, nz=1, dx=0.1, dy=0.1, dz=0.1, dt=0.01, etabar=0.2, theta=1.8,
+                             conformal=True, shear=False, bulk=False)
+    a, b = coarse["state"], ref["state"]
+    errs = {k: float(np.max(np.abs(L.interior(a[k]) - L.interior(b[k]))) / np.max(np.abs(L.interior(b[k]))))
+            for k in ("e", "ux", "uy", "ttt")}
+    assert max(errs.values()) <= 1e-10, errs

@@ -8,7 +8,10 @@
    iso-value, unequal edges), and an error exactly where the reference exits.
 """
 import ctypes
+import json
 import os
+import subprocess
+import sys
 
 import numpy as np
 import pytest
@@ -104,17 +107,18 @@ def test_error_where_reference_exits(dim, v, dx):
     L = lib()
     rc, _, _ = ours(L, dim, np.array(v), np.array(dx), 0.5)
     assert rc == gvh.GVH_ERR_NUMERIC
-    pid = os.fork()
-    if pid == 0:  # the reference in a child: its exit must not end the test process
-        os.dup2(os.open(os.devnull, os.O_WRONLY), 1)
-        R = ctypes.CDLL(REF_LIB)
-        R.gvh_refc_find.argtypes = [ctypes.c_int, dp, dp, ctypes.c_double, dp, dp, ctypes.c_int]
-        va, da, buf = np.array(v), np.array(dx), np.zeros(40)
-        R.gvh_refc_find(dim, va.ctypes.data_as(dp), da.ctypes.data_as(dp), 0.5, buf.ctypes.data_as(dp),
-                        buf.ctypes.data_as(dp), 10)
-        os._exit(0)
-    _, status = os.waitpid(pid, 0)
-    assert os.WIFEXITED(status) and os.WEXITSTATUS(status) == 1
+    # the reference in a separate process: its exit must not end the test process
+    child = ("import ctypes, json, sys\n"
+             "import numpy as np\n"
+             "dp = ctypes.POINTER(ctypes.c_double)\n"
+             "R = ctypes.CDLL(sys.argv[1])\n"
+             "R.gvh_refc_find.argtypes = [ctypes.c_int, dp, dp, ctypes.c_double, dp, dp, ctypes.c_int]\n"
+             "va, da, buf = np.array(json.loads(sys.argv[2])), np.array(json.loads(sys.argv[3])), np.zeros(40)\n"
+             "R.gvh_refc_find(int(sys.argv[4]), va.ctypes.data_as(dp), da.ctypes.data_as(dp), 0.5,\n"
+             "                buf.ctypes.data_as(dp), buf.ctypes.data_as(dp), 10)\n")
+    r = subprocess.run([sys.executable, "-c", child, REF_LIB, json.dumps(list(v)), json.dumps(list(dx)), str(dim)],
+                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL, timeout=60)
+    assert r.returncode == 1
 
 
 def test_normals_point_to_lower_values_and_close():
