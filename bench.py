@@ -500,8 +500,9 @@ def serving_mix_requests(n, seed=64):
 
 def fp64_single_path_requests(reqs, device, max_steps=6000):
     """The plain FP64 single-event path on the given requests, one after another: generate
-    the initial state, run the event alone on a gvh.Lattice the way the reference's loop runs
-    it (max e against e(T_fo) before every step, stop after 11 all-frozen checks,
+    the initial state (the sources on the host, the lattice fill on the device, as the serving
+    path does), run the event alone on a gvh.Lattice the way the reference's loop runs it (max
+    e against e(T_fo) before every step, stop after 11 all-frozen checks,
     HydroPlugin.cpp:396-413), or until a NaN status bit retires it. events_per_hour counts
     the events that reached freeze-out over the total time."""
     import gvh
@@ -510,12 +511,11 @@ def fp64_single_path_requests(reqs, device, max_steps=6000):
     total = 0.0
     for r in reqs:
         t0 = time.perf_counter()
-        prim = r.initial_state()
         lat = r.lattice
         L = gvh.Lattice(device=device, precision="fp64", nx=lat["nx"], ny=lat["ny"], nz=lat["nz"], dx=lat["dx"],
                         dy=lat["dy"], dz=lat["dz"], dt=lat["dt"], etabar=lat["etabar"], theta=2.0, conformal=False,
                         shear=True, bulk=True, tau0=r.tau0, T_fo_GeV=r.T_fo_GeV)
-        L.set_primitive(prim)
+        L.set_hotspots(r.hotspots())
         e_fo = gvh.energy_density_of_temperature(r.T_fo_GeV, conformal=False)
         frozen, n, t, st = 0, 0, r.tau0, 0
         while n < max_steps:
@@ -544,7 +544,8 @@ def fp64_single_path_requests(reqs, device, max_steps=6000):
             "per_grid_mean_seconds": {f"{g[0]}x{g[1]}x{g[2]}": float(np.mean([x["seconds"] for x in runs
                                                                               if tuple(x["grid"]) == g]))
                                       for g in sorted(set(tuple(x["grid"]) for x in runs))},
-            "path": "gvh.Lattice, plain FP64, one event at a time, initial state generated inside the timing"}
+            "path": "gvh.Lattice, plain FP64, one event at a time, initial state generated inside the timing "
+                    "(sources on the host, lattice fill on the device)"}
 
 
 def serving_run(args, device, rate=None, seconds=None):
