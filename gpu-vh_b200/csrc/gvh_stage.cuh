@@ -463,7 +463,7 @@ __host__ __device__ inline bool cell_stencil_ok(const StageArgs &a, int i, int j
   return true;
 }
 
-// speed: max over the three axes of the local propagation speed over the lattice spacing,
+// speed: max over the axes with more than one cell of the local propagation speed over the lattice spacing,
 // a / dx_axis (the CFL bound of the step is dt times its maximum over cells).
 template <int EOS, bool SHEAR, bool BULK, bool STAGE2, bool MIXED>
 __device__ __forceinline__ double stage_cell_ijk(const StageArgs &a, int i, int j, int k, double &speed) {
@@ -500,6 +500,13 @@ __device__ __forceinline__ double stage_cell_ijk(const StageArgs &a, int i, int 
   for (int axis = 0; axis < 3; ++axis) {
     const int idx = axis == 0 ? i : axis == 1 ? j : k;
     const int n_axis = axis == 0 ? a.nx : axis == 1 ? a.ny : a.nz;
+    // An axis with one cell (eta of a 2+1D lattice) adds nothing: its clamped stencil is the
+    // cell five times, so both faces carry the cell's own state, their two KT fluxes are the
+    // same number and their difference is exactly 0, as are the centred pi, Pi derivatives.
+    // The reference computes it anyway (EulerStep.cu:1011-1277); skipping its four face
+    // recoveries changes at most the sign of a zero. Such an axis has no faces for the CFL
+    // bound either.
+    if (n_axis == 1) continue;
     const int stride = axis == 0 ? 1 : axis == 1 ? (int)a.sy : (int)a.sz;
     const double inv_spacing = axis == 0 ? a.inv_dx : axis == 1 ? a.inv_dy : a.inv_dz;
     const double as = axis_update<EOS, SHEAR, BULK, MIXED>(a, (int)s, axis, idx, n_axis, stride, inv_spacing, g0,

@@ -224,7 +224,8 @@ const char *gvh_noalloc_last_error(void);
 int gvh_max_energy_density(gvh_handle *h, double *out);
 
 /* The CFL bound of the step: the largest local propagation speed over the lattice spacing,
- * max over interior cells, both faces and the three axes of a / dx_axis, where a is the KT
+ * max over interior cells, both faces and the axes with more than one cell of a / dx_axis
+ * (a one-cell axis, eta of a 2+1D lattice, has no faces), where a is the KT
  * spectral radius max(|u^i/u^tau| left, |u^i/u^tau| right) of the face
  * (SpectralRadius.cu:17-30, LocalPropagationSpeed.cu:15-24), in fm^-1 (dtau times it is the
  * CFL number). The first stage of every gvh_rk2_step keeps a running maximum of it, reduced on

@@ -539,7 +539,9 @@ static void euler_axis_cell(kt_lattice *L, int s, int axis, double t, double **c
 	kt_flux(P, nq, I, H, 1, axis, t, e[s], &af);
 	for (int n = 0; n < nq; ++n) result[n] = -H[n];
 	kt_flux(P, nq, I, H, 0, axis, t, e[s], &ab);
-	L->speed[s] = fmax(L->speed[s], fmax(af, ab) * (1.0 / d));
+	/* the CFL bound counts the axes with more than one cell (a one-cell axis has no faces) */
+	const int n_axis = axis == 1 ? P->nx : axis == 2 ? P->ny : P->nz;
+	if (n_axis > 1) L->speed[s] = fmax(L->speed[s], fmax(af, ab) * (1.0 / d));
 	for (int n = 0; n < nq; ++n) {
 		result[n] += H[n];
 		result[n] /= d;
