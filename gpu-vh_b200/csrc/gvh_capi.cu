@@ -123,22 +123,31 @@ int ensure_staging(gvh_handle *h) {
 int ensure_async(gvh_handle *h) {
   if (h->async_ready) return GVH_OK;
   const size_t bytes = (size_t)(h->nq + 10) * h->ng * sizeof(double);
-  if (cudaMalloc(&h->staging_in, bytes) != cudaSuccess) return fail(GVH_ERR_NOMEM, "async staging allocation failed");
-  if (cudaMalloc(&h->staging_out, bytes) != cudaSuccess) {
-    cudaFree(h->staging_in);
-    return fail(GVH_ERR_NOMEM, "async staging allocation failed");
+  double *areas[4] = {};
+  for (int a = 0; a < 4; ++a)
+    if (cudaMalloc(&areas[a], bytes) != cudaSuccess) {
+      for (int b = 0; b < a; ++b) cudaFree(areas[b]);
+      return fail(GVH_ERR_NOMEM, "async staging allocation failed");
+    }
+  for (int a = 0; a < 2; ++a) {
+    h->staging_in[a] = areas[a];
+    h->staging_out[a] = areas[2 + a];
   }
+  h->in_slot = h->out_slot = 0;
   GVH_CUDA(cudaStreamCreateWithFlags(&h->s_h2d, cudaStreamNonBlocking));
   GVH_CUDA(cudaStreamCreateWithFlags(&h->s_d2h, cudaStreamNonBlocking));
   GVH_CUDA(cudaEventCreateWithFlags(&h->ev_in_ready, cudaEventDisableTiming));
-  GVH_CUDA(cudaEventCreateWithFlags(&h->ev_in_free, cudaEventDisableTiming));
   GVH_CUDA(cudaEventCreateWithFlags(&h->ev_out_ready, cudaEventDisableTiming));
-  GVH_CUDA(cudaEventCreateWithFlags(&h->ev_out_free, cudaEventDisableTiming));
   GVH_CUDA(cudaEventCreateWithFlags(&h->ev_fence, cudaEventDisableTiming));
   // the events start recorded (complete), so the first waits pass
-  GVH_CUDA(cudaEventRecord(h->ev_in_free, h->stream));
-  GVH_CUDA(cudaEventRecord(h->ev_out_free, h->stream));
+  for (int a = 0; a < 2; ++a) {
+    GVH_CUDA(cudaEventCreateWithFlags(&h->ev_in_free[a], cudaEventDisableTiming));
+    GVH_CUDA(cudaEventCreateWithFlags(&h->ev_out_free[a], cudaEventDisableTiming));
+    GVH_CUDA(cudaEventRecord(h->ev_in_free[a], h->stream));
+    GVH_CUDA(cudaEventRecord(h->ev_out_free[a], h->stream));
+  }
   GVH_CUDA(cudaEventRecord(h->ev_in_ready, h->stream));
+  GVH_CUDA(cudaEventRecord(h->ev_out_ready, h->stream));
   h->async_ready = 1;
   return GVH_OK;
 }
@@ -257,14 +266,16 @@ int gvh_destroy(gvh_handle *h) {
   if (h->async_ready) {
     cudaStreamSynchronize(h->s_h2d);
     cudaStreamSynchronize(h->s_d2h);
-    cudaFree(h->staging_in);
-    cudaFree(h->staging_out);
+    for (int a = 0; a < 2; ++a) {
+      cudaFree(h->staging_in[a]);
+      cudaFree(h->staging_out[a]);
+      cudaEventDestroy(h->ev_in_free[a]);
+      cudaEventDestroy(h->ev_out_free[a]);
+    }
     cudaStreamDestroy(h->s_h2d);
     cudaStreamDestroy(h->s_d2h);
     cudaEventDestroy(h->ev_in_ready);
-    cudaEventDestroy(h->ev_in_free);
     cudaEventDestroy(h->ev_out_ready);
-    cudaEventDestroy(h->ev_out_free);
     cudaEventDestroy(h->ev_fence);
   }
   delete h;
@@ -664,8 +675,10 @@ int gvh_set_state_async(gvh_handle *h, const double *const *fields, int n_fields
   FieldTable dst = {};
   internal_fields(h, dst.p);
   const size_t fb = h->ng * sizeof(double);
-  // the input staging is free once the previous pack has read it
-  GVH_CUDA(cudaStreamWaitEvent(h->s_h2d, h->ev_in_free, 0));
+  // this call's staging area is free once the pack that last read it (two calls back) is done
+  const int slot = h->in_slot;
+  double *const staging = h->staging_in[slot];
+  GVH_CUDA(cudaStreamWaitEvent(h->s_h2d, h->ev_in_free[slot], 0));
   const double *srcs[32];
   for (int f = 0; f < n_fields; ++f) {
     const double *src = fields[f];
@@ -679,15 +692,15 @@ int gvh_set_state_async(gvh_handle *h, const double *const *fields, int n_fields
   for (int f = 0; f < n_fields;) {
     int g = f + 1;
     while (g < n_fields && srcs[g] == srcs[f] + (size_t)(g - f) * h->ng) ++g;
-    GVH_CUDA(cudaMemcpyAsync(h->staging_in + f * h->ng, srcs[f], (g - f) * fb, cudaMemcpyDefault, h->s_h2d));
+    GVH_CUDA(cudaMemcpyAsync(staging + f * h->ng, srcs[f], (g - f) * fb, cudaMemcpyDefault, h->s_h2d));
     f = g;
   }
   GVH_CUDA(cudaEventRecord(h->ev_in_ready, h->s_h2d));
   GVH_CUDA(cudaStreamWaitEvent(h->stream, h->ev_in_ready, 0));
-  pack_kernel<<<(unsigned)((h->ncells + 255) / 256), 256, 0, h->stream>>>(make_pack(h), n_fields, h->staging_in,
-                                                                            dst);
+  pack_kernel<<<(unsigned)((h->ncells + 255) / 256), 256, 0, h->stream>>>(make_pack(h), n_fields, staging, dst);
   GVH_CUDA(cudaGetLastError());
-  GVH_CUDA(cudaEventRecord(h->ev_in_free, h->stream));
+  GVH_CUDA(cudaEventRecord(h->ev_in_free[slot], h->stream));
+  h->in_slot = slot ^ 1;
   return GVH_OK;
 }
 
@@ -700,10 +713,12 @@ int gvh_get_state_async(gvh_handle *h, double *const *fields, int n_fields) {
   internal_fields(h, src.p);
   for (int f = 0; f < n_fields; ++f)
     if (!fields[f]) src.p[f] = nullptr;
-  // the output staging is free once the previous copy to the host has read it
-  GVH_CUDA(cudaStreamWaitEvent(h->stream, h->ev_out_free, 0));
-  unpack_kernel<<<(unsigned)((h->ng + 255) / 256), 256, 0, h->stream>>>(make_pack(h), n_fields, src,
-                                                                          h->staging_out);
+  // this call's staging area is free once the copy to the host that last read it (two calls
+  // back) is done
+  const int slot = h->out_slot;
+  double *const staging = h->staging_out[slot];
+  GVH_CUDA(cudaStreamWaitEvent(h->stream, h->ev_out_free[slot], 0));
+  unpack_kernel<<<(unsigned)((h->ng + 255) / 256), 256, 0, h->stream>>>(make_pack(h), n_fields, src, staging);
   GVH_CUDA(cudaGetLastError());
   GVH_CUDA(cudaEventRecord(h->ev_out_ready, h->stream));
   GVH_CUDA(cudaStreamWaitEvent(h->s_d2h, h->ev_out_ready, 0));
@@ -712,10 +727,11 @@ int gvh_get_state_async(gvh_handle *h, double *const *fields, int n_fields) {
     if (!fields[f]) { ++f; continue; }
     int g = f + 1;
     while (g < n_fields && fields[g] && fields[g] == fields[f] + (size_t)(g - f) * h->ng) ++g;
-    GVH_CUDA(cudaMemcpyAsync(fields[f], h->staging_out + f * h->ng, (g - f) * fb, cudaMemcpyDefault, h->s_d2h));
+    GVH_CUDA(cudaMemcpyAsync(fields[f], staging + f * h->ng, (g - f) * fb, cudaMemcpyDefault, h->s_d2h));
     f = g;
   }
-  GVH_CUDA(cudaEventRecord(h->ev_out_free, h->s_d2h));
+  GVH_CUDA(cudaEventRecord(h->ev_out_free[slot], h->s_d2h));
+  h->out_slot = slot ^ 1;
   return GVH_OK;
 }
 
@@ -725,8 +741,9 @@ int gvh_join_async(gvh_handle *h) {
   GVH_CUDA(cudaSetDevice(h->device));
   // the handle's stream waits for every queued copy, then the copy streams wait for
   // everything queued on the handle's stream up to here
+  // (each copy stream runs in order, so its last recorded event covers all its copies)
   GVH_CUDA(cudaStreamWaitEvent(h->stream, h->ev_in_ready, 0));
-  GVH_CUDA(cudaStreamWaitEvent(h->stream, h->ev_out_free, 0));
+  GVH_CUDA(cudaStreamWaitEvent(h->stream, h->ev_out_free[h->out_slot ^ 1], 0));
   GVH_CUDA(cudaEventRecord(h->ev_fence, h->stream));
   GVH_CUDA(cudaStreamWaitEvent(h->s_h2d, h->ev_fence, 0));
   GVH_CUDA(cudaStreamWaitEvent(h->s_d2h, h->ev_fence, 0));

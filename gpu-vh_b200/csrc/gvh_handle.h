@@ -19,11 +19,14 @@ struct gvh_handle {
   double *staging;          // reference-layout fields for set/get, allocated on first use
   double *diag;             // validity diagnostics (allocated by gvh_enable_validity)
   int validity_on;
-  // asynchronous set/get (allocated on first use): separate input and output staging, one
-  // copy stream each way, events that order them with the handle's stream
-  double *staging_in, *staging_out;
+  // asynchronous set/get (allocated on first use): two input and two output staging areas
+  // used in turn (a copy into one overlaps the pack of the other; an unpack into one overlaps
+  // the copy out of the other), one copy stream each way, events that order them with the
+  // handle's stream; in_slot / out_slot are the areas the next calls use
+  double *staging_in[2], *staging_out[2];
   cudaStream_t s_h2d, s_d2h;
-  cudaEvent_t ev_in_ready, ev_in_free, ev_out_ready, ev_out_free, ev_fence;
+  cudaEvent_t ev_in_ready, ev_in_free[2], ev_out_ready, ev_out_free[2], ev_fence;
+  int in_slot, out_slot;
   int async_ready;
   // mapped pinned word for small results read on the host (allocated on first use): a
   // kernel writes it, so the read needs no copy that could queue behind another stream's

@@ -168,9 +168,11 @@ int gvh_gather_state_device(gvh_handle *h, const void *const *fields, int n_fiel
 int gvh_scatter_state_device(gvh_handle *h, void *const *fields, int n_fields, int elem_bytes);
 /* Pipelined set/get for a caller that streams states through the handle (a new state in,
  * one or more steps, the result out, again and again): the copies go on the handle's own
- * copy streams, one each way, with separate device staging for inputs and outputs, and are
- * ordered with the handle's stream by events, so the next state's copy in, the step and the
- * last result's copy out overlap. The calls return without waiting. Host arrays should be
+ * copy streams, one each way, through two device staging areas each way used in turn (four
+ * copies of the ghosted state, allocated on the first call), and are ordered with the
+ * handle's stream by events, so the next state's copy in, the step and the last result's
+ * copy out overlap, and neither direction's copies wait for the layout conversion of the
+ * call before. The calls return without waiting. Host arrays should be
  * pinned (pageable memory still works but the copies then serialise) and must not be
  * touched until gvh_synchronize(h) returns. gvh_join_async(h) joins the handle's stream
  * and its copy streams both ways: work queued on the handle's stream afterwards waits for

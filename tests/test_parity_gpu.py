@@ -139,15 +139,16 @@ def test_set_get_state_round_trip():
 
 
 def test_pipelined_set_get_matches_blocking_calls():
-    """gvh_set_state_async / gvh_get_state_async with three different states in flight at
-    once (each: copy in, one step, copy out, nothing waited for in between) give exactly the
+    """gvh_set_state_async / gvh_get_state_async with five different states in flight at
+    once (each: copy in, one step, copy out, nothing waited for in between; the calls take
+    the two staging areas each way in turn, so the third to fifth reuse them) give exactly the
     blocking calls' results, state by state."""
     import torch
     lat_kw, _, _, st_kw = make_golden.CASES["qcd_bulk"]
     G = gvh.Lattice(**lat_kw)
     names = G.field_names
     states = []
-    for seed in range(3):
+    for seed in range(5):
         G.set_primitive(rich_state(G, **dict(st_kw, seed=seed)))
         G.step(0.5, lat_kw["dt"])
         states.append(G.get_state())
