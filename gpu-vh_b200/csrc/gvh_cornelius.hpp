@@ -62,17 +62,19 @@ struct Segment {
   GVH_HD void flip() { s = 1 - s; }
 };
 
+// A chain of segments of one cube, as indices into that cube's segment array.
 struct Polygon {
-  Segment *seg[kMaxSegsPerPoly];
-  int n;
-  int ax[3];  // the cube's free axes, ascending
-  int cax;    // the cube's constant axis
+  unsigned char seg[kMaxSegsPerPoly];
+  unsigned char n;
+  unsigned char ax[3];  // the cube's free axes, ascending
+  unsigned char cax;    // the cube's constant axis
   bool has_centroid;
   double centroid[kDim];
 };
 
+// A group of polygons of one hypercube, as indices into the hypercube's polygon list.
 struct Polyhedron {
-  Polygon *poly[kMaxPolysPerHcube];
+  unsigned char poly[kMaxPolysPerHcube];
   int n;
   int ntet;
 };
@@ -185,24 +187,26 @@ GVH_HD inline int square_segments(const double v[2][2], int c0, double w0, int c
 
 // Centroid and normal of a segment of a 2-cube (constant axes 0 and 1; free axes 2 and 3).
 GVH_HD inline void segment_element(const Segment &g, double *centroid, double *normal) {
-  const double *p0 = g.start(), *p1 = g.end();
+  const double *p0 = g.start(), *p1 = g.end(), *outp = g.out;
   for (int k = 0; k < kDim; ++k) centroid[k] = (p0[k] + p1[k]) / 2.0;
   normal[2] = -(p1[3] - p0[3]);
   normal[3] = p1[2] - p0[2];
   normal[0] = 0;
   normal[1] = 0;
-  orient(normal, g.out, centroid);
+  orient(normal, outp, centroid);
 }
 
 // ---- polygons ------------------------------------------------------------------------
+// A polygon's segments live in its cube's segment array `segs`, which every polygon function
+// takes beside the polygon.
 
 GVH_HD inline void polygon_init(Polygon &P, int cax) {
   P.n = 0;
-  P.cax = cax;
+  P.cax = (unsigned char)cax;
   P.has_centroid = false;
   int m = 0;
   for (int k = 0; k < kDim; ++k)
-    if (k != cax) P.ax[m++] = k;
+    if (k != cax) P.ax[m++] = (unsigned char)k;
 }
 
 GVH_HD inline double l1_distance(const double *x, const double *y) {
@@ -211,32 +215,33 @@ GVH_HD inline double l1_distance(const double *x, const double *y) {
   return d;
 }
 
-// Appends g when it continues the chain (its start or end is the last segment's end).
-GVH_HD inline bool polygon_extend(Polygon &P, Segment *g) {
+// Appends segment g when it continues the chain (its start or end is the last segment's end).
+GVH_HD inline bool polygon_extend(Polygon &P, Segment *segs, int g) {
   if (P.n == 0) {
-    P.seg[0] = g;
+    P.seg[0] = (unsigned char)g;
     P.n = 1;
     return true;
   }
-  const double *tail = P.seg[P.n - 1]->end();
-  const double d_start = l1_distance(g->start(), tail);
-  const double d_end = l1_distance(g->end(), tail);
+  const double *tail = segs[P.seg[P.n - 1]].end();
+  const double *g0 = segs[g].start(), *g1 = segs[g].end();
+  const double d_start = l1_distance(g0, tail);
+  const double d_end = l1_distance(g1, tail);
   if (d_start < kSameTol || d_end < kSameTol) {
-    if (d_end < kSameTol) g->flip();
-    P.seg[P.n] = g;
+    if (d_end < kSameTol) segs[g].flip();
+    P.seg[P.n] = (unsigned char)g;
     ++P.n;
     return true;
   }
   return false;
 }
 
-GVH_HD inline void polygon_add(Polygon &P, Segment *g) { P.seg[P.n++] = g; }
+GVH_HD inline void polygon_add(Polygon &P, int g) { P.seg[P.n++] = (unsigned char)g; }
 
-GVH_HD inline const double *polygon_centroid(Polygon &P) {
+GVH_HD inline const double *polygon_centroid(Polygon &P, const Segment *segs) {
   if (P.has_centroid) return P.centroid;
   double mean[kDim] = {0, 0, 0, 0};
   for (int i = 0; i < P.n; ++i) {
-    const double *p0 = P.seg[i]->start(), *p1 = P.seg[i]->end();
+    const double *p0 = segs[P.seg[i]].start(), *p1 = segs[P.seg[i]].end();
     for (int k = 0; k < kDim; ++k) mean[k] += p0[k] + p1[k];
   }
   for (int k = 0; k < kDim; ++k) mean[k] = mean[k] / double(2.0 * P.n);
@@ -249,7 +254,7 @@ GVH_HD inline const double *polygon_centroid(Polygon &P) {
   double wsum[kDim] = {0, 0, 0, 0};
   double area = 0;
   for (int i = 0; i < P.n; ++i) {
-    const double *p0 = P.seg[i]->start(), *p1 = P.seg[i]->end();
+    const double *p0 = segs[P.seg[i]].start(), *p1 = segs[P.seg[i]].end();
     double cm[kDim], u[kDim], w[kDim];
     for (int k = 0; k < kDim; ++k) cm[k] = (p0[k] + p1[k] + mean[k]) / 3.0;
     for (int k = 0; k < kDim; ++k) {
@@ -266,12 +271,12 @@ GVH_HD inline const double *polygon_centroid(Polygon &P) {
   return P.centroid;
 }
 
-GVH_HD inline void polygon_normal(Polygon &P, double *normal) {
-  const double *c = polygon_centroid(P);
+GVH_HD inline void polygon_normal(Polygon &P, const Segment *segs, double *normal) {
+  const double *c = polygon_centroid(P, segs);
   const int x = P.ax[0], y = P.ax[1], z = P.ax[2];
   for (int k = 0; k < kDim; ++k) normal[k] = 0;
   for (int i = 0; i < P.n; ++i) {
-    const double *p0 = P.seg[i]->start(), *p1 = P.seg[i]->end();
+    const double *p0 = segs[P.seg[i]].start(), *p1 = segs[P.seg[i]].end(), *outp = segs[P.seg[i]].out;
     double u[kDim], w[kDim], t[kDim];
     for (int k = 0; k < kDim; ++k) {
       u[k] = p0[k] - c[k];
@@ -281,7 +286,7 @@ GVH_HD inline void polygon_normal(Polygon &P, double *normal) {
     t[y] = -0.5 * (u[x] * w[z] - u[z] * w[x]);
     t[z] = 0.5 * (u[x] * w[y] - u[y] * w[x]);
     t[P.cax] = 0;
-    orient(t, P.seg[i]->out, c);
+    orient(t, outp, c);
     for (int k = 0; k < kDim; ++k) normal[k] += t[k];
   }
 }
@@ -322,7 +327,7 @@ GVH_HD inline int cube_polygons(const double v[2][2][2], int cax, double w, cons
   if (cw.nseg == 0) return OK;
   if (!cw.ambiguous) {
     polygon_init(cw.poly[0], cax);
-    for (int i = 0; i < cw.nseg; ++i) polygon_add(cw.poly[0], &cw.seg[i]);
+    for (int i = 0; i < cw.nseg; ++i) polygon_add(cw.poly[0], i);
     cw.npoly = 1;
     return OK;
   }
@@ -337,7 +342,7 @@ GVH_HD inline int cube_polygons(const double v[2][2][2], int cax, double w, cons
     // second segment (the first one is always in the first polygon)
     int i = 0;
     while (i < cw.nseg) {
-      if (!used[i] && polygon_extend(P, &cw.seg[i])) {
+      if (!used[i] && polygon_extend(P, cw.seg, i)) {
         used[i] = true;
         ++nused;
         i = 1;
@@ -352,10 +357,19 @@ GVH_HD inline int cube_polygons(const double v[2][2][2], int cax, double w, cons
 
 // ---- polyhedra -----------------------------------------------------------------------
 
+struct HypercubeWork {
+  CubeWork cube[8];
+  // the hypercube's polygons in the order they were found: cube, then index in that cube
+  unsigned char pcube[kMaxPolysPerHcube], pidx[kMaxPolysPerHcube];
+  Polyhedron hedra[kMaxPolyhedra];
+  GVH_HD Polygon &polygon(int q) { return cube[pcube[q]].poly[pidx[q]]; }
+  GVH_HD Segment *segments(int q) { return cube[pcube[q]].seg; }
+};
+
 // Segments l (of the new polygon) and m (already in the polyhedron) share a point: m's start
 // is one of l's end points.
-GVH_HD inline bool segments_touch(const Segment *l, const Segment *m) {
-  const double *l0 = l->start(), *l1 = l->end(), *m0 = m->start();
+GVH_HD inline bool segments_touch(const Segment &l, const Segment &m) {
+  const double *l0 = l.start(), *l1 = l.end(), *m0 = m.start();
   double d0 = 0, d1 = 0;
   for (int k = 0; k < kDim; ++k) {
     d0 += fabs(l0[k] - m0[k]);
@@ -365,21 +379,28 @@ GVH_HD inline bool segments_touch(const Segment *l, const Segment *m) {
   return true;
 }
 
-GVH_HD inline bool polyhedron_extend(Polyhedron &H, Polygon *P) {
+// Adds the hypercube's polygon q to H when H is empty or q shares a point with one of H's
+// polygons.
+GVH_HD inline bool polyhedron_extend(Polyhedron &H, HypercubeWork &hw, int q) {
+  const Polygon &P = hw.polygon(q);
   if (H.n == 0) {
-    H.poly[0] = P;
+    H.poly[0] = (unsigned char)q;
     H.n = 1;
-    H.ntet = P->n;
+    H.ntet = P.n;
     return true;
   }
-  for (int i = 0; i < H.n; ++i)
-    for (int j = 0; j < P->n; ++j)
-      for (int k = 0; k < H.poly[i]->n; ++k)
-        if (segments_touch(P->seg[j], H.poly[i]->seg[k])) {
-          H.poly[H.n++] = P;
-          H.ntet += P->n;
+  const Segment *ps = hw.segments(q);
+  for (int i = 0; i < H.n; ++i) {
+    const Polygon &Q = hw.polygon(H.poly[i]);
+    const Segment *qs = hw.segments(H.poly[i]);
+    for (int j = 0; j < P.n; ++j)
+      for (int k = 0; k < Q.n; ++k)
+        if (segments_touch(ps[P.seg[j]], qs[Q.seg[k]])) {
+          H.poly[H.n++] = (unsigned char)q;
+          H.ntet += P.n;
           return true;
         }
+  }
   return false;
 }
 
@@ -397,20 +418,25 @@ GVH_HD inline void tetra_normal(const double *a, const double *b, const double *
   n[3] = -1.0 / 6.0 * (a[0] * bc12 - a[1] * bc02 + a[2] * bc01);
 }
 
-GVH_HD inline void polyhedron_element(Polyhedron &H, double *centroid, double *normal) {
+GVH_HD inline void polyhedron_element(const Polyhedron &H, HypercubeWork &hw, double *centroid, double *normal) {
   double mean[kDim] = {0, 0, 0, 0};
-  for (int i = 0; i < H.n; ++i)
-    for (int j = 0; j < H.poly[i]->n; ++j) {
-      const double *p0 = H.poly[i]->seg[j]->start(), *p1 = H.poly[i]->seg[j]->end();
+  for (int i = 0; i < H.n; ++i) {
+    const Polygon &P = hw.polygon(H.poly[i]);
+    const Segment *ps = hw.segments(H.poly[i]);
+    for (int j = 0; j < P.n; ++j) {
+      const double *p0 = ps[P.seg[j]].start(), *p1 = ps[P.seg[j]].end();
       for (int k = 0; k < kDim; ++k) mean[k] += p0[k] + p1[k];
     }
+  }
   for (int k = 0; k < kDim; ++k) mean[k] = mean[k] / double(2.0 * H.ntet);
   double wsum[kDim] = {0, 0, 0, 0};
   double vol = 0;
   for (int i = 0; i < H.n; ++i) {
-    const double *pc = polygon_centroid(*H.poly[i]);
-    for (int j = 0; j < H.poly[i]->n; ++j) {
-      const double *p0 = H.poly[i]->seg[j]->start(), *p1 = H.poly[i]->seg[j]->end();
+    Polygon &P = hw.polygon(H.poly[i]);
+    const Segment *ps = hw.segments(H.poly[i]);
+    const double *pc = polygon_centroid(P, ps);
+    for (int j = 0; j < P.n; ++j) {
+      const double *p0 = ps[P.seg[j]].start(), *p1 = ps[P.seg[j]].end();
       double cm[kDim], a[kDim], b[kDim], c[kDim], n[kDim];
       for (int k = 0; k < kDim; ++k) cm[k] = (p0[k] + p1[k] + pc[k] + mean[k]) / 4.0;
       for (int k = 0; k < kDim; ++k) {
@@ -429,17 +455,19 @@ GVH_HD inline void polyhedron_element(Polyhedron &H, double *centroid, double *n
   for (int k = 0; k < kDim; ++k) centroid[k] = wsum[k] / vol;
   for (int k = 0; k < kDim; ++k) normal[k] = 0;
   for (int i = 0; i < H.n; ++i) {
-    const double *pc = polygon_centroid(*H.poly[i]);
-    for (int j = 0; j < H.poly[i]->n; ++j) {
-      const Segment *g = H.poly[i]->seg[j];
+    Polygon &P = hw.polygon(H.poly[i]);
+    const Segment *ps = hw.segments(H.poly[i]);
+    const double *pc = polygon_centroid(P, ps);
+    for (int j = 0; j < P.n; ++j) {
+      const double *p0 = ps[P.seg[j]].start(), *p1 = ps[P.seg[j]].end(), *outp = ps[P.seg[j]].out;
       double a[kDim], b[kDim], c[kDim], n[kDim];
       for (int k = 0; k < kDim; ++k) {
-        a[k] = g->start()[k] - centroid[k];
-        b[k] = g->end()[k] - centroid[k];
+        a[k] = p0[k] - centroid[k];
+        b[k] = p1[k] - centroid[k];
         c[k] = pc[k] - centroid[k];
       }
       tetra_normal(a, b, c, n);
-      orient(n, g->out, centroid);
+      orient(n, outp, centroid);
       for (int k = 0; k < kDim; ++k) normal[k] += n[k];
     }
   }
@@ -471,19 +499,13 @@ GVH_HD inline int find_3d(const double v[2][2][2], const double *dx4, double iso
   if (rc) return rc;
   if (cw.npoly > kMaxElements) return ERR_OVERFLOW;
   for (int i = 0; i < cw.npoly; ++i) {
-    const double *c = polygon_centroid(cw.poly[i]);
+    const double *c = polygon_centroid(cw.poly[i], cw.seg);
     for (int k = 0; k < kDim; ++k) r.centroid[i][k] = c[k];
-    polygon_normal(cw.poly[i], r.normal[i]);
+    polygon_normal(cw.poly[i], cw.seg, r.normal[i]);
   }
   r.n = cw.npoly;
   return OK;
 }
-
-struct HypercubeWork {
-  CubeWork cube[8];
-  Polygon *poly[kMaxPolysPerHcube];
-  Polyhedron hedra[kMaxPolyhedra];
-};
 
 // 4-cube: corner values v[i][j][k][l] over axes 0..3.
 GVH_HD inline int find_4d(const double v[2][2][2][2], const double *dx4, double iso, Result &r, HypercubeWork &hw) {
@@ -502,10 +524,15 @@ GVH_HD inline int find_4d(const double v[2][2][2][2], const double *dx4, double 
                           : ax == 1 ? v[i][side][j][k]
                           : ax == 2 ? v[i][j][side][k]
                                     : v[i][j][k][side];
-      CubeWork &cw = hw.cube[2 * ax + side];
+      const int c = 2 * ax + side;
+      CubeWork &cw = hw.cube[c];
       const int rc = cube_polygons(cu, ax, side * dx4[ax], dx4, iso, cw);
       if (rc) return rc;
-      for (int p = 0; p < cw.npoly; ++p) hw.poly[npoly++] = &cw.poly[p];
+      for (int p = 0; p < cw.npoly; ++p) {
+        hw.pcube[npoly] = (unsigned char)c;
+        hw.pidx[npoly] = (unsigned char)p;
+        ++npoly;
+      }
       nseg += cw.nseg;
       amb_cubes += cw.ambiguous;
     }
@@ -521,8 +548,8 @@ GVH_HD inline int find_4d(const double v[2][2][2][2], const double *dx4, double 
     H.n = 0;
     H.ntet = 0;
     for (int p = 0; p < npoly; ++p) {
-      H.poly[H.n++] = hw.poly[p];
-      H.ntet += hw.poly[p]->n;
+      H.poly[H.n++] = (unsigned char)p;
+      H.ntet += hw.polygon(p).n;
     }
     nh = 1;
   } else {
@@ -535,7 +562,7 @@ GVH_HD inline int find_4d(const double v[2][2][2][2], const double *dx4, double 
       H.ntet = 0;
       int i = 0;
       while (i < npoly) {
-        if (!used[i] && polyhedron_extend(H, hw.poly[i])) {
+        if (!used[i] && polyhedron_extend(H, hw, i)) {
           used[i] = true;
           ++nused;
           i = 1;
@@ -547,7 +574,7 @@ GVH_HD inline int find_4d(const double v[2][2][2][2], const double *dx4, double 
     }
   }
   if (nh > kMaxElements) return ERR_OVERFLOW;
-  for (int h = 0; h < nh; ++h) polyhedron_element(hw.hedra[h], r.centroid[h], r.normal[h]);
+  for (int h = 0; h < nh; ++h) polyhedron_element(hw.hedra[h], hw, r.centroid[h], r.normal[h]);
   r.n = nh;
   return OK;
 }

@@ -105,8 +105,7 @@ struct RowWork {
   // the corner (a, b, k)'s kRowVars values at the lower then the upper time level, read in
   // place from the slab's point table; null for the absent eta layer of a 3-cube
   const double *corner[2][2][2];
-  iso::HypercubeWork hw;
-  iso::CubeWork cw;
+  iso::HypercubeWork hw;  // a 3-cube uses its first cube's work space
 };
 
 // Field q at the corners, as f[t][a][b][k] (0 for an absent corner).
@@ -139,7 +138,7 @@ GVH_HD inline int cube_rows(const RowGeometry &g, int key, RowWork &w, double *r
     // cornelius is set up with the spacings of the dimensions in use (HydroPlugin.cpp
     // :155-182); in 3D its first axis has unit length and is not used
     const double dx3[4] = {1.0, g.dt, g.dx, g.dy};
-    rc = iso::find_3d(v3, dx3, g.iso, w.res, w.cw);
+    rc = iso::find_3d(v3, dx3, g.iso, w.res, w.hw.cube[0]);
   }
   if (rc) return rc;
   const double cell_x = (double)ix * g.dx - (((double)(g.nx - 1)) / 2.0 * g.dx);
