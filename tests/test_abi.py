@@ -67,3 +67,60 @@ def test_create_rejects_bad_lattice_without_gpu(lib):
         o.theta = bad
         assert L.gvh_create(ctypes.byref(lat), ctypes.byref(hyd), ctypes.byref(o), ctypes.byref(h)) == -1
         assert b"theta" in L.gvh_last_error()
+
+
+def test_null_and_bad_arguments_are_rejected_without_gpu(lib):
+    """Every entry point that takes a handle, batch or surface refuses a null one (and bad
+    sizes or ids) with a negative code and a message, before any CUDA call; destroying null
+    is a no-op, as free(NULL) is."""
+    L = gvh.load()
+    gvh._bind_batch(L)
+    gvh._bind_surface(L)
+    d = ctypes.c_double()
+    u = ctypes.c_uint()
+    t = ctypes.c_longlong()
+    n = ctypes.c_int()
+    calls = [
+        ("gvh_rk2_step", (None, 0.5, 0.01, 0.0)),
+        ("gvh_set_state", (None, None, 25)),
+        ("gvh_get_state", (None, None, 25)),
+        ("gvh_set_state_async", (None, None, 25)),
+        ("gvh_get_state_async", (None, None, 25)),
+        ("gvh_join_async", (None,)),
+        ("gvh_status", (None, ctypes.byref(u))),
+        ("gvh_clear_status", (None,)),
+        ("gvh_synchronize", (None,)),
+        ("gvh_max_energy_density", (None, ctypes.byref(d))),
+        ("gvh_max_propagation_speed", (None, ctypes.byref(d))),
+        ("gvh_set_hotspot_state", (None, None)),
+        ("gvh_gather_state_device", (None, None, 25, 8)),
+        ("gvh_scatter_state_device", (None, None, 25, 8)),
+        ("gvh_enable_validity", (None, 1)),
+        ("gvh_set_stream", (None, None)),
+        ("gvh_save_state", (None, b"/nonexistent/x", 0.5, 0)),
+        ("gvh_load_state", (None, b"/nonexistent/x", ctypes.byref(d), ctypes.byref(t))),
+    ]
+    for name, args in calls:
+        rc = getattr(L, name)(*args)
+        assert rc < 0, (name, rc)
+        assert L.gvh_last_error(), name
+    batch_calls = [
+        ("gvh_batch_step", (None, 1)),
+        ("gvh_batch_round", (None, 1, ctypes.byref(t))),
+        ("gvh_batch_poll", (None, 0, 0, None, None, ctypes.byref(n), None)),
+        ("gvh_batch_remove_event", (None, 0)),
+        ("gvh_batch_synchronize", (None,)),
+    ]
+    for name, args in batch_calls:
+        rc = getattr(L, name)(*args)
+        assert rc < 0, (name, rc)
+        assert L.gvh_batch_last_error(), name
+    zero, one = ctypes.c_double(0.0), ctypes.c_double(1.0)
+    for name, args in [("gvh_surface_find", (None, zero, one, ctypes.byref(t))),
+                       ("gvh_surface_find_begin", (None, zero, one)),
+                       ("gvh_surface_find_end", (None, ctypes.byref(t))),
+                       ("gvh_surface_set_lower", (None,))]:
+        rc = getattr(L, name)(*args)
+        assert rc < 0, (name, rc)
+        assert L.gvh_surface_last_error(), name
+    assert L.gvh_destroy(None) == 0

@@ -220,3 +220,33 @@ def test_tile_shapes_compute_the_same_values(tile_x):
         sa, sb = A.get_state(ea), B.get_state(eb)
         for k in sa:
             np.testing.assert_array_equal(sa[k], sb[k])
+
+
+def test_empty_batch_and_bad_ids():
+    """A batch with no events steps and serves rounds as no-ops; ids that were never admitted
+    or were removed are refused; the last event removed leaves an empty batch that admits
+    again."""
+    B = gvh.Batch(1 << 26, precision="fp64")
+    assert B.num_events == 0
+    B.step(3)
+    t0 = B.round(2)
+    t1 = B.round(2)
+    infos, ms = B.poll(t0)
+    assert infos == {} and ms >= 0
+    infos, _ = B.poll(t1)
+    assert infos == {}
+    for bad in (-1, 0, 7):
+        with pytest.raises(gvh.GvhError):
+            B.remove_event(bad)
+    kw, prim, t0_ev = make_events(False, True, True)[0]
+    eid = B.add_event(**kw, prim=prim, tau0=t0_ev)
+    assert eid is not None and B.num_events == 1
+    B.step(1)
+    B.remove_event(eid)
+    with pytest.raises(gvh.GvhError):
+        B.remove_event(eid)
+    assert B.num_events == 0
+    B.step(2)
+    again = B.add_event(**kw, prim=prim, tau0=t0_ev)
+    B.step(1)
+    assert B.info(again).step == 1
