@@ -69,6 +69,7 @@ struct EventDev {
   long long sy, sz, cs, ncells;
   double dx, dy, dz, dt, etabar, theta, e_reg, e_fo;
   double inv_dx, inv_dy, inv_dz, inv_dt;  // reciprocals, computed on the host at admission
+  int cartesian;        // the batch's coordinates (GVH_COORDINATES_CARTESIAN)
   double t0;            // initial proper time; the step from t0 + n dt is step n + 1
   long long step;       // completed steps
   double *qA, *qB, *e, *pA, *pB, *u[3];
@@ -87,6 +88,7 @@ __device__ __forceinline__ StageArgs make_args(EventDev &E, bool stage2) {
   a.dx = E.dx; a.dy = E.dy; a.dz = E.dz; a.dt = E.dt;
   a.inv_dx = E.inv_dx; a.inv_dy = E.inv_dy; a.inv_dz = E.inv_dz; a.inv_dt = E.inv_dt;
   a.etabar = E.etabar; a.theta = E.theta; a.e_reg = E.e_reg;
+  a.cartesian = E.cartesian;
   a.status = &E.status;
   a.diag = nullptr;       // validity diagnostics are a single-lattice option
   a.speed_max = nullptr;  // so is the propagation-speed maximum
@@ -471,6 +473,8 @@ int gvh_batch_create(const gvh_options *opts, long long arena_bytes, gvh_batch *
     return bfail(GVH_ERR_INVALID, "unknown precision");
   if (arena_bytes <= 0) return bfail(GVH_ERR_INVALID, "arena_bytes must be > 0");
   if (!(o.theta > 0)) return bfail(GVH_ERR_INVALID, "the limiter's theta must be > 0");
+  if (o.coordinates != GVH_COORDINATES_MILNE && o.coordinates != GVH_COORDINATES_CARTESIAN)
+    return bfail(GVH_ERR_INVALID, "unknown coordinates %d", o.coordinates);
   int dev = o.device;
   if (dev < 0) BCUDA(cudaGetDevice(&dev));
   BCUDA(cudaSetDevice(dev));
@@ -681,6 +685,7 @@ int admit_event(gvh_batch *b, const gvh_lattice_params *L, const gvh_hydro_param
   E.inv_dx = 1.0 / E.dx; E.inv_dy = 1.0 / E.dy; E.inv_dz = 1.0 / E.dz; E.inv_dt = 1.0 / E.dt;
   E.etabar = H->shearViscosityToEntropyDensity;
   E.theta = b->opts.theta;
+  E.cartesian = b->opts.coordinates == GVH_COORDINATES_CARTESIAN;
   const double T_reg = H->regulationTemperatureGeV / kHbarc;
   const double T_fo = H->freezeoutTemperatureGeV / kHbarc;
   if (b->opts.eos == GVH_EOS_CONFORMAL) {

@@ -120,34 +120,67 @@ int ensure_staging(gvh_handle *h) {
   return GVH_OK;
 }
 
+// Releases whatever ensure_async made (null members are skipped), so a failed set-up leaves
+// the handle as it was and the next call starts over.
+void release_async(gvh_handle *h) {
+  for (int a = 0; a < 2; ++a) {
+    if (h->staging_in[a]) cudaFree(h->staging_in[a]);
+    if (h->staging_out[a]) cudaFree(h->staging_out[a]);
+    if (h->ev_in_free[a]) cudaEventDestroy(h->ev_in_free[a]);
+    if (h->ev_out_free[a]) cudaEventDestroy(h->ev_out_free[a]);
+    h->staging_in[a] = h->staging_out[a] = nullptr;
+    h->ev_in_free[a] = h->ev_out_free[a] = nullptr;
+  }
+  if (h->s_h2d) cudaStreamDestroy(h->s_h2d);
+  if (h->s_d2h) cudaStreamDestroy(h->s_d2h);
+  if (h->ev_in_ready) cudaEventDestroy(h->ev_in_ready);
+  if (h->ev_out_ready) cudaEventDestroy(h->ev_out_ready);
+  if (h->ev_fence) cudaEventDestroy(h->ev_fence);
+  h->s_h2d = h->s_d2h = nullptr;
+  h->ev_in_ready = h->ev_out_ready = h->ev_fence = nullptr;
+  h->async_ready = 0;
+}
+
 int ensure_async(gvh_handle *h) {
   if (h->async_ready) return GVH_OK;
   const size_t bytes = (size_t)(h->nq + 10) * h->ng * sizeof(double);
-  double *areas[4] = {};
-  for (int a = 0; a < 4; ++a)
-    if (cudaMalloc(&areas[a], bytes) != cudaSuccess) {
-      for (int b = 0; b < a; ++b) cudaFree(areas[b]);
-      return fail(GVH_ERR_NOMEM, "async staging allocation failed");
-    }
+  bool ok = true;
   for (int a = 0; a < 2; ++a) {
-    h->staging_in[a] = areas[a];
-    h->staging_out[a] = areas[2 + a];
+    ok = ok && cudaMalloc(&h->staging_in[a], bytes) == cudaSuccess;
+    ok = ok && cudaMalloc(&h->staging_out[a], bytes) == cudaSuccess;
+  }
+  if (!ok) {
+    release_async(h);
+    cudaGetLastError();
+    return fail(GVH_ERR_NOMEM, "async staging allocation failed");
   }
   h->in_slot = h->out_slot = 0;
-  GVH_CUDA(cudaStreamCreateWithFlags(&h->s_h2d, cudaStreamNonBlocking));
-  GVH_CUDA(cudaStreamCreateWithFlags(&h->s_d2h, cudaStreamNonBlocking));
-  GVH_CUDA(cudaEventCreateWithFlags(&h->ev_in_ready, cudaEventDisableTiming));
-  GVH_CUDA(cudaEventCreateWithFlags(&h->ev_out_ready, cudaEventDisableTiming));
-  GVH_CUDA(cudaEventCreateWithFlags(&h->ev_fence, cudaEventDisableTiming));
-  // the events start recorded (complete), so the first waits pass
+  cudaError_t ec = cudaSuccess;
+  auto step = [&ec](cudaError_t e) {
+    if (ec == cudaSuccess) ec = e;
+  };
+  step(cudaStreamCreateWithFlags(&h->s_h2d, cudaStreamNonBlocking));
+  step(cudaStreamCreateWithFlags(&h->s_d2h, cudaStreamNonBlocking));
+  step(cudaEventCreateWithFlags(&h->ev_in_ready, cudaEventDisableTiming));
+  step(cudaEventCreateWithFlags(&h->ev_out_ready, cudaEventDisableTiming));
+  step(cudaEventCreateWithFlags(&h->ev_fence, cudaEventDisableTiming));
   for (int a = 0; a < 2; ++a) {
-    GVH_CUDA(cudaEventCreateWithFlags(&h->ev_in_free[a], cudaEventDisableTiming));
-    GVH_CUDA(cudaEventCreateWithFlags(&h->ev_out_free[a], cudaEventDisableTiming));
-    GVH_CUDA(cudaEventRecord(h->ev_in_free[a], h->stream));
-    GVH_CUDA(cudaEventRecord(h->ev_out_free[a], h->stream));
+    step(cudaEventCreateWithFlags(&h->ev_in_free[a], cudaEventDisableTiming));
+    step(cudaEventCreateWithFlags(&h->ev_out_free[a], cudaEventDisableTiming));
   }
-  GVH_CUDA(cudaEventRecord(h->ev_in_ready, h->stream));
-  GVH_CUDA(cudaEventRecord(h->ev_out_ready, h->stream));
+  // the events start recorded (complete), so the first waits pass
+  if (ec == cudaSuccess) {
+    for (int a = 0; a < 2; ++a) {
+      step(cudaEventRecord(h->ev_in_free[a], h->stream));
+      step(cudaEventRecord(h->ev_out_free[a], h->stream));
+    }
+    step(cudaEventRecord(h->ev_in_ready, h->stream));
+    step(cudaEventRecord(h->ev_out_ready, h->stream));
+  }
+  if (ec != cudaSuccess) {
+    release_async(h);
+    return fail(GVH_ERR_CUDA, "async set-up: %s", cudaGetErrorString(ec));
+  }
   h->async_ready = 1;
   return GVH_OK;
 }
@@ -177,6 +210,7 @@ void gvh_default_options(gvh_options *o) {
   o->precision = GVH_PRECISION_FP64;
   o->theta = 2.0;
   o->device = -1;
+  o->coordinates = GVH_COORDINATES_MILNE;
 }
 
 const char *gvh_last_error(void) { return g_last_error.c_str(); }
@@ -198,6 +232,8 @@ int gvh_create(const gvh_lattice_params *L, const gvh_hydro_params *H, const gvh
   if (o.shear && !(H->shearViscosityToEntropyDensity > 0))
     return fail(GVH_ERR_INVALID, "gvh_create: eta/s must be > 0 with shear");
   if (!(o.theta > 0)) return fail(GVH_ERR_INVALID, "gvh_create: the limiter's theta must be > 0");
+  if (o.coordinates != GVH_COORDINATES_MILNE && o.coordinates != GVH_COORDINATES_CARTESIAN)
+    return fail(GVH_ERR_INVALID, "gvh_create: unknown coordinates %d", o.coordinates);
   int dev = o.device;
   if (dev < 0) GVH_CUDA(cudaGetDevice(&dev));
   GVH_CUDA(cudaSetDevice(dev));
@@ -225,6 +261,7 @@ int gvh_create(const gvh_lattice_params *L, const gvh_hydro_params *H, const gvh
   h->dt_lattice = L->latticeSpacingProperTime;
   h->etabar = H->shearViscosityToEntropyDensity;
   h->theta = o.theta;
+  h->cartesian = o.coordinates == GVH_COORDINATES_CARTESIAN;
   h->eos = o.eos; h->shear = o.shear; h->bulk = o.bulk; h->precision = o.precision; h->device = dev;
   h->ucur = 0; h->uprev = 1; h->ufree = 2;
 
@@ -266,17 +303,7 @@ int gvh_destroy(gvh_handle *h) {
   if (h->async_ready) {
     cudaStreamSynchronize(h->s_h2d);
     cudaStreamSynchronize(h->s_d2h);
-    for (int a = 0; a < 2; ++a) {
-      cudaFree(h->staging_in[a]);
-      cudaFree(h->staging_out[a]);
-      cudaEventDestroy(h->ev_in_free[a]);
-      cudaEventDestroy(h->ev_out_free[a]);
-    }
-    cudaStreamDestroy(h->s_h2d);
-    cudaStreamDestroy(h->s_d2h);
-    cudaEventDestroy(h->ev_in_ready);
-    cudaEventDestroy(h->ev_out_ready);
-    cudaEventDestroy(h->ev_fence);
+    release_async(h);
   }
   delete h;
   return GVH_OK;
@@ -448,6 +475,7 @@ int gvh_rk2_step(gvh_handle *h, double t, double dt, double T_reg) {
   a.dx = h->dx; a.dy = h->dy; a.dz = h->dz; a.dt = h->dt_lattice;
   set_inverse_spacings(a);
   a.etabar = h->etabar; a.theta = h->theta;
+  a.cartesian = h->cartesian;
   a.e_reg = (h->eos == GVH_EOS_CONFORMAL) ? energy_density_of_T<EOS_CONFORMAL>(T_reg)
                                           : energy_density_of_T<EOS_QCD>(T_reg);
   a.status = h->status;

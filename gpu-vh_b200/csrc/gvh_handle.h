@@ -10,6 +10,7 @@ struct gvh_handle {
   long long sy, sz, cs;     // internal strides
   double dx, dy, dz, dt_lattice, etabar, theta;
   int eos, shear, bulk, precision, device;
+  int cartesian;            // GVH_COORDINATES_CARTESIAN
   cudaStream_t stream;      // where work is queued (own_stream unless the caller set one)
   cudaStream_t own_stream;
   double *block;

@@ -132,6 +132,8 @@ int gvh_rk2_step_noalloc(const gvh_lattice_params *L, const gvh_hydro_params *H,
   if (o.precision != GVH_PRECISION_FP64 && o.precision != GVH_PRECISION_MIXED)
     return nfail(GVH_ERR_INVALID, "gvh_rk2_step_noalloc: unknown precision");
   if (!(o.theta > 0)) return nfail(GVH_ERR_INVALID, "gvh_rk2_step_noalloc: the limiter's theta must be > 0");
+  if (o.coordinates != GVH_COORDINATES_MILNE && o.coordinates != GVH_COORDINATES_CARTESIAN)
+    return nfail(GVH_ERR_INVALID, "gvh_rk2_step_noalloc: unknown coordinates %d", o.coordinates);
   if (u_next == u || u_next == u_prev)
     return nfail(GVH_ERR_INVALID, "gvh_rk2_step_noalloc: u_next must not alias u or u_prev");
   const int nq = 4 + (o.shear ? 10 : 0) + (o.bulk ? 1 : 0);
@@ -175,6 +177,7 @@ int gvh_rk2_step_noalloc(const gvh_lattice_params *L, const gvh_hydro_params *H,
   set_inverse_spacings(a);
   a.etabar = H->shearViscosityToEntropyDensity;
   a.theta = o.theta;
+  a.cartesian = o.coordinates == GVH_COORDINATES_CARTESIAN;
   a.e_reg = (o.eos == GVH_EOS_CONFORMAL) ? energy_density_of_T<EOS_CONFORMAL>(T_reg) : energy_density_of_T<EOS_QCD>(T_reg);
   a.status = status;
   a.e = e;

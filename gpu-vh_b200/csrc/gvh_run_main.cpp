@@ -2,7 +2,7 @@
 // HydroWrapper.cpp:17-87, flags of CommandLineArguments.cpp:17-24): -c <config dir> with
 // lattice/hydro/ic.properties, -o <output dir>; the initial state is read from
 // <cwd>/input/*.dat (initial-condition type 10). Extra flags select the reference's
-// compile-time switches: --conformal, --no-bulk, --ideal, --theta <v>, --mixed; --no-dump and
+// compile-time switches: --conformal, --no-bulk, --ideal, --theta <v>, --mixed, --cartesian; --no-dump and
 // --no-surface turn off the field dumps and <output dir>/surface.dat.
 #include <stdio.h>
 #include <stdlib.h>
@@ -27,12 +27,13 @@ int main(int argc, char **argv) {
     else if (a == "--ideal") { o.bulk = 0; o.shear = 0; }
     else if (a == "--theta" && i + 1 < argc) o.theta = atof(argv[++i]);
     else if (a == "--mixed") o.precision = GVH_PRECISION_MIXED;
+    else if (a == "--cartesian") o.coordinates = GVH_COORDINATES_CARTESIAN;
     else if (a == "--no-dump") outputs &= ~GVH_RUN_FIELDS;
     else if (a == "--no-surface") outputs &= ~GVH_RUN_SURFACE;
     else if (a == "-h" || a == "-t") continue;  // the reference accepts these too
     else {
       fprintf(stderr, "usage: %s [-c config_dir] [-o output_dir] [--conformal] [--no-bulk] [--ideal] "
-                      "[--theta v] [--mixed] [--no-dump] [--no-surface]\n", argv[0]);
+                      "[--theta v] [--mixed] [--cartesian] [--no-dump] [--no-surface]\n", argv[0]);
       return 2;
     }
   }

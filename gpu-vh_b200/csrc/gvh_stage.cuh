@@ -59,6 +59,7 @@ struct StageArgs {
                           // q^n pi^{mu nu}, Pi (components 13..23) for the validity diagnostics
   unsigned long long *speed_max;  // stage 1, optional: running max of a / dx_axis over cells, as
                                   // the bit pattern of a non-negative double (see kt_stage_kernel)
+  int cartesian;          // GVH_COORDINATES_CARTESIAN: no Milne geometric sources (stage_source)
 };
 
 // Components of the validity block (VALIDITY_DOMAIN, DynamicalVariables.cuh:82-98, in that
@@ -345,11 +346,18 @@ __device__ __forceinline__ void stage_source(const StageArgs &a, long long s, in
   const R dyvy = (f.dyuy - vy * f.dyut) * iut;
   const R dnvn = (f.dnun - vn * f.dnut) * iut;
   const R dkvk = dxvx + dyvy + dnvn;
+  // The Milne geometry enters through gi = 1/tau and gt = tau (the geometric sources) and
+  // gn = 1/tau (the eta derivative's metric factor, taken twice). Cartesian coordinates
+  // (USE_CARTESIAN_COORDINATES, SourceTerms.cu:738-743) drop the geometric sources and the
+  // factor: gi = gt = 0 and gn = 1 give exactly the reference's Cartesian terms (the dropped
+  // products are zeros that adding leaves out), and the Milne expressions keep their form.
+  // The pi^{mu nu} sources below keep their Milne terms in both, as in the reference.
+  const R gi = a.cartesian ? R(0) : it, gt = a.cartesian ? R(0) : t, gn = a.cartesian ? R(1) : it;
   R S[NQ];
-  S[0] = -(q[0] * it + t * tnn) + dkvk * (pitt - pc - Pi) - vx * dxp - vy * dyp - vn * dnp;
-  S[1] = -q[1] * it - dxp + dkvk * pitx;
-  S[2] = -q[2] * it - dyp + dkvk * pity;
-  S[3] = R(-3) * q[3] * it - dnp * it * it + dkvk * pitn;
+  S[0] = -(q[0] * gi + gt * tnn) + dkvk * (pitt - pc - Pi) - vx * dxp - vy * dyp - vn * dnp;
+  S[1] = -q[1] * gi - dxp + dkvk * pitx;
+  S[2] = -q[2] * gi - dyp + dkvk * pity;
+  S[3] = R(-3) * q[3] * gi - dnp * gn * gn + dkvk * pitn;
   if (SHEAR) {
     ShearT<R> pi{q[4], q[5], q[6], q[7], q[8], q[9], q[10], q[11], q[12], q[13]};
     R rhs[11];

@@ -91,6 +91,9 @@ void twoStepRungeKutta(PRECISION t, PRECISION dt, CONSERVED_VARIABLES *__restric
 #ifdef CONFORMAL_EOS
     o.eos = GVH_EOS_CONFORMAL;
 #endif
+#ifdef USE_CARTESIAN_COORDINATES
+    o.coordinates = GVH_COORDINATES_CARTESIAN;
+#endif
     o.shear = NUMBER_CONSERVED_VARIABLES >= 14;
     o.bulk = NUMBER_CONSERVED_VARIABLES == 15;
     o.theta = GVH_THETA;

@@ -22,6 +22,8 @@ GVH_EOS_QCD = 0
 GVH_EOS_CONFORMAL = 1
 GVH_PRECISION_FP64 = 0
 GVH_PRECISION_MIXED = 1
+GVH_COORDINATES_MILNE = 0
+GVH_COORDINATES_CARTESIAN = 1
 GVH_OK = 0
 GVH_ERR_INVALID = -1
 GVH_ERR_CUDA = -2
@@ -74,7 +76,8 @@ GVH_RUN_SURFACE = 2
 
 class Options(ctypes.Structure):
     _fields_ = [("eos", ctypes.c_int), ("shear", ctypes.c_int), ("bulk", ctypes.c_int),
-                ("precision", ctypes.c_int), ("theta", ctypes.c_double), ("device", ctypes.c_int)]
+                ("precision", ctypes.c_int), ("theta", ctypes.c_double), ("device", ctypes.c_int),
+                ("coordinates", ctypes.c_int)]
 
 
 _lib = None
@@ -153,7 +156,7 @@ class Lattice:
     """One hydro lattice on the GPU (a libgvh handle)."""
 
     def __init__(self, nx, ny, nz, dx, dy, dz, dt, etabar, theta=2.0, conformal=False, shear=True, bulk=True,
-                 precision="fp64", device=-1, tau0=0.5, T_fo_GeV=0.15, T_reg_GeV=0.0):
+                 precision="fp64", device=-1, tau0=0.5, T_fo_GeV=0.15, T_reg_GeV=0.0, cartesian=False):
         self._L = load()
         self.nx, self.ny, self.nz = nx, ny, nz
         self.ncx, self.ncy, self.ncz = nx + 4, ny + 4, nz + 4
@@ -169,6 +172,7 @@ class Lattice:
         o.eos = GVH_EOS_CONFORMAL if conformal else GVH_EOS_QCD
         o.shear, o.bulk, o.theta, o.device = int(shear), int(bulk), float(theta), int(device)
         o.precision = {"fp64": GVH_PRECISION_FP64, "mixed": GVH_PRECISION_MIXED}[precision]
+        o.coordinates = GVH_COORDINATES_CARTESIAN if cartesian else GVH_COORDINATES_MILNE
         self.options = o
         h = ctypes.c_void_p()
         _check(self._L.gvh_create(ctypes.byref(self.lattice), ctypes.byref(self.hydro), ctypes.byref(o),
@@ -431,13 +435,15 @@ class Batch:
     """Many events in one HBM arena, advanced together by one persistent launch per stage
     and a CUDA graph per RK2 step. All events share the physics options."""
 
-    def __init__(self, arena_bytes, conformal=False, shear=True, bulk=True, precision="fp64", theta=2.0, device=-1):
+    def __init__(self, arena_bytes, conformal=False, shear=True, bulk=True, precision="fp64", theta=2.0, device=-1,
+                 cartesian=False):
         self._L = _bind_batch(load())
         o = Options()
         self._L.gvh_default_options(ctypes.byref(o))
         o.eos = GVH_EOS_CONFORMAL if conformal else GVH_EOS_QCD
         o.shear, o.bulk, o.theta, o.device = int(shear), int(bulk), float(theta), int(device)
         o.precision = {"fp64": GVH_PRECISION_FP64, "mixed": GVH_PRECISION_MIXED}[precision]
+        o.coordinates = GVH_COORDINATES_CARTESIAN if cartesian else GVH_COORDINATES_MILNE
         self.options = o
         self.shear, self.bulk = bool(shear), bool(bulk)
         self.qnames = q_names(self.shear, self.bulk)

@@ -62,6 +62,9 @@ extern "C" {
 #define GVH_EOS_QCD 0              /* Wuppertal-Budapest fit (the reference default) */
 #define GVH_EOS_CONFORMAL 1        /* p = e/3 (CONFORMAL_EOS, EquationOfState.cuh:16) */
 
+#define GVH_COORDINATES_MILNE 0     /* (tau, x, y, eta): the reference's default */
+#define GVH_COORDINATES_CARTESIAN 1 /* (t, x, y, z): USE_CARTESIAN_COORDINATES, SourceTerms.cu:25 */
+
 #define GVH_PRECISION_FP64 0       /* plain FP64 path */
 #define GVH_PRECISION_MIXED 1      /* FP32 fluxes/limiter/sources, FP64 state and root find */
 
@@ -98,12 +101,16 @@ typedef struct gvh_options {
 	int precision;  /* GVH_PRECISION_* (reference: PRECISION macro, DynamicalVariables.cuh:44) */
 	double theta;   /* minmod limiter slope, > 0 (reference: THETA 2.0, FluxLimiter.cu:15) */
 	int device;     /* CUDA device ordinal; -1 = current device */
+	int coordinates; /* GVH_COORDINATES_* (reference: USE_CARTESIAN_COORDINATES, off as shipped:
+	                    SourceTerms.cu:25). Cartesian replaces only the geometric sources of
+	                    T^{tau mu} (SourceTerms.cu:738-743), as the reference's switch does; the
+	                    rest of the step keeps its Milne form there too */
 } gvh_options;
 
 typedef struct gvh_handle gvh_handle;
 
 /* Fills opts with the reference's shipped configuration: QCD EoS, shear + bulk, theta 2.0,
- * FP64, current device. */
+ * FP64, current device, Milne coordinates. */
 void gvh_default_options(gvh_options *opts);
 
 int gvh_create(const gvh_lattice_params *lattice, const gvh_hydro_params *hydro, const gvh_options *opts,

@@ -61,7 +61,8 @@ class KtParams(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
                 ("dx", ctypes.c_double), ("dy", ctypes.c_double), ("dz", ctypes.c_double),
                 ("dt", ctypes.c_double), ("etabar", ctypes.c_double), ("theta", ctypes.c_double),
-                ("conformal", ctypes.c_int), ("shear", ctypes.c_int), ("bulk", ctypes.c_int)]
+                ("conformal", ctypes.c_int), ("shear", ctypes.c_int), ("bulk", ctypes.c_int),
+                ("cartesian", ctypes.c_int)]
 
 
 _oracle = None
@@ -101,13 +102,14 @@ def _ptrs(arrays):
 class _Base:
     """Shared geometry and numpy plumbing."""
 
-    def __init__(self, nx, ny, nz, dx, dy, dz, dt, etabar, theta, conformal, shear, bulk):
+    def __init__(self, nx, ny, nz, dx, dy, dz, dt, etabar, theta, conformal, shear, bulk, cartesian=False):
         self.nx, self.ny, self.nz = nx, ny, nz
         self.ncx, self.ncy, self.ncz = nx + 4, ny + 4, nz + 4
         self.ng = self.ncx * self.ncy * self.ncz
         self.conformal, self.shear, self.bulk = bool(conformal), bool(shear), bool(bulk)
+        self.cartesian = bool(cartesian)
         self.params = dict(nx=nx, ny=ny, nz=nz, dx=dx, dy=dy, dz=dz, dt=dt, etabar=etabar, theta=theta,
-                           conformal=int(conformal), shear=int(shear), bulk=int(bulk))
+                           conformal=int(conformal), shear=int(shear), bulk=int(bulk), cartesian=int(cartesian))
         self.qnames = q_names(shear, bulk)
         self.nq = len(self.qnames)
         self.field_names = self.qnames + PRIM_NAMES
@@ -187,9 +189,9 @@ class OracleLattice(_Base):
         return [o.value for o in outs]
 
 
-def ref_variant(precision: str, conformal: bool, shear: bool, bulk: bool) -> str:
+def ref_variant(precision: str, conformal: bool, shear: bool, bulk: bool, cartesian: bool = False) -> str:
     phys = "bulk" if bulk else ("shear" if shear else "ideal")
-    return f"{precision}_{'conf' if conformal else 'qcd'}_{phys}"
+    return f"{precision}_{'conf' if conformal else 'qcd'}_{phys}" + ("_cart" if cartesian else "")
 
 
 def ref_available(variant: str = "fp64_conf_shear") -> bool:
@@ -203,7 +205,7 @@ class RefLattice(_Base):
         super().__init__(**kw)
         if self.bulk and not self.shear:
             raise ValueError("bulk without shear is not a valid reference build")
-        self.variant = ref_variant(precision, self.conformal, self.shear, self.bulk)
+        self.variant = ref_variant(precision, self.conformal, self.shear, self.bulk, self.cartesian)
         path = os.path.join(REF_DIR, f"libref_{self.variant}.so")
         if not os.path.exists(path):
             raise FileNotFoundError(path)
@@ -320,6 +322,8 @@ class RefGpuLattice(_Base):
 
     def __init__(self, precision="fp64", dropin=False, **kw):
         super().__init__(**kw)
+        if self.cartesian:
+            raise ValueError("the reference's CUDA builds here are Milne-coordinate builds")
         self.variant = ref_gpu_variant(precision, self.conformal, self.shear, self.bulk, kw["theta"])
         # dropin: the same program with gpu-vh_b200/dropin/twoStepRungeKutta_gvh.cu in place of
         # FullyDiscreteKurganovTadmorScheme.cu (libgvh's step behind the reference's loop)

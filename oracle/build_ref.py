@@ -18,6 +18,9 @@ Variants (compile-time switches the reference exposes as macros):
   precision  fp64 (PRECISION double + double intrinsics, via the shim) | fp32 (as shipped)
   eos        conf (CONFORMAL_EOS, EquationOfState.cuh:16) | qcd (default WB fit)
   physics    bulk (PIMUNU+PI: 15 components) | shear (PI off: 14) | ideal (4)
+  coords     Milne (as shipped) | _cart suffix: USE_CARTESIAN_COORDINATES defined on the
+             command line (SourceTerms.cu:25 leaves it commented out; its #ifdef at 738-743
+             then takes the Cartesian source terms), for three FP64 physics variants
 """
 from __future__ import annotations
 
@@ -55,8 +58,11 @@ EOS = {"conf": ["-DCONFORMAL_EOS"], "qcd": []}
 PHYSICS = {"bulk": [], "shear": ["-DGVH_REF_NO_BULK"], "ideal": ["-DGVH_REF_IDEAL"]}
 
 
+CARTESIAN_VARIANTS = ["fp64_conf_ideal_cart", "fp64_conf_shear_cart", "fp64_qcd_bulk_cart"]
+
+
 def variant_names():
-    return ["_".join(v) for v in itertools.product(PRECISIONS, EOS, PHYSICS)]
+    return ["_".join(v) for v in itertools.product(PRECISIONS, EOS, PHYSICS)] + CARTESIAN_VARIANTS
 
 
 def lib_path(name: str) -> str:
@@ -104,8 +110,8 @@ def _run(cmd):
 
 
 def build_variant(name: str, flux_limiter: str, validity: str) -> str:
-    prec, eos, phys = name.split("_")
-    flags = PRECISIONS[prec] + EOS[eos] + PHYSICS[phys]
+    prec, eos, phys, *coords = name.split("_")
+    flags = PRECISIONS[prec] + EOS[eos] + PHYSICS[phys] + (["-DUSE_CARTESIAN_COORDINATES"] if coords == ["cart"] else [])
     obj_dir = os.path.join(OUT, "obj", name)
     os.makedirs(obj_dir, exist_ok=True)
     src_dir = os.path.join(REF_ROOT, "rhic", "src")

@@ -514,6 +514,12 @@ static void euler_source_cell(kt_lattice *L, int s, double t, double **cur, doub
 	S[1] = -ttx / t - dxp + dkvk * pitx;
 	S[2] = -tty / t - dyp + dkvk * pity;
 	S[3] = -3 * ttn / t - dnp / pow(t, 2) + dkvk * pitn;
+	if (P->cartesian) { /* SourceTerms.cu:738-743 replaces the four Milne terms */
+		S[0] = dkvk * (pitt - pc - Pi) - vx * dxp - vy * dyp - vn * dnp;
+		S[1] = -dxp + dkvk * pitx;
+		S[2] = -dyp + dkvk * pity;
+		S[3] = -dnp + dkvk * pitn;
+	}
 	if (P->shear) {
 		double rhs[11];
 		pimunu_source(P, rhs, t, e[s], pc, ut, ux, uy, un, up[0][s], up[1][s], up[2][s], up[3][s], pitt, pitx, pity,

@@ -20,6 +20,7 @@ typedef struct {
 	int conformal;        /* CONFORMAL_EOS */
 	int shear;            /* PIMUNU: evolve pi^{mu nu} */
 	int bulk;             /* PI: evolve the bulk pressure (requires shear) */
+	int cartesian;        /* USE_CARTESIAN_COORDINATES (SourceTerms.cu:25, 738-743) */
 } kt_params;
 
 typedef struct kt_lattice kt_lattice;

@@ -40,6 +40,9 @@ CASES = {
                                 conformal=False, shear=True, bulk=True), 4, 0.0, dict(seed=5, emin=0.02, e0=3.0, spacing=1.5)),
     "conf_shear_line": (dict(nx=1, ny=1, nz=12, dx=0.3, dy=0.3, dz=0.3, dt=0.02, etabar=0.2, theta=1.8,
                              conformal=True, shear=True, bulk=False), 4, 0.0, dict(seed=6)),
+    # USE_CARTESIAN_COORDINATES (SourceTerms.cu:738-743), the reference built with it defined
+    "conf_shear_cart": (dict(nx=8, ny=9, nz=6, dx=0.3, dy=0.3, dz=0.3, dt=0.02, etabar=0.2, theta=1.8,
+                             conformal=True, shear=True, bulk=False, cartesian=True), 4, 0.0, dict(seed=7)),
 }
 
 TAU0 = 0.5
@@ -96,9 +99,11 @@ def scalar_tables():
     return out
 
 
-def main():
+def main(names=None):
     build_ref.build()
     for name, (lat_kw, steps, T_reg, st_kw) in CASES.items():
+        if names and name not in names:
+            continue
         L, prim, s0, s1 = run_case(oracle.RefLattice, lat_kw, steps, T_reg, st_kw)
         data = {"steps": steps, "T_reg": T_reg, "tau0": TAU0}
         for k, v in s0.items():
@@ -107,9 +112,11 @@ def main():
             data["final_" + k] = L.interior(v)
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **data)
         print("wrote", name)
-    np.savez_compressed(os.path.join(HERE, "scalars.npz"), **scalar_tables())
-    print("wrote scalars")
+    if not names or "scalars" in names:
+        np.savez_compressed(os.path.join(HERE, "scalars.npz"), **scalar_tables())
+        print("wrote scalars")
 
 
 if __name__ == "__main__":
-    main()
+    # optional arguments: the case names to (re)write; none writes every case and the scalars
+    main(sys.argv[1:] or None)

@@ -89,3 +89,27 @@ def test_oracle_matches_reference_build_live(conformal, phys):
     sa, sb = A.get_state(), B.get_state()
     for k in A.field_names:
         np.testing.assert_array_equal(A.interior(sa[k]), A.interior(sb[k]), err_msg=k)
+
+
+@pytest.mark.parametrize("variant", ["fp64_conf_ideal_cart", "fp64_conf_shear_cart", "fp64_qcd_bulk_cart"])
+@pytest.mark.skipif(not oracle.ref_available("fp64_conf_ideal_cart"), reason="Cartesian reference builds not built")
+def test_oracle_cartesian_matches_reference_build_live(variant):
+    """The reference compiled with USE_CARTESIAN_COORDINATES defined (SourceTerms.cu:738-743)
+    against the oracle's Cartesian switch, bit for bit."""
+    _, eos, phys, _ = variant.split("_")
+    kw = dict(nx=9, ny=6, nz=5, dx=0.25, dy=0.3, dz=0.2, dt=0.015, etabar=0.12, theta=1.6, conformal=eos == "conf",
+              shear=phys != "ideal", bulk=phys == "bulk", cartesian=True)
+    A = oracle.OracleLattice(**kw)
+    B = oracle.RefLattice(**kw)
+    assert B.variant == variant
+    prim = rich_state(A, seed=12, vel=0.2)
+    A.set_primitive(prim)
+    B.set_primitive(prim)
+    t = 0.6
+    for n in range(1, 6):
+        A.step(t, kw["dt"], 0.0)
+        B.step(t, kw["dt"], 0.0)
+        t = 0.6 + n * kw["dt"]
+    sa, sb = A.get_state(), B.get_state()
+    for k in A.field_names:
+        np.testing.assert_array_equal(A.interior(sa[k]), A.interior(sb[k]), err_msg=k)
