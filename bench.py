@@ -733,6 +733,16 @@ def run_ours(args):
         Lm.close()
         extras["mixed_cell_updates_per_s"] = cells / (ms_mixed / 1e3)
         extras["mixed_ms_per_step"] = ms_mixed
+        # the same FP64 step with the validity diagnostics on (the reference's checkValidity,
+        # which its step runs every time; opt-in here, one kernel after stage 2)
+        Lv = _g.Lattice(device=local, **w.lattice_kwargs())
+        Lv.set_primitive(prim)
+        Lv.set_stream(stream.cuda_stream)
+        Lv.enable_validity(True)
+        ms_val = time_steps(Lv, w, max(5, args.steps // 2), 3, stream)
+        Lv.close()
+        extras["fp64_with_validity"] = {"ms_per_step": ms_val, "cell_updates_per_s": cells / (ms_val / 1e3),
+                                        "validity_ms_per_step": ms_val - ms_max / args.steps}
         # the 33x33x17 conformal configuration (its 100 steps, after 5 warm-up steps)
         w1 = workloads.CONFIG1
         L1 = _g.Lattice(device=local, **w1.lattice_kwargs())
