@@ -65,6 +65,30 @@ def test_event_same_alone_and_in_batch(precision, conformal, shear, bulk):
         assert np.isclose(info.max_energy_density, interior(shape, inb["e"]).max(), rtol=1e-15)
 
 
+def test_cartesian_event_same_alone_and_in_batch():
+    """A batch in Cartesian coordinates (the reference's USE_CARTESIAN_COORDINATES) advances
+    each event as a Cartesian single lattice does, and differently from Milne."""
+    evs = make_events(True, True, False)
+    B = gvh.Batch(1 << 26, conformal=True, shear=True, bulk=False, cartesian=True)
+    ids = [B.add_event(**kw, prim=prim, tau0=t0) for kw, prim, t0 in evs]
+    B.step(4)
+    for eid, (kw, prim, t0) in zip(ids, evs):
+        out = {}
+        for cart in (True, False):
+            L = gvh.Lattice(conformal=True, shear=True, bulk=False, cartesian=cart, **kw)
+            L.set_primitive(prim)
+            for n in range(4):
+                L.step(t0 + n * kw["dt"], kw["dt"])
+            out[cart] = L.get_state()
+        inb = B.get_state(eid)
+        shape = (kw["nx"], kw["ny"], kw["nz"])
+        for k in ("ttt", "ttx", "pixx", "e"):
+            a, b, m = (interior(shape, out[True][k]), interior(shape, inb[k]), interior(shape, out[False][k]))
+            scale = np.abs(a).max()
+            assert np.abs(a - b).max() <= 1e-12 * scale, k
+        assert np.abs(interior(shape, out[True]["ttt"]) - interior(shape, out[False]["ttt"])).max() > 1e-3
+
+
 def test_freezeout_stop_rule():
     """Below e(T_fo) from the start: the initial check counts, then one per step; the event
     is frozen out after 11 checks (FOFREQ+1), as the reference's run loop stops."""

@@ -48,15 +48,17 @@ def rel(a, b):
 
 HBARC = 0.197326938
 
-# (eos, shear, bulk, T_reg [fm^-1], state kwargs): the scratch holds nq + 5 values per cell,
-# so each component count (4, 14, 15) lays it out differently; T_reg > 0 on a state with
-# large pi regulates cells (the regulation branch of the stage kernel).
+# (eos, shear, bulk, T_reg [fm^-1], state kwargs[, Cartesian coordinates]): the scratch holds
+# nq + 5 values per cell, so each component count (4, 14, 15) lays it out differently;
+# T_reg > 0 on a state with large pi regulates cells (the regulation branch of the stage
+# kernel); the last case takes the options' Cartesian coordinates through the same call.
 CASES = {
     "qcd_shear_bulk": (False, True, True, 0.0, dict(seed=31)),
     "qcd_shear": (False, True, False, 0.0, dict(seed=32)),
     "conformal_ideal": (True, False, False, 0.0, dict(seed=33)),
     "conformal_shear": (True, True, False, 0.0, dict(seed=34)),
     "qcd_shear_regulated": (False, True, False, 0.5 / HBARC, dict(seed=35, pi=0.3)),
+    "conformal_shear_cartesian": (True, True, False, 0.0, dict(seed=36), True),
 }
 
 
@@ -65,10 +67,10 @@ CASES = {
 def test_noalloc_step_matches_handle_on_two_calls(case, precision):
     import torch
 
-    conformal, shear, bulk, T_reg, st_kw = CASES[case]
+    conformal, shear, bulk, T_reg, st_kw, *cart = CASES[case]
     L = bound()
     kw = dict(nx=12, ny=10, nz=7, dx=0.3, dy=0.3, dz=0.3, dt=0.01, etabar=0.16, theta=2.0, conformal=conformal,
-              shear=shear, bulk=bulk)
+              shear=shear, bulk=bulk, cartesian=bool(cart and cart[0]))
     G = gvh.Lattice(precision=precision, **kw)
     G.set_primitive(rich_state(G, **st_kw))
     s = G.get_state()
