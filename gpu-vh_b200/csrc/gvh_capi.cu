@@ -59,8 +59,16 @@ namespace {
 
 template <int EOS, bool SHEAR, bool BULK, bool MIXED>
 int launch_stage_p(const gvh_handle *h, const StageArgs &a, bool stage2) {
-  const dim3 grid = stage_grid(h->ncells);
   const size_t smem = stage_smem_bytes<SHEAR, BULK>();
+  if (h->ncells < h->split_below) {
+    // fewer cells than one wave of the one-thread-per-cell kernel: four warps per 32 cells
+    const dim3 grid = split_grid(h->ncells);
+    if (stage2) kt_stage_split_kernel<EOS, SHEAR, BULK, true, MIXED><<<grid, kThreads, smem, h->stream>>>(a);
+    else kt_stage_split_kernel<EOS, SHEAR, BULK, false, MIXED><<<grid, kThreads, smem, h->stream>>>(a);
+    GVH_CUDA(cudaGetLastError());
+    return GVH_OK;
+  }
+  const dim3 grid = stage_grid(h->ncells);
   if (stage2) kt_stage_kernel<EOS, SHEAR, BULK, true, MIXED><<<grid, kThreads, smem, h->stream>>>(a);
   else kt_stage_kernel<EOS, SHEAR, BULK, false, MIXED><<<grid, kThreads, smem, h->stream>>>(a);
   GVH_CUDA(cudaGetLastError());
@@ -244,9 +252,13 @@ int gvh_create(const gvh_lattice_params *L, const gvh_hydro_params *H, const gvh
     std::lock_guard<std::mutex> lock(mu);
     if (dev < 64 && !(prepared & (1ull << dev))) {
       GVH_CUDA(allow_all_stage_kernels());
+      GVH_CUDA(allow_all_split_kernels());
       prepared |= 1ull << dev;
     }
   }
+
+  int sms = 0;
+  GVH_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
 
   gvh_handle *h = new gvh_handle();
   memset(h, 0, sizeof(*h));
@@ -263,6 +275,8 @@ int gvh_create(const gvh_lattice_params *L, const gvh_hydro_params *H, const gvh
   h->theta = o.theta;
   h->cartesian = o.coordinates == GVH_COORDINATES_CARTESIAN;
   h->eos = o.eos; h->shear = o.shear; h->bulk = o.bulk; h->precision = o.precision; h->device = dev;
+  // one wave of the one-thread-per-cell stage kernel: below it the split kernel runs
+  h->split_below = (long long)sms * GVH_MIN_BLOCKS * kThreads;
   h->ucur = 0; h->uprev = 1; h->ufree = 2;
 
   size_t nbuf = 2 * (size_t)h->nq + 3 + 12;

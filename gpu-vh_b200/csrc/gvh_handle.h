@@ -11,6 +11,7 @@ struct gvh_handle {
   double dx, dy, dz, dt_lattice, etabar, theta;
   int eos, shear, bulk, precision, device;
   int cartesian;            // GVH_COORDINATES_CARTESIAN
+  long long split_below;    // lattices with fewer cells take the split stage kernel
   cudaStream_t stream;      // where work is queued (own_stream unless the caller set one)
   cudaStream_t own_stream;
   double *block;

@@ -221,7 +221,9 @@ __device__ __forceinline__ void axis_pi_sources(const StageArgs &a, int s, int a
 }
 
 // Returns the axis's local propagation speed, max(a(i+1/2), a(i-1/2)) (SpectralRadius.cu:17-30).
-template <int EOS, bool SHEAR, bool BULK, bool MIXED>
+// INCREMENT: store each component's increment before the factor dt in out instead of adding
+// dt times it (the split kernel, whose source warp adds them in axis order).
+template <int EOS, bool SHEAR, bool BULK, bool MIXED, bool INCREMENT = false>
 __device__ __forceinline__ double axis_update(const StageArgs &a, int s, int axis, int idx, int n_axis, int stride,
                                               double inv_spacing, const GuessEos &g0, const double *uc, double *out,
                                               double *cache, unsigned &status) {
@@ -251,7 +253,8 @@ __device__ __forceinline__ double axis_update(const StageArgs &a, int s, int axi
     R r = flux_from_states<R>((R)c[0], (R)c[kBlock], (R)c[2 * kBlock], (R)c[3 * kBlock], f);
     r = r * half_inv_d;
     if (SHEAR && n < 4) r += Sa[n];
-    out[n * kBlock] += (double)r * a.dt;
+    if (INCREMENT) out[n * kBlock] = (double)r;
+    else out[n * kBlock] += (double)r * a.dt;
   }
   // pi^{ij} from the lattice, two components' stencil loads in flight at once (2 measured
   // faster than 1, 3 and 6)
@@ -259,7 +262,8 @@ __device__ __forceinline__ double axis_update(const StageArgs &a, int s, int axi
 #pragma unroll 2
     for (int n = 8; n < 14; ++n) {
       R r = flux_difference<R>(th, a.qin + (size_t)n * a.cs + s, o, f);
-      out[n * kBlock] += (double)(r * half_inv_d) * a.dt;
+      if (INCREMENT) out[n * kBlock] = (double)(r * half_inv_d);
+      else out[n * kBlock] += (double)(r * half_inv_d) * a.dt;
     }
   }
   return fmax(fd.af, fd.ab);
@@ -563,6 +567,90 @@ __global__ void __launch_bounds__(kBlock, GVH_MIN_BLOCKS) kt_stage_kernel(const 
   }
 }
 
+// ---- lattices too small to fill the GPU: one cell's stage on four warps -----------------
+// With fewer cells than the GPU has thread slots (148 SMs x 4 blocks x kBlock) SMs sit idle
+// and the time is one thread's dependency chain: the source term, then the three axes one
+// after another. Here a block takes kSplitCells cells and each of its four warps does one part
+// of every cell: warp 0 the source term, warps 1-3 the x, y and eta fluxes. An axis warp
+// leaves its components' increments (before the factor dt) in its own shared-memory column;
+// after a barrier warp 0 adds them to its Euler update in axis order, in the same expression
+// as the one-thread-per-cell kernel's running update, and finishes the cell. The same
+// functions in the same order of operations: the state is the same bit for bit.
+constexpr int kSplitCells = kBlock / 4;
+static_assert(kSplitCells == 32, "one warp per part of a cell's stage");
+
+inline dim3 split_grid(long long ncells) { return dim3((unsigned)((ncells + kSplitCells - 1) / kSplitCells)); }
+
+template <int EOS, bool SHEAR, bool BULK, bool STAGE2, bool MIXED>
+__global__ void __launch_bounds__(kBlock, GVH_MIN_BLOCKS) kt_stage_split_kernel(const StageArgs a) {
+  constexpr int NQ = NComp<SHEAR, BULK>::value;
+  const int lane = threadIdx.x % kSplitCells;
+  const int part = threadIdx.x / kSplitCells;  // 0: source and finish; 1..3: axis part - 1
+  const long long id = (long long)blockIdx.x * kSplitCells + lane;
+  extern __shared__ double gvh_stage_smem[];
+  double *out = gvh_stage_smem + threadIdx.x;
+  double *cache = gvh_stage_smem + NQ * kBlock + threadIdx.x;
+  double speed = 0.0;
+  bool live = id < a.ncells;
+  int i = 0, j = 0, k = 0;
+  long long s = 0;
+  if (live) {
+    i = (int)(id % a.nx);
+    j = (int)((id / a.nx) % a.ny);
+    k = (int)(id / ((long long)a.nx * a.ny));
+    s = i + a.sy * j + a.sz * k;
+#ifdef GVH_BOUNDS_CHECK
+    if (!cell_stencil_ok(a, i, j, k)) {
+      if (part == 0) atomicOr(a.status, STATUS_BOUNDS);
+      live = false;
+    }
+#endif
+  }
+  unsigned status = 0;
+  double ePrev = 0.0;
+  if (live) {
+    ePrev = a.e[s];
+    double uc[4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) uc[m] = __ldg(a.uin + m * a.cs + s);
+    if (part == 0) {
+      stage_source<EOS, SHEAR, BULK, MIXED, kBlock>(a, s, i, j, k, ePrev, uc, out);
+    } else {
+      const int axis = part - 1;
+      const int idx = axis == 0 ? i : axis == 1 ? j : k;
+      const int n_axis = axis == 0 ? a.nx : axis == 1 ? a.ny : a.nz;
+      // the FP64 kernel's one-cell axes are skipped, as in kt_stage_kernel
+      if (MIXED || n_axis > 1) {
+        const int stride = axis == 0 ? 1 : axis == 1 ? (int)a.sy : (int)a.sz;
+        const double inv_spacing = axis == 0 ? a.inv_dx : axis == 1 ? a.inv_dy : a.inv_dz;
+        const GuessEos g0 = guess_eos<EOS>(ePrev);
+        const double as = axis_update<EOS, SHEAR, BULK, MIXED, true>(a, (int)s, axis, idx, n_axis, stride,
+                                                                     inv_spacing, g0, uc, out, cache, status);
+        speed = n_axis > 1 ? as * inv_spacing : 0.0;
+        if (status) atomicOr(a.status, status);
+      }
+    }
+  }
+  __syncthreads();
+  if (live && part == 0) {
+#pragma unroll 1
+    for (int axis = 0; axis < 3; ++axis) {
+      const int n_axis = axis == 0 ? a.nx : axis == 1 ? a.ny : a.nz;
+      if (!MIXED && n_axis == 1) continue;
+      const double *inc = gvh_stage_smem + (axis + 1) * kSplitCells + lane;
+#pragma unroll
+      for (int n = 0; n < NQ; ++n) out[n * kBlock] += inc[n * kBlock] * a.dt;
+    }
+    stage_finish<EOS, SHEAR, BULK, STAGE2, kBlock>(a, s, out, guess_eos<EOS>(ePrev), status);
+  }
+  if (!STAGE2 && a.speed_max) {
+    unsigned long long b = (unsigned long long)__double_as_longlong(fmax(speed, 0.0));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) b = max(b, __shfl_xor_sync(0xffffffffu, b, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(a.speed_max, b);
+  }
+}
+
 // Raises a stage kernel's dynamic shared-memory limit to what it is launched with. A kernel
 // template instantiated in several translation units has one copy in each, so each file that
 // launches one calls this for its own copies (host only; done once per device, before any
@@ -581,6 +669,21 @@ inline cudaError_t allow_all_stage_kernels() {
   if (e == cudaSuccess) e = allow_stage_smem(kt_stage_kernel<EOS_, SH, BU, true, false>, stage_smem_bytes<SH, BU>());  \
   if (e == cudaSuccess) e = allow_stage_smem(kt_stage_kernel<EOS_, SH, BU, false, true>, stage_smem_bytes<SH, BU>());  \
   if (e == cudaSuccess) e = allow_stage_smem(kt_stage_kernel<EOS_, SH, BU, true, true>, stage_smem_bytes<SH, BU>());
+  GVH_ALLOW(EOS_QCD, false, false) GVH_ALLOW(EOS_QCD, true, false) GVH_ALLOW(EOS_QCD, true, true)
+  GVH_ALLOW(EOS_CONFORMAL, false, false) GVH_ALLOW(EOS_CONFORMAL, true, false) GVH_ALLOW(EOS_CONFORMAL, true, true)
+#undef GVH_ALLOW
+  return e;
+}
+
+// All 24 kt_stage_split_kernel instantiations of the calling translation unit, as
+// allow_all_stage_kernels (only the single-lattice handle launches them).
+inline cudaError_t allow_all_split_kernels() {
+  cudaError_t e = cudaSuccess;
+#define GVH_ALLOW(EOS_, SH, BU)                                                                                      \
+  if (e == cudaSuccess) e = allow_stage_smem(kt_stage_split_kernel<EOS_, SH, BU, false, false>, stage_smem_bytes<SH, BU>()); \
+  if (e == cudaSuccess) e = allow_stage_smem(kt_stage_split_kernel<EOS_, SH, BU, true, false>, stage_smem_bytes<SH, BU>());  \
+  if (e == cudaSuccess) e = allow_stage_smem(kt_stage_split_kernel<EOS_, SH, BU, false, true>, stage_smem_bytes<SH, BU>());  \
+  if (e == cudaSuccess) e = allow_stage_smem(kt_stage_split_kernel<EOS_, SH, BU, true, true>, stage_smem_bytes<SH, BU>());
   GVH_ALLOW(EOS_QCD, false, false) GVH_ALLOW(EOS_QCD, true, false) GVH_ALLOW(EOS_QCD, true, true)
   GVH_ALLOW(EOS_CONFORMAL, false, false) GVH_ALLOW(EOS_CONFORMAL, true, false) GVH_ALLOW(EOS_CONFORMAL, true, true)
 #undef GVH_ALLOW

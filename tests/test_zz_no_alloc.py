@@ -23,6 +23,12 @@ from helpers import rich_state
 pytestmark = pytest.mark.gpu
 
 REL_TOL = 1e-12
+# The handle runs small lattices on its split stage kernel (four warps per 32 cells), the
+# allocation-free step on the one-thread-per-cell kernel: the same code compiled into two
+# kernels, whose multiply-add contraction of the mixed path's FP32 arithmetic may differ. The
+# mixed path's bar, as between a batched event and the same event alone (far inside its 1e-4
+# accuracy against the FP64 oracle).
+MIXED_TOL = 1e-6
 
 
 def bound():
@@ -99,12 +105,13 @@ def test_noalloc_step_matches_handle_on_two_calls(case, precision):
         assert status.value == G.status(), (call, status.value, G.status())
         ref = G.get_state()
         torch.cuda.synchronize()
+        tol = REL_TOL if precision == "fp64" else MIXED_TOL
         for n, name in enumerate(G.qnames):
-            assert rel(q[n].cpu().numpy(), G.interior(ref[name]).reshape(-1)) <= REL_TOL, (call, name)
-        assert rel(e.cpu().numpy(), G.interior(ref["e"]).reshape(-1)) <= REL_TOL
-        assert rel(p.cpu().numpy(), G.interior(ref["p"]).reshape(-1)) <= REL_TOL
+            assert rel(q[n].cpu().numpy(), G.interior(ref[name]).reshape(-1)) <= tol, (call, name)
+        assert rel(e.cpu().numpy(), G.interior(ref["e"]).reshape(-1)) <= tol
+        assert rel(p.cpu().numpy(), G.interior(ref["p"]).reshape(-1)) <= tol
         for m, name in enumerate(["ut", "ux", "uy", "un"]):
-            assert rel(u_next[m].cpu().numpy(), G.interior(ref[name]).reshape(-1)) <= REL_TOL, (call, name)
+            assert rel(u_next[m].cpu().numpy(), G.interior(ref[name]).reshape(-1)) <= tol, (call, name)
         # next step: u^n becomes the previous level, u^{n+1} the current one
         u_prev, u, u_next = u, u_next, u_prev
         t = 0.5 + (call + 1) * kw["dt"]
