@@ -66,9 +66,10 @@ def parse():
     ap.add_argument("--serving-rate", type=float, default=4.0)
     ap.add_argument("--batch64-seconds", type=float, default=120.0,
                     help="time limit of the 64-event batched run (0 skips it)")
-    ap.add_argument("--stage-case", default="", choices=["", "fp64", "mixed"],
-                    help="only --warmup + --steps RK2 steps of the 131x131x61 event in this precision "
-                         "(a small case for profiling the stage kernel); prints one JSON line")
+    ap.add_argument("--stage-case", default="", choices=["", "fp64", "mixed", "config1"],
+                    help="only --warmup + --steps RK2 steps of the 131x131x61 event in this precision, "
+                         "or of the 33x33x17 configuration (config1, FP64: the split stage kernel's "
+                         "case), for profiling the stage kernels; prints one JSON line")
     ap.add_argument("--surface-slabs", type=int, default=0,
                     help="only the freeze-out surface of N slabs of the 131x131x61 event after "
                          "300 steps (text only, as the run loop keeps it); for profiling its kernels")
@@ -826,8 +827,13 @@ def stage_case(precision, steps, warmup):
 
     import gvh
 
-    w, prim, _ = make_event(workloads.CONFIG2, 0)
-    L = gvh.Lattice(device=0, precision=precision, **w.lattice_kwargs())
+    if precision == "config1":
+        # the 33x33x17 conformal configuration in FP64 (the split kernel's case)
+        w, prim = workloads.CONFIG1, workloads.gaussian_profile(workloads.CONFIG1)
+        L = gvh.Lattice(device=0, precision="fp64", **w.lattice_kwargs())
+    else:
+        w, prim, _ = make_event(workloads.CONFIG2, 0)
+        L = gvh.Lattice(device=0, precision=precision, **w.lattice_kwargs())
     L.set_primitive(prim)
     stream = torch.cuda.Stream()
     L.set_stream(stream.cuda_stream)
